@@ -1,0 +1,917 @@
+// C ABI of the Paillier / Paillier-Lookup path (see include/cuhe_paillier.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cuhe_paillier.h"
+#include "host_bigint.h"
+#include "paillier_kernels.cuh"
+
+using cuhe::host::Limbs;
+
+namespace {
+
+std::string g_create_error;
+
+struct Variant {
+  int K, TPI, W;
+};
+
+// (K, TPI, W) combinations compiled into the library.
+#define CUHE_VARIANTS(X) \
+  X(64, 8, 4)            \
+  X(64, 16, 4)           \
+  X(128, 8, 4)           \
+  X(128, 16, 4)          \
+  X(128, 16, 5)          \
+  X(128, 32, 4)          \
+  X(256, 16, 4)          \
+  X(256, 32, 4)          \
+  X(256, 32, 5)
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t grow = std::max(need, size_t(1) << 20);
+    cudaError_t e = cudaMalloc(&ptr, grow);
+    if (e == cudaSuccess) bytes = grow;
+    return e;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
+bool is_device_pointer(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+
+struct cuhe_paillier {
+  int device = 0;
+  int K = 0;
+  int n_words = 0;
+  int tpi = 0, window = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  uint32_t* d_consts = nullptr;
+  int* d_status = nullptr;
+  cuhe::KeyScalars ks{};
+  Limbs n, n2;
+  Limbs secret_exp;  // empty until set
+  bool have_secret = false;
+  int32_t* d_ops_n = nullptr;
+  int nops_n = 0;
+  int32_t* d_ops_sec = nullptr;
+  int nops_sec = 0;
+  uint32_t* d_gtab = nullptr;
+  int message_chunks = 0;
+  uint32_t* d_noise = nullptr;
+  int noise_entries = 0;
+  DeviceBuffer work;
+  DeviceBuffer tmp_ops;
+  std::string error;
+  std::mutex mu;
+};
+
+namespace {
+
+int fail(cuhe_paillier* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->error = msg; else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(cuhe_paillier* ctx, cudaError_t e, const char* where) {
+  return fail(ctx, CUHE_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorName(e) + " (" +
+                                         cudaGetErrorString(e) + ")");
+}
+
+#define CUHE_CUDA(ctx, call, where)                   \
+  do {                                                \
+    cudaError_t _e = (call);                          \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+  } while (0)
+
+// ---- kernel launchers -----------------------------------------------------
+
+template <int K, int TPI, int W>
+size_t modexp_smem() {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  return size_t(5 * K + IPB * cuhe::inst_stride_words<K>((1 << (W - 1)) + 1)) * 4;
+}
+
+template <int K, int TPI, int W>
+cudaError_t launch_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* aux, uint32_t* out,
+                          long long count, const int32_t* ops, int nops, int mode, int pop_words) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = modexp_smem<K, TPI, W>();
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp<K, TPI, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_modexp<K, TPI, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      base, aux, K, out, count, ctx->d_consts, ctx->ks, ops, nops, mode, pop_words, ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int K, int TPI>
+cudaError_t launch_modexp_var(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* exps, int exp_words,
+                              int windows, uint32_t* out, long long count) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = size_t(2 * K + IPB * cuhe::inst_stride_words<K>(17)) * 4;
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp_var<K, TPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_modexp_var<K, TPI><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      base, exps, exp_words, windows, out, count, ctx->d_consts, ctx->ks, ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int K, int TPI>
+cudaError_t launch_mulmod(cuhe_paillier* ctx, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                          long long count) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = size_t(K + IPB * cuhe::inst_stride_words<K>(1)) * 4;
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_mulmod<K, TPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_mulmod<K, TPI><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      a, b, out, count, ctx->d_consts, ctx->ks, ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int K, int TPI>
+cudaError_t launch_convert(cuhe_paillier* ctx, const uint32_t* in, uint32_t* out, long long count, int to_mont) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = size_t(K) * 4;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_convert<K, TPI><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      in, out, count, ctx->d_consts, ctx->ks, to_mont, ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int K, int TPI>
+cudaError_t launch_outer(cuhe_paillier* ctx, const uint32_t* qmont, long long nq, const uint32_t* index,
+                         long long nx, uint32_t* out) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = size_t(K) * 4;
+  const long long bx = (nx + IPB - 1) / IPB;
+  for (long long q0 = 0; q0 < nq; q0 += 65535) {
+    const long long qn = std::min<long long>(65535, nq - q0);
+    cuhe::k_mulmod_outer<K, TPI><<<dim3(unsigned(bx), unsigned(qn)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+        qmont + q0 * K, qn, index, nx, out + q0 * nx * K, ctx->d_consts, ctx->ks, ctx->d_status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <int K, int TPI>
+cudaError_t launch_lookup(cuhe_paillier* ctx, const uint8_t* bits, int embed_len, int chunk_len, int chunk_num,
+                          const uint32_t* plain, long long count, const uint8_t* idx, uint32_t* out) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t rows_bytes = size_t(IPB) * ctx->message_chunks * 2;
+  const size_t smem = size_t(K + IPB * cuhe::inst_stride_words<K>(1)) * 4 + ((rows_bytes + 15) & ~size_t(15));
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_lookup_encrypt<K, TPI>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_lookup_encrypt<K, TPI><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      bits, embed_len, chunk_len, chunk_num, plain, K, count, ctx->message_chunks, ctx->d_gtab, ctx->d_noise,
+      ctx->noise_entries, idx, out, ctx->d_consts, ctx->ks, ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int K, int TPI>
+cudaError_t launch_table_rows(cuhe_paillier* ctx, const uint32_t* bases, int rows, uint32_t* gtab) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = size_t(IPB * cuhe::inst_stride_words<K>(2)) * 4;
+  const long long blocks = ((long long)rows * 16 + IPB - 1) / IPB;
+  cuhe::k_table_rows<K, TPI><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      bases, rows, gtab, ctx->d_consts, ctx->ks);
+  return cudaGetLastError();
+}
+
+// Runtime dispatch over the compiled variants.
+struct Dispatch {
+  cudaError_t (*modexp)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long, const int32_t*,
+                        int, int, int) = nullptr;
+  cudaError_t (*modexp_var)(cuhe_paillier*, const uint32_t*, const uint32_t*, int, int, uint32_t*, long long) = nullptr;
+  cudaError_t (*mulmod)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long) = nullptr;
+  cudaError_t (*convert)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int) = nullptr;
+  cudaError_t (*outer)(cuhe_paillier*, const uint32_t*, long long, const uint32_t*, long long, uint32_t*) = nullptr;
+  cudaError_t (*lookup)(cuhe_paillier*, const uint8_t*, int, int, int, const uint32_t*, long long, const uint8_t*,
+                        uint32_t*) = nullptr;
+  cudaError_t (*table_rows)(cuhe_paillier*, const uint32_t*, int, uint32_t*) = nullptr;
+};
+
+bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
+#define CUHE_MATCH(k, t, w)                                        \
+  if (K == k && TPI == t && W == w) {                              \
+    d->modexp = &launch_modexp<k, t, w>;                           \
+    d->modexp_var = &launch_modexp_var<k, t>;                      \
+    d->mulmod = &launch_mulmod<k, t>;                              \
+    d->convert = &launch_convert<k, t>;                            \
+    d->outer = &launch_outer<k, t>;                                \
+    d->lookup = &launch_lookup<k, t>;                              \
+    d->table_rows = &launch_table_rows<k, t>;                      \
+    return true;                                                   \
+  }
+  CUHE_VARIANTS(CUHE_MATCH)
+#undef CUHE_MATCH
+  return false;
+}
+
+void default_tuning(int K, int* tpi, int* w) {
+  *w = 4;
+  *tpi = K / 8;  // eight limbs per lane
+}
+
+// ---- staging of host buffers ----------------------------------------------
+
+struct Staged {
+  const void* src;
+  void* dev;
+  size_t bytes;
+  bool in;    // copy host->device before
+  bool out;   // copy device->host after
+  void* host_out;
+};
+
+class Stager {
+ public:
+  explicit Stager(cuhe_paillier* ctx) : ctx_(ctx) {}
+  // Reserve space for all buffers first, then bind.
+  void add(const void* host_or_dev, size_t bytes, bool in, bool out) {
+    items_.push_back({host_or_dev, nullptr, bytes, in, out, const_cast<void*>(host_or_dev)});
+  }
+  // Device scratch that lives in the workspace for the duration of the call.
+  void add_scratch(size_t bytes) { items_.push_back({nullptr, nullptr, bytes, false, false, nullptr}); }
+  int bind() {
+    size_t total = 0;
+    for (auto& it : items_) {
+      if ((!it.src || !is_device_pointer(it.src)) && it.bytes) total += (it.bytes + 255) & ~size_t(255);
+    }
+    if (total) {
+      cudaError_t e = ctx_->work.reserve(total);
+      if (e != cudaSuccess) return cuda_fail(ctx_, e, "workspace allocation");
+    }
+    size_t off = 0;
+    for (auto& it : items_) {
+      if (!it.bytes) { it.dev = nullptr; continue; }
+      if (!it.src) {
+        it.dev = static_cast<char*>(ctx_->work.ptr) + off;
+        off += (it.bytes + 255) & ~size_t(255);
+        continue;
+      }
+      if (is_device_pointer(it.src)) {
+        it.dev = const_cast<void*>(it.src);
+        it.in = it.out = false;
+      } else {
+        it.dev = static_cast<char*>(ctx_->work.ptr) + off;
+        off += (it.bytes + 255) & ~size_t(255);
+        staged_ = true;
+        if (it.in) {
+          cudaError_t e = cudaMemcpyAsync(it.dev, it.src, it.bytes, cudaMemcpyHostToDevice, ctx_->stream);
+          if (e != cudaSuccess) return cuda_fail(ctx_, e, "host to device copy");
+        }
+      }
+    }
+    return CUHE_OK;
+  }
+  void* dev(size_t i) const { return items_[i].dev; }
+  int finish() {
+    for (auto& it : items_) {
+      if (it.out) {
+        cudaError_t e = cudaMemcpyAsync(it.host_out, it.dev, it.bytes, cudaMemcpyDeviceToHost, ctx_->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx_, e, "device to host copy");
+      }
+    }
+    if (staged_) {
+      cudaError_t e = cudaStreamSynchronize(ctx_->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx_, e, "stream synchronize");
+    }
+    return CUHE_OK;
+  }
+  bool staged() const { return staged_; }
+
+ private:
+  cuhe_paillier* ctx_;
+  std::vector<Staged> items_;
+  bool staged_ = false;
+};
+
+int check_status(cuhe_paillier* ctx, bool synchronous) {
+  // Range errors are reported by the kernels through d_status; reading it
+  // needs a synchronisation, done only for calls that already synchronise.
+  if (!synchronous) return CUHE_OK;
+  int status = 0;
+  cudaError_t e = cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "status read");
+  if (status) {
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+    return fail(ctx, CUHE_RANGE, "input outside its valid range (ciphertext >= n^2, plaintext >= n, or noise index)");
+  }
+  return CUHE_OK;
+}
+
+int upload_schedule(cuhe_paillier* ctx, const Limbs& e, int32_t** dptr, int* nops) {
+  std::vector<int32_t> ops = cuhe::host::window_schedule(e, ctx->window);
+  if (*dptr) cudaFree(*dptr);
+  *dptr = nullptr;
+  *nops = int(ops.size());
+  if (ops.empty()) return CUHE_OK;
+  CUHE_CUDA(ctx, cudaMalloc(dptr, ops.size() * sizeof(int32_t)), "schedule allocation");
+  CUHE_CUDA(ctx, cudaMemcpy(*dptr, ops.data(), ops.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+            "schedule upload");
+  return CUHE_OK;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* cuhe_version(void) { return "cuhe_b200 paillier 1"; }
+
+int cuhe_window_schedule(const uint32_t* exponent, int exponent_words, int window, int32_t* ops, int capacity) {
+  if (!exponent || exponent_words <= 0 || window < 1 || window > 8 || capacity < 0) return CUHE_INVALID_ARGUMENT;
+  Limbs e(exponent, exponent + exponent_words);
+  std::vector<int32_t> sched = cuhe::host::window_schedule(e, window);
+  for (int i = 0; i < capacity && i < int(sched.size()); ++i) ops[i] = sched[size_t(i)];
+  return int(sched.size());
+}
+
+const char* cuhe_last_error(const cuhe_paillier* ctx) {
+  return ctx ? ctx->error.c_str() : g_create_error.c_str();
+}
+
+int cuhe_paillier_words(const cuhe_paillier* ctx) { return ctx ? ctx->K : 0; }
+
+int cuhe_paillier_create(const uint32_t* n_in, int n_words, int device, cuhe_paillier** out) {
+  if (!out || !n_in || n_words <= 0) return fail(nullptr, CUHE_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  Limbs n(n_in, n_in + n_words);
+  while (!n.empty() && n.back() == 0) n.pop_back();
+  if (n.empty() || (n[0] & 1u) == 0) return fail(nullptr, CUHE_INVALID_ARGUMENT, "n must be odd and nonzero");
+  const size_t nbits = cuhe::host::bit_length(n);
+  int K = 0;
+  for (int cand : {64, 128, 256}) {
+    if (nbits <= size_t(cand) * 16) { K = cand; break; }
+  }
+  if (!K) return fail(nullptr, CUHE_INVALID_ARGUMENT, "n wider than 4096 bits is not supported");
+  int count = 0;
+  cudaError_t ce = cudaGetDeviceCount(&count);
+  if (ce != cudaSuccess || count == 0) return fail(nullptr, CUHE_CUDA_ERROR, "no CUDA device available");
+  if (device < 0 || device >= count) return fail(nullptr, CUHE_INVALID_ARGUMENT, "invalid device ordinal");
+  DeviceGuard guard(device);
+
+  auto* ctx = new (std::nothrow) cuhe_paillier();
+  if (!ctx) return fail(nullptr, CUHE_OUT_OF_MEMORY, "context allocation");
+  ctx->device = device;
+  ctx->K = K;
+  ctx->n_words = K / 2;
+  default_tuning(K, &ctx->tpi, &ctx->window);
+
+  const size_t k = size_t(K);
+  Limbs nk = cuhe::host::resized(n.data(), n.size(), k);
+  Limbs n2 = cuhe::host::mul(nk, nk, k);
+  ctx->n = nk;
+  ctx->n2 = n2;
+  // R mod N = 2^(32K) mod N via doubling from 1; likewise R^2 = R * 2^(32K)
+  Limbs one(k, 0u);
+  one[0] = 1u;
+  Limbs rm = cuhe::host::shift_mod(one, 32 * k, n2);
+  Limbs r2 = cuhe::host::shift_mod(rm, 32 * k, n2);
+  Limbs rmn = cuhe::host::shift_mod(one, 32 * k, nk);
+  Limbs r2n = cuhe::host::shift_mod(rmn, 32 * k, nk);
+  Limbs nneg(k, 0u);
+  cuhe::host::sub_in_place(nneg, nk);  // 2^(32K) - n (mod 2^(32K))
+  Limbs nr = cuhe::host::shift_mod(nk, 32 * k, n2);  // n < n^2
+  Limbs multr(k, 0u);
+
+  std::vector<uint32_t> block(size_t(cuhe::C_ROWS) * k, 0u);
+  auto put = [&](int row, const Limbs& v) { std::memcpy(block.data() + size_t(row) * k, v.data(), 4 * k); };
+  put(cuhe::C_N2, n2);
+  put(cuhe::C_R2, r2);
+  put(cuhe::C_ONE, one);
+  put(cuhe::C_RM, rm);
+  put(cuhe::C_N, nk);
+  put(cuhe::C_R2N, r2n);
+  put(cuhe::C_NNEG, nneg);
+  put(cuhe::C_NR, nr);
+  put(cuhe::C_MULTR, multr);
+  ctx->ks.ninv2 = 0u - cuhe::host::inv32(n2[0]);
+  ctx->ks.ninv1 = 0u - cuhe::host::inv32(nk[0]);
+  ctx->ks.ndiv = cuhe::host::inv32(nk[0]);
+  ctx->ks.mult_is_zero = 1u;
+
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_consts, block.size() * 4);
+  if (e == cudaSuccess) e = cudaMemcpy(ctx->d_consts, block.data(), block.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_status, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_status, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "context setup");
+    cuhe_paillier_destroy(ctx);
+    return rc;
+  }
+  ctx->stream = ctx->own_stream;
+  if (upload_schedule(ctx, nk, &ctx->d_ops_n, &ctx->nops_n) != CUHE_OK) {
+    g_create_error = ctx->error;
+    cuhe_paillier_destroy(ctx);
+    return CUHE_CUDA_ERROR;
+  }
+  *out = ctx;
+  return CUHE_OK;
+}
+
+void cuhe_paillier_destroy(cuhe_paillier* ctx) {
+  if (!ctx) return;
+  DeviceGuard guard(ctx->device);
+  if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+  if (ctx->stream && ctx->stream != ctx->own_stream) cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->d_consts);
+  cudaFree(ctx->d_status);
+  cudaFree(ctx->d_ops_n);
+  cudaFree(ctx->d_ops_sec);
+  cudaFree(ctx->d_gtab);
+  cudaFree(ctx->d_noise);
+  ctx->work.release();
+  ctx->tmp_ops.release();
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+int cuhe_paillier_set_stream(cuhe_paillier* ctx, void* stream) {
+  if (!ctx) return CUHE_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return CUHE_OK;
+}
+
+int cuhe_synchronize(cuhe_paillier* ctx) {
+  if (!ctx) return CUHE_INVALID_ARGUMENT;
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "synchronize");
+  return check_status(ctx, true);
+}
+
+int cuhe_paillier_set_tuning(cuhe_paillier* ctx, int tpi, int window) {
+  if (!ctx) return CUHE_INVALID_ARGUMENT;
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  int dt, dw;
+  default_tuning(ctx->K, &dt, &dw);
+  if (!tpi) tpi = dt;
+  if (!window) window = dw;
+  Dispatch d;
+  if (!find_dispatch(ctx->K, tpi, window, &d))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "tuning (threads per instance, window) not compiled for this width");
+  const bool changed = window != ctx->window;
+  ctx->tpi = tpi;
+  ctx->window = window;
+  if (changed) {
+    int rc = upload_schedule(ctx, ctx->n, &ctx->d_ops_n, &ctx->nops_n);
+    if (rc) return rc;
+    if (ctx->have_secret) {
+      rc = upload_schedule(ctx, ctx->secret_exp, &ctx->d_ops_sec, &ctx->nops_sec);
+      if (rc) return rc;
+    }
+  }
+  return CUHE_OK;
+}
+
+int cuhe_paillier_get_tuning(const cuhe_paillier* ctx, int* tpi, int* window) {
+  if (!ctx) return CUHE_INVALID_ARGUMENT;
+  if (tpi) *tpi = ctx->tpi;
+  if (window) *window = ctx->window;
+  return CUHE_OK;
+}
+
+int cuhe_paillier_set_secret(cuhe_paillier* ctx, const uint32_t* exponent, int exponent_words,
+                             const uint32_t* multiplier, int multiplier_words) {
+  if (!ctx || !exponent || !multiplier || exponent_words <= 0 || multiplier_words <= 0)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "null secret");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  const size_t k = size_t(ctx->K);
+  if (!cuhe::host::fits(exponent, size_t(exponent_words), k))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "secret exponent wider than n^2");
+  if (!cuhe::host::fits(multiplier, size_t(multiplier_words), k))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "secret multiplier too wide");
+  Limbs e = cuhe::host::resized(exponent, size_t(exponent_words), k);
+  Limbs mult = cuhe::host::resized(multiplier, size_t(multiplier_words), k);
+  if (cuhe::host::cmp(mult, ctx->n) >= 0) {
+    // the reference reduces (x * mult) mod n; reduce the multiplier first
+    while (cuhe::host::cmp(mult, ctx->n) >= 0) cuhe::host::sub_in_place(mult, ctx->n);
+  }
+  Limbs multr = cuhe::host::shift_mod(mult, 32 * k, ctx->n);
+  CUHE_CUDA(ctx, cudaMemcpy(ctx->d_consts + size_t(cuhe::C_MULTR) * k, multr.data(), 4 * k, cudaMemcpyHostToDevice),
+            "secret upload");
+  ctx->ks.mult_is_zero = cuhe::host::is_zero(mult) ? 1u : 0u;
+  ctx->secret_exp = e;
+  ctx->have_secret = true;
+  return upload_schedule(ctx, e, &ctx->d_ops_sec, &ctx->nops_sec);
+}
+
+int cuhe_paillier_encrypt(cuhe_paillier* ctx, const uint32_t* m, const uint32_t* r, uint32_t* c, int64_t count) {
+  if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (count == 0) return CUHE_OK;
+  if (!m || !r || !c) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t bytes = size_t(count) * ctx->K * 4;
+  Stager st(ctx);
+  st.add(m, bytes, true, false);
+  st.add(r, bytes, true, false);
+  st.add(c, bytes, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(1), (const uint32_t*)st.dev(0), (uint32_t*)st.dev(2), count,
+                          ctx->d_ops_n, ctx->nops_n, cuhe::EXP_ENCRYPT, 0),
+            "encrypt launch");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+int cuhe_paillier_decrypt(cuhe_paillier* ctx, const uint32_t* c, uint32_t* m, int64_t count) {
+  if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (!ctx->have_secret) return fail(ctx, CUHE_NOT_READY, "decrypt: secret key not installed");
+  if (count == 0) return CUHE_OK;
+  if (!c || !m) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t bytes = size_t(count) * ctx->K * 4;
+  Stager st(ctx);
+  st.add(c, bytes, true, false);
+  st.add(m, bytes, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, (uint32_t*)st.dev(1), count, ctx->d_ops_sec,
+                          ctx->nops_sec, cuhe::EXP_DECRYPT, 0),
+            "decrypt launch");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t vectors, int chunk_num,
+                                 int chunk_len, int64_t* distance) {
+  if (!ctx || vectors < 0 || chunk_num <= 0 || chunk_len <= 0 || chunk_len % 32)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid decode layout");
+  if (!ctx->have_secret) return fail(ctx, CUHE_NOT_READY, "decode: secret key not installed");
+  if (vectors == 0) return CUHE_OK;
+  if (!c || !distance) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  if (chunk_len / 32 > ctx->K) return fail(ctx, CUHE_INVALID_ARGUMENT, "chunk_len wider than n^2");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const int64_t total = vectors * chunk_num;
+  Stager st(ctx);
+  st.add(c, size_t(total) * ctx->K * 4, true, false);
+  st.add_scratch(size_t(total) * 4);  // per-chunk popcounts
+  st.add(distance, size_t(vectors) * 8, false, true);
+  if (int rc = st.bind()) return rc;
+  uint32_t* d_counts = static_cast<uint32_t*>(st.dev(1));
+  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, d_counts, total, ctx->d_ops_sec, ctx->nops_sec,
+                          cuhe::EXP_DECODE, chunk_len / 32),
+            "decode launch");
+  cuhe::k_sum_chunks<<<unsigned((vectors + 255) / 256), 256, 0, ctx->stream>>>(
+      d_counts, vectors, chunk_num, reinterpret_cast<long long*>(st.dev(2)));
+  CUHE_CUDA(ctx, cudaGetLastError(), "decode reduction");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+int cuhe_imad_peak(int device, double* word_products_per_second) {
+  if (!word_products_per_second) return fail(nullptr, CUHE_INVALID_ARGUMENT, "null output");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    return fail(nullptr, CUHE_CUDA_ERROR, "no such CUDA device");
+  DeviceGuard guard(device);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  uint32_t* sink = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaMalloc(&sink, 4);
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  const int iters = 4096, blocks = sms * 8, threads = 256;
+  float ms = 0.f;
+  if (e == cudaSuccess) {
+    cuhe::k_imad_probe<<<blocks, threads>>>(sink, iters, 1u);  // warm-up
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) cuhe::k_imad_probe<<<blocks, threads>>>(sink, iters, 2u + r);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "imad probe");
+  const double pairs = 5.0 * blocks * threads * double(iters) * 8.0;
+  *word_products_per_second = pairs / (double(ms) * 1e-3);
+  return CUHE_OK;
+}
+
+int cuhe_paillier_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* exponent, int exponent_words,
+                         uint32_t* out, int64_t count) {
+  if (!ctx || count < 0 || !exponent || exponent_words <= 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (count == 0) return CUHE_OK;
+  if (!base || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  // exponent of any width: build its schedule
+  Limbs e(exponent, exponent + exponent_words);
+  while (e.size() > 1 && e.back() == 0) e.pop_back();
+  std::vector<int32_t> ops = cuhe::host::window_schedule(e, ctx->window);
+  if (!ops.empty()) {
+    if (cudaError_t ce = ctx->tmp_ops.reserve(ops.size() * 4)) return cuda_fail(ctx, ce, "schedule allocation");
+    CUHE_CUDA(ctx, cudaMemcpyAsync(ctx->tmp_ops.ptr, ops.data(), ops.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+              "schedule upload");
+  }
+  const size_t bytes = size_t(count) * ctx->K * 4;
+  Stager st(ctx);
+  st.add(base, bytes, true, false);
+  st.add(out, bytes, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, (uint32_t*)st.dev(1), count,
+                          (const int32_t*)ctx->tmp_ops.ptr, int(ops.size()), cuhe::EXP_POW, 0),
+            "modexp launch");
+  if (int rc = st.finish()) return rc;
+  // the schedule buffer is reused by the next call: keep host order
+  if (!st.staged()) CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "modexp synchronize");
+  return check_status(ctx, true);
+}
+
+int cuhe_paillier_modexp_each(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* exponents,
+                              int exponent_words, uint32_t* out, int64_t count) {
+  if (!ctx || count < 0 || exponent_words <= 0 || exponent_words > ctx->K)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (count == 0) return CUHE_OK;
+  if (!base || !exponents || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t bytes = size_t(count) * ctx->K * 4;
+  Stager st(ctx);
+  st.add(base, bytes, true, false);
+  st.add(exponents, size_t(count) * exponent_words * 4, true, false);
+  st.add(out, bytes, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.modexp_var(ctx, (const uint32_t*)st.dev(0), (const uint32_t*)st.dev(1), exponent_words,
+                              exponent_words * 8, (uint32_t*)st.dev(2), count),
+            "modexp_each launch");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+int cuhe_paillier_mulmod(cuhe_paillier* ctx, const uint32_t* a, const uint32_t* b, uint32_t* out, int64_t count) {
+  if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (count == 0) return CUHE_OK;
+  if (!a || !b || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t bytes = size_t(count) * ctx->K * 4;
+  Stager st(ctx);
+  st.add(a, bytes, true, false);
+  st.add(b, bytes, true, false);
+  st.add(out, bytes, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.mulmod(ctx, (const uint32_t*)st.dev(0), (const uint32_t*)st.dev(1), (uint32_t*)st.dev(2), count),
+            "mulmod launch");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+int cuhe_paillier_mulmod_outer(cuhe_paillier* ctx, const uint32_t* query, int64_t nq, const uint32_t* index,
+                               int64_t nx, uint32_t* out) {
+  if (!ctx || nq < 0 || nx < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (nq == 0 || nx == 0) return CUHE_OK;
+  if (!query || !index || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t kb = size_t(ctx->K) * 4;
+  Stager st(ctx);
+  st.add(query, size_t(nq) * kb, true, false);
+  st.add(index, size_t(nx) * kb, true, false);
+  st.add(out, size_t(nq) * size_t(nx) * kb, false, true);
+  st.add_scratch(size_t(nq) * kb);  // queries in Montgomery form
+  if (int rc = st.bind()) return rc;
+  uint32_t* qm = static_cast<uint32_t*>(st.dev(3));
+  CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(0), qm, nq, 1), "query conversion");
+  CUHE_CUDA(ctx, d.outer(ctx, qm, nq, (const uint32_t*)st.dev(1), nx, (uint32_t*)st.dev(2)), "mulmod_outer launch");
+  if (int rc = st.finish()) return rc;
+  // the scratch slice is reused by the next call: keep host order
+  if (!st.staged()) CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "mulmod_outer synchronize");
+  return check_status(ctx, true);
+}
+
+int cuhe_lookup_set_tables(cuhe_paillier* ctx, const uint32_t* g_table, int message_chunks, const uint32_t* noise,
+                           int noise_entries) {
+  if (!ctx || !g_table || !noise || message_chunks <= 0 || noise_entries <= 0 || noise_entries > 256)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid tables");
+  if (message_chunks * 256 > 65536) return fail(ctx, CUHE_INVALID_ARGUMENT, "too many message chunks");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t kb = size_t(ctx->K) * 4;
+  const size_t gbytes = size_t(message_chunks) * 256 * kb;
+  cudaFree(ctx->d_gtab);
+  cudaFree(ctx->d_noise);
+  ctx->d_gtab = nullptr;
+  ctx->d_noise = nullptr;
+  ctx->message_chunks = 0;
+  ctx->noise_entries = 0;
+  CUHE_CUDA(ctx, cudaMalloc(&ctx->d_gtab, gbytes), "table allocation");
+  CUHE_CUDA(ctx, cudaMalloc(&ctx->d_noise, size_t(noise_entries) * kb), "table allocation");
+  Stager st(ctx);
+  st.add(g_table, gbytes, true, false);
+  st.add(noise, size_t(noise_entries) * kb, true, false);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(0), ctx->d_gtab, (long long)message_chunks * 256, 1),
+            "table conversion");
+  CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(1), ctx->d_noise, noise_entries, 1), "table conversion");
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "table synchronize");
+  if (int rc = check_status(ctx, true)) return rc;
+  ctx->message_chunks = message_chunks;
+  ctx->noise_entries = noise_entries;
+  return CUHE_OK;
+}
+
+int cuhe_lookup_build_tables(cuhe_paillier* ctx, const uint32_t* g, int message_chunks, const uint32_t* noise,
+                             int noise_entries) {
+  if (!ctx || !g || message_chunks <= 0 || message_chunks * 256 > 65536)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid table request");
+  if (noise && (noise_entries <= 0 || noise_entries > 256)) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid noise");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t k = size_t(ctx->K), kb = k * 4;
+  // base_i = g^(2^(8i)) for all rows: one batched modexp per row exponent is
+  // wasteful; square on the device 8 times per row in one group instead.
+  std::vector<uint32_t> gk(k, 0u);
+  std::memcpy(gk.data(), g, kb);  // caller passes K words
+  DeviceBuffer bases, gdev, pows;
+  CUHE_CUDA(ctx, bases.reserve(size_t(message_chunks) * kb), "table scratch");
+  CUHE_CUDA(ctx, gdev.reserve(kb), "table scratch");
+  CUHE_CUDA(ctx, cudaMemcpyAsync(gdev.ptr, gk.data(), kb, cudaMemcpyHostToDevice, ctx->stream), "upload g");
+  // bases: row i = g^(2^(8i)); computed as a batched modexp over rows with
+  // per-row exponent 2^(8i) is not fixed-exponent, so use successive
+  // fixed-exponent launches of 2^8 on the previous row (message_chunks launches).
+  std::vector<int32_t> ops256 = cuhe::host::window_schedule(Limbs{256u}, ctx->window);
+  CUHE_CUDA(ctx, pows.reserve(ops256.size() * 4), "table scratch");
+  CUHE_CUDA(ctx, cudaMemcpyAsync(pows.ptr, ops256.data(), ops256.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+            "upload schedule");
+  uint32_t* b = static_cast<uint32_t*>(bases.ptr);
+  CUHE_CUDA(ctx, cudaMemcpyAsync(b, gdev.ptr, kb, cudaMemcpyDeviceToDevice, ctx->stream), "row 0");
+  for (int i = 1; i < message_chunks; ++i) {
+    CUHE_CUDA(ctx, d.modexp(ctx, b + (i - 1) * k, nullptr, b + i * k, 1, (const int32_t*)pows.ptr, int(ops256.size()),
+                            cuhe::EXP_POW, 0),
+              "row base");
+  }
+  // to Montgomery form, then fill rows
+  DeviceBuffer bm;
+  CUHE_CUDA(ctx, bm.reserve(size_t(message_chunks) * kb), "table scratch");
+  CUHE_CUDA(ctx, d.convert(ctx, b, (uint32_t*)bm.ptr, message_chunks, 1), "row conversion");
+  cudaFree(ctx->d_gtab);
+  ctx->d_gtab = nullptr;
+  ctx->message_chunks = 0;
+  CUHE_CUDA(ctx, cudaMalloc(&ctx->d_gtab, size_t(message_chunks) * 256 * kb), "table allocation");
+  CUHE_CUDA(ctx, d.table_rows(ctx, (const uint32_t*)bm.ptr, message_chunks, ctx->d_gtab), "table rows");
+  if (noise) {
+    cudaFree(ctx->d_noise);
+    ctx->d_noise = nullptr;
+    ctx->noise_entries = 0;
+    CUHE_CUDA(ctx, cudaMalloc(&ctx->d_noise, size_t(noise_entries) * kb), "noise allocation");
+    Stager st(ctx);
+    st.add(noise, size_t(noise_entries) * kb, true, false);
+    if (int rc = st.bind()) return rc;
+    CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(0), ctx->d_noise, noise_entries, 1), "noise conversion");
+  }
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "table synchronize");
+  bases.release();
+  gdev.release();
+  pows.release();
+  bm.release();
+  if (int rc = check_status(ctx, true)) return rc;
+  ctx->message_chunks = message_chunks;
+  if (noise) ctx->noise_entries = noise_entries;
+  return CUHE_OK;
+}
+
+int cuhe_lookup_get_g_table(cuhe_paillier* ctx, uint32_t* out) {
+  if (!ctx || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  if (!ctx->d_gtab) return fail(ctx, CUHE_NOT_READY, "tables not installed");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const long long entries = (long long)ctx->message_chunks * 256;
+  Stager st(ctx);
+  st.add(out, size_t(entries) * ctx->K * 4, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.convert(ctx, ctx->d_gtab, (uint32_t*)st.dev(0), entries, 0), "table export");
+  if (int rc = st.finish()) return rc;
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "table export");
+  return check_status(ctx, true);
+}
+
+int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t vectors, int embed_len, int chunk_len,
+                             int chunk_num, const uint8_t* noise_index, uint32_t* out) {
+  if (!ctx || vectors < 0 || embed_len <= 0 || chunk_len <= 0 || chunk_num <= 0)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid layout");
+  if (!ctx->d_gtab || !ctx->d_noise) return fail(ctx, CUHE_NOT_READY, "lookup tables not installed");
+  if (int64_t(chunk_num) * chunk_len < 2 * int64_t(embed_len))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "chunks do not cover the padded embedding");
+  if (vectors == 0) return CUHE_OK;
+  if (!bits || !noise_index || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const int64_t total = vectors * chunk_num;
+  Stager st(ctx);
+  st.add(bits, size_t(vectors) * embed_len, true, false);
+  st.add(noise_index, size_t(total) * cuhe::kNoiseMultiples, true, false);
+  st.add(out, size_t(total) * ctx->K * 4, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.lookup(ctx, (const uint8_t*)st.dev(0), embed_len, chunk_len, chunk_num, nullptr, total,
+                          (const uint8_t*)st.dev(1), (uint32_t*)st.dev(2)),
+            "lookup encrypt launch");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t count, const uint8_t* noise_index,
+                             uint32_t* out) {
+  if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (!ctx->d_gtab || !ctx->d_noise) return fail(ctx, CUHE_NOT_READY, "lookup tables not installed");
+  if (count == 0) return CUHE_OK;
+  if (!m || !noise_index || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  Stager st(ctx);
+  st.add(m, size_t(count) * ctx->K * 4, true, false);
+  st.add(noise_index, size_t(count) * cuhe::kNoiseMultiples, true, false);
+  st.add(out, size_t(count) * ctx->K * 4, false, true);
+  if (int rc = st.bind()) return rc;
+  CUHE_CUDA(ctx, d.lookup(ctx, nullptr, 0, 0, 1, (const uint32_t*)st.dev(0), count, (const uint8_t*)st.dev(1),
+                          (uint32_t*)st.dev(2)),
+            "lookup encrypt launch");
+  if (int rc = st.finish()) return rc;
+  return check_status(ctx, st.staged());
+}
+
+}  // extern "C"

@@ -1,0 +1,585 @@
+// Paillier / Paillier-Lookup kernels for sm_100a.
+//
+// One instance (ciphertext) is owned by a TPI-lane group (see bigint_group.cuh);
+// a 128-thread block holds 128/TPI instances.  All arithmetic mod n^2 is in the
+// Montgomery domain with R = 2^(32K); arithmetic mod n uses the same K-limb
+// routines with n zero-padded to K limbs.
+#pragma once
+#include <cstdint>
+#include "bigint_group.cuh"
+
+namespace cuhe {
+
+// Rows of the per-key constant block (each row K words).
+enum ConstRow : int {
+  C_N2 = 0,     // n^2
+  C_R2 = 1,     // R^2 mod n^2
+  C_ONE = 2,    // 1
+  C_RM = 3,     // R mod n^2  (Montgomery form of 1)
+  C_N = 4,      // n, zero-padded
+  C_R2N = 5,    // R^2 mod n
+  C_NNEG = 6,   // 2^(32K) - n
+  C_NR = 7,     // n * R mod n^2
+  C_MULTR = 8,  // (secret multiplier) * R mod n
+  C_ROWS = 9
+};
+
+struct KeyScalars {
+  uint32_t ninv2;  // -(n^2)^-1 mod 2^32
+  uint32_t ninv1;  // -n^-1 mod 2^32
+  uint32_t ndiv;   // n^-1 mod 2^32 (exact division)
+  uint32_t mult_is_zero;
+};
+
+// status bits written by kernels
+enum StatusBits : int { ST_RANGE = 1 };
+
+enum ExpMode : int { EXP_POW = 0, EXP_ENCRYPT = 1, EXP_DECRYPT = 2, EXP_DECODE = 3 };
+
+constexpr int kBlockThreads = 128;
+
+template <int K>
+__host__ __device__ constexpr int inst_stride_words(int buffers) {
+  return buffers * K + 4;  // +4 words shifts consecutive instances by 4 banks
+}
+
+// -- helpers shared by kernels ---------------------------------------------
+
+template <int K, int TPI>
+__device__ __forceinline__ void copy_rows_to_smem(uint32_t* dst, const uint32_t* consts, const int* rows,
+                                                  int nrows) {
+  for (int r = 0; r < nrows; ++r)
+    for (int i = threadIdx.x; i < K; i += blockDim.x) dst[r * K + i] = consts[rows[r] * K + i];
+}
+
+// x + small (small < 2^32) over the group, with lookahead carry resolution.
+template <int K, int TPI>
+__device__ __forceinline__ void add_small(const Group<K, TPI>& g, uint32_t (&x)[K / TPI], uint32_t small) {
+  constexpr int L = K / TPI;
+  uint32_t add0 = (g.gl == 0) ? small : 0u;
+  x[0] = add_cc(x[0], add0);
+#pragma unroll
+  for (int j = 1; j < L; ++j) x[j] = addc_cc(x[j], 0u);
+  const uint32_t carry = addc(0u, 0u);
+  uint32_t ones = x[0];
+#pragma unroll
+  for (int j = 1; j < L; ++j) ones &= x[j];
+  const bool cin = g.lookahead(carry != 0u, ones == 0xffffffffu, nullptr);
+  if (cin) {
+    x[0] = add_cc(x[0], 1u);
+#pragma unroll
+    for (int j = 1; j < L; ++j) x[j] = addc_cc(x[j], 0u);
+    (void)addc(0u, 0u);
+  }
+}
+
+// x - y for x >= y over the group.
+template <int K, int TPI>
+__device__ __forceinline__ void sub_group(const Group<K, TPI>& g, uint32_t (&x)[K / TPI],
+                                          const uint32_t (&y)[K / TPI]) {
+  constexpr int L = K / TPI;
+  x[0] = sub_cc(x[0], y[0]);
+#pragma unroll
+  for (int j = 1; j < L; ++j) x[j] = subc_cc(x[j], y[j]);
+  const uint32_t borrow = subc(0u, 0u) & 1u;
+  uint32_t zero = x[0];
+#pragma unroll
+  for (int j = 1; j < L; ++j) zero |= x[j];
+  const bool bin = g.lookahead(borrow != 0u, zero == 0u, nullptr);
+  if (bin) {
+    x[0] = sub_cc(x[0], 1u);
+#pragma unroll
+    for (int j = 1; j < L; ++j) x[j] = subc_cc(x[j], 0u);
+    (void)subc(0u, 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-exponent modular exponentiation with per-instance bases.
+//   EXP_POW     out = base^e mod n^2
+//   EXP_ENCRYPT out = base^e * (1 + aux*n) mod n^2          (Paillier encrypt, g = n+1)
+//   EXP_DECRYPT out = floor((base^e mod n^2 - 1)/n) * mult mod n
+//   EXP_DECODE  out32 = popcount of the even bits of the EXP_DECRYPT value
+// The exponent is a host-built sliding-window schedule (host_bigint.h).
+// ---------------------------------------------------------------------------
+template <int K, int TPI, int W>
+__global__ void __launch_bounds__(kBlockThreads)
+k_modexp(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, int aux_words,
+         uint32_t* __restrict__ out, long long count, const uint32_t* __restrict__ consts, KeyScalars ks,
+         const int32_t* __restrict__ ops, int nops, int mode, int pop_words, int* status) {
+  constexpr int L = K / TPI;
+  constexpr int T = 1 << (W - 1);
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int STRIDE = inst_stride_words<K>(T + 1);
+  extern __shared__ __align__(16) uint32_t smem[];
+  // block rows: ONE, R2, NR, R2N, MULTR
+  uint32_t* s_one = smem;
+  uint32_t* s_r2 = smem + K;
+  uint32_t* s_nr = smem + 2 * K;
+  uint32_t* s_r2n = smem + 3 * K;
+  uint32_t* s_multr = smem + 4 * K;
+  {
+    const int rows[5] = {C_ONE, C_R2, C_NR, C_R2N, C_MULTR};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 5);
+  }
+  __syncthreads();
+
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;  // whole groups leave together
+  uint32_t* s_inst = smem + 5 * K + slot * STRIDE;
+  uint32_t* s_x = s_inst;               // current value (b operand of squarings)
+  uint32_t* s_tab = s_inst + K;         // T odd powers
+
+  uint32_t n2[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  uint32_t x[L], acc[L];
+  g.load(x, base + inst * K);
+  if (!g.less_than(x, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  // odd-power table in Montgomery form
+  g.mont_mul(acc, x, s_r2, n2, ks.ninv2);  // x*R
+  g.publish(s_tab, acc);
+  if (T > 1) {
+    uint32_t sq[L];
+    g.mont_mul(sq, acc, s_tab, n2, ks.ninv2);  // x^2 R
+    g.publish(s_x, sq);
+#pragma unroll 1
+    for (int t = 1; t < T; ++t) {
+      g.mont_mul(acc, acc, s_x, n2, ks.ninv2);
+      g.publish(s_tab + t * K, acc);
+    }
+  }
+  // exponent schedule
+  if (nops == 0) {
+    g.load(acc, s_tab);  // unused value, replaced below by R mod n^2
+    uint32_t rm[L];
+    g.load_ro(rm, consts + C_RM * K);
+#pragma unroll
+    for (int j = 0; j < L; ++j) acc[j] = rm[j];
+  } else {
+    const int first = __ldg(ops) & 0xffff;
+    g.load(acc, s_tab + (first - 1) * K);
+  }
+  g.publish(s_x, acc);
+#pragma unroll 1
+  for (int o = 1; o < nops; ++o) {
+    const int op = __ldg(ops + o);
+    const int sq = op >> 16;
+    const int idx = op & 0xffff;
+#pragma unroll 1
+    for (int s = 0; s < sq; ++s) {
+      g.mont_mul(acc, acc, s_x, n2, ks.ninv2);
+      g.publish(s_x, acc);
+    }
+    if (idx) {
+      g.mont_mul(acc, acc, s_tab + (idx - 1) * K, n2, ks.ninv2);
+      g.publish(s_x, acc);
+    }
+  }
+
+  if (mode == EXP_POW) {
+    g.mont_mul(x, acc, s_one, n2, ks.ninv2);
+    g.store(out + inst * K, x);
+    return;
+  }
+  if (mode == EXP_ENCRYPT) {
+    uint32_t m[L];
+    g.load(m, aux + inst * aux_words);  // aux_words == K (zero-padded m < n)
+    uint32_t nn[L];
+    g.load_ro(nn, consts + C_N * K);
+    if (!g.less_than(m, nn)) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
+    }
+    g.mont_mul(x, m, s_nr, n2, ks.ninv2);  // m*n (exact, < n^2)
+    add_small<K, TPI>(g, x, 1u);           // 1 + m*n = g^m mod n^2
+    g.publish(s_x, x);
+    g.mont_mul(x, acc, s_x, n2, ks.ninv2);  // r^n * g^m
+    g.store(out + inst * K, x);
+    return;
+  }
+  // decrypt / decode: y = base^e mod n^2 - 1
+  g.mont_mul(x, acc, s_one, n2, ks.ninv2);
+  uint32_t nn[L];
+  g.load_ro(nn, consts + C_N * K);
+  uint32_t res[L];
+  if (g.is_zero(x)) {
+    // floor(-1/n) = -1  ->  (-mult) mod n
+    uint32_t multr[L], mult[L];
+    g.load(multr, s_multr);
+    g.mont_mul(mult, multr, s_one, nn, ks.ninv1);
+#pragma unroll
+    for (int j = 0; j < L; ++j) res[j] = nn[j];
+    if (ks.mult_is_zero) {
+#pragma unroll
+      for (int j = 0; j < L; ++j) res[j] = 0u;
+    } else {
+      sub_group<K, TPI>(g, res, mult);
+    }
+  } else {
+    uint32_t one[L];
+#pragma unroll
+    for (int j = 0; j < L; ++j) one[j] = (g.gl == 0 && j == 0) ? 1u : 0u;
+    sub_group<K, TPI>(g, x, one);                 // y
+    uint32_t t1[L];
+    g.mont_mul(t1, x, s_one, nn, ks.ninv1);       // y R^-1 mod n
+    uint32_t rem[L];
+    g.mont_mul(rem, t1, s_r2n, nn, ks.ninv1);     // y mod n
+    sub_group<K, TPI>(g, x, rem);                 // y - (y mod n) = q*n
+    uint32_t q[L], mneg[L];
+    g.load_ro(mneg, consts + C_NNEG * K);
+    g.exact_div(q, x, mneg, ks.ndiv, K / 2);      // q = floor(y/n) < n
+    g.mont_mul(res, q, s_multr, nn, ks.ninv1);    // q * mult mod n
+  }
+  if (mode == EXP_DECRYPT) {
+    g.store(out + inst * K, res);
+    return;
+  }
+  // EXP_DECODE
+  int pc = 0;
+#pragma unroll
+  for (int j = 0; j < L; ++j)
+    if (g.gl * L + j < pop_words) pc += __popc(res[j] & 0x55555555u);
+#pragma unroll
+  for (int off = TPI / 2; off > 0; off >>= 1) pc += __shfl_xor_sync(g.mask, pc, off, TPI);
+  if (g.gl == 0) out[inst] = uint32_t(pc);
+}
+
+// ---------------------------------------------------------------------------
+// Modular exponentiation with a per-instance exponent (fixed 4-bit windows, so
+// every group of a warp follows the same schedule):
+//   out[i] = base[i]^exps[i] mod n^2, exps[i] held in exp_words words.
+// ---------------------------------------------------------------------------
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_modexp_var(const uint32_t* __restrict__ base, const uint32_t* __restrict__ exps, int exp_words, int windows,
+             uint32_t* __restrict__ out, long long count, const uint32_t* __restrict__ consts, KeyScalars ks,
+             int* status) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int T = 16;
+  constexpr int STRIDE = inst_stride_words<K>(T + 1);
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_one = smem;
+  uint32_t* s_r2 = smem + K;
+  {
+    const int rows[2] = {C_ONE, C_R2};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 2);
+  }
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;
+  uint32_t* s_x = smem + 2 * K + slot * STRIDE;
+  uint32_t* s_tab = s_x + K;
+  uint32_t n2[L], x[L], acc[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load(x, base + inst * K);
+  if (!g.less_than(x, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  g.load_ro(acc, consts + C_RM * K);
+  g.publish(s_tab, acc);                   // x^0
+  g.mont_mul(acc, x, s_r2, n2, ks.ninv2);  // x^1
+  g.publish(s_tab + K, acc);
+  g.publish(s_x, acc);
+#pragma unroll 1
+  for (int t = 2; t < T; ++t) {
+    g.mont_mul(acc, acc, s_x, n2, ks.ninv2);
+    g.publish(s_tab + t * K, acc);
+  }
+  const uint32_t* e = exps + inst * exp_words;
+  g.load_ro(acc, consts + C_RM * K);
+  g.publish(s_x, acc);
+  bool started = false;
+#pragma unroll 1
+  for (int w = windows - 1; w >= 0; --w) {
+    const int bit = 4 * w;
+    const int digit = (bit / 32 < exp_words) ? int((__ldg(e + bit / 32) >> (bit % 32)) & 15u) : 0;
+    if (started) {
+#pragma unroll 1
+      for (int s = 0; s < 4; ++s) {
+        g.mont_mul(acc, acc, s_x, n2, ks.ninv2);
+        g.publish(s_x, acc);
+      }
+    }
+    if (digit) {
+      g.mont_mul(acc, acc, s_tab + digit * K, n2, ks.ninv2);
+      g.publish(s_x, acc);
+      started = true;
+    }
+  }
+  g.mont_mul(x, acc, s_one, n2, ks.ninv2);
+  g.store(out + inst * K, x);
+}
+
+// distance[v] = sum of the chunk_num per-chunk popcounts of vector v.
+__global__ void k_sum_chunks(const uint32_t* __restrict__ counts, long long vectors, int chunk_num,
+                             long long* __restrict__ distance) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= vectors) return;
+  long long s = 0;
+  for (int c = 0; c < chunk_num; ++c) s += counts[v * chunk_num + c];
+  distance[v] = s;
+}
+
+// Integer multiply-add throughput probe: every iteration issues one
+// mad.lo.u32 and one mad.hi.u32 (one 32x32->64 word product) on each of 16
+// independent accumulators.  Used to state the IMAD roofline of the chip.
+__global__ void __launch_bounds__(256) k_imad_probe(uint32_t* sink, int iters, uint32_t seed) {
+  uint32_t lo[8], hi[8];
+  const uint32_t a = seed ^ threadIdx.x, b = seed * 2654435761u + blockIdx.x;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) { lo[j] = a + j; hi[j] = b - j; }
+#pragma unroll 1
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(lo[j]) : "r"(hi[j]), "r"(b));
+      asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(hi[j]) : "r"(lo[j]), "r"(a));
+    }
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x ^= lo[j] ^ hi[j];
+  if (x == 0x9e3779b9u) sink[0] = x;
+}
+
+// ---------------------------------------------------------------------------
+// Pointwise modular multiplication: out[i] = a[i] * b[i] mod n^2.
+// ---------------------------------------------------------------------------
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_mulmod(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b, uint32_t* __restrict__ out,
+         long long count, const uint32_t* __restrict__ consts, KeyScalars ks, int* status) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int STRIDE = inst_stride_words<K>(1);
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_r2 = smem;
+  {
+    const int rows[1] = {C_R2};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 1);
+  }
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;
+  uint32_t* s_b = smem + K + slot * STRIDE;
+  uint32_t n2[L], x[L], y[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load(x, a + inst * K);
+  g.load(y, b + inst * K);
+  if (!g.less_than(x, n2) || !g.less_than(y, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  g.publish(s_b, y);
+  g.mont_mul(x, x, s_b, n2, ks.ninv2);   // a b R^-1
+  g.mont_mul(x, x, s_r2, n2, ks.ninv2);  // a b
+  g.store(out + inst * K, x);
+}
+
+// out[q][j] = query[q] * index[j] mod n^2 with queries given in Montgomery form
+// (query * R mod n^2).  One Montgomery product per output.
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_mulmod_outer(const uint32_t* __restrict__ qmont, long long nq, const uint32_t* __restrict__ index,
+               long long nx, uint32_t* __restrict__ out, const uint32_t* __restrict__ consts, KeyScalars ks,
+               int* status) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  extern __shared__ __align__(16) uint32_t smem[];
+  const long long qi = blockIdx.y;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) smem[i] = qmont[qi * K + i];
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long j = (long long)blockIdx.x * IPB + slot;
+  if (j >= nx) return;
+  uint32_t n2[L], x[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load_ro(x, index + j * K);
+  if (!g.less_than(x, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  g.mont_mul(x, x, smem, n2, ks.ninv2);
+  g.store(out + (qi * nx + j) * K, x);
+}
+
+// out[i] = in[i] * R mod n^2 (to Montgomery form), or in[i] * R^-1 (from).
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_convert(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long long count,
+          const uint32_t* __restrict__ consts, KeyScalars ks, int to_mont, int* status) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  extern __shared__ __align__(16) uint32_t smem[];
+  {
+    const int rows[1] = {to_mont ? (int)C_R2 : (int)C_ONE};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 1);
+  }
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;
+  uint32_t n2[L], x[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load(x, in + inst * K);
+  if (!g.less_than(x, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  g.mont_mul(x, x, smem, n2, ks.ninv2);
+  g.store(out + inst * K, x);
+}
+
+// ---------------------------------------------------------------------------
+// Paillier-Lookup encryption by fixed-base table product:
+//   c = prod_i G[i][digit_i(m)] * prod_k NOISE[idx_k]  mod n^2
+// G and NOISE are device-resident in Montgomery form.  The plaintext digits
+// come either from binary embeddings (Hamming padding "0b" per bit, read as
+// MSB-first chunks of chunk_len bits) or from little-endian plaintext words.
+// ---------------------------------------------------------------------------
+constexpr int kNoiseMultiples = 14;
+
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len, int chunk_num,
+                 const uint32_t* __restrict__ plain, int plain_words, long long count, int message_chunks,
+                 const uint32_t* __restrict__ gtab, const uint32_t* __restrict__ noise, int noise_entries,
+                 const uint8_t* __restrict__ noise_idx, uint32_t* __restrict__ out,
+                 const uint32_t* __restrict__ consts, KeyScalars ks, int* status) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int ACC_STRIDE = inst_stride_words<K>(1);
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_one = smem;
+  {
+    const int rows[1] = {C_ONE};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 1);
+  }
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;
+  uint32_t* s_acc = smem + K + slot * ACC_STRIDE;
+  uint16_t* s_rows = reinterpret_cast<uint16_t*>(smem + K + IPB * ACC_STRIDE) + slot * message_chunks;
+  __shared__ int s_count[IPB];
+
+  // nonzero digits -> list of table rows (lane 0 of the group)
+  if (g.gl == 0) {
+    int cnt = 0;
+    if (bits) {
+      const long long vec = inst / chunk_num;
+      const int chunk = int(inst % chunk_num);
+      const int padded_total = 2 * embed_len;
+      const int cbase = chunk * chunk_len;
+      int avail = padded_total - cbase;
+      if (avail > chunk_len) avail = chunk_len;
+      if (avail < 0) avail = 0;
+      const uint8_t* vb = bits + vec * embed_len;
+      for (int i = 0; i < message_chunks; ++i) {
+        int d = 0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+          const int e = 8 * i + b;  // exponent within the chunk value
+          if (e < avail) {
+            const int p = cbase + (avail - 1 - e);  // padded MSB-first position
+            if (p & 1) d |= (vb[p >> 1] & 1) << b;
+          }
+        }
+        if (d) s_rows[cnt++] = uint16_t(i * 256 + d);
+      }
+    } else {
+      const uint8_t* mb = reinterpret_cast<const uint8_t*>(plain + inst * plain_words);
+      const int bytes = plain_words * 4 < message_chunks ? plain_words * 4 : message_chunks;
+      for (int i = 0; i < bytes; ++i) {
+        const int d = mb[i];
+        if (d) s_rows[cnt++] = uint16_t(i * 256 + d);
+      }
+    }
+    s_count[slot] = cnt;
+  }
+  __syncwarp(g.mask);
+  const int cnt = s_count[slot];
+
+  uint32_t n2[L], acc[L], a[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load_ro(acc, consts + C_RM * K);  // Montgomery one
+  g.publish(s_acc, acc);
+#pragma unroll 1
+  for (int j = 0; j < cnt; ++j) {
+    const int row = s_rows[j];
+    g.load_ro(a, gtab + (long long)row * K);
+    g.mont_mul(acc, a, s_acc, n2, ks.ninv2);
+    g.publish(s_acc, acc);
+  }
+  const uint8_t* idx = noise_idx + inst * kNoiseMultiples;
+#pragma unroll 1
+  for (int k = 0; k < kNoiseMultiples; ++k) {
+    const int r = idx[k];
+    if (r >= noise_entries) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
+    }
+    g.load_ro(a, noise + (long long)r * K);
+    g.mont_mul(acc, a, s_acc, n2, ks.ninv2);
+    g.publish(s_acc, acc);
+  }
+  g.mont_mul(a, acc, s_one, n2, ks.ninv2);
+  g.store(out + inst * K, a);
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-base table construction: rows i of G = base_i^j, j = 0..255, with
+// base_i = g^(2^(8i)) (all in Montgomery form).  One group per (row, chunk of
+// 16 consecutive j); thread-level work is 16 sequential products.
+// ---------------------------------------------------------------------------
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_table_rows(const uint32_t* __restrict__ bases_mont, int rows, uint32_t* __restrict__ gtab,
+             const uint32_t* __restrict__ consts, KeyScalars ks) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int STRIDE = inst_stride_words<K>(2);
+  extern __shared__ __align__(16) uint32_t smem[];
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;  // row * 16 + block of j
+  if (inst >= (long long)rows * 16) return;
+  const int row = int(inst / 16);
+  const int jb = int(inst % 16);
+  uint32_t* s_base = smem + slot * STRIDE;
+  uint32_t* s_pow = s_base + K;
+  uint32_t n2[L], b[L], p[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load_ro(b, bases_mont + (long long)row * K);
+  g.publish(s_base, b);
+  // p = base^(16*jb) via square-and-multiply over the 8-bit exponent
+  g.load_ro(p, consts + C_RM * K);
+  const int e = 16 * jb;
+#pragma unroll 1
+  for (int bit = 7; bit >= 0; --bit) {
+    g.publish(s_pow, p);
+    g.mont_mul(p, p, s_pow, n2, ks.ninv2);
+    if ((e >> bit) & 1) g.mont_mul(p, p, s_base, n2, ks.ninv2);
+  }
+#pragma unroll 1
+  for (int t = 0; t < 16; ++t) {
+    g.store(gtab + ((long long)row * 256 + e + t) * K, p);
+    g.mont_mul(p, p, s_base, n2, ks.ninv2);
+  }
+}
+
+}  // namespace cuhe

@@ -1,0 +1,162 @@
+/* C ABI of the B200 Paillier / Paillier-Lookup kernels (libcuhe_b200.so).
+ *
+ * Conventions
+ *  - Big integers are arrays of little-endian 32-bit words.  A key of
+ *    key_len-bit primes has an n of 2*key_len bits and an n^2 of 4*key_len
+ *    bits; the library works with K = key_len/8 words per value mod n^2
+ *    (64, 128 or 256 words for key_len 512, 1024, 2048).  Every batched
+ *    array below uses a stride of K words per item, plaintexts included
+ *    (plaintexts < n occupy the low K/2 words, the rest are zero).
+ *  - Pointers may be host or device memory.  Host buffers are staged through
+ *    a context-owned device workspace and the call returns when the result is
+ *    back on the host.  Device buffers are processed on the context stream
+ *    and the call returns after queueing; cuhe_synchronize() waits.
+ *  - Every function returns 0 on success or a negative cuhe_status; the
+ *    message of the last failure is available from cuhe_last_error().
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the cuhepy project).
+ */
+#ifndef CUHE_PAILLIER_H
+#define CUHE_PAILLIER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cuhe_status {
+  CUHE_OK = 0,
+  CUHE_INVALID_ARGUMENT = -1, /* reference raises ValueError / RuntimeError */
+  CUHE_OUT_OF_MEMORY = -2,
+  CUHE_CUDA_ERROR = -3,
+  CUHE_NOT_READY = -4,        /* keys or tables not loaded */
+  CUHE_RANGE = -5             /* an input is outside [0, n^2) or [0, n) */
+} cuhe_status;
+
+typedef struct cuhe_paillier cuhe_paillier;
+
+/* Library version string and the last error of a context (or of the last
+ * failed cuhe_paillier_create when ctx is NULL). */
+const char* cuhe_version(void);
+const char* cuhe_last_error(const cuhe_paillier* ctx);
+
+/* Create a context for the public modulus n (n_words words).  Replaces the
+ * key material held inside PaillierGPUClient / PaillierGPULookupClient
+ * (src/cuhepy/paillier/_gpu_ext/paillier_GPU_client.cu:747-760;
+ *  _lookup_gpu_ext/paillier_GPU_lookup_client.cu:1570-1612) and the pk dict
+ * of Paillier.encrypt (src/cuhepy/paillier/scheme.py:63-83). */
+int cuhe_paillier_create(const uint32_t* n, int n_words, int device, cuhe_paillier** out);
+void cuhe_paillier_destroy(cuhe_paillier* ctx);
+/* Words per value mod n^2 (K) used by this context. */
+int cuhe_paillier_words(const cuhe_paillier* ctx);
+/* Use a caller stream (cudaStream_t passed as void*); NULL restores the
+ * context's own stream. */
+int cuhe_paillier_set_stream(cuhe_paillier* ctx, void* stream);
+int cuhe_synchronize(cuhe_paillier* ctx);
+
+/* Install the secret decryption exponent and multiplier:
+ *   textbook Paillier: exponent = phi, multiplier = phi^-1 mod n
+ *     (src/cuhepy/paillier/scheme.py:86-104)
+ *   Paillier-Lookup:   exponent = a,   multiplier = g_a_inv
+ *     (src/cuhepy/paillier/lookup.py:257-278) */
+int cuhe_paillier_set_secret(cuhe_paillier* ctx, const uint32_t* exponent, int exponent_words,
+                             const uint32_t* multiplier, int multiplier_words);
+
+/* c[i] = (1 + m[i]*n) * r[i]^n mod n^2, i.e. g^m r^n with g = n + 1.
+ * Replaces Paillier.encrypt (src/cuhepy/paillier/scheme.py:63-83) with the
+ * randomness r supplied by the caller, and the device half of
+ * PaillierGPUClient.encrypt (paillier_GPU_client.cu:873-974, 458-546). */
+int cuhe_paillier_encrypt(cuhe_paillier* ctx, const uint32_t* m, const uint32_t* r, uint32_t* c,
+                          int64_t count);
+
+/* m[i] = floor((c[i]^e mod n^2 - 1) / n) * multiplier mod n (the installed
+ * secret).  Replaces Paillier.decrypt (scheme.py:86-104),
+ * PaillierLookup.decrypt (lookup.py:257-278) and decrypt_only_kernel
+ * (paillier_GPU_lookup_client.cu:1014-1050, 2440-2499). */
+int cuhe_paillier_decrypt(cuhe_paillier* ctx, const uint32_t* c, uint32_t* m, int64_t count);
+
+/* Hamming decode: distance[v] = sum over the chunk_num chunks of vector v of
+ * popcount(even bits of decrypt(c)).  Replaces decode_hamming_client
+ * (paillier_GPU_lookup_client.cu:2338-2437: decrypt_only_kernel +
+ * odd_popcount_kernel + host sum; hamming/paillier_lookup.py:221-242). */
+int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t vectors, int chunk_num,
+                                 int chunk_len, int64_t* distance);
+
+/* out[i] = base[i]^exponent mod n^2 (generic fixed-exponent batch). */
+int cuhe_paillier_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* exponent,
+                         int exponent_words, uint32_t* out, int64_t count);
+
+/* out[i] = base[i]^exponents[i] mod n^2 with a per-item exponent of
+ * exponent_words words (fixed 4-bit windows).  Replaces the per-entry
+ * gmpy2.powmod of precompute_noise_table (src/cuhepy/paillier/lookup.py:113-117;
+ * paillier_GPU_lookup_client.cu:593-626). */
+int cuhe_paillier_modexp_each(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* exponents,
+                              int exponent_words, uint32_t* out, int64_t count);
+
+/* out[i] = a[i] * b[i] mod n^2.  Replaces Paillier.add / PaillierLookup.add
+ * (scheme.py:107-119; lookup.py:282-294) and modmul_pointwise_kernel behind
+ * encode_hamming_server (paillier_GPU_lookup_client.cu:811-835, 2312-2335). */
+int cuhe_paillier_mulmod(cuhe_paillier* ctx, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                         int64_t count);
+
+/* out[q*nx + j] = query[q] * index[j] mod n^2: encode_hamming_server for a
+ * batch of queries against a resident index (one Montgomery product each). */
+int cuhe_paillier_mulmod_outer(cuhe_paillier* ctx, const uint32_t* query, int64_t nq,
+                               const uint32_t* index, int64_t nx, uint32_t* out);
+
+/* Install the fixed-base tables of Paillier-Lookup in normal (non-Montgomery)
+ * form: g_table[(i*256 + j)*K ...] = g_table[i][j] and noise[k*K ...].
+ * Replaces load_config(tables) / ensure_device_tables_
+ * (paillier_GPU_lookup_client.cu:1771-1836, 2625-2652). */
+int cuhe_lookup_set_tables(cuhe_paillier* ctx, const uint32_t* g_table, int message_chunks,
+                           const uint32_t* noise, int noise_entries);
+/* Build g_table[i][j] = (g^(2^(8i)))^j on the device (lookup.py:104-110;
+ * precompute_g_table, paillier_GPU_lookup_client.cu:550-588) and install the
+ * given noise table.  noise may be NULL to keep the current one. */
+int cuhe_lookup_build_tables(cuhe_paillier* ctx, const uint32_t* g, int message_chunks,
+                             const uint32_t* noise, int noise_entries);
+/* Copy the installed g_table back in normal form (dump_tables,
+ * paillier_GPU_lookup_client.cu:1838-1862).  out holds message_chunks*256*K words. */
+int cuhe_lookup_get_g_table(cuhe_paillier* ctx, uint32_t* out);
+
+/* Encrypt binary embeddings bits[vectors][embed_len] (0/1 bytes) into
+ * vectors*chunk_num ciphertexts (chunk_len = 2*key_len bits of Hamming-padded
+ * plaintext per chunk) using 14 caller-supplied noise indices per ciphertext.
+ * Replaces PaillierGPULookupClient.encrypt / encrypt_kernel
+ * (paillier_GPU_lookup_client.cu:1873-2002, 839-948) and
+ * PaillierLookupCPU.encrypt (hamming/paillier_lookup.py:199-219). */
+int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t vectors, int embed_len,
+                             int chunk_len, int chunk_num, const uint8_t* noise_index, uint32_t* out);
+
+/* Encrypt plaintexts m[i] < n (K-word stride) by table product.  Replaces
+ * PaillierLookup.encrypt (lookup.py:213-252) and encrypt_cts
+ * (paillier_GPU_lookup_client.cu:2006-2131, 951-1011). */
+int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t count,
+                             const uint8_t* noise_index, uint32_t* out);
+
+/* Measure the integer multiply roofline of a device: 32x32->64-bit word
+ * products per second (one mad.lo.u32 + one mad.hi.u32 each) sustained by a
+ * dependency-light probe kernel over all SMs.  No counterpart in the
+ * reference; it provides the denominator of the modexp roofline. */
+int cuhe_imad_peak(int device, double* word_products_per_second);
+
+/* Host-only helper (no device needed): the left-to-right sliding-window
+ * schedule used for a fixed exponent.  Writes at most capacity ops, each
+ * (squarings << 16) | (odd-power index + 1), and returns the op count.  It
+ * has no counterpart in the reference; it exists so the schedule can be
+ * checked on a machine without a GPU. */
+int cuhe_window_schedule(const uint32_t* exponent, int exponent_words, int window, int32_t* ops, int capacity);
+
+/* Select (threads per instance, window) for this context's width; 0 picks the
+ * built-in default.  Used by the autotuner. */
+int cuhe_paillier_set_tuning(cuhe_paillier* ctx, int threads_per_instance, int window);
+int cuhe_paillier_get_tuning(const cuhe_paillier* ctx, int* threads_per_instance, int* window);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUHE_PAILLIER_H */
