@@ -330,19 +330,21 @@ __global__ void k_sum_chunks(const uint32_t* __restrict__ counts, long long vect
 }
 
 // Integer multiply-add throughput probe: every iteration issues one
-// mad.lo.u32 and one mad.hi.u32 (one 32x32->64 word product) on each of 16
-// independent accumulators.  Used to state the IMAD roofline of the chip.
+// mad.lo.u32 and one mad.hi.u32 (one 32x32->64 word product) per operand
+// pair into 16 accumulators that depend only on themselves, so the probe is
+// bound by issue/pipe throughput, not latency.  Used to state the IMAD
+// roofline of the chip.
 __global__ void __launch_bounds__(256) k_imad_probe(uint32_t* sink, int iters, uint32_t seed) {
-  uint32_t lo[8], hi[8];
+  uint32_t lo[8], hi[8], x[8];
   const uint32_t a = seed ^ threadIdx.x, b = seed * 2654435761u + blockIdx.x;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) { lo[j] = a + j; hi[j] = b - j; }
+  for (int j = 0; j < 8; ++j) { lo[j] = a + j; hi[j] = b - j; x[j] = (a * 33u) ^ (b + 7u * j); }
 #pragma unroll 1
   for (int i = 0; i < iters; ++i) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(lo[j]) : "r"(hi[j]), "r"(b));
-      asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(hi[j]) : "r"(lo[j]), "r"(a));
+      asm volatile("mad.lo.u32 %0, %1, %2, %0;" : "+r"(lo[j]) : "r"(x[j]), "r"(b));
+      asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(hi[j]) : "r"(x[j]), "r"(b));
     }
   }
   uint32_t x = 0;
