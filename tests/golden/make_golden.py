@@ -174,18 +174,84 @@ def lookup_fixture(lookup, number, key_len: int, alpha_len: int, hamming_vectors
     }
 
 
+class SeededSecrets(RecordingSecrets):
+    """Seeded source whose randbelow/randbits match random.Random(seed)."""
+
+
+def load_reference_native() -> None:
+    """Make the compiled reference _bfv_rns (oracle/_ref) importable as the
+    reference package's own extension module."""
+    import importlib.util
+
+    sys.path.insert(0, str(REPO / "oracle" / "_ref"))
+    import _bfv_rns  # noqa: F401  (built by oracle/Makefile)
+
+    sys.modules["cuhepy.bfv._cpu_ext._bfv_rns"] = _bfv_rns
+    assert importlib.util.find_spec("cuhepy.bfv._cpu_ext") is not None
+
+
+def bfv_fixture(bfv_scheme, n: int, t: int, bits: int, gadget: int, embed_len: int,
+                vectors: list[list[int]], query: list[int], seed: int, backends: tuple[str, ...]) -> dict:
+    """BFVClient (hamming/bfv.py) with rns_modulus=True: keys, a packed index, one
+    query and encode_hamming_server_packed on several server backends."""
+    import json as _json
+
+    load_reference_native()
+    import cuhepy.hamming.bfv as hb
+
+    rec = SeededSecrets(seed)
+    bfv_scheme.secrets = rec
+    client = hb.BFVClient(embed_len, n, t, bits, gadget, response_modulus_bits=40, rns_modulus=True)
+    q_wire = client.encrypt_vec_one(query)
+    index = client.encrypt_vec_packed(vectors)
+    results = {}
+    for backend in backends:
+        server = hb.BFVClient(skip_key_gen=True, server_backend=backend)
+        server.load_config(_json.loads(client.stringify_config()))
+        server.load_stringified_keys(client.stringify_pk())
+        for compact in (False, True):
+            res = server.encode_hamming_server_packed(q_wire, index, len(vectors), compact=compact)
+            results[f"{backend}_{'compact' if compact else 'full'}"] = [[h(v) for v in ct] for ct in res]
+    first = next(iter(results))
+    for name, value in results.items():
+        other = first if name.endswith("full") == first.endswith("full") else None
+        if other and value != results[other]:
+            raise AssertionError(f"backend {name} differs from {other}")
+    compacted = [[int(v, 16) for v in ct] for ct in results[f"{backends[0]}_compact"]]
+    distances = client.decode_hamming_client_packed(compacted, len(vectors))
+    return {
+        "seed": seed, "n": n, "t": t, "q_bits": bits, "gadget_bits": gadget, "embed_len": embed_len,
+        "response_modulus_bits": 40, "eta": 21,
+        "vectors": ["".join(map(str, v)) for v in vectors], "query": "".join(map(str, query)),
+        "key_id": client._pk()["key_id"],
+        "query_wire": [h(v) for v in q_wire], "index_wire": [[h(v) for v in ct] for ct in index],
+        "results": results, "distances": distances,
+    }
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference", type=Path)
     parser.add_argument("--only", default="")
     args = parser.parse_args()
     scheme, lookup, bfv_scheme, number = setup(args.reference)
+    small_vectors = [[0, 1, 0], [1, 0, 1], [0, 0, 0]] * 13
+    rng = random.Random(1337)
+    mid_vectors = [[rng.getrandbits(1) for _ in range(20)] for _ in range(77)]
+    mid_query = [rng.getrandbits(1) for _ in range(20)]
+    all_backends = ("residue", "native", "rns", "optimized", "reference")
     jobs = {
         "paillier_512": lambda: paillier_fixture(scheme, number, 512),
         "paillier_1024": lambda: paillier_fixture(scheme, number, 1024),
         "lookup_512": lambda: lookup_fixture(lookup, number, 512, 280, 0),
         "lookup_1024": lambda: lookup_fixture(lookup, number, 1024, 280, 6),
     }
+    for bits, gadget in ((60, 4), (120, 15), (180, 30), (180, 61), (480, 127)):
+        jobs[f"bfv_n16_q{bits}_g{gadget}"] = (
+            lambda b=bits, g=gadget: bfv_fixture(bfv_scheme, 16, 97, b, g, 3, small_vectors, [0, 1, 0],
+                                                 100 + b + g, all_backends))
+    jobs["bfv_n256_q180_g30"] = lambda: bfv_fixture(
+        bfv_scheme, 256, 7681, 180, 30, 20, mid_vectors, mid_query, 4242, ("residue", "native", "reference"))
     for name, job in jobs.items():
         if args.only and args.only not in name:
             continue
