@@ -31,6 +31,11 @@ LIBRARIES = {
         "depends": ["bigint_group.cuh", "paillier_kernels.cuh", "host_bigint.h"],
         "headers": ["cuhe_paillier.h"],
     },
+    "libcuhe_bfv_b200.so": {
+        "sources": ["cuhe_bfv.cu"],
+        "depends": ["bfv_arith.cuh", "bfv_host.h", "bfv_kernels.cuh"],
+        "headers": ["cuhe_bfv.h", "cuhe_paillier.h"],
+    },
 }
 
 

@@ -1,0 +1,677 @@
+// BFV residue-ring kernels for sm_100a.
+//
+// Layout in HBM: residues are u64 planes [poly][prime][N] in coefficient or
+// NTT (bit-reversed) order; composed integers are [poly][N][W] little-endian
+// u64 words (W = ceil(bits(Q)/64)).  The negacyclic NTT of one N-point plane
+// runs inside one CTA in shared memory (N <= 16384).
+#pragma once
+#include <cstdint>
+
+#include "bfv_arith.cuh"
+
+namespace cuhe {
+namespace bfv {
+
+constexpr int kMaxPrimes = 17;
+constexpr int kMaxResidue = 8;
+constexpr int kCrtWordsDev = 18;
+constexpr int kMaxWords = 8;  // composed coefficient words (Q <= 512 bits)
+
+struct BaseDev {
+  int start, count, tstart, tcount;
+  u64 inv[kMaxPrimes], inv_q[kMaxPrimes];
+  u64 partial_mod_target[kMaxPrimes][kMaxPrimes];  // [k][j]
+  u64 product_mod_target[kMaxPrimes], product_mod_target_q[kMaxPrimes];
+  u64 partial_words[kMaxPrimes][kCrtWordsDev];
+  u64 product_words[kCrtWordsDev];
+};
+
+struct RingDev {
+  int n, logn, primes, residue, tensor, digits, digit_bits, words;
+  Prime prime[kMaxPrimes];
+  const u64* fwd[kMaxPrimes];
+  const u64* fwd_q[kMaxPrimes];
+  const u64* inv[kMaxPrimes];
+  const u64* inv_q[kMaxPrimes];
+  u64 n_inv[kMaxPrimes], n_inv_q[kMaxPrimes], last[kMaxPrimes], last_q[kMaxPrimes];
+  u64 garner[kMaxResidue][kMaxResidue], garner_q[kMaxResidue][kMaxResidue];
+  u64 q_words[kMaxWords];       // Q
+  u64 pow64_mod[kMaxPrimes][kMaxWords];  // 2^(64i) mod p_j
+  // exact scale-and-round (valid when has_scale)
+  int has_scale;
+  u64 t;
+  BaseDev q_to_b, b_to_q;
+  u64 inv_q_mod_b[kMaxPrimes], inv_q_mod_b_q[kMaxPrimes];
+  u64 t_mod[kMaxPrimes], t_mod_q[kMaxPrimes];  // t mod p_j (Shoup)
+};
+
+// ---- negacyclic NTT of one plane in shared memory ---------------------------
+// Forward: decimation in frequency with psi^bitrev twiddles; output bit-reversed.
+__device__ __forceinline__ void ntt_forward_smem(u64* a, const RingDev& R, int j) {
+  const int n = R.n;
+  const u64 p = R.prime[j].p, two_p = 2 * p;
+  const u64* __restrict__ w = R.fwd[j];
+  const u64* __restrict__ wq = R.fwd_q[j];
+  int shift = R.logn - 1;  // log2(gap)
+  for (int m = 1; m < n; m <<= 1, --shift) {
+    const int gap = 1 << shift;
+    for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
+      const int group = b >> shift, jj = b & (gap - 1);
+      const int i0 = (group << (shift + 1)) + jj, i1 = i0 + gap;
+      const u64 root = __ldg(w + m + group), rq = __ldg(wq + m + group);
+      u64 u = a[i0];
+      if (u >= two_p) u -= two_p;
+      const u64 v = shoup_lazy(a[i1], root, rq, p);
+      a[i0] = u + v;
+      a[i1] = u + two_p - v;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    u64 x = a[i];
+    if (x >= two_p) x -= two_p;
+    if (x >= p) x -= p;
+    a[i] = x;
+  }
+  __syncthreads();
+}
+
+// Inverse: decimation in time, 1/N fused into the last stage; canonical output.
+__device__ __forceinline__ void ntt_inverse_smem(u64* a, const RingDev& R, int j) {
+  const int n = R.n;
+  const u64 p = R.prime[j].p, two_p = 2 * p;
+  const u64* __restrict__ w = R.inv[j];
+  const u64* __restrict__ wq = R.inv_q[j];
+  int shift = 0;
+  for (int m = n / 2; m > 1; m >>= 1, ++shift) {
+    const int gap = 1 << shift;
+    for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
+      const int group = b >> shift, jj = b & (gap - 1);
+      const int i0 = (group << (shift + 1)) + jj, i1 = i0 + gap;
+      const u64 root = __ldg(w + m + group), rq = __ldg(wq + m + group);
+      const u64 u = a[i0], v = a[i1];
+      const u64 s = u + v;
+      a[i0] = s >= two_p ? s - two_p : s;
+      a[i1] = shoup_lazy(u + two_p - v, root, rq, p);
+    }
+    __syncthreads();
+  }
+  const int half = n / 2;
+  for (int b = threadIdx.x; b < half; b += blockDim.x) {
+    const u64 u = a[b], v = a[b + half];
+    a[b] = shoup(u + v, R.n_inv[j], R.n_inv_q[j], p);
+    a[b + half] = shoup(u + two_p - v, R.last[j], R.last_q[j], p);
+  }
+  __syncthreads();
+}
+
+// Batched transform: plane b of `data` (stride n) uses prime prime_of(b).
+// prime = (b / prime_block) % prime_mod + prime_base.
+__global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block,
+                      int inverse) {
+  extern __shared__ __align__(16) u64 s_plane[];
+  const RingDev& R = *ring;
+  const int n = R.n;
+  const long long b = blockIdx.x;
+  const int j = prime_base + int((b / prime_block) % prime_mod);
+  u64* plane = data + b * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[i] = plane[i];
+  __syncthreads();
+  if (inverse) ntt_inverse_smem(s_plane, R, j);
+  else ntt_forward_smem(s_plane, R, j);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[i];
+}
+
+// ---- wire unpacking ---------------------------------------------------------
+__device__ __forceinline__ u64 load_word_bytes(const uint8_t* data, long long nbytes, long long offset) {
+  u64 r = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const long long at = offset + k;
+    if (at < nbytes) r |= u64(data[at]) << (8 * k);
+  }
+  return r;
+}
+
+// words[poly][i][W] from `bits`-bit packed little-endian coefficients; each
+// coefficient must be < Q (status bit 1 otherwise).
+__global__ void k_unpack(const uint8_t* __restrict__ wire, long long poly_bytes, int bits, int polys,
+                         u64* __restrict__ words, const RingDev* __restrict__ ring, int* status) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)polys * R.n;
+  if (idx >= total) return;
+  const long long poly = idx / R.n;
+  const long long i = idx % R.n;
+  const uint8_t* src = wire + poly * poly_bytes;
+  const long long bit0 = i * bits;
+  const long long off = (bit0 / 64) * 8;
+  const int sh = int(bit0 % 64);
+  const int W = R.words;
+  const int nw = (bits + 63) / 64;
+  u64 v[kMaxWords];
+#pragma unroll
+  for (int k = 0; k < kMaxWords; ++k) v[k] = 0;
+  for (int k = 0; k < nw; ++k) {
+    u64 x = load_word_bytes(src, poly_bytes, off + 8 * k) >> sh;
+    if (sh) x |= load_word_bytes(src, poly_bytes, off + 8 * k + 8) << (64 - sh);
+    v[k] = x;
+  }
+  if (bits % 64) v[nw - 1] &= (u64(1) << (bits % 64)) - 1;
+  // v < Q ?
+  bool less = false, decided = false;
+  for (int k = W - 1; k >= 0 && !decided; --k) {
+    if (v[k] != R.q_words[k]) { less = v[k] < R.q_words[k]; decided = true; }
+  }
+  if (!less) atomicOr(status, 1);
+  u64* dst = words + idx * W;
+  for (int k = 0; k < W; ++k) dst[k] = v[k];
+}
+
+// value mod p_j of a composed W-word integer (Horner over 64-bit words)
+__device__ __forceinline__ u64 words_mod(const u64* v, int W, const RingDev& R, int j) {
+  u128 acc = 0;
+  for (int k = 0; k < W; ++k) acc += u128(v[k]) * R.pow64_mod[j][k];
+  return reduce128(acc, R.prime[j]);
+}
+
+// out[poly][j][i] = words[poly][i] mod p_j for j < primes_out
+__global__ void k_words_to_residues(const u64* __restrict__ words, long long polys, int primes_out,
+                                    u64* __restrict__ out, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const u64* w = words + idx * R.words;
+  for (int j = 0; j < primes_out; ++j) out[(poly * primes_out + j) * R.n + i] = words_mod(w, R.words, R, j);
+}
+
+// residues[t][c][j][i] of (query - tile) mod Q for c in {0,1}, j < primes_out.
+__global__ void k_diff_residues(const u64* __restrict__ query_words, const u64* __restrict__ tile_words,
+                                int tiles, int primes_out, u64* __restrict__ out, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per_tile = 2LL * R.n;
+  if (idx >= tiles * per_tile) return;
+  const long long t = idx / per_tile;
+  const int c = int((idx % per_tile) / R.n);
+  const int i = int(idx % R.n);
+  const int W = R.words;
+  const u64* a = query_words + ((long long)c * R.n + i) * W;
+  const u64* b = tile_words + ((t * 2 + c) * R.n + i) * W;
+  u64 d[kMaxWords];
+  u64 borrow = 0;
+  for (int k = 0; k < W; ++k) {
+    const u128 x = u128(a[k]) - b[k] - borrow;
+    d[k] = u64(x);
+    borrow = u64(x >> 64) ? 1 : 0;
+  }
+  if (borrow) {
+    u64 carry = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 s = u128(d[k]) + R.q_words[k] + carry;
+      d[k] = u64(s);
+      carry = u64(s >> 64);
+    }
+  }
+  for (int j = 0; j < primes_out; ++j)
+    out[((t * 2 + c) * primes_out + j) * R.n + i] = words_mod(d, W, R, j);
+}
+
+// NTT-domain tensor of (x0, x1) and (y0, y1): out = (x0 y0, x0 y1 + x1 y0, x1 y1).
+__global__ void k_tensor(const u64* __restrict__ x, const u64* __restrict__ y, int polys, int primes,
+                         u64* __restrict__ out, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = (long long)primes * R.n;
+  if (idx >= polys * per) return;
+  const long long t = idx / per;
+  const int j = int((idx % per) / R.n);
+  const int i = int(idx % R.n);
+  const Prime& m = R.prime[j];
+  const u64 a0 = x[((t * 2 + 0) * primes + j) * R.n + i], a1 = x[((t * 2 + 1) * primes + j) * R.n + i];
+  const u64 b0 = y[((t * 2 + 0) * primes + j) * R.n + i], b1 = y[((t * 2 + 1) * primes + j) * R.n + i];
+  out[((t * 3 + 0) * primes + j) * R.n + i] = reduce128(u128(a0) * b0, m);
+  out[((t * 3 + 1) * primes + j) * R.n + i] = reduce128(u128(a0) * b1 + u128(a1) * b0, m);
+  out[((t * 3 + 2) * primes + j) * R.n + i] = reduce128(u128(a1) * b1, m);
+}
+
+// NTT-domain square of (x0, x1): out = (x0^2, 2 x0 x1, x1^2) per prime.
+__global__ void k_tensor_square(const u64* __restrict__ x, int tiles, int primes, u64* __restrict__ out,
+                                const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per_tile = (long long)primes * R.n;
+  if (idx >= tiles * per_tile) return;
+  const long long t = idx / per_tile;
+  const int j = int((idx % per_tile) / R.n);
+  const int i = int(idx % R.n);
+  const Prime& m = R.prime[j];
+  const u64 a = x[((t * 2 + 0) * primes + j) * R.n + i];
+  const u64 b = x[((t * 2 + 1) * primes + j) * R.n + i];
+  const u128 ab = u128(a) * b;
+  out[((t * 3 + 0) * primes + j) * R.n + i] = reduce128(u128(a) * a, m);
+  // x0*x1 + x1*x0 (< 2^121, exact in 128 bits)
+  out[((t * 3 + 1) * primes + j) * R.n + i] = reduce128(ab + ab, m);
+  out[((t * 3 + 2) * primes + j) * R.n + i] = reduce128(u128(b) * b, m);
+}
+
+// ---- exact RNS scale-and-round (round(t z / Q) mod Q from z mod P) -----------
+__device__ __forceinline__ void words_addmul(u64 (&v)[kCrtWordsDev], const u64* src, u64 m) {
+  u128 c = 0;
+#pragma unroll 1
+  for (int i = 0; i < kCrtWordsDev; ++i) {
+    c += u128(src[i]) * m + v[i];
+    v[i] = u64(c);
+    c >>= 64;
+  }
+}
+
+__device__ __forceinline__ bool words_ge(const u64 (&a)[kCrtWordsDev], const u64 (&b)[kCrtWordsDev]) {
+  for (int i = kCrtWordsDev - 1; i >= 0; --i)
+    if (a[i] != b[i]) return a[i] > b[i];
+  return true;
+}
+
+struct Normalized {
+  u64 terms[kMaxPrimes];
+  u64 alpha;
+};
+
+// A = sum terms_j M_j, theta = A/M; alpha = floor(theta) or round(theta),
+// certified by a fixed-point interval with an exact multiword fallback.
+__device__ __forceinline__ void normalize(const BaseDev& B, const RingDev& R, const u64* residues, bool centered,
+                                          Normalized& out) {
+  u128 frac = 0;
+  for (int j = 0; j < B.count; ++j) {
+    const Prime& m = R.prime[B.start + j];
+    out.terms[j] = shoup(residues[j], B.inv[j], B.inv_q[j], m.p);
+    frac += fraction64(out.terms[j], m);
+  }
+  const u128 bias = centered ? (u128(1) << 63) : 0;
+  out.alpha = u64((frac + bias) >> 64);
+  if (out.alpha != u64((frac + u128(B.count) + bias) >> 64)) {
+    u64 sum[kCrtWordsDev], rhs[kCrtWordsDev];
+    for (int i = 0; i < kCrtWordsDev; ++i) sum[i] = rhs[i] = 0;
+    for (int j = 0; j < B.count; ++j) words_addmul(sum, B.partial_words[j], out.terms[j]);
+    if (centered) {
+      u64 twice[kCrtWordsDev];
+      for (int i = 0; i < kCrtWordsDev; ++i) twice[i] = 0;
+      words_addmul(twice, sum, 2);
+      words_addmul(rhs, B.product_words, 2 * out.alpha + 1);
+      if (words_ge(twice, rhs)) ++out.alpha;
+    } else {
+      words_addmul(rhs, B.product_words, out.alpha + 1);
+      if (words_ge(sum, rhs)) ++out.alpha;
+    }
+  }
+}
+
+__device__ __forceinline__ void convert(const BaseDev& B, const RingDev& R, const Normalized& v, u64* out) {
+  for (int k = 0; k < B.tcount; ++k) {
+    const Prime& m = R.prime[B.tstart + k];
+    u128 s = 0;
+    for (int j = 0; j < B.count; ++j) s += u128(v.terms[j]) * B.partial_mod_target[k][j];
+    const u64 residue = reduce128(s, m);
+    const u64 corr = shoup(v.alpha, B.product_mod_target[k], B.product_mod_target_q[k], m.p);
+    out[k] = submod(residue, corr, m.p);
+  }
+}
+
+// round(t r / M) for r = A - alpha M (the canonical lift)
+__device__ __forceinline__ u64 round_fraction(const BaseDev& B, const RingDev& R, const Normalized& v, u64 t) {
+  u64 whole = 0;
+  u128 frac = 0;
+  for (int j = 0; j < B.count; ++j) {
+    const Prime& m = R.prime[B.start + j];
+    u64 q, r;
+    divide128(u128(t) * v.terms[j], m, &q, &r);
+    whole += q;
+    frac += fraction64(r, m);
+  }
+  const u128 half = u128(1) << 63;
+  u64 rounded = whole + u64((frac + half) >> 64);
+  if (((frac + half) >> 64) != ((frac + u128(B.count) + half) >> 64)) {
+    u64 sum[kCrtWordsDev], lhs[kCrtWordsDev], rhs[kCrtWordsDev];
+    for (int i = 0; i < kCrtWordsDev; ++i) sum[i] = lhs[i] = rhs[i] = 0;
+    for (int j = 0; j < B.count; ++j) words_addmul(sum, B.partial_words[j], v.terms[j]);
+    words_addmul(lhs, sum, 2 * t);
+    words_addmul(rhs, B.product_words, 2 * rounded + 1);
+    if (words_ge(lhs, rhs)) ++rounded;
+  }
+  return rounded - t * v.alpha;
+}
+
+// tensor[poly][K][N] (coefficient domain, residues of the signed product z)
+// -> out[poly][L][N] = round(t z / Q) mod Q, per coefficient.
+__global__ void k_rns_scale(const u64* __restrict__ tensor, long long polys, u64* __restrict__ out,
+                            const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const int L = R.residue, K = R.tensor;
+  const u64* z = tensor + poly * K * R.n + i;
+  u64 rem[kMaxPrimes], quot[kMaxPrimes], rb[kMaxPrimes], kq[kMaxPrimes];
+  for (int j = 0; j < L; ++j) rem[j] = z[j * R.n];
+  Normalized nq;
+  normalize(R.q_to_b, R, rem, false, nq);
+  convert(R.q_to_b, R, nq, rb);
+  const u64 rounded = round_fraction(R.q_to_b, R, nq, R.t);
+  for (int j = 0; j < K - L; ++j) {
+    const u64 p = R.prime[L + j].p;
+    const u64 residue = submod(z[(L + j) * R.n], rb[j], p);
+    quot[j] = shoup(residue, R.inv_q_mod_b[j], R.inv_q_mod_b_q[j], p);
+  }
+  Normalized nb;
+  normalize(R.b_to_q, R, quot, true, nb);
+  convert(R.b_to_q, R, nb, kq);
+  for (int j = 0; j < L; ++j) {
+    const u64 p = R.prime[j].p;
+    const u64 r = rounded >= p ? rounded - p : rounded;
+    const u64 c = shoup(kq[j], R.t_mod[j], R.t_mod_q[j], p) + r;
+    out[(poly * L + j) * R.n + i] = c >= p ? c - p : c;
+  }
+}
+
+// ---- key switching ------------------------------------------------------------
+// One key-switch job: out_k = base_k + [k == 0] sigma_g(x0) + KS(sigma_g(x1))_k,
+// with sigma_g the Galois automorphism X -> X^g (g = 1: identity).
+struct SwitchOp {
+  const u64* base;   // [2][L][N] or null
+  const u64* x0;     // [L][N] or null
+  const u64* words;  // composed sigma_g(x1): [N][W]
+  const u64* key;    // [D][2][L][N] NTT domain
+  u64* out;          // [2][L][N]
+  unsigned g_inv;    // inverse of g mod 2N (gather for x0)
+  unsigned pad;
+};
+
+struct ComposeOp {
+  const u64* x1;  // [L][N] coefficient residues
+  u64* words;     // [N][W] output
+  unsigned g;
+  unsigned pad;
+};
+
+// Garner: canonical integer in [0, Q) of each coefficient, written to the
+// position of X^g (negated when the exponent wraps past N).
+__global__ void k_compose(const ComposeOp* __restrict__ ops, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const ComposeOp op = ops[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R.n) return;
+  const int L = R.residue, W = R.words;
+  u64 digit[kMaxResidue];
+  for (int j = 0; j < L; ++j) {
+    const u64 p = R.prime[j].p;
+    u64 value = op.x1[(long long)j * R.n + i];
+    for (int k = 0; k < j; ++k) {
+      const u64 d = digit[k] >= p ? digit[k] - p : digit[k];
+      value = shoup(value + p - d, R.garner[j][k], R.garner_q[j][k], p);
+    }
+    digit[j] = value;
+  }
+  u64 w[kMaxWords];
+  for (int k = 0; k < kMaxWords; ++k) w[k] = 0;
+  w[0] = digit[L - 1];
+  int used = 1;
+  for (int j = L - 1; j > 0; --j) {
+    u64 carry = digit[j - 1];
+    const u64 p = R.prime[j - 1].p;
+    for (int k = 0; k < used; ++k) {
+      const u128 prod = u128(w[k]) * p + carry;
+      w[k] = u64(prod);
+      carry = u64(prod >> 64);
+    }
+    if (carry) w[used++] = carry;
+  }
+  const unsigned at = unsigned((unsigned long long)i * op.g % (2u * unsigned(R.n)));
+  const int dst = int(at % unsigned(R.n));
+  bool nonzero = false;
+  for (int k = 0; k < W; ++k) nonzero |= w[k] != 0;
+  if (at >= unsigned(R.n) && nonzero) {
+    u64 borrow = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 x = u128(R.q_words[k]) - w[k] - borrow;
+      w[k] = u64(x);
+      borrow = u64(x >> 64) ? 1 : 0;
+    }
+  }
+  u64* o = op.words + (long long)dst * W;
+  for (int k = 0; k < W; ++k) o[k] = w[k];
+}
+
+// digit d of a composed integer, reduced mod p_j
+__device__ __forceinline__ u64 gadget_digit(const u64* w, int W, int d, const RingDev& R, int j) {
+  const int bits = R.digit_bits;
+  const int start = d * bits;
+  const Prime& m = R.prime[j];
+  if (bits <= 64) {
+    const int limb = start / 64, off = start % 64;
+    u64 v = limb < W ? (w[limb] >> off) : 0;
+    if (off && limb + 1 < W) v |= w[limb + 1] << (64 - off);
+    if (bits < 64) v &= (u64(1) << bits) - 1;
+    if (bits <= 60) return v >= m.p ? v - m.p : v;
+    return v % m.p;
+  }
+  // wide digit: Horner over 64-bit chunks from the top of [start, start+bits)
+  u64 r = 0;
+  int remaining = bits;
+  while (remaining > 0) {
+    const int take = remaining > 64 ? 64 : remaining;
+    const int lo = start + remaining - take;
+    const int limb = lo / 64, off = lo % 64;
+    u64 v = limb < W ? (w[limb] >> off) : 0;
+    if (off && limb + 1 < W) v |= w[limb + 1] << (64 - off);
+    if (take < 64) v &= (u64(1) << take) - 1;
+    const u128 shifted = take == 64 ? (u128(r) << 64) : (u128(r) << take);
+    r = reduce128(shifted + v, m);
+    remaining -= take;
+  }
+  return r;
+}
+
+constexpr int kSwitchThreads = 512;
+
+// CTA per (op, prime j < L): D forward NTTs of the digits, multiply-accumulate
+// with the key in the NTT domain, two inverse NTTs, epilogue additions.
+template <int kSwitchPer>  // coefficients per thread: N / kSwitchThreads (rounded up)
+__global__ void __launch_bounds__(kSwitchThreads)
+k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) {
+  extern __shared__ __align__(16) u64 s_plane[];
+  const RingDev& R = *ring;
+  const SwitchOp op = ops[blockIdx.x];
+  const int j = blockIdx.y;
+  const int n = R.n, L = R.residue, W = R.words;
+  const Prime& m = R.prime[j];
+  // positions owned by this thread: threadIdx.x + k * kSwitchThreads < n
+  const int per = (n - int(threadIdx.x) + kSwitchThreads - 1) / kSwitchThreads;
+  u64 acc0[kSwitchPer], acc1[kSwitchPer];
+#pragma unroll
+  for (int k = 0; k < kSwitchPer; ++k) { acc0[k] = 0; acc1[k] = 0; }
+  for (int d = 0; d < R.digits; ++d) {
+    for (int i = threadIdx.x; i < n; i += kSwitchThreads)
+      s_plane[i] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
+    __syncthreads();
+    ntt_forward_smem(s_plane, R, j);
+    const u64* k0 = op.key + ((long long)(d * 2 + 0) * L + j) * n;
+    const u64* k1 = op.key + ((long long)(d * 2 + 1) * L + j) * n;
+#pragma unroll
+    for (int k = 0; k < kSwitchPer; ++k) {
+      if (k < per) {
+        const int i = threadIdx.x + k * kSwitchThreads;
+        const u64 v = s_plane[i];
+        acc0[k] = addmod(acc0[k], reduce128(u128(v) * __ldg(k0 + i), m), m.p);
+        acc1[k] = addmod(acc1[k], reduce128(u128(v) * __ldg(k1 + i), m), m.p);
+      }
+    }
+    __syncthreads();
+  }
+  for (int comp = 0; comp < 2; ++comp) {
+#pragma unroll
+    for (int k = 0; k < kSwitchPer; ++k)
+      if (k < per) s_plane[threadIdx.x + k * kSwitchThreads] = comp ? acc1[k] : acc0[k];
+    __syncthreads();
+    ntt_inverse_smem(s_plane, R, j);
+    u64* out = op.out + ((long long)comp * L + j) * n;
+    const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
+    for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
+      u64 v = s_plane[i];
+      if (base) v = addmod(v, base[i], m.p);
+      if (comp == 0 && op.x0) {
+        const unsigned s = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));
+        u64 x = s < unsigned(n) ? op.x0[(long long)j * n + s] : op.x0[(long long)j * n + (s - n)];
+        if (s >= unsigned(n) && x) x = m.p - x;
+        v = addmod(v, x, m.p);
+      }
+      out[i] = v;
+    }
+    __syncthreads();
+  }
+}
+
+// ---- elementwise ------------------------------------------------------------------
+// data[b][j][N] *= plain[j][N] (NTT domain), j = plane % L
+__global__ void k_mul_plain(u64* __restrict__ data, long long planes, int L, const u64* __restrict__ plain,
+                            const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= planes * R.n) return;
+  const long long plane = idx / R.n;
+  const int i = int(idx % R.n);
+  const int j = int(plane % L);
+  data[idx] = reduce128(u128(data[idx]) * plain[(long long)j * R.n + i], R.prime[j]);
+}
+
+// out = a + b elementwise over planes of L primes
+__global__ void k_add(const u64* __restrict__ a, const u64* __restrict__ b, u64* __restrict__ out, long long planes,
+                      int L, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= planes * R.n) return;
+  const int j = int((idx / R.n) % L);
+  out[idx] = addmod(a[idx], b[idx], R.prime[j].p);
+}
+
+// Compaction: c' = floor((2*target*c + Q) / (2Q)) mod target on composed words
+// (bfv_server.h:142-151), by binary long division.
+__global__ void k_compact(u64* __restrict__ words, long long coeffs, const u64* __restrict__ target_words,
+                          int target_nwords, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= coeffs) return;
+  const int W = R.words;
+  constexpr int NW = 2 * kMaxWords + 2;
+  u64* c = words + idx * W;
+  // num = 2 * target * c + Q
+  u64 num[NW], den[NW], rem[NW], quo[NW];
+  for (int k = 0; k < NW; ++k) num[k] = den[k] = rem[k] = quo[k] = 0;
+  for (int a = 0; a < target_nwords; ++a) {
+    u128 carry = 0;
+    for (int b = 0; b < W; ++b) {
+      carry += u128(target_words[a]) * c[b] + num[a + b];
+      num[a + b] = u64(carry);
+      carry >>= 64;
+    }
+    for (int k = a + W; carry && k < NW; ++k) {
+      carry += num[k];
+      num[k] = u64(carry);
+      carry >>= 64;
+    }
+  }
+  // *2
+  u64 top = 0;
+  for (int k = 0; k < NW; ++k) {
+    const u64 nt = num[k] >> 63;
+    num[k] = (num[k] << 1) | top;
+    top = nt;
+  }
+  u128 carry = 0;
+  for (int k = 0; k < NW; ++k) {
+    carry += u128(num[k]) + (k < W ? R.q_words[k] : 0);
+    num[k] = u64(carry);
+    carry >>= 64;
+  }
+  // den = 2Q
+  top = 0;
+  for (int k = 0; k < NW; ++k) {
+    const u64 qk = k < W ? R.q_words[k] : 0;
+    den[k] = (qk << 1) | top;
+    top = qk >> 63;
+  }
+  int nbits = 0;
+  for (int k = NW - 1; k >= 0; --k)
+    if (num[k]) { nbits = k * 64 + 64 - __clzll(num[k]); break; }
+  for (int bit = nbits - 1; bit >= 0; --bit) {
+    u64 t2 = 0;
+    for (int k = 0; k < NW; ++k) {
+      const u64 nt = rem[k] >> 63;
+      rem[k] = (rem[k] << 1) | t2;
+      t2 = nt;
+    }
+    rem[0] |= (num[bit / 64] >> (bit % 64)) & 1;
+    bool ge = true;
+    for (int k = NW - 1; k >= 0; --k)
+      if (rem[k] != den[k]) { ge = rem[k] > den[k]; break; }
+    if (ge) {
+      u64 borrow = 0;
+      for (int k = 0; k < NW; ++k) {
+        const u128 x = u128(rem[k]) - den[k] - borrow;
+        rem[k] = u64(x);
+        borrow = u64(x >> 64) ? 1 : 0;
+      }
+      quo[bit / 64] |= u64(1) << (bit % 64);
+    }
+  }
+  // quotient <= target; reduce mod target (one subtraction)
+  bool ge = true;
+  for (int k = NW - 1; k >= 0; --k) {
+    const u64 tk = k < target_nwords ? target_words[k] : 0;
+    if (quo[k] != tk) { ge = quo[k] > tk; break; }
+  }
+  if (ge) {
+    u64 borrow = 0;
+    for (int k = 0; k < NW; ++k) {
+      const u64 tk = k < target_nwords ? target_words[k] : 0;
+      const u128 x = u128(quo[k]) - tk - borrow;
+      quo[k] = u64(x);
+      borrow = u64(x >> 64) ? 1 : 0;
+    }
+  }
+  for (int k = 0; k < W; ++k) c[k] = quo[k];
+}
+
+// Pack composed words into `bits`-bit little-endian coefficients: thread per
+// output 64-bit word gathers the (at most bits/64 + 2) overlapping coefficients.
+__global__ void k_pack(const u64* __restrict__ words, int W, int n, int bits, int polys, u64* __restrict__ out,
+                       long long out_words_per_poly) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)polys * out_words_per_poly) return;
+  const long long poly = idx / out_words_per_poly;
+  const long long ow = idx % out_words_per_poly;
+  const long long lo_bit = ow * 64, hi_bit = lo_bit + 64;
+  long long first = lo_bit / bits, last = (hi_bit - 1) / bits;
+  if (last >= n) last = n - 1;
+  u64 acc = 0;
+  for (long long i = first; i <= last; ++i) {
+    const u64* c = words + (poly * n + i) * W;
+    const long long cb = i * bits;  // coefficient start bit
+    // bits of coefficient overlapping [lo_bit, hi_bit)
+    for (int k = 0; k < W; ++k) {
+      const long long wb = cb + 64LL * k;  // global bit of c[k]'s bit 0
+      if (64LL * k >= bits) break;
+      u64 v = c[k];
+      if (64LL * (k + 1) > bits) v &= (bits - 64 * k) >= 64 ? ~u64(0) : ((u64(1) << (bits - 64 * k)) - 1);
+      const long long rel = wb - lo_bit;
+      if (rel >= 64 || rel <= -64) continue;
+      acc |= rel >= 0 ? (v << rel) : (v >> (-rel));
+    }
+  }
+  out[idx] = acc;
+}
+
+}  // namespace bfv
+}  // namespace cuhe

@@ -1,0 +1,1184 @@
+// C ABI of the BFV residue evaluator (see include/cuhe_bfv.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cuhe_bfv.h"
+#include "../../include/cuhe_paillier.h"
+#include "bfv_host.h"
+#include "bfv_kernels.cuh"
+
+using namespace cuhe::bfv;
+namespace H = cuhe::bfv::host;
+
+namespace {
+
+thread_local std::string t_error;
+
+int fail(int code, const std::string& msg) {
+  t_error = msg;
+  return code;
+}
+
+#define BFV_CUDA(call, where)                                                                 \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(CUHE_CUDA_ERROR, std::string(where) + ": " + cudaGetErrorName(e_) + " (" +  \
+                                       cudaGetErrorString(e_) + ")");                         \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Growable device workspace carved into aligned slices for one call.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  ~Arena() { if (base) cudaFree(base); }
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&base, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+  bool overflow = false;
+  void reset() { used = 0; overflow = false; }
+  // Slices past the reserved capacity are never handed out: the call is
+  // marked as overflowed and receives a null pointer, checked before launch.
+  template <class T> T* take(size_t count) {
+    const size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    if (!base || used + bytes > cap) {
+      overflow = true;
+      return nullptr;
+    }
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+#define BFV_ARENA(arena)                                                                  \
+  do {                                                                                    \
+    if ((arena).overflow) return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted"); \
+  } while (0)
+
+size_t slice(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+}  // namespace
+
+struct cuhe_bfv_ring {
+  std::atomic<int> refs{1};
+  int device = 0;
+  H::RingPlan plan;
+  bool residue = false, fast = false;
+  unsigned kernel_level = 0;
+  size_t switch_prime_count = 0;
+  u64* d_tables = nullptr;
+  size_t table_bytes = 0;
+  RingDev host_dev{};
+  std::map<u64, RingDev*> dev_for_t;  // t == 0: no scale constants
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  Arena arena;
+
+  ~cuhe_bfv_ring() {
+    DeviceGuard g(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& kv : dev_for_t) cudaFree(kv.second);
+    if (d_tables) cudaFree(d_tables);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+struct cuhe_bfv_key {
+  std::atomic<int> refs{1};
+  cuhe_bfv_ring* ring = nullptr;
+  u64* d_key = nullptr;  // [D][2][L][N] NTT domain
+  size_t bytes = 0;
+  ~cuhe_bfv_key() {
+    if (d_key) {
+      DeviceGuard g(ring->device);
+      cudaFree(d_key);
+    }
+    cuhe_bfv_ring_release(ring);
+  }
+};
+
+struct cuhe_bfv_server {
+  std::atomic<int> refs{1};
+  cuhe_bfv_ring* ring = nullptr;
+  cuhe_bfv_key* relin = nullptr;
+  std::map<u64, cuhe_bfv_key*> keys;
+  size_t padded = 0, lanes = 0, capacity = 0;
+  u64 t = 0;
+  H::Big target;
+  unsigned target_bits = 0;
+  std::vector<u64> target_words;
+  std::vector<u64> left, right;
+  u64* d_full_mask = nullptr;  // [L][N] NTT domain
+  u64* d_target = nullptr;
+  std::map<size_t, u64*> partial_masks;
+  RingDev* d_ring = nullptr;
+  double profile_ms[6] = {0, 0, 0, 0, 0, 0};
+  ~cuhe_bfv_server() {
+    {
+      DeviceGuard g(ring->device);
+      if (d_full_mask) cudaFree(d_full_mask);
+      if (d_target) cudaFree(d_target);
+      for (auto& kv : partial_masks) cudaFree(kv.second);
+    }
+    for (auto& kv : keys) cuhe_bfv_key_release(kv.second);
+    cuhe_bfv_key_release(relin);
+    cuhe_bfv_ring_release(ring);
+  }
+};
+
+namespace {
+
+unsigned log2u(size_t n) {
+  unsigned l = 0;
+  while ((size_t(1) << l) < n) ++l;
+  return l;
+}
+
+// Device copy of the ring constants; t != 0 adds the exact scale constants.
+int device_ring(cuhe_bfv_ring* r, u64 t, RingDev** out) {
+  auto it = r->dev_for_t.find(t);
+  if (it != r->dev_for_t.end()) { *out = it->second; return CUHE_OK; }
+  RingDev dev = r->host_dev;
+  if (t) {
+    H::RingPlan plan = r->plan;
+    try {
+      H::build_scale(plan, t);
+    } catch (const std::invalid_argument& e) {
+      return fail(CUHE_INVALID_ARGUMENT, e.what());
+    }
+    auto fill = [&](BaseDev& b, const H::ExactBase& h) {
+      b.start = int(h.base.front());
+      b.count = int(h.base.size());
+      b.tstart = int(h.target.front());
+      b.tcount = int(h.target.size());
+      for (size_t j = 0; j < h.base.size(); ++j) {
+        b.inv[j] = h.inv[j];
+        b.inv_q[j] = h.inv_q[j];
+        for (int w = 0; w < kCrtWordsDev; ++w) b.partial_words[j][w] = h.partial_words[j][size_t(w)];
+      }
+      for (size_t k = 0; k < h.target.size(); ++k) {
+        b.product_mod_target[k] = h.product_mod_target[k];
+        b.product_mod_target_q[k] = h.product_mod_target_q[k];
+        for (size_t j = 0; j < h.base.size(); ++j) b.partial_mod_target[k][j] = h.partial_mod_target[k][j];
+      }
+      for (int w = 0; w < kCrtWordsDev; ++w) b.product_words[w] = h.product_words[size_t(w)];
+    };
+    fill(dev.q_to_b, plan.q_to_b);
+    fill(dev.b_to_q, plan.b_to_q);
+    for (size_t j = 0; j < plan.inv_q_mod_b.size(); ++j) {
+      dev.inv_q_mod_b[j] = plan.inv_q_mod_b[j];
+      dev.inv_q_mod_b_q[j] = plan.inv_q_mod_b_q[j];
+    }
+    for (size_t j = 0; j < plan.primes.size(); ++j) {
+      dev.t_mod[j] = t % plan.primes[j];
+      dev.t_mod_q[j] = H::shoup_quotient(dev.t_mod[j], plan.primes[j]);
+    }
+    dev.has_scale = 1;
+    dev.t = t;
+  }
+  RingDev* d = nullptr;
+  BFV_CUDA(cudaMalloc(&d, sizeof(RingDev)), "ring constants");
+  BFV_CUDA(cudaMemcpy(d, &dev, sizeof(RingDev), cudaMemcpyHostToDevice), "ring constants");
+  r->dev_for_t[t] = d;
+  *out = d;
+  return CUHE_OK;
+}
+
+// fixed-width little-endian coefficient bytes -> words, validated < q
+int parse_polys(const cuhe_bfv_ring* r, const uint8_t* data, size_t polys, std::vector<u64>& words) {
+  const auto& P = r->plan;
+  const size_t n = P.n, cb = P.coefficient_bytes, W = size_t(r->host_dev.words);
+  words.assign(polys * n * W, 0);
+  for (size_t k = 0; k < polys * n; ++k) {
+    const uint8_t* src = data + k * cb;
+    u64* dst = words.data() + k * W;
+    for (size_t b = 0; b < cb; ++b) dst[b / 8] |= u64(src[b]) << (8 * (b % 8));
+    // compare with q
+    int c = 0;
+    for (size_t w = W; w-- > 0 && c == 0;) {
+      const u64 qw = w < P.q.w.size() ? P.q.w[w] : 0;
+      if (dst[w] != qw) c = dst[w] < qw ? -1 : 1;
+    }
+    if (c >= 0) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical polynomial coefficient");
+  }
+  return CUHE_OK;
+}
+
+void words_to_bytes(const cuhe_bfv_ring* r, const std::vector<u64>& words, size_t polys, uint8_t* out) {
+  const size_t n = r->plan.n, cb = r->plan.coefficient_bytes, W = size_t(r->host_dev.words);
+  for (size_t k = 0; k < polys * n; ++k) {
+    const u64* src = words.data() + k * W;
+    for (size_t b = 0; b < cb; ++b) out[k * cb + b] = uint8_t(src[b / 8] >> (8 * (b % 8)));
+  }
+}
+
+unsigned blocks_for(long long items, int threads) { return unsigned((items + threads - 1) / threads); }
+
+size_t ntt_smem(const cuhe_bfv_ring* r) { return r->plan.n * sizeof(u64); }
+
+cudaError_t launch_ntt(cuhe_bfv_ring* r, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
+                       int prime_block, int inverse) {
+  if (planes <= 0) return cudaSuccess;
+  const size_t smem = ntt_smem(r);
+  cudaError_t e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const int threads = r->plan.n >= 2048 ? 1024 : int(std::max<size_t>(32, r->plan.n / 2));
+  k_ntt<<<unsigned(planes), threads, smem, r->stream>>>(data, d, prime_base, prime_mod, prime_block, inverse);
+  return cudaGetLastError();
+}
+
+// Compose ops then key-switch ops (one launch each).
+int run_switch(cuhe_bfv_ring* r, RingDev* d, const std::vector<ComposeOp>& cops, const std::vector<SwitchOp>& sops,
+               ComposeOp* d_cops, SwitchOp* d_sops) {
+  const auto& P = r->plan;
+  if (!cops.empty()) {
+    BFV_CUDA(cudaMemcpyAsync(d_cops, cops.data(), cops.size() * sizeof(ComposeOp), cudaMemcpyHostToDevice, r->stream),
+             "compose ops");
+    dim3 grid(blocks_for((long long)(P.n), 256), unsigned(cops.size()));
+    k_compose<<<grid, 256, 0, r->stream>>>(d_cops, d);
+    BFV_CUDA(cudaGetLastError(), "compose launch");
+  }
+  if (!sops.empty()) {
+    BFV_CUDA(cudaMemcpyAsync(d_sops, sops.data(), sops.size() * sizeof(SwitchOp), cudaMemcpyHostToDevice, r->stream),
+             "switch ops");
+    const size_t smem = ntt_smem(r);
+    dim3 grid(unsigned(sops.size()), unsigned(P.residue_count));
+    if (P.n <= 8192) {
+      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
+      k_keyswitch<16><<<grid, kSwitchThreads, smem, r->stream>>>(d_sops, d);
+    } else {
+      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
+      k_keyswitch<32><<<grid, kSwitchThreads, smem, r->stream>>>(d_sops, d);
+    }
+    BFV_CUDA(cudaGetLastError(), "keyswitch launch");
+  }
+  // op tables are reused by the next call; keep host order
+  BFV_CUDA(cudaStreamSynchronize(r->stream), "switch synchronize");
+  return CUHE_OK;
+}
+
+unsigned inverse_mod_2n(u64 g, size_t n) {
+  const u64 m = 2 * u64(n);
+  for (u64 x = 1; x < m; x += 2)
+    if ((g * x) % m == 1) return unsigned(x);
+  return 0;
+}
+
+// host words of a composed result (after k_compose) -> bytes
+int download_words(cuhe_bfv_ring* r, const u64* d_words, size_t polys, uint8_t* out) {
+  std::vector<u64> words(polys * r->plan.n * size_t(r->host_dev.words));
+  BFV_CUDA(cudaMemcpyAsync(words.data(), d_words, words.size() * 8, cudaMemcpyDeviceToHost, r->stream), "download");
+  BFV_CUDA(cudaStreamSynchronize(r->stream), "download");
+  words_to_bytes(r, words, polys, out);
+  return CUHE_OK;
+}
+
+// mask(count) of the Hamming server (bfv_server.h:80-99): the polynomial
+// m(X) mod t with m(psi^{+-3^lane}) = 1 on the selected slots and 0 on the
+// others, i.e. m_i = N^-1 * sum_{e in S} psi^(-e i) mod t.
+std::vector<u64> hamming_mask(size_t n, u64 t, size_t lanes, size_t count) {
+  u64 psi = 0;
+  for (u64 c = 2;; ++c) {
+    const u64 root = H::powmod(c, (t - 1) / (2 * n), t);
+    if (H::powmod(root, n, t) == t - 1) { psi = root; break; }
+  }
+  const u64 psi_inv = H::powmod(psi, t - 2, t);
+  std::vector<u64> exps;
+  u64 g = 1;
+  for (size_t lane = 0; lane < lanes; ++lane) {
+    for (size_t row = 0; row < 2; ++row) {
+      if (row * lanes + lane >= count) continue;
+      exps.push_back(row ? 2 * n - g : g);
+    }
+    g = g * 3 % (2 * n);
+  }
+  std::vector<u64> m(n, 0);
+  const u64 n_inv = H::powmod(n % t, t - 2, t);
+  for (u64 e : exps) {
+    const u64 step = H::powmod(psi_inv, e, t);  // psi^-e
+    u64 w = 1;
+    for (size_t i = 0; i < n; ++i) {
+      m[i] = (m[i] + w) % t;
+      w = u64(u128(w) * step % t);
+    }
+  }
+  for (auto& v : m) v = u64(u128(v) * n_inv % t);
+  return m;
+}
+
+// residues mod the first L primes of a small nonnegative polynomial, NTT'd
+int upload_plain_ntt(cuhe_bfv_ring* r, RingDev* d, const std::vector<u64>& coeffs_words, u64** out) {
+  const auto& P = r->plan;
+  const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
+  u64* d_words = nullptr;
+  u64* d_res = nullptr;
+  BFV_CUDA(cudaMalloc(&d_words, n * W * 8), "plain alloc");
+  BFV_CUDA(cudaMalloc(&d_res, L * n * 8), "plain alloc");
+  BFV_CUDA(cudaMemcpyAsync(d_words, coeffs_words.data(), n * W * 8, cudaMemcpyHostToDevice, r->stream), "plain");
+  k_words_to_residues<<<blocks_for((long long)(n), 256), 256, 0, r->stream>>>(d_words, 1, int(L), d_res, d);
+  BFV_CUDA(cudaGetLastError(), "plain residues");
+  BFV_CUDA(launch_ntt(r, d, d_res, (long long)(L), 0, int(L), 1, 0), "plain ntt");
+  BFV_CUDA(cudaStreamSynchronize(r->stream), "plain");
+  cudaFree(d_words);
+  *out = d_res;
+  return CUHE_OK;
+}
+
+std::vector<u64> small_to_words(const std::vector<u64>& v, size_t W) {
+  std::vector<u64> w(v.size() * W, 0);
+  for (size_t i = 0; i < v.size(); ++i) w[i * W] = v[i];
+  return w;
+}
+
+// Tile circuit for `ct` tiles resident as residues: tensor square of
+// (query - tile) with exact scale, relinearization, the given rotations and
+// the masks.  dist_out receives [ct][2][L][N] coefficient-domain residues.
+struct TileArgs {
+  const u64* q_words;   // [2][N][W]
+  const u64* t_words;   // [ct][2][N][W]
+  size_t ct;
+  cuhe_bfv_key* relin;
+  std::vector<u64> exps;                 // rotation exponents (1 = double)
+  std::vector<cuhe_bfv_key*> keys;
+  std::vector<const u64*> masks;         // per tile mask NTT [L][N]
+};
+
+int tile_circuit(cuhe_bfv_ring* r, RingDev* d, const TileArgs& a, u64* dist, double* ms) {
+  const auto& P = r->plan;
+  const size_t n = P.n, L = P.residue_count, T = P.tensor_count, W = size_t(r->host_dev.words);
+  const size_t ct = a.ct;
+  Arena& ar = r->arena;
+  u64* diff = ar.take<u64>(ct * 2 * T * n);
+  u64* tens = ar.take<u64>(ct * 3 * T * n);
+  u64* scaled = ar.take<u64>(ct * 3 * L * n);
+  u64* words = ar.take<u64>(ct * n * W);
+  u64* other = ar.take<u64>(ct * 2 * L * n);
+  ComposeOp* d_cops = ar.take<ComposeOp>(ct);
+  SwitchOp* d_sops = ar.take<SwitchOp>(ct);
+  BFV_ARENA(ar);
+  cudaEvent_t ev[5];
+  for (auto& e : ev) cudaEventCreate(&e);
+  cudaEventRecord(ev[0], r->stream);
+  k_diff_residues<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, r->stream>>>(a.q_words, a.t_words, int(ct), int(T),
+                                                                                    diff, d);
+  BFV_CUDA(cudaGetLastError(), "diff residues");
+  BFV_CUDA(launch_ntt(r, d, diff, (long long)(ct * 2 * T), 0, int(T), 1, 0), "tensor ntt");
+  k_tensor_square<<<blocks_for((long long)(ct * T * n), 256), 256, 0, r->stream>>>(diff, int(ct), int(T), tens, d);
+  BFV_CUDA(cudaGetLastError(), "tensor");
+  BFV_CUDA(launch_ntt(r, d, tens, (long long)(ct * 3 * T), 0, int(T), 1, 1), "tensor intt");
+  k_rns_scale<<<blocks_for((long long)(ct * 3 * n), 128), 128, 0, r->stream>>>(tens, (long long)(ct * 3), scaled, d);
+  BFV_CUDA(cudaGetLastError(), "rns scale");
+  cudaEventRecord(ev[1], r->stream);
+  // relinearize: dist = (c0, c1) + KS(c2)
+  std::vector<ComposeOp> cops(ct);
+  std::vector<SwitchOp> sops(ct);
+  for (size_t t = 0; t < ct; ++t) {
+    cops[t] = ComposeOp{scaled + (t * 3 + 2) * L * n, words + t * n * W, 1u, 0u};
+    sops[t] = SwitchOp{scaled + t * 3 * L * n, nullptr, words + t * n * W, a.relin->d_key, dist + t * 2 * L * n, 1u, 0u};
+  }
+  if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
+  cudaEventRecord(ev[2], r->stream);
+  // rotations: dist += rotate(dist, g)
+  u64* cur = dist;
+  u64* nxt = other;
+  for (size_t k = 0; k < a.exps.size(); ++k) {
+    const u64 g = a.exps[k];
+    if (g == 1) {
+      k_add<<<blocks_for((long long)(ct * 2 * L * n), 256), 256, 0, r->stream>>>(cur, cur, nxt, (long long)(ct * 2 * L), int(L), d);
+      BFV_CUDA(cudaGetLastError(), "double");
+    } else {
+      const unsigned ginv = inverse_mod_2n(g, n);
+      for (size_t t = 0; t < ct; ++t) {
+        cops[t] = ComposeOp{cur + (t * 2 + 1) * L * n, words + t * n * W, unsigned(g), 0u};
+        sops[t] = SwitchOp{cur + t * 2 * L * n, cur + t * 2 * L * n, words + t * n * W, a.keys[k]->d_key,
+                           nxt + t * 2 * L * n, ginv, 0u};
+      }
+      if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
+    }
+    std::swap(cur, nxt);
+  }
+  cudaEventRecord(ev[3], r->stream);
+  // masks in the NTT domain
+  BFV_CUDA(launch_ntt(r, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 0), "mask ntt");
+  for (size_t t = 0; t < ct; ++t) {
+    const u64* m = a.masks[t];
+    size_t run = 1;
+    while (t + run < ct && a.masks[t + run] == m) ++run;
+    k_mul_plain<<<blocks_for((long long)(run * 2 * L * n), 256), 256, 0, r->stream>>>(cur + t * 2 * L * n,
+                                                                                      (long long)(run * 2 * L), int(L), m, d);
+    BFV_CUDA(cudaGetLastError(), "mask");
+    t += run - 1;
+  }
+  BFV_CUDA(launch_ntt(r, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 1), "mask intt");
+  if (cur != dist)
+    BFV_CUDA(cudaMemcpyAsync(dist, cur, ct * 2 * L * n * 8, cudaMemcpyDeviceToDevice, r->stream), "dist copy");
+  cudaEventRecord(ev[4], r->stream);
+  BFV_CUDA(cudaStreamSynchronize(r->stream), "tile circuit");
+  if (ms) {
+    float x;
+    cudaEventElapsedTime(&x, ev[0], ev[1]); ms[0] += x;
+    cudaEventElapsedTime(&x, ev[1], ev[2]); ms[1] += x;
+    cudaEventElapsedTime(&x, ev[2], ev[3]); ms[2] += x;
+    cudaEventElapsedTime(&x, ev[3], ev[4]); ms[3] += x;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return CUHE_OK;
+}
+
+size_t tile_arena_bytes(const cuhe_bfv_ring* r, size_t ct) {
+  const auto& P = r->plan;
+  const size_t n = P.n, L = P.residue_count, T = P.tensor_count, W = size_t(r->host_dev.words);
+  return slice(ct * 2 * T * n * 8) + slice(ct * 3 * T * n * 8) + slice(ct * 3 * L * n * 8) + slice(ct * n * W * 8) +
+         slice(ct * 2 * L * n * 8) + slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cuhe_bfv_last_error(void) { return t_error.c_str(); }
+
+int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int fast, int residue,
+                         uint64_t kernel_level, int device, cuhe_bfv_ring** out) {
+  if (!out || !q_hex) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  const size_t len = std::strlen(q_hex);
+  if (n > 32768 || digit_bits > 512 || kernel_level > 2)
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid native BFV ring parameters or kernel level");
+  if (len < 1 || len > 128 || (len > 1 && q_hex[0] == '0'))
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid or oversized native modulus encoding");
+  if (kernel_level && !residue)
+    return fail(CUHE_INVALID_ARGUMENT,
+                "Kernel level must be 0..2, with nonzero levels requiring the residue backend");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(CUHE_CUDA_ERROR, "no CUDA device available");
+  }
+  if (device < 0 || device >= count) return fail(CUHE_INVALID_ARGUMENT, "invalid device ordinal");
+  auto* r = new (std::nothrow) cuhe_bfv_ring();
+  if (!r) return fail(CUHE_OUT_OF_MEMORY, "ring allocation");
+  try {
+    const H::Big q = H::from_hex(q_hex);
+    r->plan = H::build_ring(size_t(n), q, unsigned(digit_bits));
+    if (r->plan.n > 16384) throw std::invalid_argument("the B200 evaluator supports N <= 16384");
+    if (r->plan.primes.size() > size_t(kMaxPrimes)) throw std::invalid_argument("too many auxiliary primes");
+    if (!residue) {
+      const H::Big qm1 = H::sub(q, H::Big(1));
+      const H::Big sb = H::mul(H::mul_small(H::Big(u64(n)), u64(r->plan.digits)),
+                               H::mul(H::sub(H::shl(H::Big(1), size_t(digit_bits)), H::Big(1)), qm1));
+      r->switch_prime_count = H::prime_count_for(r->plan.primes, sb);
+    } else {
+      r->switch_prime_count = r->plan.residue_count;
+    }
+  } catch (const std::invalid_argument& e) {
+    delete r;
+    return fail(CUHE_INVALID_ARGUMENT, e.what());
+  }
+  r->device = device;
+  r->residue = residue != 0;
+  r->fast = fast != 0;
+  r->kernel_level = unsigned(kernel_level);
+  DeviceGuard guard(device);
+  const auto& P = r->plan;
+  const size_t K = P.primes.size(), N = P.n;
+  r->table_bytes = K * 4 * N * 8;
+  std::vector<u64> tables(K * 4 * N);
+  for (size_t j = 0; j < K; ++j) {
+    std::memcpy(&tables[(j * 4 + 0) * N], P.ntt[j].fwd.data(), N * 8);
+    std::memcpy(&tables[(j * 4 + 1) * N], P.ntt[j].fwd_q.data(), N * 8);
+    std::memcpy(&tables[(j * 4 + 2) * N], P.ntt[j].inv.data(), N * 8);
+    std::memcpy(&tables[(j * 4 + 3) * N], P.ntt[j].inv_q.data(), N * 8);
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&r->d_tables, r->table_bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(r->d_tables, tables.data(), r->table_bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    delete r;
+    return fail(CUHE_CUDA_ERROR, std::string("ring setup: ") + cudaGetErrorString(e));
+  }
+  RingDev& dev = r->host_dev;
+  std::memset(&dev, 0, sizeof(dev));
+  dev.n = int(N);
+  dev.logn = int(log2u(N));
+  dev.primes = int(K);
+  dev.residue = int(P.residue_count);
+  dev.tensor = int(P.tensor_count);
+  dev.digits = int(P.digits);
+  dev.digit_bits = int(P.digit_bits);
+  dev.words = int((P.q_bits + 63) / 64);
+  for (size_t j = 0; j < K; ++j) {
+    dev.prime[j] = H::make_prime(P.primes[j]);
+    dev.fwd[j] = r->d_tables + (j * 4 + 0) * N;
+    dev.fwd_q[j] = r->d_tables + (j * 4 + 1) * N;
+    dev.inv[j] = r->d_tables + (j * 4 + 2) * N;
+    dev.inv_q[j] = r->d_tables + (j * 4 + 3) * N;
+    dev.n_inv[j] = P.ntt[j].n_inv;
+    dev.n_inv_q[j] = P.ntt[j].n_inv_q;
+    dev.last[j] = P.ntt[j].last;
+    dev.last_q[j] = P.ntt[j].last_q;
+    u64 pw = 1 % P.primes[j];
+    const u64 two64 = u64((u128(1) << 64) % P.primes[j]);
+    for (int w = 0; w < kMaxWords; ++w) {
+      dev.pow64_mod[j][w] = pw;
+      pw = u64(u128(pw) * two64 % P.primes[j]);
+    }
+  }
+  for (size_t j = 0; j < P.residue_count; ++j)
+    for (size_t k = 0; k < j; ++k) {
+      dev.garner[j][k] = P.garner_inv[j][k];
+      dev.garner_q[j][k] = P.garner_inv_q[j][k];
+    }
+  for (size_t w = 0; w < P.q.w.size() && w < size_t(kMaxWords); ++w) dev.q_words[w] = P.q.w[w];
+  RingDev* dummy = nullptr;
+  if (int rc = device_ring(r, 0, &dummy)) {
+    delete r;
+    return rc;
+  }
+  *out = r;
+  return CUHE_OK;
+}
+
+void cuhe_bfv_ring_release(cuhe_bfv_ring* ring) {
+  if (ring && --ring->refs == 0) delete ring;
+}
+
+int cuhe_bfv_ring_info(const cuhe_bfv_ring* ring, uint64_t* primes, int capacity, int* prime_count,
+                       int* switch_prime_count, int* residue_prime_count, uint64_t* table_bytes,
+                       uint64_t* coefficient_bytes, int* kernel_level, int* fast) {
+  if (!ring) return fail(CUHE_INVALID_ARGUMENT, "null ring");
+  const auto& P = ring->plan;
+  for (int i = 0; i < capacity && size_t(i) < P.primes.size(); ++i) primes[i] = P.primes[size_t(i)];
+  if (prime_count) *prime_count = int(P.primes.size());
+  if (switch_prime_count) *switch_prime_count = int(ring->switch_prime_count);
+  if (residue_prime_count) *residue_prime_count = ring->residue ? int(P.residue_count) : 0;
+  if (table_bytes) *table_bytes = ring->table_bytes;
+  if (coefficient_bytes) *coefficient_bytes = P.coefficient_bytes;
+  if (kernel_level) *kernel_level = int(ring->kernel_level);
+  if (fast) *fast = ring->fast ? 1 : 0;
+  return CUHE_OK;
+}
+
+int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t digits, cuhe_bfv_key** out) {
+  if (!ring || !key_polys || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  const auto& P = ring->plan;
+  if (digits != P.digits) return fail(CUHE_INVALID_ARGUMENT, "Incorrect gadget digit count");
+  std::lock_guard<std::mutex> lock(ring->mu);
+  DeviceGuard guard(ring->device);
+  std::vector<u64> words;
+  if (int rc = parse_polys(ring, key_polys, size_t(2 * digits), words)) return rc;
+  const size_t n = P.n, L = P.residue_count, W = size_t(ring->host_dev.words);
+  auto* key = new (std::nothrow) cuhe_bfv_key();
+  if (!key) return fail(CUHE_OUT_OF_MEMORY, "key allocation");
+  key->ring = ring;
+  ++ring->refs;
+  key->bytes = size_t(digits) * 2 * L * n * 8;
+  RingDev* d = nullptr;
+  int rc = device_ring(ring, 0, &d);
+  u64* d_words = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (!rc) e = cudaMalloc(&key->d_key, key->bytes);
+  if (!rc && e == cudaSuccess) e = cudaMalloc(&d_words, words.size() * 8);
+  if (!rc && e == cudaSuccess)
+    e = cudaMemcpyAsync(d_words, words.data(), words.size() * 8, cudaMemcpyHostToDevice, ring->stream);
+  if (!rc && e == cudaSuccess) {
+    // layout: [digit][component][prime][N] == residues of polys in order b_0, a_0, b_1, ...
+    k_words_to_residues<<<blocks_for((long long)(2 * digits * n), 256), 256, 0, ring->stream>>>(
+        d_words, (long long)(2 * digits), int(L), key->d_key, d);
+    e = cudaGetLastError();
+  }
+  if (!rc && e == cudaSuccess) e = launch_ntt(ring, d, key->d_key, (long long)(2 * digits * L), 0, int(L), 1, 0);
+  if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ring->stream);
+  if (d_words) cudaFree(d_words);
+  if (rc || e != cudaSuccess) {
+    cuhe_bfv_key_release(key);
+    return rc ? rc : fail(CUHE_CUDA_ERROR, std::string("compile_key: ") + cudaGetErrorString(e));
+  }
+  *out = key;
+  return CUHE_OK;
+}
+
+void cuhe_bfv_key_release(cuhe_bfv_key* key) {
+  if (key && --key->refs == 0) delete key;
+}
+
+uint64_t cuhe_bfv_key_bytes(const cuhe_bfv_key* key) { return key ? key->bytes : 0; }
+
+namespace {
+
+// upload fixed-width polys as words and residues (mod the first `primes` primes)
+int upload_polys(cuhe_bfv_ring* r, RingDev* d, const uint8_t* data, size_t polys, size_t primes, u64** d_words,
+                 u64** d_res) {
+  std::vector<u64> words;
+  if (int rc = parse_polys(r, data, polys, words)) return rc;
+  const size_t n = r->plan.n;
+  *d_words = r->arena.take<u64>(words.size());
+  BFV_ARENA(r->arena);
+  BFV_CUDA(cudaMemcpyAsync(*d_words, words.data(), words.size() * 8, cudaMemcpyHostToDevice, r->stream), "upload");
+  if (d_res) {
+    *d_res = r->arena.take<u64>(polys * primes * n);
+    BFV_ARENA(r->arena);
+    k_words_to_residues<<<blocks_for((long long)(polys * n), 256), 256, 0, r->stream>>>(*d_words, (long long)(polys),
+                                                                                        int(primes), *d_res, d);
+    BFV_CUDA(cudaGetLastError(), "residues");
+  }
+  BFV_CUDA(cudaStreamSynchronize(r->stream), "upload");
+  return CUHE_OK;
+}
+
+int compose_out(cuhe_bfv_ring* r, RingDev* d, const u64* res, size_t polys, uint8_t* out) {
+  const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  u64* words = r->arena.take<u64>(polys * n * W);
+  ComposeOp* d_cops = r->arena.take<ComposeOp>(polys);
+  BFV_ARENA(r->arena);
+  std::vector<ComposeOp> cops(polys);
+  for (size_t k = 0; k < polys; ++k) cops[k] = ComposeOp{res + k * L * n, words + k * n * W, 1u, 0u};
+  if (int rc = run_switch(r, d, cops, {}, d_cops, nullptr)) return rc;
+  return download_words(r, words, polys, out);
+}
+
+}  // namespace
+
+int cuhe_bfv_apply_key(cuhe_bfv_key* key, const uint8_t* poly, uint8_t* out) {
+  if (!key || !poly || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  cuhe_bfv_ring* r = key->ring;
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, 0, &d)) return rc;
+  const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  BFV_CUDA(r->arena.reserve(slice(n * W * 8) * 3 + slice(2 * L * n * 8) * 2 + 4096), "workspace");
+  r->arena.reset();
+  u64* words = nullptr;
+  if (int rc = upload_polys(r, d, poly, 1, L, &words, nullptr)) return rc;
+  u64* res = r->arena.take<u64>(2 * L * n);
+  SwitchOp* d_sops = r->arena.take<SwitchOp>(1);
+  BFV_ARENA(r->arena);
+  std::vector<SwitchOp> sops{SwitchOp{nullptr, nullptr, words, key->d_key, res, 1u, 0u}};
+  if (int rc = run_switch(r, d, {}, sops, nullptr, d_sops)) return rc;
+  return compose_out(r, d, res, 2, out);
+}
+
+int cuhe_bfv_rotate_rows(cuhe_bfv_key* key, const uint8_t* ct, uint64_t exponent, uint8_t* out) {
+  if (!key || !ct || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  cuhe_bfv_ring* r = key->ring;
+  const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  if (!(exponent & 1) || exponent >= 2 * n) return fail(CUHE_INVALID_ARGUMENT, "Invalid Galois exponent");
+  if (exponent == 1) {
+    std::vector<u64> words;
+    if (int rc = parse_polys(r, ct, 2, words)) return rc;
+    std::memcpy(out, ct, 2 * n * r->plan.coefficient_bytes);
+    return CUHE_OK;
+  }
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, 0, &d)) return rc;
+  BFV_CUDA(r->arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * L * n * 8) * 3 + slice(n * W * 8) + 8192), "workspace");
+  r->arena.reset();
+  u64 *words = nullptr, *res = nullptr;
+  if (int rc = upload_polys(r, d, ct, 2, L, &words, &res)) return rc;
+  u64* sw = r->arena.take<u64>(n * W);
+  u64* outres = r->arena.take<u64>(2 * L * n);
+  ComposeOp* d_cops = r->arena.take<ComposeOp>(1);
+  SwitchOp* d_sops = r->arena.take<SwitchOp>(1);
+  BFV_ARENA(r->arena);
+  std::vector<ComposeOp> cops{ComposeOp{res + L * n, sw, unsigned(exponent), 0u}};
+  std::vector<SwitchOp> sops{SwitchOp{nullptr, res, sw, key->d_key, outres, inverse_mod_2n(exponent, n), 0u}};
+  if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
+  return compose_out(r, d, outres, 2, out);
+}
+
+int cuhe_bfv_ring_product(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* rhs, uint8_t* out) {
+  if (!r || !lhs || !rhs || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, 0, &d)) return rc;
+  const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  BFV_CUDA(r->arena.reserve(slice(n * W * 8) * 4 + slice(L * n * 8) * 3 + 8192), "workspace");
+  r->arena.reset();
+  u64 *wa, *wb, *ra, *rb;
+  if (int rc = upload_polys(r, d, lhs, 1, L, &wa, &ra)) return rc;
+  if (int rc = upload_polys(r, d, rhs, 1, L, &wb, &rb)) return rc;
+  BFV_CUDA(launch_ntt(r, d, ra, (long long)(L), 0, int(L), 1, 0), "ntt");
+  BFV_CUDA(launch_ntt(r, d, rb, (long long)(L), 0, int(L), 1, 0), "ntt");
+  k_mul_plain<<<blocks_for((long long)(L * n), 256), 256, 0, r->stream>>>(ra, (long long)(L), int(L), rb, d);
+  BFV_CUDA(cudaGetLastError(), "product");
+  BFV_CUDA(launch_ntt(r, d, ra, (long long)(L), 0, int(L), 1, 1), "intt");
+  return compose_out(r, d, ra, 1, out);
+}
+
+int cuhe_bfv_multiply(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* rhs, uint64_t t, uint8_t* out) {
+  if (!r || !lhs || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  if (t < 2 || t >= (u64(1) << 60) || H::cmp(H::Big(t), r->plan.q) >= 0)
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid plaintext modulus");
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, t, &d)) return rc;
+  const size_t n = r->plan.n, L = r->plan.residue_count, T = r->plan.tensor_count, W = size_t(r->host_dev.words);
+  BFV_CUDA(r->arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * T * n * 8) * 2 + slice(3 * T * n * 8) +
+                            slice(3 * L * n * 8) + slice(3 * n * W * 8) + 8192),
+           "workspace");
+  r->arena.reset();
+  u64 *wa, *ra, *wb = nullptr, *rb = nullptr;
+  if (int rc = upload_polys(r, d, lhs, 2, T, &wa, &ra)) return rc;
+  if (rhs) {
+    if (int rc = upload_polys(r, d, rhs, 2, T, &wb, &rb)) return rc;
+  }
+  u64* tens = r->arena.take<u64>(3 * T * n);
+  u64* scaled = r->arena.take<u64>(3 * L * n);
+  BFV_ARENA(r->arena);
+  BFV_CUDA(launch_ntt(r, d, ra, (long long)(2 * T), 0, int(T), 1, 0), "ntt");
+  if (rb) BFV_CUDA(launch_ntt(r, d, rb, (long long)(2 * T), 0, int(T), 1, 0), "ntt");
+  k_tensor<<<blocks_for((long long)(T * n), 256), 256, 0, r->stream>>>(ra, rb ? rb : ra, 1, int(T), tens, d);
+  BFV_CUDA(cudaGetLastError(), "tensor");
+  BFV_CUDA(launch_ntt(r, d, tens, (long long)(3 * T), 0, int(T), 1, 1), "intt");
+  k_rns_scale<<<blocks_for((long long)(3 * n), 128), 128, 0, r->stream>>>(tens, 3, scaled, d);
+  BFV_CUDA(cudaGetLastError(), "scale");
+  return compose_out(r, d, scaled, 3, out);
+}
+
+int cuhe_bfv_hamming_tile(cuhe_bfv_key* relin, const uint8_t* query, const uint8_t* tile, const uint64_t* exponents,
+                          cuhe_bfv_key* const* keys, uint64_t rotations, const uint8_t* mask, uint64_t t,
+                          uint8_t* out) {
+  if (!relin || !query || !tile || !mask || !out || (rotations && (!exponents || !keys)))
+    return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  cuhe_bfv_ring* r = relin->ring;
+  const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  if (t < 2 || t >= (u64(1) << 60) || H::cmp(H::Big(t), r->plan.q) >= 0)
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid plaintext modulus");
+  for (uint64_t k = 0; k < rotations; ++k) {
+    if (!(exponents[k] & 1) || exponents[k] >= 2 * n) return fail(CUHE_INVALID_ARGUMENT, "Invalid Galois exponent");
+    if (!keys[k] || keys[k]->ring != r) return fail(CUHE_INVALID_ARGUMENT, "Rotation key belongs to another native ring");
+  }
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, t, &d)) return rc;
+  BFV_CUDA(r->arena.reserve(tile_arena_bytes(r, 1) + slice(2 * n * W * 8) * 2 + slice(n * W * 8) + slice(L * n * 8) * 2 +
+                            slice(2 * L * n * 8) + slice(2 * n * W * 8) + 16384),
+           "workspace");
+  r->arena.reset();
+  u64 *qw, *tw, *mw, *mres;
+  if (int rc = upload_polys(r, d, query, 2, 0, &qw, nullptr)) return rc;
+  if (int rc = upload_polys(r, d, tile, 2, 0, &tw, nullptr)) return rc;
+  if (int rc = upload_polys(r, d, mask, 1, L, &mw, &mres)) return rc;
+  BFV_CUDA(launch_ntt(r, d, mres, (long long)(L), 0, int(L), 1, 0), "mask ntt");
+  u64* dist = r->arena.take<u64>(2 * L * n);
+  BFV_ARENA(r->arena);
+  TileArgs a;
+  a.q_words = qw;
+  a.t_words = tw;
+  a.ct = 1;
+  a.relin = relin;
+  for (uint64_t k = 0; k < rotations; ++k) {
+    a.exps.push_back(exponents[k]);
+    a.keys.push_back(keys[k]);
+  }
+  a.masks = {mres};
+  if (int rc = tile_circuit(r, d, a, dist, nullptr)) return rc;
+  return compose_out(r, d, dist, 2, out);
+}
+
+int cuhe_bfv_create_server(cuhe_bfv_key* relin, const uint64_t* exponents, cuhe_bfv_key* const* keys, uint64_t count,
+                           uint64_t padded, uint64_t t, const char* target_hex, cuhe_bfv_server** out) {
+  if (!relin || !out || !target_hex || (count && (!exponents || !keys)))
+    return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  cuhe_bfv_ring* r = relin->ring;
+  const auto& P = r->plan;
+  const size_t n = P.n;
+  if (t < 2 || t >= (u64(1) << 60) || H::cmp(H::Big(t), P.q) >= 0)
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid plaintext modulus");
+  if (!padded || padded > n / 2 || (padded & (padded - 1)) || t % (2 * n) != 1 || !H::is_prime64(t))
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid native server layout or plaintext modulus");
+  const size_t tlen = std::strlen(target_hex);
+  if (tlen < 1 || tlen > (P.q_bits + 3) / 4 || (tlen > 1 && target_hex[0] == '0'))
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid or oversized native modulus encoding");
+  H::Big target;
+  try {
+    target = H::from_hex(target_hex);
+  } catch (const std::invalid_argument&) {
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid or oversized native modulus encoding");
+  }
+  if (H::cmp(target, H::Big(t)) <= 0 || H::cmp(target, P.q) > 0)
+    return fail(CUHE_INVALID_ARGUMENT, "Invalid native response modulus");
+  std::map<u64, cuhe_bfv_key*> keymap;
+  for (uint64_t k = 0; k < count; ++k) {
+    const u64 g = exponents[k];
+    if (!(g & 1) || g >= 2 * n) return fail(CUHE_INVALID_ARGUMENT, "Invalid Galois exponent");
+    if (!keys[k] || keys[k]->ring != r) return fail(CUHE_INVALID_ARGUMENT, "Rotation key belongs to another native ring");
+    if (!keymap.emplace(g, keys[k]).second) return fail(CUHE_INVALID_ARGUMENT, "Duplicate rotation key");
+  }
+  const size_t lanes = n / (2 * padded);
+  auto exponent = [&](size_t step) { return H::powmod(3, step % (n / 2), 2 * n); };
+  std::vector<u64> left, right;
+  for (size_t size = 1; size < padded; size *= 2) {
+    left.push_back(exponent(lanes * size));
+    right.push_back(exponent(n / 2 - lanes * size));
+    if (!keymap.count(left.back()) || !keymap.count(right.back()))
+      return fail(CUHE_INVALID_ARGUMENT, "Missing native server rotation key");
+  }
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, t, &d)) return rc;
+  auto* s = new (std::nothrow) cuhe_bfv_server();
+  if (!s) return fail(CUHE_OUT_OF_MEMORY, "server allocation");
+  s->ring = r;
+  ++r->refs;
+  s->relin = relin;
+  ++relin->refs;
+  for (auto& kv : keymap) {
+    s->keys[kv.first] = kv.second;
+    ++kv.second->refs;
+  }
+  s->padded = padded;
+  s->lanes = lanes;
+  s->capacity = 2 * lanes;
+  s->t = t;
+  s->target = target;
+  s->target_bits = unsigned(target.bits());
+  s->target_words = target.w;
+  s->left = left;
+  s->right = right;
+  s->d_ring = d;
+  const size_t W = size_t(r->host_dev.words);
+  int rc = upload_plain_ntt(r, d, small_to_words(hamming_mask(n, t, lanes, s->capacity), W), &s->d_full_mask);
+  cudaError_t e = cudaSuccess;
+  if (!rc) e = cudaMalloc(&s->d_target, 8 * std::max<size_t>(1, target.w.size()));
+  if (!rc && e == cudaSuccess)
+    e = cudaMemcpy(s->d_target, target.w.data(), 8 * target.w.size(), cudaMemcpyHostToDevice);
+  if (rc || e != cudaSuccess) {
+    cuhe_bfv_server_release(s);
+    return rc ? rc : fail(CUHE_CUDA_ERROR, "server setup");
+  }
+  *out = s;
+  return CUHE_OK;
+}
+
+void cuhe_bfv_server_release(cuhe_bfv_server* server) {
+  if (server && --server->refs == 0) delete server;
+}
+
+uint64_t cuhe_bfv_server_bytes(const cuhe_bfv_server* s) {
+  if (!s) return 0;
+  return s->ring->plan.residue_count * s->ring->plan.n * 8;
+}
+
+int cuhe_bfv_server_layout(const cuhe_bfv_server* s, uint64_t* capacity, uint64_t* padded,
+                           uint64_t* input_packed_bytes, uint64_t* output_packed_bytes,
+                           uint64_t* compact_packed_bytes) {
+  if (!s) return fail(CUHE_INVALID_ARGUMENT, "null server");
+  const auto& P = s->ring->plan;
+  if (capacity) *capacity = s->capacity;
+  if (padded) *padded = s->padded;
+  if (input_packed_bytes) *input_packed_bytes = (P.n * P.q_bits + 7) / 8;
+  if (output_packed_bytes) *output_packed_bytes = (P.n * P.q_bits + 7) / 8;
+  if (compact_packed_bytes) *compact_packed_bytes = (P.n * s->target_bits + 7) / 8;
+  return CUHE_OK;
+}
+
+int cuhe_bfv_last_profile(const cuhe_bfv_server* s, double* ms, int capacity) {
+  if (!s || !ms) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  for (int i = 0; i < capacity && i < 6; ++i) ms[i] = s->profile_ms[i];
+  return CUHE_OK;
+}
+
+}  // extern "C"
+
+struct cuhe_bfv_index {
+  cuhe_bfv_server* server = nullptr;
+  u64* d_words = nullptr;  // [tiles][2][N][W] composed coefficients
+  uint64_t tiles = 0;
+  ~cuhe_bfv_index() {
+    if (d_words) {
+      DeviceGuard g(server->ring->device);
+      cudaFree(d_words);
+    }
+    cuhe_bfv_server_release(server);
+  }
+};
+
+namespace {
+
+// The Hamming search over tiles given either as packed host bytes (index) or
+// as composed words already resident in HBM (resident).
+int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, const u64* resident,
+                uint64_t tiles, uint64_t count, int compact, uint8_t* out, uint64_t out_capacity,
+                uint64_t* responses) {
+  if (!s || !query || (tiles && !index && !resident) || !responses) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  if (count > UINT64_MAX - s->capacity || (count + s->capacity - 1) / s->capacity != tiles)
+    return fail(CUHE_INVALID_ARGUMENT, "vector_count does not match the packed ciphertext count");
+  cuhe_bfv_ring* r = s->ring;
+  const auto& P = r->plan;
+  const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
+  const size_t in_bytes = (n * P.q_bits + 7) / 8;
+  const unsigned out_bits = compact ? s->target_bits : unsigned(P.q_bits);
+  const size_t out_bytes = (n * out_bits + 7) / 8;
+  const size_t groups = (size_t(tiles) + s->padded - 1) / s->padded;
+  *responses = 0;
+  if (groups * 2 * out_bytes > out_capacity) return fail(CUHE_INVALID_ARGUMENT, "output buffer too small");
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = s->d_ring;
+  for (double& v : s->profile_ms) v = 0;
+  // partial mask for the last tile
+  const u64* partial = nullptr;
+  if (count % s->capacity) {
+    auto it = s->partial_masks.find(size_t(count % s->capacity));
+    if (it == s->partial_masks.end()) {
+      u64* m = nullptr;
+      if (int rc = upload_plain_ntt(r, d, small_to_words(hamming_mask(n, s->t, s->lanes, size_t(count % s->capacity)), W), &m))
+        return rc;
+      it = s->partial_masks.emplace(size_t(count % s->capacity), m).first;
+    }
+    partial = it->second;
+  }
+  if (tiles == 0) return CUHE_OK;
+  // chunks of whole groups, at most ~1024 tiles each
+  const size_t max_tiles = std::max<size_t>(s->padded, 1024 / s->padded * s->padded);
+  const size_t out_words = (n * out_bits + 63) / 64;
+  for (size_t g0 = 0; g0 < groups;) {
+    const size_t first = g0 * s->padded;
+    size_t ct = std::min<size_t>(size_t(tiles) - first, max_tiles);
+    const size_t gc = (ct + s->padded - 1) / s->padded;
+    ct = std::min<size_t>(size_t(tiles) - first, gc * s->padded);
+    const size_t need = tile_arena_bytes(r, ct) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) +
+                        slice(2 * n * W * 8) + slice(ct * 2 * n * W * 8) + slice(ct * 2 * L * n * 8) +
+                        slice(gc * 2 * n * W * 8) + slice(gc * 2 * out_words * 8) + slice(sizeof(int)) +
+                        slice(ct * n * W * 8) + slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp)) + 65536;
+    BFV_CUDA(r->arena.reserve(need), "workspace");
+    r->arena.reset();
+    uint8_t* d_qb = r->arena.take<uint8_t>(2 * in_bytes);
+    uint8_t* d_ib = resident ? nullptr : r->arena.take<uint8_t>(ct * 2 * in_bytes);
+    u64* qw = r->arena.take<u64>(2 * n * W);
+    u64* tw = resident ? const_cast<u64*>(resident) + first * 2 * n * W : r->arena.take<u64>(ct * 2 * n * W);
+    u64* dist = r->arena.take<u64>(ct * 2 * L * n);
+    u64* ow = r->arena.take<u64>(gc * 2 * n * W);
+    u64* packed = r->arena.take<u64>(gc * 2 * out_words);
+    int* d_status = r->arena.take<int>(1);
+    BFV_ARENA(r->arena);
+    BFV_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), r->stream), "status");
+    BFV_CUDA(cudaMemcpyAsync(d_qb, query, 2 * in_bytes, cudaMemcpyHostToDevice, r->stream), "query upload");
+    k_unpack<<<blocks_for((long long)(2 * n), 256), 256, 0, r->stream>>>(d_qb, (long long)(in_bytes), int(P.q_bits), 2, qw, d,
+                                                                         d_status);
+    if (!resident) {
+      BFV_CUDA(cudaMemcpyAsync(d_ib, index + first * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice,
+                               r->stream),
+               "index upload");
+      k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, r->stream>>>(
+          d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), tw, d, d_status);
+    }
+    BFV_CUDA(cudaGetLastError(), "unpack");
+    int status = 0;
+    BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, r->stream), "status");
+    BFV_CUDA(cudaStreamSynchronize(r->stream), "unpack");
+    if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
+    TileArgs a;
+    a.q_words = qw;
+    a.t_words = tw;
+    a.ct = ct;
+    a.relin = s->relin;
+    for (u64 g : s->left) {
+      a.exps.push_back(g);
+      a.keys.push_back(s->keys.at(g));
+    }
+    a.masks.assign(ct, s->d_full_mask);
+    if (partial && first + ct == size_t(tiles)) a.masks[ct - 1] = partial;
+    if (int rc = tile_circuit(r, d, a, dist, s->profile_ms)) return rc;
+    // merge tree (bfv_server.h:15-45), executed in waves of independent merges
+    cudaEvent_t m0, m1;
+    cudaEventCreate(&m0);
+    cudaEventCreate(&m1);
+    cudaEventRecord(m0, r->stream);
+    struct Merge { size_t left, right; size_t level; size_t wave; };
+    std::vector<Merge> merges;
+    std::vector<size_t> result_slot;
+    for (size_t gs = 0; gs < ct; gs += s->padded) {
+      struct Node { size_t slot, ready; };
+      std::vector<std::pair<Node, size_t>> stack;
+      const size_t ge = std::min(gs + s->padded, ct);
+      for (size_t at = gs; at < ge; ++at) {
+        Node node{at, 0};
+        size_t size = 1, level = 0;
+        while (!stack.empty() && stack.back().second == size) {
+          const Node left = stack.back().first;
+          stack.pop_back();
+          const size_t wave = std::max(left.ready, node.ready);
+          merges.push_back({left.slot, node.slot, level, wave});
+          node = Node{left.slot, wave + 1};
+          size *= 2;
+          ++level;
+        }
+        stack.emplace_back(node, size);
+      }
+      Node result = stack.back().first;
+      stack.pop_back();
+      while (!stack.empty()) {
+        const size_t size = stack.back().second;
+        size_t level = 0;
+        while ((size_t(1) << level) < size) ++level;
+        const Node left = stack.back().first;
+        stack.pop_back();
+        const size_t wave = std::max(left.ready, result.ready);
+        merges.push_back({left.slot, result.slot, level, wave});
+        result = Node{left.slot, wave + 1};
+      }
+      result_slot.push_back(result.slot);
+    }
+    size_t waves = 0;
+    for (const auto& m : merges) waves = std::max(waves, m.wave + 1);
+    u64* mwords = r->arena.take<u64>(std::max<size_t>(1, ct) * n * W);
+    ComposeOp* d_cops = r->arena.take<ComposeOp>(std::max<size_t>(1, ct));
+    SwitchOp* d_sops = r->arena.take<SwitchOp>(std::max<size_t>(1, ct));
+    BFV_ARENA(r->arena);
+    for (size_t w = 0; w < waves; ++w) {
+      std::vector<ComposeOp> cops;
+      std::vector<SwitchOp> sops;
+      for (const auto& m : merges) {
+        if (m.wave != w) continue;
+        const u64 g = s->right.at(m.level);
+        u64* words = mwords + cops.size() * n * W;
+        cops.push_back(ComposeOp{dist + (m.right * 2 + 1) * L * n, words, unsigned(g), 0u});
+        sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, s->keys.at(g)->d_key,
+                                dist + m.left * 2 * L * n, inverse_mod_2n(g, n), 0u});
+      }
+      if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
+    }
+    cudaEventRecord(m1, r->stream);
+    // outputs: compose, optional compaction, packing
+    std::vector<ComposeOp> cops;
+    for (size_t gi = 0; gi < gc; ++gi)
+      for (size_t comp = 0; comp < 2; ++comp)
+        cops.push_back(ComposeOp{dist + (result_slot[gi] * 2 + comp) * L * n, ow + (gi * 2 + comp) * n * W, 1u, 0u});
+    if (int rc = run_switch(r, d, cops, {}, d_cops, nullptr)) return rc;
+    if (compact) {
+      k_compact<<<blocks_for((long long)(gc * 2 * n), 128), 128, 0, r->stream>>>(ow, (long long)(gc * 2 * n), s->d_target,
+                                                                                 int(s->target_words.size()), d);
+      BFV_CUDA(cudaGetLastError(), "compact");
+    }
+    k_pack<<<blocks_for((long long)(gc * 2 * out_words), 256), 256, 0, r->stream>>>(ow, int(W), int(n), int(out_bits),
+                                                                                   int(gc * 2), packed, (long long)(out_words));
+    BFV_CUDA(cudaGetLastError(), "pack");
+    std::vector<u64> host(gc * 2 * out_words);
+    BFV_CUDA(cudaMemcpyAsync(host.data(), packed, host.size() * 8, cudaMemcpyDeviceToHost, r->stream), "download");
+    cudaEvent_t o1;
+    cudaEventCreate(&o1);
+    cudaEventRecord(o1, r->stream);
+    BFV_CUDA(cudaStreamSynchronize(r->stream), "search");
+    float x = 0;
+    cudaEventElapsedTime(&x, m0, m1);
+    s->profile_ms[4] += x;
+    cudaEventElapsedTime(&x, m1, o1);
+    s->profile_ms[5] += x;
+    cudaEventDestroy(m0);
+    cudaEventDestroy(m1);
+    cudaEventDestroy(o1);
+    for (size_t gi = 0; gi < gc * 2; ++gi)
+      std::memcpy(out + (g0 * 2 + gi) * out_bytes, reinterpret_cast<const uint8_t*>(host.data() + gi * out_words),
+                  out_bytes);
+    g0 += gc;
+  }
+  *responses = groups;
+  return CUHE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cuhe_bfv_packed_search(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, uint64_t tiles,
+                           uint64_t count, int compact, uint8_t* out, uint64_t out_capacity, uint64_t* responses) {
+  return search_impl(s, query, index, nullptr, tiles, count, compact, out, out_capacity, responses);
+}
+
+int cuhe_bfv_upload_index(cuhe_bfv_server* s, const uint8_t* index, uint64_t tiles, cuhe_bfv_index** out) {
+  if (!s || !out || (tiles && !index)) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  cuhe_bfv_ring* r = s->ring;
+  const auto& P = r->plan;
+  const size_t n = P.n, W = size_t(r->host_dev.words);
+  const size_t in_bytes = (n * P.q_bits + 7) / 8;
+  std::lock_guard<std::mutex> lock(r->mu);
+  DeviceGuard guard(r->device);
+  auto* idx = new (std::nothrow) cuhe_bfv_index();
+  if (!idx) return fail(CUHE_OUT_OF_MEMORY, "index allocation");
+  idx->server = s;
+  ++s->refs;
+  idx->tiles = tiles;
+  if (tiles) {
+    const size_t chunk = 256;
+    if (cudaMalloc(&idx->d_words, size_t(tiles) * 2 * n * W * 8) != cudaSuccess) {
+      cudaGetLastError();
+      delete idx;
+      return fail(CUHE_OUT_OF_MEMORY, "index does not fit in device memory");
+    }
+    const size_t need = slice(chunk * 2 * in_bytes) + slice(sizeof(int));
+    if (r->arena.reserve(need) != cudaSuccess) {
+      delete idx;
+      return fail(CUHE_OUT_OF_MEMORY, "workspace");
+    }
+    r->arena.reset();
+    uint8_t* d_ib = r->arena.take<uint8_t>(chunk * 2 * in_bytes);
+    int* d_status = r->arena.take<int>(1);
+    if (r->arena.overflow) { delete idx; return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted"); }
+    cudaMemsetAsync(d_status, 0, sizeof(int), r->stream);
+    for (size_t t0 = 0; t0 < tiles; t0 += chunk) {
+      const size_t ct = std::min<size_t>(chunk, size_t(tiles) - t0);
+      cudaMemcpyAsync(d_ib, index + t0 * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice, r->stream);
+      k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, r->stream>>>(
+          d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), idx->d_words + t0 * 2 * n * W, s->d_ring, d_status);
+      cudaStreamSynchronize(r->stream);  // the staging slice is reused by the next chunk
+    }
+    int status = 0;
+    cudaError_t e = cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { delete idx; return fail(CUHE_CUDA_ERROR, "index upload"); }
+    if (status) { delete idx; return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient"); }
+  }
+  *out = idx;
+  return CUHE_OK;
+}
+
+void cuhe_bfv_index_release(cuhe_bfv_index* index) { delete index; }
+
+int cuhe_bfv_search_index(cuhe_bfv_server* s, cuhe_bfv_index* index, const uint8_t* query, uint64_t count,
+                          int compact, uint8_t* out, uint64_t out_capacity, uint64_t* responses) {
+  if (!index || index->server != s) return fail(CUHE_INVALID_ARGUMENT, "index belongs to another server");
+  return search_impl(s, query, nullptr, index->d_words, index->tiles, count, compact, out, out_capacity, responses);
+}
+
+}  // extern "C"

@@ -347,10 +347,10 @@ __global__ void __launch_bounds__(256) k_imad_probe(uint32_t* sink, int iters, u
       asm volatile("mad.hi.u32 %0, %1, %2, %0;" : "+r"(hi[j]) : "r"(x[j]), "r"(b));
     }
   }
-  uint32_t x = 0;
+  uint32_t folded = 0;
 #pragma unroll
-  for (int j = 0; j < 8; ++j) x ^= lo[j] ^ hi[j];
-  if (x == 0x9e3779b9u) sink[0] = x;
+  for (int j = 0; j < 8; ++j) folded ^= lo[j] ^ hi[j];
+  if (folded == 0x9e3779b9u) sink[0] = folded;
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,105 @@
+/* C ABI of the B200 BFV residue evaluator (libcuhe_bfv_b200.so).
+ *
+ * Replaces the CPython module _bfv_rns (ABI_VERSION 4) of the reference,
+ * src/cuhepy/bfv/_cpu_ext/bindings.cpp:405-433, for rings whose ciphertext
+ * modulus Q is a product of the first 60-bit NTT primes (the reference's
+ * "residue" backend).  Handles are reference counted: a key keeps its ring
+ * alive and a server keeps its keys alive (bindings.cpp:25-38).
+ *
+ * Buffers: a "poly" is N coefficients of coefficient_bytes little-endian
+ * bytes each (bindings.cpp:43-82); a "packed poly" is N coefficients of
+ * bits(modulus) bits each, bit-packed little-endian (packed_wire.h:21-60).
+ * All pointers are host memory.  Return codes follow cuhe_status of
+ * cuhe_paillier.h; cuhe_bfv_last_error() gives the message of the last
+ * failure on the calling thread.
+ */
+#ifndef CUHE_BFV_H
+#define CUHE_BFV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cuhe_bfv_ring cuhe_bfv_ring;
+typedef struct cuhe_bfv_key cuhe_bfv_key;
+typedef struct cuhe_bfv_server cuhe_bfv_server;
+
+const char* cuhe_bfv_last_error(void);
+
+/* create_ring(n, q_hex, digit_bits, fast, residue, kernel_level)
+ * (bindings.cpp:120-136).  Only residue rings are served by the device. */
+int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int fast, int residue,
+                         uint64_t kernel_level, int device, cuhe_bfv_ring** out);
+void cuhe_bfv_ring_release(cuhe_bfv_ring* ring);
+/* ring_info (bindings.cpp:254-270): primes (capacity entries), counts and
+ * the bytes of the NTT tables. */
+int cuhe_bfv_ring_info(const cuhe_bfv_ring* ring, uint64_t* primes, int capacity, int* prime_count,
+                       int* switch_prime_count, int* residue_prime_count, uint64_t* table_bytes,
+                       uint64_t* coefficient_bytes, int* kernel_level, int* fast);
+
+/* compile_key(ring, ((b, a),) * digits) (bindings.cpp:194-208): the key as
+ * digits*2 consecutive polys b_0, a_0, b_1, a_1, ... */
+int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t digits, cuhe_bfv_key** out);
+void cuhe_bfv_key_release(cuhe_bfv_key* key);
+uint64_t cuhe_bfv_key_bytes(const cuhe_bfv_key* key);
+
+/* apply_key(key, poly) -> (b, a) (bindings.cpp:210-220). out: 2 polys. */
+int cuhe_bfv_apply_key(cuhe_bfv_key* key, const uint8_t* poly, uint8_t* out);
+/* ring_product(ring, lhs, rhs) mod q (bindings.cpp:222-236). */
+int cuhe_bfv_ring_product(cuhe_bfv_ring* ring, const uint8_t* lhs, const uint8_t* rhs, uint8_t* out);
+/* multiply(ring, lhs2, rhs2 or NULL, t) -> 3 polys (bindings.cpp:238-252). */
+int cuhe_bfv_multiply(cuhe_bfv_ring* ring, const uint8_t* lhs, const uint8_t* rhs, uint64_t t, uint8_t* out);
+/* rotate_rows(key, ct2, exponent) -> 2 polys (bindings.cpp:154-165). */
+int cuhe_bfv_rotate_rows(cuhe_bfv_key* key, const uint8_t* ct, uint64_t exponent, uint8_t* out);
+/* hamming_tile(relin, query2, tile2, ((g, key),...), mask, t) -> 2 polys
+ * (bindings.cpp:167-192). */
+int cuhe_bfv_hamming_tile(cuhe_bfv_key* relin, const uint8_t* query, const uint8_t* tile,
+                          const uint64_t* exponents, cuhe_bfv_key* const* keys, uint64_t rotations,
+                          const uint8_t* mask, uint64_t t, uint8_t* out);
+
+/* create_server(relin, ((g, key),...), padded, t, target_hex)
+ * (bindings.cpp:278-313). */
+int cuhe_bfv_create_server(cuhe_bfv_key* relin, const uint64_t* exponents, cuhe_bfv_key* const* keys,
+                           uint64_t count, uint64_t padded, uint64_t t, const char* target_hex,
+                           cuhe_bfv_server** out);
+void cuhe_bfv_server_release(cuhe_bfv_server* server);
+uint64_t cuhe_bfv_server_bytes(const cuhe_bfv_server* server);
+/* Geometry of a server: vectors per tile (capacity), bytes of one packed
+ * input poly, and of one packed output poly with and without compaction. */
+int cuhe_bfv_server_layout(const cuhe_bfv_server* server, uint64_t* capacity, uint64_t* padded,
+                           uint64_t* input_packed_bytes, uint64_t* output_packed_bytes,
+                           uint64_t* compact_packed_bytes);
+
+/* packed_search(server, (b, a), ((b, a),...), count, compact)
+ * (bindings.cpp:329-367): query = 2 packed polys, index = tiles*2 packed
+ * polys, tiles == ceil(count / capacity).  Writes responses*2 packed polys
+ * (responses = ceil(tiles / padded)) into out, whose size must be
+ * out_capacity bytes or more; *responses receives the count. */
+int cuhe_bfv_packed_search(cuhe_bfv_server* server, const uint8_t* query, const uint8_t* index,
+                           uint64_t tiles, uint64_t count, int compact, uint8_t* out, uint64_t out_capacity,
+                           uint64_t* responses);
+
+/* Serving form of packed_search: upload an encrypted index once (validated,
+ * unpacked and kept resident in HBM), then search it with any number of
+ * queries.  Results are identical to packed_search on the same bytes.  No
+ * counterpart in the reference, whose packed_search re-imports the index on
+ * every call (bindings.cpp:340-351). */
+typedef struct cuhe_bfv_index cuhe_bfv_index;
+int cuhe_bfv_upload_index(cuhe_bfv_server* server, const uint8_t* index, uint64_t tiles, cuhe_bfv_index** out);
+void cuhe_bfv_index_release(cuhe_bfv_index* index);
+int cuhe_bfv_search_index(cuhe_bfv_server* server, cuhe_bfv_index* index, const uint8_t* query, uint64_t count,
+                          int compact, uint8_t* out, uint64_t out_capacity, uint64_t* responses);
+
+/* Per-phase device times (milliseconds) of the last packed_search on this
+ * server, in the phase order tensor, relinearize, rotate, mask, merge,
+ * output.  No counterpart in the reference; it feeds the profile_* calls. */
+int cuhe_bfv_last_profile(const cuhe_bfv_server* server, double* ms, int capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUHE_BFV_H */

@@ -29,6 +29,29 @@ def test_paillier_library_exports_every_declared_symbol():
     assert lib.cuhe_version().startswith(b"cuhe_b200")
 
 
+def test_bfv_library_exports_every_declared_symbol():
+    from cuhepy_b200.bfv import _bfv_rns
+
+    lib = _bfv_rns.lib()
+    names = declared("cuhe_bfv.h")
+    assert "cuhe_bfv_packed_search" in names and len(names) > 15
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _bfv_rns.BFV_SIGNATURES, name
+    assert _bfv_rns.ABI_VERSION == 4
+
+
+def test_bfv_boundary_validation_without_a_device():
+    from cuhepy_b200.bfv import _bfv_rns
+
+    with pytest.raises(TypeError):
+        _bfv_rns.create_ring(16, 7, 4)
+    with pytest.raises(ValueError):
+        _bfv_rns.create_ring(1 << 20, "f", 4, True, True)
+    with pytest.raises((TypeError, ValueError, OverflowError)):
+        _bfv_rns.create_ring(16, "f", 4, True, True, -1)
+
+
 def test_context_creation_reports_errors_without_crashing():
     lib = _native.paillier_lib()
     handle = ctypes.c_void_p()
