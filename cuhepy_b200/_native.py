@@ -46,6 +46,8 @@ PAILLIER_SIGNATURES: dict[str, tuple] = {
     "cuhe_paillier_decrypt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]),
     "cuhe_paillier_decode_hamming": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                                     ctypes.c_int, ctypes.c_void_p]),
+    "cuhe_paillier_decode_hamming_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                           ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "cuhe_paillier_modexp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_u32_p, ctypes.c_int,
                                             ctypes.c_void_p, ctypes.c_int64]),
     "cuhe_paillier_modexp_each": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,

@@ -15,6 +15,11 @@
 
 using cuhe::host::Limbs;
 
+// Scratch of cuhe_paillier_decode_hamming_static: one popcount per ciphertext
+// chunk.  Host code must not pass this name to a kernel (on the host it is a
+// stand-in, not a device address); the device address is looked up per device.
+static __device__ __align__(256) uint32_t g_static_decode_counts[CUHE_STATIC_DECODE_MAX_CHUNKS];
+
 namespace {
 
 std::string g_create_error;
@@ -620,6 +625,62 @@ int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t 
   CUHE_CUDA(ctx, cudaGetLastError(), "decode reduction");
   if (int rc = st.finish()) return rc;
   return check_status(ctx, st.staged());
+}
+
+}  // extern "C"
+
+namespace {
+
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_mu;
+uint32_t* g_static_counts[kMaxStaticDevices] = {};
+
+// Device address of g_static_decode_counts on `device` (which is current).
+int static_counts(cuhe_paillier* ctx, int device, uint32_t** out) {
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (device < 0 || device >= kMaxStaticDevices) return fail(ctx, CUHE_INVALID_ARGUMENT, "device ordinal out of range");
+  if (!g_static_counts[device]) {
+    void* address = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&address, g_static_decode_counts);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "static scratch address");
+    g_static_counts[device] = static_cast<uint32_t*>(address);
+  }
+  *out = g_static_counts[device];
+  return CUHE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cuhe_paillier_decode_hamming_static(cuhe_paillier* ctx, const uint32_t* c, int64_t vectors, int chunk_num,
+                                        int chunk_len, int64_t* distance) {
+  if (!ctx || vectors < 0 || chunk_num <= 0 || chunk_len <= 0 || chunk_len % 32)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid decode layout");
+  if (!ctx->have_secret) return fail(ctx, CUHE_NOT_READY, "decode: secret key not installed");
+  if (vectors == 0) return CUHE_OK;
+  if (!c || !distance) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  if (chunk_len / 32 > ctx->K) return fail(ctx, CUHE_INVALID_ARGUMENT, "chunk_len wider than n^2");
+  if (vectors > CUHE_STATIC_DECODE_MAX_CHUNKS / chunk_num)
+    return fail(ctx, CUHE_INVALID_ARGUMENT,
+                "decode_hamming_static: vectors*chunk_num exceeds the static scratch of " +
+                    std::to_string(CUHE_STATIC_DECODE_MAX_CHUNKS) + " ciphertext chunks");
+  DeviceGuard guard(ctx->device);
+  if (!is_device_pointer(c) || !is_device_pointer(distance))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "decode_hamming_static needs device buffers for c and distance");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  uint32_t* counts = nullptr;
+  if (int rc = static_counts(ctx, ctx->device, &counts)) return rc;
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const int64_t total = vectors * chunk_num;
+  CUHE_CUDA(ctx, d.modexp(ctx, c, nullptr, counts, total, ctx->d_ops_sec, ctx->nops_sec, cuhe::EXP_DECODE,
+                          chunk_len / 32),
+            "static decode launch");
+  cuhe::k_sum_chunks<<<unsigned((vectors + 255) / 256), 256, 0, ctx->stream>>>(
+      counts, vectors, chunk_num, reinterpret_cast<long long*>(distance));
+  CUHE_CUDA(ctx, cudaGetLastError(), "static decode reduction");
+  return CUHE_OK;
 }
 
 int cuhe_imad_peak(int device, double* word_products_per_second) {

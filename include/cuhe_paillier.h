@@ -85,6 +85,34 @@ int cuhe_paillier_decrypt(cuhe_paillier* ctx, const uint32_t* c, uint32_t* m, in
 int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t vectors, int chunk_num,
                                  int chunk_len, int64_t* distance);
 
+/* Allocation-free variant of cuhe_paillier_decode_hamming.  It has no
+ * counterpart in the reference.  It is for callers that cannot allocate GPU
+ * memory while they run: code inside a CUDA graph capture, and serving
+ * processes whose device memory is owned by a caching allocator or a fixed
+ * reservation.  cuhe_paillier_decode_hamming takes its per-chunk scratch from
+ * the context workspace, which cudaMalloc's on growth; this entry point instead
+ * keeps that scratch in a file-scope device array of
+ * CUHE_STATIC_DECODE_MAX_CHUNKS uint32 counts (256 KiB), which every GPU that
+ * loads the library holds until the process exits.
+ *  - c (vectors*chunk_num ciphertexts, K words each) and distance (vectors
+ *    int64) must be device memory; host pointers are rejected, because staging
+ *    them would allocate.
+ *  - vectors*chunk_num above CUHE_STATIC_DECODE_MAX_CHUNKS is rejected with
+ *    CUHE_INVALID_ARGUMENT before anything is launched.
+ *  - The first call on a device, with that device current, looks up the
+ *    array's device address once (cudaGetSymbolAddress); make that first call
+ *    before any stream capture.
+ *  - Work is queued on the context stream and the call returns without waiting;
+ *    range errors surface at the next cuhe_synchronize.
+ *  - All calls in the process share the one array per device, so two calls
+ *    whose work overlaps on the GPU race on it: serialise them (one stream, or
+ *    wait between calls).  Each call writes every count it later reads, so
+ *    nothing has to be cleared between calls.
+ * Calls no cudaMalloc, cudaFree or other allocating routine. */
+#define CUHE_STATIC_DECODE_MAX_CHUNKS 65536
+int cuhe_paillier_decode_hamming_static(cuhe_paillier* ctx, const uint32_t* c, int64_t vectors, int chunk_num,
+                                        int chunk_len, int64_t* distance);
+
 /* out[i] = base[i]^exponent mod n^2 (generic fixed-exponent batch). */
 int cuhe_paillier_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* exponent,
                          int exponent_words, uint32_t* out, int64_t count);
