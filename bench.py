@@ -355,11 +355,160 @@ def run_gpu(args) -> dict | None:
                 "path": "C ABI with pinned host buffers, every stage staged over PCIe"},
         "gpu_launches": 6 * args.steps,
     }
+    if not args.no_bfv:
+        result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
     if not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if dist:
         dist.destroy_process_group()
     return result
+
+
+BFV_N, BFV_Q_BITS, BFV_GADGET, BFV_T, BFV_EMBED = 8192, 180, 30, 65537, 512
+BFV_VECTORS = 16384
+
+
+def bfv_setup(seed: int = 8192):
+    """N=8192, Q = 3 x 60-bit NTT primes, 30-bit gadget, t=65537, embed 512
+    (16 vectors per ciphertext, 1,024 index ciphertexts for 16,384 vectors).
+    Keys and ciphertexts are uniform residues from a seeded generator: the
+    evaluator's work is independent of the values, and bit-exactness on real
+    encryptions is covered by the parity tests."""
+    from oracle import bfv as ob
+
+    q = 1
+    for p in ob.rns_primes(BFV_N, BFV_Q_BITS):
+        q *= p
+    layout = ob.Layout(BFV_N, BFV_EMBED)
+    exps = sorted(set(layout.left()) | set(layout.right()))
+    rng = np.random.default_rng(seed)
+    width = (q.bit_length() + 7) // 8
+
+    def poly_fixed():
+        # uniform residues below q: three 60-bit limbs, each < its prime, via CRT-free rejection
+        vals = [int(x) for x in rng.integers(0, 1 << 62, size=BFV_N, dtype=np.int64)]
+        hi = [int(x) for x in rng.integers(0, 1 << 62, size=BFV_N, dtype=np.int64)]
+        lo = [int(x) for x in rng.integers(0, 1 << 62, size=BFV_N, dtype=np.int64)]
+        return b"".join((((v << 124) | (h << 62) | w) % q).to_bytes(width, "little") for v, h, w in zip(vals, hi, lo))
+
+    def key():
+        return tuple((poly_fixed(), poly_fixed()) for _ in range(6))
+
+    keys = [key() for _ in range(1 + len(exps))]
+    bits = q.bit_length()
+
+    def packed_ct():
+        out = []
+        for _ in range(2):
+            vals = [int(x) for x in rng.integers(0, 1 << 62, size=(BFV_N, 3), dtype=np.int64).reshape(-1)]
+            coeffs = [((vals[3 * i] << 124) | (vals[3 * i + 1] << 62) | vals[3 * i + 2]) % q for i in range(BFV_N)]
+            out.append(ob.pack_poly(coeffs, bits))
+        return tuple(out)
+
+    query = packed_ct()
+    base_tiles = [packed_ct() for _ in range(8)]
+    tiles = BFV_VECTORS // layout.capacity
+    index = tuple(base_tiles[i % len(base_tiles)] for i in range(tiles))
+    target = ob.coefficient_modulus(50)
+    return q, layout, exps, keys, query, index, target
+
+
+def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
+    """BFV packed Hamming kNN: one step = one encrypted query against the
+    resident 16,384-vector index (1,024 tiles, 2 compacted responses)."""
+    from cuhepy_b200.bfv import _bfv_rns as m
+
+    q, layout, exps, keys, query, index, target = bfv_setup()
+    ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+    relin = m.compile_key(ring, keys[0])
+    galois = tuple((g, m.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
+    server = m.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
+    resident = m.upload_index(server, index)
+    for _ in range(warmup):
+        m.search_index(server, resident, query, BFV_VECTORS, True)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        resp = m.search_index(server, resident, query, BFV_VECTORS, True)
+        times.append(time.perf_counter() - t0)
+    _, prof = m.profile_packed_search(server, query, index, BFV_VECTORS, True)
+    e2e_t = []
+    for _ in range(max(1, min(steps, 2))):
+        t0 = time.perf_counter()
+        resp2 = m.packed_search(server, query, index, BFV_VECTORS, True)
+        e2e_t.append(time.perf_counter() - t0)
+    if resp2 != resp:
+        raise RuntimeError("BFV resident and packed searches differ")
+    # per-operation form: one hamming_tile call per tile (no batching across tiles)
+    width = (q.bit_length() + 7) // 8
+    from oracle import bfv as ob
+    unpack = [ob.unpack_poly(c, q.bit_length(), BFV_N) for c in query]
+    qf = tuple(b"".join(int(v).to_bytes(width, "little") for v in poly) for poly in unpack)
+    mask = b"".join(int(v).to_bytes(width, "little")
+                    for v in ob.batch_encode(layout.mask_slots(layout.capacity), BFV_N, BFV_T))
+    rot = tuple((g, k) for g, k in galois if g in layout.left())
+    rot = tuple(sorted(rot, key=lambda e: layout.left().index(e[0])))
+    m.hamming_tile(relin, qf, qf, rot, mask, BFV_T)
+    t0 = time.perf_counter()
+    plain_tiles = 8
+    for _ in range(plain_tiles):
+        m.hamming_tile(relin, qf, qf, rot, mask, BFV_T)
+    per_tile = (time.perf_counter() - t0) / plain_tiles
+    tiles = len(index)
+    out = {
+        "metric": "BFV kNN queries/s (N=8192, Q=3x60-bit, 16,384 x 512-bit index resident, compacted responses)",
+        "value": 1.0 / statistics.mean(times), "unit": "queries/s",
+        "p50_ms": 1e3 * statistics.median(times), "p99_ms": 1e3 * float(np.percentile(times, 99)),
+        "phase_ms": {k: 1e3 * v["seconds"] for k, v in prof.items() if k != "other"},
+        "e2e": {"value": 1.0 / statistics.mean(e2e_t), "unit": "queries/s",
+                "path": "_bfv_rns.packed_search with the packed index as host bytes (re-imported every call)",
+                "h2d_bytes_per_step": int((tiles + 1) * 2 * len(index[0][0])),
+                "d2h_bytes_per_step": int(sum(len(a) + len(b) for a, b in resp))},
+        "plain_value": 1.0 / (per_tile * tiles),
+        "plain": "one hamming_tile call per tile (merge tree not included)",
+        "tiles": tiles,
+        "data": "seeded uniform keys and ciphertexts (evaluation work is value-independent)",
+    }
+    if cpu:
+        out["cpu_baseline"] = bfv_cpu_baseline(q, layout, exps, keys, query, index, target)
+    return out
+
+
+def bfv_cpu_baseline(q, layout, exps, keys, query, index, target, sample_tiles: int = 2) -> dict:
+    """The reference's own compiled _bfv_rns (oracle/_ref) on the host cores:
+    one search of `sample_tiles` tiles per thread (the module releases the GIL),
+    extrapolated linearly to the 1,024-tile query."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    sys.path.insert(0, str(REPO / "tests"))
+    from bfv_helpers import reference_native
+
+    ref = reference_native()
+    if ref is None:
+        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref not built on this machine"}
+    ring = ref.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+    relin = ref.compile_key(ring, keys[0])
+    galois = tuple((g, ref.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
+    server = ref.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
+    sample = index[:sample_tiles]
+    count = sample_tiles * layout.capacity
+    ref.packed_search(server, query, sample, count, True)
+    cores = len(os.sched_getaffinity(0))
+    t0 = time.perf_counter()
+    ref.packed_search(server, query, sample, count, True)
+    single = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(cores) as pool:
+        list(pool.map(lambda _: ref.packed_search(server, query, sample, count, True), range(cores)))
+    multi = time.perf_counter() - t0
+    tiles = len(index)
+    per_query_1 = single / sample_tiles * tiles
+    per_query_all = multi / (cores * sample_tiles) * tiles
+    return {"value": 1.0 / per_query_all, "unit": "queries/s", "cores": cores, "kind": "reference",
+            "single_thread_value": 1.0 / per_query_1,
+            "sample": f"reference _bfv_rns.packed_search (oracle/_ref, GMP 6.3.0) over {sample_tiles} tiles "
+                      f"per thread on {cores} threads, extrapolated to {tiles} tiles"}
 
 
 def ctypes_imad_peak(native, device: int) -> float:
@@ -418,12 +567,48 @@ def _cpu_worker(payload):
     return done, time.perf_counter() - t0
 
 
+def seeded_lookup_keys_cpu(seed: int = 0) -> dict:
+    """The same seeded Paillier-Lookup keys as seeded_lookup_keys, computed on
+    the host only (tables by the oracle), for the CPU arms."""
+    import math as _math
+
+    from cuhepy_b200 import _numbers
+    from cuhepy_b200.paillier import lookup
+    from oracle import gmp as ogmp
+    from oracle import paillier as oracle
+
+    fake = SeededSecrets(seed)
+    saved = (_numbers.secrets, lookup.secrets)
+    _numbers.secrets = lookup.secrets = fake
+    try:
+        while True:
+            q_bits = min(KEY_LEN, ALPHA_LEN)
+            p1, q1, g1 = lookup.PaillierLookup.gen_dsa_params_custom(KEY_LEN, q_bits // 2)
+            p2, q2, g2 = lookup.PaillierLookup.gen_dsa_params_custom(KEY_LEN, q_bits - q_bits // 2)
+            n = p1 * p2
+            n2 = n * n
+            g, _ = lookup.PaillierLookup.crt_pair((g1 % p1) * (1 + p1) % (p1 * p1), p1 * p1,
+                                                  (g2 % p2) * (1 + p2) % (p2 * p2), p2 * p2)
+            a = _math.lcm(q1, q2)
+            if ogmp.powmod(g, n * a, n2) == 1 and ogmp.powmod(g, n, n2) != 1:
+                break
+        g_a_inv = pow((ogmp.powmod(g, a, n2) - 1) // n, -1, n)
+        exps = [lookup.PaillierLookup.generate_random_r(n) for _ in range(256)]
+    finally:
+        _numbers.secrets, lookup.secrets = saved
+    chunks = oracle.message_chunks(KEY_LEN)
+    table = oracle.g_table(g, n, KEY_LEN)
+    return {"pk": {"g": g, "n": n, "n_squared": n2}, "sk": {"a": a, "g_a_inv": g_a_inv},
+            "g_table": dict(enumerate(table)), "noise_table": oracle.noise_table(g, n, exps),
+            "message_chunks": chunks}
+
+
 def cpu_baseline(seconds: float = 20.0) -> dict:
     import multiprocessing as mp
 
     from oracle import paillier as oracle
 
-    keys = seeded_lookup_keys(0)
+    keys = seeded_lookup_keys_cpu(0)
     keys_plain = {"pk": dict(keys["pk"]), "sk": dict(keys["sk"])}
     table = [keys["g_table"][i] for i in range(keys["message_chunks"])]
     noise = list(keys["noise_table"])
@@ -467,6 +652,47 @@ def run_reference(args) -> dict | None:
     }
 
 
+def profile_case(which: str) -> None:
+    """Small cases of the dominant kernels, sized for ncu captures (inputs
+    larger than L2 where the kernel streams memory, a few GB at most)."""
+    import torch
+
+    if which == "paillier":
+        from cuhepy_b200.paillier.gpu import PaillierDevice
+
+        keys = seeded_lookup_keys(0)
+        pk, sk = keys["pk"], keys["sk"]
+        ctx = PaillierDevice(pk["n"])
+        ctx.set_secret(sk["a"], sk["g_a_inv"])
+        ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
+        stream = torch.cuda.Stream()
+        ctx.set_stream(stream.cuda_stream)
+        vectors = 8192
+        bits = torch.from_numpy(synthetic_bits(vectors, 1337)).cuda()
+        nidx = torch.from_numpy(noise_indices(vectors, 3)).cuda()
+        cts = torch.empty((vectors, ctx.words), dtype=torch.int32, device="cuda")
+        dist = torch.empty(vectors, dtype=torch.int64, device="cuda")
+        with torch.cuda.stream(stream):
+            for _ in range(2):  # launch 1-2: encrypt; decode follows each
+                ctx.lookup_encrypt_bits_array(bits, vectors, EMBED_LEN, 2 * KEY_LEN, 1, nidx, cts)
+                ctx.decode_array(cts, vectors, 1, 2 * KEY_LEN, dist)
+        torch.cuda.synchronize()
+        print("paillier profile case done", int(dist[:4].sum()))
+    else:
+        from cuhepy_b200.bfv import _bfv_rns as m
+
+        q, layout, exps, keys, query, index, target = bfv_setup()
+        ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+        relin = m.compile_key(ring, keys[0])
+        galois = tuple((g, m.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
+        server = m.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
+        small = index[:64]
+        resident = m.upload_index(server, small)
+        for _ in range(2):
+            m.search_index(server, resident, query, 64 * layout.capacity, True)
+        print("bfv profile case done")
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -475,7 +701,13 @@ def main() -> None:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--cpu-seconds", type=float, default=20.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-bfv", action="store_true", help="skip the BFV kNN section")
+    parser.add_argument("--profile-case", choices=["paillier", "bfv"],
+                        help="run one small step of a hot kernel (for ncu captures) and exit")
     args = parser.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     result = run_reference(args) if args.impl == "reference" else run_gpu(args)
