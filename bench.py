@@ -660,7 +660,7 @@ def profile_case(which: str) -> None:
     if which == "paillier":
         from cuhepy_b200.paillier.gpu import PaillierDevice
 
-        keys = seeded_lookup_keys(0)
+        keys = seeded_lookup_keys_cpu(0)  # host-built keys: the only k_modexp launches are the decodes
         pk, sk = keys["pk"], keys["sk"]
         ctx = PaillierDevice(pk["n"])
         ctx.set_secret(sk["a"], sk["g_a_inv"])
