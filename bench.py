@@ -39,6 +39,8 @@ import numpy as np
 REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
+from cuhepy_b200._numbers import factors_from_phi  # noqa: E402
+
 KEY_LEN = 1024
 ALPHA_LEN = 280
 EMBED_LEN = 512
@@ -167,6 +169,8 @@ def run_gpu(args) -> dict | None:
     pk, sk = keys["pk"], keys["sk"]
     ctx = PaillierDevice(pk["n"], device=local)
     ctx.set_secret(sk["a"], sk["g_a_inv"])
+    factors = factors_from_phi(pk["n"], sk["phi"])
+    ctx.set_factors(*factors)  # decode by CRT (the reference-facing clients do the same)
     ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
@@ -264,6 +268,7 @@ def run_gpu(args) -> dict | None:
     dist_p = pinned((QUERY_BATCH * INDEX_VECTORS,), torch.int64)
     e2e_ctx = PaillierDevice(pk["n"], device=local)
     e2e_ctx.set_secret(sk["a"], sk["g_a_inv"])
+    e2e_ctx.set_factors(*factors)
     e2e_ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
 
     def e2e_step():
@@ -301,15 +306,32 @@ def run_gpu(args) -> dict | None:
         stream.synchronize()
     plain_value = plain_n / (time.perf_counter() - t0)
 
-    # ---- roofline of the dominant kernel (decode: c^a modexp) --------------
+    # ---- the same decode batch on the direct kernel mod n^2 (no CRT) ------
+    ctx.set_factors(None, None)
+    direct_ms = []
+    for _ in range(2):
+        flush.fill_(1)
+        a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a_ev.record(stream)
+            ctx.decode_array(prod, QUERY_BATCH * INDEX_VECTORS, 1, chunk_len, dist_out)
+            b_ev.record(stream)
+        b_ev.synchronize()
+        direct_ms.append(a_ev.elapsed_time(b_ev))
+    ctx.set_factors(*factors)
+
+    # ---- roofline of the dominant kernel (decode: c^a by CRT) --------------
     peak = ctypes_imad_peak(_native, local)
     k = words
+    kh = k // 2
     a_bits = int(sk["a"]).bit_length()
     mm = a_bits + math.ceil(a_bits / 6) + 16
-    wp_per_decode = mm * (2 * k * k + k)
+    wp_per_decode = 2 * mm * (2 * kh * kh + kh)
     decode_ms = statistics.mean(kernel_ms["decode"])
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    nominal = torch.cuda.get_device_properties(local).multi_processor_count * 64 * sm_mhz * 1e6 / 2
     achieved = QUERY_BATCH * INDEX_VECTORS * wp_per_decode / (decode_ms / 1e3)
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(QUERY_BATCH * INDEX_VECTORS)
     clock_summary = clocks.summary()
     if rank != 0:
         if dist:
@@ -338,16 +360,23 @@ def run_gpu(args) -> dict | None:
             "tuning": {"threads_per_instance": ctx.tuning()[0], "window": ctx.tuning()[1]},
         },
         "stage_ms": {name: statistics.mean(v) for name, v in kernel_ms.items()},
+        "decode_direct_ms": statistics.mean(direct_ms),
+        "decode_direct": "the same decode batch on k_modexp (c^a mod n^2, no CRT), outside the timed steps",
         "p50_ms": statistics.median(step_ms),
         "p99_ms": float(np.percentile(step_ms, 99)),
         "plain_value": plain_value,
         "plain": "decode one ciphertext per launch (batch 1), host-synchronised",
         "roofline": {
-            "bound": "imad", "kernel": "k_modexp<128,16,4> decode (c^a, |a|=%d bits)" % a_bits,
+            "bound": "imad",
+            "kernel": "k_modexp_crt<64,8,4> decode (c^a mod p^2 and mod q^2, |a|=%d bits)" % a_bits,
             "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Twp/s",
             "frac": achieved / peak, "traffic": traffic,
-            "peak_source": "measured by cuhe_imad_peak (mad.lo+mad.hi word products) in this run",
-            "work_per_unit": f"MM(e)=e+ceil(e/6)+16={mm} modmuls x (2k^2+k)={2 * k * k + k} wp, k={k}",
+            "peak_nominal": nominal / 1e12, "frac_of_nominal": achieved / nominal,
+            "peak_nominal_source": "SMs x 64 IMAD/clk x median SM clock / 2 IMAD per word product",
+            "traffic_source": "ncu dram bytes of an 8,192-decode launch, scaled by decodes per launch",
+            "peak_source": "measured by cuhe_imad_peak in this run (best of mad.lo+mad.hi, mad.wide, carry-chain probes)",
+            "work_per_unit": (f"2 sides x MM(e)=e+ceil(e/6)+16={mm} modmuls x (2kh^2+kh)={2 * kh * kh + kh} wp, "
+                              f"kh={kh} (recombination and epilogue, under 2%, not counted)"),
         },
         "clocks": clock_summary,
         "e2e": {"value": e2e_value, "unit": "modexp/s", "h2d_bytes_per_step": int(h2d),
@@ -522,15 +551,17 @@ def ctypes_imad_peak(native, device: int) -> float:
     return out.value
 
 
-def ncu_traffic():
-    """DRAM bytes per decode launch from the committed ncu summary, if any."""
-    path = REPO / "profiles" / "traffic.json"
-    if path.exists():
-        try:
-            return json.loads(path.read_text()).get(WORKLOAD)
-        except (ValueError, OSError):
-            return None
-    return None
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_modexp_crt<64,8,4>
+# decode launch of 8,192 ciphertexts (ncu --set full, key_len 1024):
+# 4,350,976 + 0 bytes.  Each ciphertext is read once, so the traffic of a
+# larger launch scales with the number of decodes.
+DECODE_TRAFFIC_BYTES, DECODE_TRAFFIC_ITEMS = 4_350_976, 8192
+
+
+def ncu_traffic(items: int) -> float:
+    """DRAM bytes of one decode launch of `items` ciphertexts, scaled from
+    the measured small-case capture."""
+    return DECODE_TRAFFIC_BYTES * items / DECODE_TRAFFIC_ITEMS
 
 
 # ---------------------------------------------------------------------------
@@ -598,7 +629,7 @@ def seeded_lookup_keys_cpu(seed: int = 0) -> dict:
         _numbers.secrets, lookup.secrets = saved
     chunks = oracle.message_chunks(KEY_LEN)
     table = oracle.g_table(g, n, KEY_LEN)
-    return {"pk": {"g": g, "n": n, "n_squared": n2}, "sk": {"a": a, "g_a_inv": g_a_inv},
+    return {"pk": {"g": g, "n": n, "n_squared": n2}, "sk": {"phi": (p1 - 1) * (p2 - 1), "a": a, "g_a_inv": g_a_inv},
             "g_table": dict(enumerate(table)), "noise_table": oracle.noise_table(g, n, exps),
             "message_chunks": chunks}
 
@@ -664,6 +695,7 @@ def profile_case(which: str) -> None:
         pk, sk = keys["pk"], keys["sk"]
         ctx = PaillierDevice(pk["n"])
         ctx.set_secret(sk["a"], sk["g_a_inv"])
+        ctx.set_factors(*factors_from_phi(pk["n"], sk["phi"]))
         ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
         stream = torch.cuda.Stream()
         ctx.set_stream(stream.cuda_stream)

@@ -63,3 +63,21 @@ def get_random_range(a: int, b: int) -> int:
 
 def lcm(a: int, b: int) -> int:
     return math.lcm(int(a), int(b))
+
+
+def factors_from_phi(n: int, phi: int) -> tuple[int, int] | None:
+    """The primes p <= q of n = p q from phi = (p - 1)(q - 1): p + q = n - phi + 1
+    and p, q are the roots of x^2 - (p + q) x + n.  None when (n, phi) is not
+    such a pair."""
+    n, phi = int(n), int(phi)
+    s = n - phi + 1
+    disc = s * s - 4 * n
+    if s <= 0 or disc < 0:
+        return None
+    root = math.isqrt(disc)
+    if root * root != disc or (s - root) % 2:
+        return None
+    p, q = (s - root) // 2, (s + root) // 2
+    if p <= 1 or p * q != n:
+        return None
+    return p, q

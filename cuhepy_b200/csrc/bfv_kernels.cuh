@@ -46,6 +46,136 @@ struct RingDev {
 };
 
 // ---- negacyclic NTT of one plane in shared memory ---------------------------
+// Shared-memory planes are padded by one u64 every 16 elements so that the
+// stride-1 radix-16 blocks of the last passes do not all hit one bank.
+__device__ __forceinline__ int sp(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr size_t plane_smem_words(int n) { return size_t(n) + size_t(n) / 16 + 16; }
+
+// Forward (decimation in frequency, psi^bitrev twiddles, bit-reversed output)
+// as passes of up to four radix-2 stages held in registers: a block of E = 2^P
+// elements at stride `stride` runs stages s0 .. s0+P-1 without touching shared
+// memory.  Stage s has 2^s groups of gap N/2^(s+1); inside a block the group
+// of element k at stage s0+t is G*2^t + (k >> (P-t)).
+template <int P>
+__device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const u64* __restrict__ w,
+                                                 const u64* __restrict__ wq, u64 p, bool last) {
+  constexpr int E = 1 << P;
+  const int n = 1 << logn;
+  const u64 two_p = 2 * p;
+  const int g = n >> (s0 + 1);
+  const int stride = g >> (P - 1);
+  const int log_stride = (logn - s0 - 1) - (P - 1);
+  const int nblocks = n >> P;
+  for (int blk = threadIdx.x; blk < nblocks; blk += blockDim.x) {
+    const int G = blk >> log_stride, jj = blk & (stride - 1);
+    const int base = G * 2 * g + jj;
+    u64 x[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) x[k] = a[sp(base + k * stride)];
+#pragma unroll
+    for (int t = 0; t < P; ++t) {
+      const int half = E >> (t + 1);
+      const int m = 1 << (s0 + t);
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        if (k & half) continue;
+        const int idx = m + (G << t) + (k >> (P - t));
+        const u64 root = __ldg(w + idx), rq = __ldg(wq + idx);
+        u64 u = x[k];
+        if (u >= two_p) u -= two_p;
+        const u64 v = shoup_lazy(x[k + half], root, rq, p);
+        x[k] = u + v;
+        x[k + half] = u + two_p - v;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      u64 v = x[k];
+      if (last) {
+        if (v >= two_p) v -= two_p;
+        if (v >= p) v -= p;
+      }
+      a[sp(base + k * stride)] = v;
+    }
+  }
+}
+
+// Inverse (decimation in time) passes: stage u has gap 2^u and N/2^(u+1)
+// groups; the final stage (gap N/2) folds in 1/N and the inverse twist.
+template <int P>
+__device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const u64* __restrict__ w,
+                                                 const u64* __restrict__ wq, u64 p, u64 n_inv, u64 n_inv_q,
+                                                 u64 last_w, u64 last_q) {
+  constexpr int E = 1 << P;
+  const int n = 1 << logn;
+  const u64 two_p = 2 * p;
+  const int stride = 1 << u0;
+  const int nblocks = n >> P;
+  for (int blk = threadIdx.x; blk < nblocks; blk += blockDim.x) {
+    const int G = blk >> u0, jj = blk & (stride - 1);
+    const int base = (G << (u0 + P)) + jj;
+    u64 x[E];
+#pragma unroll
+    for (int k = 0; k < E; ++k) x[k] = a[sp(base + k * stride)];
+#pragma unroll
+    for (int t = 0; t < P; ++t) {
+      const int half = 1 << t;
+      const int stage = u0 + t;
+      const bool final_stage = stage == logn - 1;
+      const int m = n >> (stage + 1);
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        if (k & half) continue;
+        const u64 u = x[k], v = x[k + half];
+        if (final_stage) {
+          x[k] = shoup(u + v, n_inv, n_inv_q, p);
+          x[k + half] = shoup(u + two_p - v, last_w, last_q, p);
+        } else {
+          const int idx = m + (G << (P - t - 1)) + (k >> (t + 1));
+          const u64 root = __ldg(w + idx), rq = __ldg(wq + idx);
+          const u64 s = u + v;
+          x[k] = s >= two_p ? s - two_p : s;
+          x[k + half] = shoup_lazy(u + two_p - v, root, rq, p);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) a[sp(base + k * stride)] = x[k];
+  }
+}
+
+// Whole transforms over a padded shared-memory plane (all threads of the CTA).
+__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j) {
+  const int logn = R.logn;
+  const u64 p = R.prime[j].p;
+  for (int s0 = 0; s0 < logn; s0 += 4) {
+    const int P = logn - s0 < 4 ? logn - s0 : 4;
+    const bool last = s0 + P == logn;
+    switch (P) {
+      case 4: ntt_forward_pass<4>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
+      case 3: ntt_forward_pass<3>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
+      case 2: ntt_forward_pass<2>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
+      default: ntt_forward_pass<1>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j) {
+  const int logn = R.logn;
+  const u64 p = R.prime[j].p;
+  for (int u0 = 0; u0 < logn; u0 += 4) {
+    const int P = logn - u0 < 4 ? logn - u0 : 4;
+    switch (P) {
+      case 4: ntt_inverse_pass<4>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      case 3: ntt_inverse_pass<3>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      case 2: ntt_inverse_pass<2>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      default: ntt_inverse_pass<1>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+    }
+    __syncthreads();
+  }
+}
+
 // Forward: decimation in frequency with psi^bitrev twiddles; output bit-reversed.
 __device__ __forceinline__ void ntt_forward_smem(u64* a, const RingDev& R, int j) {
   const int n = R.n;
@@ -115,11 +245,11 @@ __global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_bas
   const long long b = blockIdx.x;
   const int j = prime_base + int((b / prime_block) % prime_mod);
   u64* plane = data + b * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[i] = plane[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[sp(i)] = plane[i];
   __syncthreads();
-  if (inverse) ntt_inverse_smem(s_plane, R, j);
-  else ntt_forward_smem(s_plane, R, j);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[i];
+  if (inverse) ntt_inverse_fast(s_plane, R, j);
+  else ntt_forward_fast(s_plane, R, j);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[sp(i)];
 }
 
 // ---- wire unpacking ---------------------------------------------------------
@@ -487,39 +617,57 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
   const int j = blockIdx.y;
   const int n = R.n, L = R.residue, W = R.words;
   const Prime& m = R.prime[j];
-  // positions owned by this thread: threadIdx.x + k * kSwitchThreads < n
+  // Accumulators: kSwitchPer == 0 keeps them in shared memory after the
+  // padded plane (N <= 8192); otherwise in registers, kSwitchPer per thread.
+  constexpr bool kSmemAcc = kSwitchPer == 0;
+  constexpr int kRegs = kSmemAcc ? 1 : kSwitchPer;
+  u64* s_acc = s_plane + plane_smem_words(n);
   const int per = (n - int(threadIdx.x) + kSwitchThreads - 1) / kSwitchThreads;
-  u64 acc0[kSwitchPer], acc1[kSwitchPer];
+  u64 acc0[kRegs], acc1[kRegs];
 #pragma unroll
-  for (int k = 0; k < kSwitchPer; ++k) { acc0[k] = 0; acc1[k] = 0; }
+  for (int k = 0; k < kRegs; ++k) { acc0[k] = 0; acc1[k] = 0; }
+  if (kSmemAcc)
+    for (int i = threadIdx.x; i < 2 * n; i += kSwitchThreads) s_acc[i] = 0;
   for (int d = 0; d < R.digits; ++d) {
     for (int i = threadIdx.x; i < n; i += kSwitchThreads)
-      s_plane[i] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
+      s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
     __syncthreads();
-    ntt_forward_smem(s_plane, R, j);
+    ntt_forward_fast(s_plane, R, j);
     const u64* k0 = op.key + ((long long)(d * 2 + 0) * L + j) * n;
     const u64* k1 = op.key + ((long long)(d * 2 + 1) * L + j) * n;
+    if (kSmemAcc) {
+      for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
+        const u64 v = s_plane[sp(i)];
+        s_acc[i] = addmod(s_acc[i], reduce128(u128(v) * __ldg(k0 + i), m), m.p);
+        s_acc[n + i] = addmod(s_acc[n + i], reduce128(u128(v) * __ldg(k1 + i), m), m.p);
+      }
+    } else {
 #pragma unroll
-    for (int k = 0; k < kSwitchPer; ++k) {
-      if (k < per) {
-        const int i = threadIdx.x + k * kSwitchThreads;
-        const u64 v = s_plane[i];
-        acc0[k] = addmod(acc0[k], reduce128(u128(v) * __ldg(k0 + i), m), m.p);
-        acc1[k] = addmod(acc1[k], reduce128(u128(v) * __ldg(k1 + i), m), m.p);
+      for (int k = 0; k < kRegs; ++k) {
+        if (k < per) {
+          const int i = threadIdx.x + k * kSwitchThreads;
+          const u64 v = s_plane[sp(i)];
+          acc0[k] = addmod(acc0[k], reduce128(u128(v) * __ldg(k0 + i), m), m.p);
+          acc1[k] = addmod(acc1[k], reduce128(u128(v) * __ldg(k1 + i), m), m.p);
+        }
       }
     }
     __syncthreads();
   }
   for (int comp = 0; comp < 2; ++comp) {
+    if (kSmemAcc) {
+      for (int i = threadIdx.x; i < n; i += kSwitchThreads) s_plane[sp(i)] = s_acc[comp * n + i];
+    } else {
 #pragma unroll
-    for (int k = 0; k < kSwitchPer; ++k)
-      if (k < per) s_plane[threadIdx.x + k * kSwitchThreads] = comp ? acc1[k] : acc0[k];
+      for (int k = 0; k < kRegs; ++k)
+        if (k < per) s_plane[sp(threadIdx.x + k * kSwitchThreads)] = comp ? acc1[k] : acc0[k];
+    }
     __syncthreads();
-    ntt_inverse_smem(s_plane, R, j);
+    ntt_inverse_fast(s_plane, R, j);
     u64* out = op.out + ((long long)comp * L + j) * n;
     const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
     for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
-      u64 v = s_plane[i];
+      u64 v = s_plane[sp(i)];
       if (base) v = addmod(v, base[i], m.p);
       if (comp == 0 && op.x0) {
         const unsigned s = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));

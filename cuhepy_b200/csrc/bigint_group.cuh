@@ -181,14 +181,10 @@ struct Group {
     for (int j = 0; j < L; ++j) r[j] = ge ? d[j] : acc[j];
   }
 
-  // r = a * b * 2^(-32K) mod N.  a: registers (< N), b: shared memory (< N).
-  __device__ __forceinline__ void mont_mul(uint32_t (&r)[L], const uint32_t (&a)[L],
-                                           const uint32_t* __restrict__ b, const uint32_t (&n)[L],
-                                           uint32_t ninv) const {
-    uint32_t acc[L];
-#pragma unroll
-    for (int j = 0; j < L; ++j) acc[j] = 0u;
-    uint32_t c0 = 0u, c1 = 0u;
+  // The K CIOS word steps of one Montgomery product, b read from shared memory.
+  __device__ __forceinline__ void cios(uint32_t (&acc)[L], uint32_t& c0, uint32_t& c1, const uint32_t (&a)[L],
+                                       const uint32_t* __restrict__ b, const uint32_t (&n)[L],
+                                       uint32_t ninv) const {
 #pragma unroll 1
     for (int base = 0; base < K; base += L) {
 #pragma unroll
@@ -200,6 +196,31 @@ struct Group {
         step(acc, c0, c1, a, n, bw.w, ninv);
       }
     }
+  }
+
+  // r = a * b * 2^(-32K) mod N.  a: registers (< N), b: shared memory (< N).
+  __device__ __forceinline__ void mont_mul(uint32_t (&r)[L], const uint32_t (&a)[L],
+                                           const uint32_t* __restrict__ b, const uint32_t (&n)[L],
+                                           uint32_t ninv) const {
+    uint32_t acc[L];
+#pragma unroll
+    for (int j = 0; j < L; ++j) acc[j] = 0u;
+    uint32_t c0 = 0u, c1 = 0u;
+    cios(acc, c0, c1, a, b, n, ninv);
+    finalize(r, acc, c0, n);
+  }
+
+  // r = (init + a * b) * 2^(-32K) mod N with the accumulator started at
+  // init.  Valid for init < 2^(32K), a < 2^(32K), b < N: the CIOS value stays
+  // below 2N, which finalize reduces.
+  __device__ __forceinline__ void mont_mul_acc(uint32_t (&r)[L], const uint32_t (&init)[L],
+                                               const uint32_t (&a)[L], const uint32_t* __restrict__ b,
+                                               const uint32_t (&n)[L], uint32_t ninv) const {
+    uint32_t acc[L];
+#pragma unroll
+    for (int j = 0; j < L; ++j) acc[j] = init[j];
+    uint32_t c0 = 0u, c1 = 0u;
+    cios(acc, c0, c1, a, b, n, ninv);
     finalize(r, acc, c0, n);
   }
 

@@ -244,7 +244,7 @@ void words_to_bytes(const cuhe_bfv_ring* r, const std::vector<u64>& words, size_
 
 unsigned blocks_for(long long items, int threads) { return unsigned((items + threads - 1) / threads); }
 
-size_t ntt_smem(const cuhe_bfv_ring* r) { return r->plan.n * sizeof(u64); }
+size_t ntt_smem(const cuhe_bfv_ring* r) { return plane_smem_words(int(r->plan.n)) * sizeof(u64); }
 
 cudaError_t launch_ntt(cuhe_bfv_ring* r, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
                        int prime_block, int inverse) {
@@ -252,7 +252,7 @@ cudaError_t launch_ntt(cuhe_bfv_ring* r, RingDev* d, u64* data, long long planes
   const size_t smem = ntt_smem(r);
   cudaError_t e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  const int threads = r->plan.n >= 2048 ? 1024 : int(std::max<size_t>(32, r->plan.n / 2));
+  const int threads = int(std::min<size_t>(1024, std::max<size_t>(32, r->plan.n / 16)));
   k_ntt<<<unsigned(planes), threads, smem, r->stream>>>(data, d, prime_base, prime_mod, prime_block, inverse);
   return cudaGetLastError();
 }
@@ -274,8 +274,10 @@ int run_switch(cuhe_bfv_ring* r, RingDev* d, const std::vector<ComposeOp>& cops,
     const size_t smem = ntt_smem(r);
     dim3 grid(unsigned(sops.size()), unsigned(P.residue_count));
     if (P.n <= 8192) {
-      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
-      k_keyswitch<16><<<grid, kSwitchThreads, smem, r->stream>>>(d_sops, d);
+      const size_t smem_acc = smem + 2 * P.n * sizeof(u64);  // accumulators after the plane
+      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_acc)),
+               "smem");
+      k_keyswitch<0><<<grid, kSwitchThreads, smem_acc, r->stream>>>(d_sops, d);
     } else {
       BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
       k_keyswitch<32><<<grid, kSwitchThreads, smem, r->stream>>>(d_sops, d);

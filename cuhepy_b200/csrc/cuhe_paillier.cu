@@ -30,13 +30,17 @@ struct Variant {
 
 // (K, TPI, W) combinations compiled into the library.
 #define CUHE_VARIANTS(X) \
+  X(64, 8, 3)            \
   X(64, 8, 4)            \
   X(64, 16, 4)           \
   X(128, 8, 4)           \
+  X(128, 16, 3)          \
   X(128, 16, 4)          \
   X(128, 16, 5)          \
+  X(128, 32, 3)          \
   X(128, 32, 4)          \
   X(256, 16, 4)          \
+  X(256, 32, 3)          \
   X(256, 32, 4)          \
   X(256, 32, 5)
 
@@ -89,6 +93,9 @@ struct cuhe_paillier {
   int nops_n = 0;
   int32_t* d_ops_sec = nullptr;
   int nops_sec = 0;
+  uint32_t* d_crt = nullptr;  // CRT constant block, present once the factors are installed
+  cuhe::CrtScalars cs{};
+  bool have_factors = false;
   uint32_t* d_gtab = nullptr;
   int message_chunks = 0;
   uint32_t* d_noise = nullptr;
@@ -136,6 +143,28 @@ cudaError_t launch_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32
   const long long blocks = (count + IPB - 1) / IPB;
   cuhe::k_modexp<K, TPI, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
       base, aux, K, out, count, ctx->d_consts, ctx->ks, ops, nops, mode, pop_words, ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int KH, int TPI, int W>
+size_t modexp_crt_smem() {
+  constexpr int IPB = cuhe::kBlockThreads / (2 * TPI);
+  return size_t(7 * 2 * KH + IPB * 2 * (((1 << (W - 1)) + 1) * KH + 4)) * 4;
+}
+
+// CRT decrypt / decode: KH = K/2 words per side, TPI lanes per side.
+template <int KH, int TPI, int W>
+cudaError_t launch_modexp_crt(cuhe_paillier* ctx, const uint32_t* base, uint32_t* out, long long count,
+                              int mode, int pop_words) {
+  constexpr int IPB = cuhe::kBlockThreads / (2 * TPI);
+  const size_t smem = modexp_crt_smem<KH, TPI, W>();
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp_crt<KH, TPI, W>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_modexp_crt<KH, TPI, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      base, out, count, ctx->d_consts, ctx->ks, ctx->d_crt, ctx->cs, ctx->d_ops_sec, ctx->nops_sec, mode,
+      pop_words, ctx->d_status);
   return cudaGetLastError();
 }
 
@@ -224,6 +253,7 @@ struct Dispatch {
   cudaError_t (*modexp)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long, const int32_t*,
                         int, int, int) = nullptr;
   cudaError_t (*modexp_var)(cuhe_paillier*, const uint32_t*, const uint32_t*, int, int, uint32_t*, long long) = nullptr;
+  cudaError_t (*modexp_crt)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int, int) = nullptr;
   cudaError_t (*mulmod)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long) = nullptr;
   cudaError_t (*convert)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int) = nullptr;
   cudaError_t (*outer)(cuhe_paillier*, const uint32_t*, long long, const uint32_t*, long long, uint32_t*) = nullptr;
@@ -237,6 +267,7 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
   if (K == k && TPI == t && W == w) {                              \
     d->modexp = &launch_modexp<k, t, w>;                           \
     d->modexp_var = &launch_modexp_var<k, t>;                      \
+    d->modexp_crt = &launch_modexp_crt<k / 2, t / 2, w>;           \
     d->mulmod = &launch_mulmod<k, t>;                              \
     d->convert = &launch_convert<k, t>;                            \
     d->outer = &launch_outer<k, t>;                                \
@@ -247,6 +278,14 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
   CUHE_VARIANTS(CUHE_MATCH)
 #undef CUHE_MATCH
   return false;
+}
+
+// Exponentiation by the secret exponent (decrypt / decode): the CRT kernel
+// when the factorisation is installed, else the direct kernel mod n^2.
+cudaError_t secret_modexp(cuhe_paillier* ctx, const Dispatch& d, const uint32_t* base, uint32_t* out,
+                          long long count, int mode, int pop_words) {
+  if (ctx->have_factors) return d.modexp_crt(ctx, base, out, count, mode, pop_words);
+  return d.modexp(ctx, base, nullptr, out, count, ctx->d_ops_sec, ctx->nops_sec, mode, pop_words);
 }
 
 void default_tuning(int K, int* tpi, int* w) {
@@ -475,6 +514,7 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_status);
   cudaFree(ctx->d_ops_n);
   cudaFree(ctx->d_ops_sec);
+  cudaFree(ctx->d_crt);
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_noise);
   ctx->work.release();
@@ -548,6 +588,8 @@ int cuhe_paillier_set_secret(cuhe_paillier* ctx, const uint32_t* exponent, int e
     while (cuhe::host::cmp(mult, ctx->n) >= 0) cuhe::host::sub_in_place(mult, ctx->n);
   }
   Limbs multr = cuhe::host::shift_mod(mult, 32 * k, ctx->n);
+  // kernels already queued may still read the previous secret
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "synchronize before secret upload");
   CUHE_CUDA(ctx, cudaMemcpy(ctx->d_consts + size_t(cuhe::C_MULTR) * k, multr.data(), 4 * k, cudaMemcpyHostToDevice),
             "secret upload");
   ctx->ks.mult_is_zero = cuhe::host::is_zero(mult) ? 1u : 0u;
@@ -555,6 +597,56 @@ int cuhe_paillier_set_secret(cuhe_paillier* ctx, const uint32_t* exponent, int e
   ctx->have_secret = true;
   return upload_schedule(ctx, e, &ctx->d_ops_sec, &ctx->nops_sec);
 }
+
+int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p_in, int p_words, const uint32_t* q_in,
+                              int q_words) {
+  if (!ctx) return CUHE_INVALID_ARGUMENT;
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  if (!p_in && !q_in) {
+    ctx->have_factors = false;
+    return CUHE_OK;
+  }
+  if (!p_in || !q_in || p_words <= 0 || q_words <= 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "null factor");
+  const size_t k = size_t(ctx->K), kh = k / 2;
+  if (!cuhe::host::fits(p_in, size_t(p_words), k) || !cuhe::host::fits(q_in, size_t(q_words), k))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "factor wider than n");
+  Limbs p = cuhe::host::resized(p_in, size_t(p_words), k), q = cuhe::host::resized(q_in, size_t(q_words), k);
+  Limbs n2k = cuhe::host::resized(ctx->n.data(), ctx->n.size(), 2 * k);
+  if (cuhe::host::cmp(cuhe::host::mul(p, q, 2 * k), n2k) != 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "p * q != n");
+  if (!(p[0] & 1u) || !(q[0] & 1u) || cuhe::host::bit_length(p) < 2 || cuhe::host::bit_length(q) < 2)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "factors must be odd and greater than 1");
+  if (cuhe::host::bit_length(p) > 16 * kh || cuhe::host::bit_length(q) > 16 * kh)
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "unbalanced factors: p^2 or q^2 wider than half of n^2");
+  Limbs one(kh, 0u);
+  one[0] = 1u;
+  Limbs side[2] = {cuhe::host::mul(p, p, kh), cuhe::host::mul(q, q, kh)};  // p^2, q^2
+  Limbs qinv;
+  if (!cuhe::host::mod_inverse_odd(cuhe::host::mod_reduce(side[1], side[0]), side[0], &qinv))
+    return fail(ctx, CUHE_INVALID_ARGUMENT, "factors are not coprime");
+  std::vector<uint32_t> block(size_t(cuhe::CR_ROWS) * k, 0u);
+  auto put_half = [&](int row, int s, const Limbs& v) {
+    std::memcpy(block.data() + size_t(row) * k + size_t(s) * kh, v.data(), 4 * kh);
+  };
+  for (int s = 0; s < 2; ++s) {
+    Limbs rm = cuhe::host::shift_mod(one, 32 * kh, side[s]);
+    put_half(cuhe::CR_M, s, side[s]);
+    put_half(cuhe::CR_RM, s, rm);
+    put_half(cuhe::CR_R3, s, cuhe::host::shift_mod(rm, 64 * kh, side[s]));
+    ctx->cs.ninv[s] = 0u - cuhe::host::inv32(side[s][0]);
+  }
+  put_half(cuhe::CR_H, 0, cuhe::host::shift_mod(qinv, 32 * kh, side[0]));
+  Limbs cq = cuhe::host::shift_mod(cuhe::host::resized(side[1].data(), kh, k), 32 * k, ctx->n2);
+  std::memcpy(block.data() + size_t(cuhe::CR_CQ) * k, cq.data(), 4 * k);
+  // kernels already queued may still read the previous constants
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "synchronize before CRT constants upload");
+  if (!ctx->d_crt) CUHE_CUDA(ctx, cudaMalloc(&ctx->d_crt, block.size() * 4), "CRT constants allocation");
+  CUHE_CUDA(ctx, cudaMemcpy(ctx->d_crt, block.data(), block.size() * 4, cudaMemcpyHostToDevice), "CRT constants upload");
+  ctx->have_factors = true;
+  return CUHE_OK;
+}
+
+int cuhe_paillier_has_factors(const cuhe_paillier* ctx) { return ctx && ctx->have_factors ? 1 : 0; }
 
 int cuhe_paillier_encrypt(cuhe_paillier* ctx, const uint32_t* m, const uint32_t* r, uint32_t* c, int64_t count) {
   if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
@@ -591,8 +683,7 @@ int cuhe_paillier_decrypt(cuhe_paillier* ctx, const uint32_t* c, uint32_t* m, in
   st.add(c, bytes, true, false);
   st.add(m, bytes, false, true);
   if (int rc = st.bind()) return rc;
-  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, (uint32_t*)st.dev(1), count, ctx->d_ops_sec,
-                          ctx->nops_sec, cuhe::EXP_DECRYPT, 0),
+  CUHE_CUDA(ctx, secret_modexp(ctx, d, (const uint32_t*)st.dev(0), (uint32_t*)st.dev(1), count, cuhe::EXP_DECRYPT, 0),
             "decrypt launch");
   if (int rc = st.finish()) return rc;
   return check_status(ctx, st.staged());
@@ -617,8 +708,7 @@ int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t 
   st.add(distance, size_t(vectors) * 8, false, true);
   if (int rc = st.bind()) return rc;
   uint32_t* d_counts = static_cast<uint32_t*>(st.dev(1));
-  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, d_counts, total, ctx->d_ops_sec, ctx->nops_sec,
-                          cuhe::EXP_DECODE, chunk_len / 32),
+  CUHE_CUDA(ctx, secret_modexp(ctx, d, (const uint32_t*)st.dev(0), d_counts, total, cuhe::EXP_DECODE, chunk_len / 32),
             "decode launch");
   cuhe::k_sum_chunks<<<unsigned((vectors + 255) / 256), 256, 0, ctx->stream>>>(
       d_counts, vectors, chunk_num, reinterpret_cast<long long*>(st.dev(2)));
@@ -674,9 +764,7 @@ int cuhe_paillier_decode_hamming_static(cuhe_paillier* ctx, const uint32_t* c, i
   Dispatch d;
   find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
   const int64_t total = vectors * chunk_num;
-  CUHE_CUDA(ctx, d.modexp(ctx, c, nullptr, counts, total, ctx->d_ops_sec, ctx->nops_sec, cuhe::EXP_DECODE,
-                          chunk_len / 32),
-            "static decode launch");
+  CUHE_CUDA(ctx, secret_modexp(ctx, d, c, counts, total, cuhe::EXP_DECODE, chunk_len / 32), "static decode launch");
   cuhe::k_sum_chunks<<<unsigned((vectors + 255) / 256), 256, 0, ctx->stream>>>(
       counts, vectors, chunk_num, reinterpret_cast<long long*>(distance));
   CUHE_CUDA(ctx, cudaGetLastError(), "static decode reduction");
@@ -697,21 +785,43 @@ int cuhe_imad_peak(int device, double* word_products_per_second) {
   if (e == cudaSuccess) e = cudaEventCreate(&a);
   if (e == cudaSuccess) e = cudaEventCreate(&b);
   const int iters = 4096, blocks = sms * 8, threads = 256;
-  float ms = 0.f;
+  float ms_pairs = 0.f, ms_chain = 0.f;
   if (e == cudaSuccess) {
     cuhe::k_imad_probe<<<blocks, threads>>>(sink, iters, 1u);  // warm-up
     cudaEventRecord(a);
     for (int r = 0; r < 5; ++r) cuhe::k_imad_probe<<<blocks, threads>>>(sink, iters, 2u + r);
     cudaEventRecord(b);
     e = cudaEventSynchronize(b);
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_pairs, a, b);
+  }
+  if (e == cudaSuccess) {
+    cuhe::k_imad_chain_probe<<<blocks, threads>>>(sink, iters, 1u);  // warm-up
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) cuhe::k_imad_chain_probe<<<blocks, threads>>>(sink, iters, 2u + r);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_chain, a, b);
+  }
+  float ms_wide = 0.f;
+  if (e == cudaSuccess) {
+    cuhe::k_imad_wide_probe<<<blocks, threads>>>(sink, iters, 1u);  // warm-up
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) cuhe::k_imad_wide_probe<<<blocks, threads>>>(sink, iters, 2u + r);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_wide, a, b);
   }
   if (a) cudaEventDestroy(a);
   if (b) cudaEventDestroy(b);
   cudaFree(sink);
   if (e != cudaSuccess) return cuda_fail(nullptr, e, "imad probe");
-  const double pairs = 5.0 * blocks * threads * double(iters) * 8.0;
-  *word_products_per_second = pairs / (double(ms) * 1e-3);
+  // word products per thread per iteration: 32 in the chain probe (4 rows of
+  // 8 limbs), 8 in the lo/hi and wide probes
+  const double products = 5.0 * blocks * threads * double(iters) * 32.0;
+  const double pairs_rate = products / 4.0 / (double(ms_pairs) * 1e-3);
+  const double chain_rate = products / (double(ms_chain) * 1e-3);
+  const double wide_rate = products / 4.0 / (double(ms_wide) * 1e-3);
+  *word_products_per_second = std::max(pairs_rate, std::max(chain_rate, wide_rate));
   return CUHE_OK;
 }
 

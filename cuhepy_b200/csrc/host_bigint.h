@@ -105,6 +105,63 @@ inline bool is_zero(const Limbs& x) {
   return true;
 }
 
+// x >>= 1 with `top` shifted into the most significant bit
+inline void shr1(Limbs& x, uint32_t top = 0u) {
+  for (size_t i = 0; i + 1 < x.size(); ++i) x[i] = (x[i] >> 1) | (x[i + 1] << 31);
+  x.back() = (x.back() >> 1) | (top << 31);
+}
+
+// x = x / 2 mod m for x < m, m odd (same limb count)
+inline void half_mod(Limbs& x, const Limbs& m) {
+  if (x[0] & 1u) {
+    const uint32_t carry = add_in_place(x, m);
+    shr1(x, carry);
+  } else {
+    shr1(x);
+  }
+}
+
+// x = x - y mod m for x, y < m
+inline void sub_mod(Limbs& x, const Limbs& y, const Limbs& m) {
+  if (sub_in_place(x, y)) add_in_place(x, m);
+}
+
+// x mod m (bitwise long division; m nonzero).  Result has m's limb count.
+inline Limbs mod_reduce(const Limbs& x, const Limbs& m) {
+  Limbs r(m.size(), 0u);
+  for (size_t i = bit_length(x); i-- > 0;) {
+    const uint32_t top = r.back() >> 31;
+    for (size_t k = r.size(); k-- > 1;) r[k] = (r[k] << 1) | (r[k - 1] >> 31);
+    r[0] = (r[0] << 1) | ((x[i / 32] >> (i % 32)) & 1u);
+    if (top || cmp(r, m) >= 0) sub_in_place(r, m);
+  }
+  return r;
+}
+
+// a^-1 mod m for odd m and 0 < a < m (binary extended Euclid).  Returns false
+// when gcd(a, m) != 1.  All values have m's limb count.
+inline bool mod_inverse_odd(const Limbs& a, const Limbs& m, Limbs* out) {
+  const size_t w = m.size();
+  Limbs one(w, 0u);
+  one[0] = 1u;
+  Limbs u = a, v = m, x1 = one, x2(w, 0u);
+  if (is_zero(u) || !(m[0] & 1u)) return false;
+  while (cmp(u, one) != 0 && cmp(v, one) != 0) {
+    if (is_zero(u) || is_zero(v)) return false;
+    while (!(u[0] & 1u)) { shr1(u); half_mod(x1, m); }
+    while (!(v[0] & 1u)) { shr1(v); half_mod(x2, m); }
+    if (cmp(u, v) >= 0) {
+      sub_in_place(u, v);
+      sub_mod(x1, x2, m);
+    } else {
+      sub_in_place(v, u);
+      sub_mod(x2, x1, m);
+    }
+  }
+  *out = cmp(u, one) == 0 ? x1 : x2;
+  return true;
+}
+
 // Left-to-right sliding-window schedule for a fixed exponent.  Each op is
 // (squarings << 16) | (odd-power table index + 1); the first op only loads
 // its table entry.  Table entry t holds base^(2t+1).

@@ -24,6 +24,21 @@ enum ConstRow : int {
   C_ROWS = 9
 };
 
+// Rows of the CRT constant block (each row K words).  Half rows hold the p^2
+// value in words [0, K/2) and the q^2 value in words [K/2, K); R_h = 2^(16K).
+enum CrtRow : int {
+  CR_M = 0,    // p^2 | q^2
+  CR_RM = 1,   // R_h mod p^2 | R_h mod q^2
+  CR_R3 = 2,   // R_h^3 mod p^2 | R_h^3 mod q^2
+  CR_H = 3,    // (q^2)^-1 R_h mod p^2 | 0
+  CR_CQ = 4,   // q^2 R mod n^2 (full row)
+  CR_ROWS = 5
+};
+
+struct CrtScalars {
+  uint32_t ninv[2];  // -(p^2)^-1, -(q^2)^-1 mod 2^32
+};
+
 struct KeyScalars {
   uint32_t ninv2;  // -(n^2)^-1 mod 2^32
   uint32_t ninv1;  // -n^-1 mod 2^32
@@ -92,6 +107,108 @@ __device__ __forceinline__ void sub_group(const Group<K, TPI>& g, uint32_t (&x)[
     for (int j = 1; j < L; ++j) x[j] = subc_cc(x[j], 0u);
     (void)subc(0u, 0u);
   }
+}
+
+// x += y over the group; returns the carry out of the top lane.
+template <int K, int TPI>
+__device__ __forceinline__ bool add_group(const Group<K, TPI>& g, uint32_t (&x)[K / TPI],
+                                          const uint32_t (&y)[K / TPI]) {
+  constexpr int L = K / TPI;
+  x[0] = add_cc(x[0], y[0]);
+#pragma unroll
+  for (int j = 1; j < L; ++j) x[j] = addc_cc(x[j], y[j]);
+  const uint32_t carry = addc(0u, 0u);
+  uint32_t ones = x[0];
+#pragma unroll
+  for (int j = 1; j < L; ++j) ones &= x[j];
+  bool out = false;
+  const bool cin = g.lookahead(carry != 0u, ones == 0xffffffffu, &out);
+  if (cin) {
+    x[0] = add_cc(x[0], 1u);
+#pragma unroll
+    for (int j = 1; j < L; ++j) x[j] = addc_cc(x[j], 0u);
+    (void)addc(0u, 0u);
+  }
+  return out;
+}
+
+// x = (x - y) mod m for x, y < m over the group.
+template <int K, int TPI>
+__device__ __forceinline__ void sub_mod(const Group<K, TPI>& g, uint32_t (&x)[K / TPI],
+                                        const uint32_t (&y)[K / TPI], const uint32_t (&m)[K / TPI]) {
+  constexpr int L = K / TPI;
+  x[0] = sub_cc(x[0], y[0]);
+#pragma unroll
+  for (int j = 1; j < L; ++j) x[j] = subc_cc(x[j], y[j]);
+  const uint32_t borrow = subc(0u, 0u) & 1u;
+  uint32_t zero = x[0];
+#pragma unroll
+  for (int j = 1; j < L; ++j) zero |= x[j];
+  bool under = false;  // x < y: the group-wide borrow (same value in every lane)
+  const bool bin = g.lookahead(borrow != 0u, zero == 0u, &under);
+  if (bin) {
+    x[0] = sub_cc(x[0], 1u);
+#pragma unroll
+    for (int j = 1; j < L; ++j) x[j] = subc_cc(x[j], 0u);
+    (void)subc(0u, 0u);
+  }
+  if (under) (void)add_group<K, TPI>(g, x, m);
+}
+
+// Epilogue shared by the decrypt / decode kernels.  x = base^e mod n^2
+// (canonical); writes floor((x - 1)/n) * mult mod n (EXP_DECRYPT) or the
+// popcount of its even bits over pop_words words (EXP_DECODE).  Block rows:
+// s_one = 1, s_r2n = R^2 mod n, s_multr = mult * R mod n.
+template <int K, int TPI>
+__device__ __forceinline__ void decrypt_epilogue(const Group<K, TPI>& g, uint32_t (&x)[K / TPI],
+                                                 uint32_t* __restrict__ out, long long inst,
+                                                 const uint32_t* __restrict__ consts, const KeyScalars& ks,
+                                                 const uint32_t* s_one, const uint32_t* s_r2n,
+                                                 const uint32_t* s_multr, int mode, int pop_words) {
+  constexpr int L = K / TPI;
+  uint32_t nn[L];
+  g.load_ro(nn, consts + C_N * K);
+  uint32_t res[L];
+  if (g.is_zero(x)) {
+    // floor(-1/n) = -1  ->  (-mult) mod n
+    uint32_t multr[L], mult[L];
+    g.load(multr, s_multr);
+    g.mont_mul(mult, multr, s_one, nn, ks.ninv1);
+#pragma unroll
+    for (int j = 0; j < L; ++j) res[j] = nn[j];
+    if (ks.mult_is_zero) {
+#pragma unroll
+      for (int j = 0; j < L; ++j) res[j] = 0u;
+    } else {
+      sub_group<K, TPI>(g, res, mult);
+    }
+  } else {
+    uint32_t one[L];
+#pragma unroll
+    for (int j = 0; j < L; ++j) one[j] = (g.gl == 0 && j == 0) ? 1u : 0u;
+    sub_group<K, TPI>(g, x, one);                 // y
+    uint32_t t1[L];
+    g.mont_mul(t1, x, s_one, nn, ks.ninv1);       // y R^-1 mod n
+    uint32_t rem[L];
+    g.mont_mul(rem, t1, s_r2n, nn, ks.ninv1);     // y mod n
+    sub_group<K, TPI>(g, x, rem);                 // y - (y mod n) = q*n
+    uint32_t q[L], mneg[L];
+    g.load_ro(mneg, consts + C_NNEG * K);
+    g.exact_div(q, x, mneg, ks.ndiv, K / 2);      // q = floor(y/n) < n
+    g.mont_mul(res, q, s_multr, nn, ks.ninv1);    // q * mult mod n
+  }
+  if (mode == EXP_DECRYPT) {
+    g.store(out + inst * K, res);
+    return;
+  }
+  // EXP_DECODE
+  int pc = 0;
+#pragma unroll
+  for (int j = 0; j < L; ++j)
+    if (g.gl * L + j < pop_words) pc += __popc(res[j] & 0x55555555u);
+#pragma unroll
+  for (int off = TPI / 2; off > 0; off >>= 1) pc += __shfl_xor_sync(g.mask, pc, off, TPI);
+  if (g.gl == 0) out[inst] = uint32_t(pc);
 }
 
 // ---------------------------------------------------------------------------
@@ -202,51 +319,144 @@ k_modexp(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, in
     g.store(out + inst * K, x);
     return;
   }
-  // decrypt / decode: y = base^e mod n^2 - 1
+  // decrypt / decode
   g.mont_mul(x, acc, s_one, n2, ks.ninv2);
-  uint32_t nn[L];
-  g.load_ro(nn, consts + C_N * K);
-  uint32_t res[L];
-  if (g.is_zero(x)) {
-    // floor(-1/n) = -1  ->  (-mult) mod n
-    uint32_t multr[L], mult[L];
-    g.load(multr, s_multr);
-    g.mont_mul(mult, multr, s_one, nn, ks.ninv1);
-#pragma unroll
-    for (int j = 0; j < L; ++j) res[j] = nn[j];
-    if (ks.mult_is_zero) {
-#pragma unroll
-      for (int j = 0; j < L; ++j) res[j] = 0u;
-    } else {
-      sub_group<K, TPI>(g, res, mult);
+  decrypt_epilogue<K, TPI>(g, x, out, inst, consts, ks, s_one, s_r2n, s_multr, mode, pop_words);
+}
+
+// ---------------------------------------------------------------------------
+// Decrypt / decode exponentiation by the Chinese remainder theorem, for keys
+// whose factorisation n = p q is known (EXP_DECRYPT / EXP_DECODE only).
+//
+// Each ciphertext is owned by 2*TPI consecutive lanes.  Its lower TPI lanes
+// (side 0) compute x_p = c^e mod p^2 and its upper TPI lanes (side 1)
+// x_q = c^e mod q^2, each a KH-word Montgomery exponentiation with
+// R_h = 2^(32 KH) on its own half of the lanes, so one modular product costs
+// a quarter of a K-word one.  Garner's recombination
+//   h = (x_p - x_q) (q^2)^-1 mod p^2,   x = x_q + q^2 h   (< n^2, exact)
+// runs on the two halves together as a K-word group, and the same epilogue
+// as k_modexp follows, so the result equals the direct c^e mod n^2 path for
+// every c < n^2.
+// ---------------------------------------------------------------------------
+template <int KH, int TPI, int W>
+__global__ void __launch_bounds__(kBlockThreads)
+k_modexp_crt(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, long long count,
+             const uint32_t* __restrict__ consts, KeyScalars ks, const uint32_t* __restrict__ crt, CrtScalars cs,
+             const int32_t* __restrict__ ops, int nops, int mode, int pop_words, int* status) {
+  constexpr int K = 2 * KH;
+  constexpr int L = KH / TPI;
+  constexpr int T = 1 << (W - 1);
+  constexpr int IPB = kBlockThreads / (2 * TPI);
+  constexpr int SIDE = (T + 1) * KH + 4;  // per side: x, then T odd powers; +4 words moves the banks
+  extern __shared__ __align__(16) uint32_t smem[];
+  // block rows: ONE, R2N, MULTR (K words each), RM, R3, H (two halves), CQ (K words)
+  uint32_t* s_one = smem;
+  uint32_t* s_r2n = smem + K;
+  uint32_t* s_multr = smem + 2 * K;
+  uint32_t* s_rm = smem + 3 * K;
+  uint32_t* s_r3 = smem + 4 * K;
+  uint32_t* s_h = smem + 5 * K;
+  uint32_t* s_cq = smem + 6 * K;
+  {
+    const int rows[3] = {C_ONE, C_R2N, C_MULTR};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 3);
+    const int crows[4] = {CR_RM, CR_R3, CR_H, CR_CQ};
+    copy_rows_to_smem<K, TPI>(smem + 3 * K, crt, crows, 4);
+  }
+  __syncthreads();
+
+  Group<K, 2 * TPI> g;   // the whole ciphertext
+  Group<KH, TPI> h;      // this side's half
+  const int side = (threadIdx.x / TPI) & 1;
+  const int slot = threadIdx.x / (2 * TPI);
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;  // both halves leave together
+  uint32_t* s_item = smem + 7 * K + slot * 2 * SIDE;
+  uint32_t* s_x = s_item + side * SIDE;
+  uint32_t* s_tab = s_x + KH;
+
+  {
+    uint32_t c[L], n2[L];
+    g.load_ro(n2, consts + C_N2 * K);
+    g.load(c, base + inst * K);
+    if (!g.less_than(c, n2)) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
     }
+  }
+  const uint32_t ninv = cs.ninv[side];
+  uint32_t m[L], lo[L], hi[L], acc[L];
+  h.load_ro(m, crt + CR_M * K + side * KH);
+  h.load(lo, base + inst * K);
+  h.load(hi, base + inst * K + KH);
+  // c = lo + hi R_h:  (lo + hi * (R_h mod M)) R_h^-1 = c R_h^-1, then * R_h^3 R_h^-1
+  h.mont_mul_acc(acc, lo, hi, s_rm + side * KH, m, ninv);
+  h.mont_mul(acc, acc, s_r3 + side * KH, m, ninv);  // c R_h mod M (Montgomery form)
+  h.publish(s_tab, acc);
+  if (T > 1) {
+    uint32_t sq[L];
+    h.mont_mul(sq, acc, s_tab, m, ninv);
+    h.publish(s_x, sq);
+#pragma unroll 1
+    for (int t = 1; t < T; ++t) {
+      h.mont_mul(acc, acc, s_x, m, ninv);
+      h.publish(s_tab + t * KH, acc);
+    }
+  }
+  if (nops == 0) {
+    h.load(acc, s_rm + side * KH);  // e = 0: Montgomery form of 1
   } else {
-    uint32_t one[L];
-#pragma unroll
-    for (int j = 0; j < L; ++j) one[j] = (g.gl == 0 && j == 0) ? 1u : 0u;
-    sub_group<K, TPI>(g, x, one);                 // y
-    uint32_t t1[L];
-    g.mont_mul(t1, x, s_one, nn, ks.ninv1);       // y R^-1 mod n
-    uint32_t rem[L];
-    g.mont_mul(rem, t1, s_r2n, nn, ks.ninv1);     // y mod n
-    sub_group<K, TPI>(g, x, rem);                 // y - (y mod n) = q*n
-    uint32_t q[L], mneg[L];
-    g.load_ro(mneg, consts + C_NNEG * K);
-    g.exact_div(q, x, mneg, ks.ndiv, K / 2);      // q = floor(y/n) < n
-    g.mont_mul(res, q, s_multr, nn, ks.ninv1);    // q * mult mod n
+    const int first = __ldg(ops) & 0xffff;
+    h.load(acc, s_tab + (first - 1) * KH);
   }
-  if (mode == EXP_DECRYPT) {
-    g.store(out + inst * K, res);
-    return;
+  h.publish(s_x, acc);
+#pragma unroll 1
+  for (int o = 1; o < nops; ++o) {
+    const int op = __ldg(ops + o);
+    const int sq = op >> 16;
+    const int idx = op & 0xffff;
+#pragma unroll 1
+    for (int s = 0; s < sq; ++s) {
+      h.mont_mul(acc, acc, s_x, m, ninv);
+      h.publish(s_x, acc);
+    }
+    if (idx) {
+      h.mont_mul(acc, acc, s_tab + (idx - 1) * KH, m, ninv);
+      h.publish(s_x, acc);
+    }
   }
-  // EXP_DECODE
-  int pc = 0;
+  uint32_t xs[L];
+  h.mont_mul(xs, acc, s_one, m, ninv);  // x_side, canonical
+  __syncwarp(g.mask);
+  h.store(s_x, xs);
+  __syncwarp(g.mask);
+  uint32_t* s_xp = s_item;
+  uint32_t* s_xq = s_item + SIDE;
+  if (side == 0) {
+    // h = x_p (q^2)^-1 - x_q (q^2)^-1 mod p^2   (x_q may exceed p^2; x_q < R_h)
+    uint32_t xq[L], v[L], u[L];
+    h.load(xq, s_xq);
+    h.mont_mul(v, xs, s_h, m, ninv);
+    h.mont_mul(u, xq, s_h, m, ninv);
+    sub_mod<KH, TPI>(h, v, u, m);
+    __syncwarp(h.mask);
+    h.store(s_xp, v);
+  }
+  __syncwarp(g.mask);
+  // x = x_q + q^2 h over the whole group: side 0 lanes hold the low words
+  uint32_t hv[L], xq[L], x[L];
+  if (side == 0) {
+    h.load(hv, s_xp);
+    h.load(xq, s_xq);
+  } else {
 #pragma unroll
-  for (int j = 0; j < L; ++j)
-    if (g.gl * L + j < pop_words) pc += __popc(res[j] & 0x55555555u);
-#pragma unroll
-  for (int off = TPI / 2; off > 0; off >>= 1) pc += __shfl_xor_sync(g.mask, pc, off, TPI);
-  if (g.gl == 0) out[inst] = uint32_t(pc);
+    for (int j = 0; j < L; ++j) hv[j] = xq[j] = 0u;
+  }
+  uint32_t n2[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.mont_mul(x, hv, s_cq, n2, ks.ninv2);  // h q^2 mod n^2 = h q^2
+  (void)add_group<K, 2 * TPI>(g, x, xq);
+  decrypt_epilogue<K, 2 * TPI>(g, x, out, inst, consts, ks, s_one, s_r2n, s_multr, mode, pop_words);
 }
 
 // ---------------------------------------------------------------------------
@@ -329,11 +539,62 @@ __global__ void k_sum_chunks(const uint32_t* __restrict__ counts, long long vect
   distance[v] = s;
 }
 
+// Integer multiply-add throughput probe in the Montgomery kernels' own
+// instruction mix: four independent 8-limb accumulators, each updated per
+// iteration by one mad.lo.cc/madc.hi.cc row (8 word products, the shape of
+// Group::mac_row) with no shuffles or memory traffic, so the probe is bound
+// only by the integer multiply pipe.  Each row is 8 word products.
+__global__ void __launch_bounds__(256) k_imad_chain_probe(uint32_t* sink, int iters, uint32_t seed) {
+  uint32_t acc[4][8], c0[4], c1[4], a[8];
+  const uint32_t b = seed * 2654435761u + blockIdx.x;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = (seed ^ threadIdx.x) * (j + 3u) + 0x9e3779b9u;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    c0[s] = c1[s] = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[s][j] = a[j] ^ s;
+  }
+#pragma unroll 1
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) Group<128, 16>::mac_row(acc[s], c0[s], c1[s], a, b + s);
+  }
+  uint32_t folded = 0;
+#pragma unroll
+  for (int s = 0; s < 4; ++s) {
+    folded ^= c0[s] ^ c1[s];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) folded ^= acc[s][j];
+  }
+  if (folded == 0x12345678u) sink[0] = folded;
+}
+
+// Integer multiply-add throughput probe in 64-bit form: every iteration
+// issues one mad.wide.u32 (a full 32x32->64 word product added to a 64-bit
+// accumulator) on each of eight independent accumulators.
+__global__ void __launch_bounds__(256) k_imad_wide_probe(uint32_t* sink, int iters, uint32_t seed) {
+  unsigned long long acc[8];
+  const uint32_t b = seed * 2654435761u + blockIdx.x;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) acc[j] = ((unsigned long long)(seed ^ threadIdx.x) << 7) + 977u * j + 1u;
+#pragma unroll 1
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint32_t lo = uint32_t(acc[j]);
+      asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc[j]) : "r"(lo), "r"(b));
+    }
+  }
+  unsigned long long folded = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) folded ^= acc[j];
+  if (folded == 0x9e3779b97f4a7c15ull) sink[0] = uint32_t(folded);
+}
+
 // Integer multiply-add throughput probe: every iteration issues one
 // mad.lo.u32 and one mad.hi.u32 (one 32x32->64 word product) per operand
-// pair into 16 accumulators that depend only on themselves, so the probe is
-// bound by issue/pipe throughput, not latency.  Used to state the IMAD
-// roofline of the chip.
+// pair into 16 accumulators that depend only on themselves.
 __global__ void __launch_bounds__(256) k_imad_probe(uint32_t* sink, int iters, uint32_t seed) {
   uint32_t lo[8], hi[8], x[8];
   const uint32_t a = seed ^ threadIdx.x, b = seed * 2654435761u + blockIdx.x;

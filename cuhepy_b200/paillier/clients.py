@@ -90,7 +90,8 @@ class PaillierGPULookupClient:
 
     def _ctx(self):
         keys = self._need_keys("device")
-        return device_for(int(keys["pk"]["n"]), (int(keys["sk"]["a"]), int(keys["sk"]["g_a_inv"])))
+        return device_for(int(keys["pk"]["n"]), (int(keys["sk"]["a"]), int(keys["sk"]["g_a_inv"])),
+                          phi=keys["sk"].get("phi"))
 
     def _install_tables(self) -> None:
         keys = self._need_keys("tables")
@@ -143,7 +144,7 @@ class PaillierGPULookupClient:
         """paillier_GPU_lookup_client.cu:2134-2286: decrypt under key_a, re-encrypt under key_b."""
         pk_a, sk_a = key_a.get("pk", key_a), key_a.get("sk", key_a)
         pk_b = key_b.get("pk", key_b)
-        plain = device_for(int(pk_a["n"]), (int(sk_a["a"]), int(sk_a["g_a_inv"]))).decrypt(
+        plain = device_for(int(pk_a["n"]), (int(sk_a["a"]), int(sk_a["g_a_inv"])), phi=sk_a.get("phi")).decrypt(
             [_as_int(c) for c in ciphers])
         n_b = int(pk_b["n"])
         chunks = int(key_b.get("message_chunks") or message_chunks_for((n_b.bit_length() + 1) // 2))
@@ -322,7 +323,8 @@ class PaillierGPUClient:
             if len(row) != self._chunk_num:
                 raise RuntimeError("decode_hamming_client: each inner list must have length == chunk_num")
             rows.append([int(str(c), 16) for c in row])
-        ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["phi"]), int(keys["sk"]["inv"])))
+        ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["phi"]), int(keys["sk"]["inv"])),
+                         phi=keys["sk"]["phi"])
         return ctx.decode_hamming(rows, self._chunk_num, self._chunk_len)
 
     def get_pk_hex(self) -> tuple[str, str]:

@@ -20,6 +20,7 @@ import numpy as np
 
 from cuhepy_b200 import _native
 from cuhepy_b200._limbs import from_limbs, to_limbs, words_for
+from cuhepy_b200._numbers import factors_from_phi
 
 NOISE_MULTIPLES = 14
 
@@ -87,6 +88,21 @@ class PaillierDevice:
             self._ctx, e.ctypes.data_as(_native.c_u32_p), e.size, m.ctypes.data_as(_native.c_u32_p), m.size))
         self.secret = (int(exponent), int(multiplier))
 
+    def set_factors(self, p: int | None, q: int | None) -> None:
+        """Install n = p q so that decrypt / decode run by the CRT (same
+        results, half-width exponentiations); None, None removes them."""
+        if p is None and q is None:
+            self._check(self._lib.cuhe_paillier_set_factors(self._ctx, None, 0, None, 0))
+            return
+        pl = to_limbs([int(p)], words_for(int(p)))[0]
+        ql = to_limbs([int(q)], words_for(int(q)))[0]
+        self._check(self._lib.cuhe_paillier_set_factors(
+            self._ctx, pl.ctypes.data_as(_native.c_u32_p), pl.size, ql.ctypes.data_as(_native.c_u32_p), ql.size))
+
+    @property
+    def has_factors(self) -> bool:
+        return bool(self._lib.cuhe_paillier_has_factors(self._ctx))
+
     def set_stream(self, stream: int | None) -> None:
         self._check(self._lib.cuhe_paillier_set_stream(self._ctx, ctypes.c_void_p(stream or 0)))
 
@@ -95,6 +111,51 @@ class PaillierDevice:
 
     def set_tuning(self, threads_per_instance: int = 0, window: int = 0) -> None:
         self._check(self._lib.cuhe_paillier_set_tuning(self._ctx, int(threads_per_instance), int(window)))
+
+    VARIANTS = {64: [(8, 3), (8, 4), (16, 4)],
+                128: [(8, 4), (16, 3), (16, 4), (16, 5), (32, 3), (32, 4)],
+                256: [(16, 4), (32, 3), (32, 4), (32, 5)]}
+
+    def autotune(self, exponent_bits: int = 0, count: int = 0, reps: int = 2) -> dict:
+        """Time every compiled (threads per instance, window) variant on a
+        fixed-exponent batch of this context's width and keep the fastest.
+
+        The measurement uses a device-resident batch (one resident wave of
+        groups per SM at least) and CUDA events on a private stream; returns
+        the timings so callers can record the choice."""
+        import torch
+
+        rng = np.random.default_rng(5)
+        count = count or 148 * (128 // 8) * 4
+        bits = exponent_bits or max(2, self.n.bit_length())
+        exponent = int(rng.integers(1, 1 << 62)) | (1 << 62)
+        while exponent.bit_length() < bits:
+            exponent = (exponent << 62) | int(rng.integers(0, 1 << 62))
+        exponent >>= max(0, exponent.bit_length() - bits)
+        raw = rng.integers(0, 1 << 32, size=(count, self.words), dtype=np.uint64).astype(np.uint32)
+        raw[:, -1] = 0  # below n^2
+        base = torch.from_numpy(raw.view(np.int32)).cuda(self.device)
+        out = torch.empty_like(base)
+        stream = torch.cuda.Stream(self.device)
+        self.set_stream(stream.cuda_stream)
+        timings = {}
+        try:
+            for tpi, window in self.VARIANTS[self.words]:
+                self.set_tuning(tpi, window)
+                with torch.cuda.stream(stream):
+                    self.modexp_array(base, exponent, out, count)
+                    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    start.record(stream)
+                    for _ in range(reps):
+                        self.modexp_array(base, exponent, out, count)
+                    end.record(stream)
+                end.synchronize()
+                timings[(tpi, window)] = start.elapsed_time(end) / reps
+        finally:
+            self.set_stream(None)
+        best = min(timings, key=timings.get)
+        self.set_tuning(*best)
+        return {"best": best, "ms": {f"{t}x{w}": v for (t, w), v in timings.items()}}
 
     def tuning(self) -> tuple[int, int]:
         tpi, w = ctypes.c_int(), ctypes.c_int()
@@ -288,9 +349,12 @@ _cache_lock = threading.Lock()
 _CACHE_MAX = 8
 
 
-def device_for(n: int, secret: tuple[int, int] | None = None, device: int = 0) -> PaillierDevice:
-    """Cached context for modulus n (and secret, when given)."""
-    key = (int(n), secret, int(device))
+def device_for(n: int, secret: tuple[int, int] | None = None, device: int = 0,
+               phi: int | None = None) -> PaillierDevice:
+    """Cached context for modulus n (and secret, when given).  With phi, the
+    factors of n are recovered and installed, so decrypt / decode use the CRT
+    kernel (identical results)."""
+    key = (int(n), secret, int(device), None if phi is None else int(phi))
     with _cache_lock:
         ctx = _cache.get(key)
         if ctx is not None:
@@ -299,6 +363,13 @@ def device_for(n: int, secret: tuple[int, int] | None = None, device: int = 0) -
     ctx = PaillierDevice(n, device)
     if secret is not None:
         ctx.set_secret(*secret)
+    if phi is not None:
+        factors = factors_from_phi(int(n), int(phi))
+        if factors is not None:
+            try:
+                ctx.set_factors(*factors)
+            except ValueError:
+                pass  # unbalanced factors: the direct kernel serves this key
     with _cache_lock:
         _cache[key] = ctx
         while len(_cache) > _CACHE_MAX:

@@ -195,7 +195,8 @@ class PaillierLookup:
         for c in ciphertexts:
             if not 0 <= int(c) < n2:
                 raise ValueError("ciphertext must be in range [0, n^2)")
-        ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["a"]), int(keys["sk"]["g_a_inv"])))
+        ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["a"]), int(keys["sk"]["g_a_inv"])),
+                         phi=keys["sk"].get("phi"))
         return ctx.decrypt([int(c) for c in ciphertexts])
 
     @staticmethod

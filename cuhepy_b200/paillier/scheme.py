@@ -79,7 +79,8 @@ class Paillier:
         for c in ciphertexts:
             if not 0 <= int(c) < n2:
                 raise ValueError("ciphertext must be in range [0, n^2)")
-        ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["phi"]), int(keys["sk"]["inv"])))
+        ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["phi"]), int(keys["sk"]["inv"])),
+                         phi=keys["sk"]["phi"])
         return ctx.decrypt([int(c) for c in ciphertexts])
 
     @staticmethod

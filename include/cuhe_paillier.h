@@ -65,6 +65,21 @@ int cuhe_synchronize(cuhe_paillier* ctx);
 int cuhe_paillier_set_secret(cuhe_paillier* ctx, const uint32_t* exponent, int exponent_words,
                              const uint32_t* multiplier, int multiplier_words);
 
+/* Install the prime factors of n (n = p * q, little-endian words) so that
+ * decrypt and decode exponentiations run by the Chinese remainder theorem:
+ * c^e mod p^2 and c^e mod q^2 on half-width lane groups, recombined to
+ * c^e mod n^2 by Garner's formula before the same L() / multiplier / popcount
+ * epilogue.  Results are identical to the direct path for every c < n^2.
+ * p = q = NULL removes the factors.  Rejects p * q != n, even or unit
+ * factors, and factors whose squares are wider than half of n^2.  No
+ * reference counterpart: the reference exponentiates mod n^2 directly
+ * (decrypt_only_kernel, src/cuhepy/paillier/_lookup_gpu_ext/
+ * paillier_GPU_lookup_client.cu:1013-1050); both of its key formats carry
+ * phi, from which the host recovers p and q. */
+int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p, int p_words, const uint32_t* q, int q_words);
+/* 1 when factors are installed (decrypt / decode use the CRT kernel). */
+int cuhe_paillier_has_factors(const cuhe_paillier* ctx);
+
 /* c[i] = (1 + m[i]*n) * r[i]^n mod n^2, i.e. g^m r^n with g = n + 1.
  * Replaces Paillier.encrypt (src/cuhepy/paillier/scheme.py:63-83) with the
  * randomness r supplied by the caller, and the device half of
@@ -166,9 +181,13 @@ int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t coun
                              const uint8_t* noise_index, uint32_t* out);
 
 /* Measure the integer multiply roofline of a device: 32x32->64-bit word
- * products per second (one mad.lo.u32 + one mad.hi.u32 each) sustained by a
- * dependency-light probe kernel over all SMs.  No counterpart in the
- * reference; it provides the denominator of the modexp roofline. */
+ * products per second over all SMs, the largest of three probe kernels: one
+ * issuing mad.lo.u32 + mad.hi.u32 pairs on independent accumulators, one
+ * issuing mad.wide.u32 on independent 64-bit accumulators, one running the
+ * modexp kernel's own carry-chained multiply-accumulate row
+ * (mad.lo.cc / madc.hi.cc) on four independent accumulator sets.  No
+ * counterpart in the reference; it provides the denominator of the modexp
+ * roofline. */
 int cuhe_imad_peak(int device, double* word_products_per_second);
 
 /* Host-only helper (no device needed): the left-to-right sliding-window

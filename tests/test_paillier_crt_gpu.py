@@ -1,0 +1,237 @@
+"""Decrypt / decode by the Chinese remainder theorem (k_modexp_crt).
+
+With the factors of n installed, c^e mod n^2 is computed as c^e mod p^2 and
+c^e mod q^2 and recombined; every result must equal the direct kernel's and
+the oracle's, for ciphertexts and for arbitrary values below n^2 (zero,
+multiples of p, p^2, q, n, ...).  Integer work: equality is exact.
+"""
+
+import random
+
+import numpy as np
+import pytest
+
+from conftest import hx, load_golden
+from oracle import paillier as oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _keys(data):
+    pk = {k: hx(v) for k, v in data["pk"].items()}
+    return pk, {"pk": pk, "sk": {k: hx(v) for k, v in data["sk"].items()}}
+
+
+def _pair(n, secret, phi):
+    """(direct context, CRT context) for the same key."""
+    from cuhepy_b200._numbers import factors_from_phi
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    direct = PaillierDevice(n)
+    direct.set_secret(*secret)
+    crt = PaillierDevice(n)
+    crt.set_secret(*secret)
+    p, q = factors_from_phi(n, phi)
+    crt.set_factors(p, q)
+    assert crt.has_factors and not direct.has_factors
+    return direct, crt, p, q
+
+
+def _awkward(n, p, q, rng, count=48):
+    """Values below n^2 that stress the recombination: zero, units, multiples
+    of p, q, p^2, q^2 and n, the top of the range, and random values."""
+    n2 = n * n
+    vals = [0, 1, 2, n - 1, n, n + 1, p, q, p * p, q * q, p * p * q, q * q * p, n2 - 1, n2 - n, n2 - p, n2 - 2]
+    vals += [p * rng.randrange(1, q * q) for _ in range(8)]
+    vals += [q * q * rng.randrange(1, p * p) for _ in range(4)]
+    vals += [rng.randrange(n2) for _ in range(count)]
+    return [v for v in vals if 0 <= v < n2]
+
+
+@pytest.mark.parametrize("name", ["paillier_512.json", "paillier_1024.json"])
+def test_crt_textbook_golden_and_edges(name):
+    data = load_golden(name)
+    pk, keys = _keys(data)
+    n = pk["n"]
+    direct, crt, p, q = _pair(n, (keys["sk"]["phi"], keys["sk"]["inv"]), keys["sk"]["phi"])
+    ms = [hx(c["m"]) for c in data["encrypt"]]
+    cs = [hx(c["c"]) for c in data["encrypt"]]
+    vals = _awkward(n, p, q, random.Random(3))
+    want = [oracle.decrypt(c, keys) for c in vals]
+    for tpi, w in crt.VARIANTS[crt.words]:
+        crt.set_tuning(tpi, w)
+        assert crt.decrypt(cs) == ms, (tpi, w)
+        assert crt.decrypt(vals) == want, (tpi, w)
+    assert direct.decrypt(vals) == want
+    sums = crt.mulmod([cs[s["i"]] for s in data["add"]], [cs[s["j"]] for s in data["add"]])
+    assert crt.decrypt(sums) == [hx(s["m"]) for s in data["add"]]
+
+
+@pytest.mark.parametrize("name", ["lookup_512.json", "lookup_1024.json"])
+def test_crt_lookup_golden_decode_and_edges(name):
+    data = load_golden(name)
+    pk, keys = _keys(data)
+    n = pk["n"]
+    direct, crt, p, q = _pair(n, (keys["sk"]["a"], keys["sk"]["g_a_inv"]), keys["sk"]["phi"])
+    ms = [hx(c["m"]) for c in data["encrypt"]]
+    cs = [hx(c["c"]) for c in data["encrypt"]]
+    vals = _awkward(n, p, q, random.Random(4))
+    want = [oracle.lookup_decrypt(c, keys) for c in vals]
+    chunk_len = 2 * data["key_len"]
+    pairs = data["hamming"]["pairs"] if data["hamming"] else []
+    for tpi, w in crt.VARIANTS[crt.words]:
+        crt.set_tuning(tpi, w)
+        assert crt.decrypt(cs) == ms, (tpi, w)
+        assert crt.decrypt(vals) == want, (tpi, w)
+        if pairs:
+            server = [[hx(pr["c"])] for pr in pairs]
+            assert crt.decode_hamming(server, 1, chunk_len) == [pr["distance"] for pr in pairs], (tpi, w)
+    # decode of arbitrary values: popcount of the even bits of the decrypted value
+    rows = [[v] for v in vals]
+    got = crt.decode_hamming(rows, 1, chunk_len)
+    assert got == direct.decode_hamming(rows, 1, chunk_len)
+    assert got == [oracle.decode_distance([m], data["key_len"]) for m in want]
+
+
+def test_crt_matches_direct_on_a_large_device_batch():
+    """A device-resident batch several waves deep, through the array API."""
+    import torch
+
+    data = load_golden("lookup_1024.json")
+    pk, keys = _keys(data)
+    n = pk["n"]
+    direct, crt, p, q = _pair(n, (keys["sk"]["a"], keys["sk"]["g_a_inv"]), keys["sk"]["phi"])
+    rng = random.Random(77)
+    vals = _awkward(n, p, q, rng, count=6000)
+    limbs = torch.from_numpy(crt.limbs(vals).view(np.int32)).cuda()
+    out_a = torch.zeros((len(vals), crt.words), dtype=torch.int32, device="cuda")
+    out_b = torch.zeros_like(out_a)
+    crt.decrypt_array(limbs, out_a, len(vals))
+    direct.decrypt_array(limbs, out_b, len(vals))
+    torch.cuda.synchronize()
+    assert torch.equal(out_a, out_b)
+    sample = rng.sample(range(len(vals)), 64)
+    got = out_a.cpu().numpy().view(np.uint32)
+    from cuhepy_b200._limbs import from_limbs
+
+    decoded = from_limbs(got[sample])
+    assert decoded == [oracle.lookup_decrypt(vals[i], keys) for i in sample]
+
+
+def test_crt_8192_bit_modulus_vs_oracle():
+    rng = random.Random(4096)
+    from oracle.gmp import powmod
+
+    def is_prime(x):
+        if x % 2 == 0:
+            return False
+        d, s = x - 1, 0
+        while d % 2 == 0:
+            d //= 2
+            s += 1
+        for _ in range(20):
+            a = rng.randrange(2, x - 1)
+            y = powmod(a, d, x)
+            if y in (1, x - 1):
+                continue
+            for _ in range(s - 1):
+                y = y * y % x
+                if y == x - 1:
+                    break
+            else:
+                return False
+        return True
+
+    def get_prime(bits):
+        while True:
+            c = rng.getrandbits(bits) | (1 << (bits - 1)) | 1
+            if all(c % s for s in (3, 5, 7, 11, 13, 17, 19, 23)) and is_prime(c):
+                return c
+
+    p, q = get_prime(2048), get_prime(2048)
+    keys = oracle.keys_from_primes(p, q)
+    pk = keys["pk"]
+    direct, crt, _, _ = _pair(pk["n"], (keys["sk"]["phi"], keys["sk"]["inv"]), keys["sk"]["phi"])
+    assert crt.words == 256
+    ms = [rng.randrange(pk["n"]) for _ in range(8)]
+    cs = [oracle.encrypt(m, rng.randrange(1, pk["n"]), pk) for m in ms]
+    vals = _awkward(pk["n"], p, q, rng, count=4)
+    want = [oracle.decrypt(c, keys) for c in vals]
+    for tpi, w in crt.VARIANTS[256]:
+        crt.set_tuning(tpi, w)
+        assert crt.decrypt(cs) == ms, (tpi, w)
+        assert crt.decrypt(vals) == want, (tpi, w)
+
+
+def test_set_factors_rejects_bad_factorisations_and_can_be_removed():
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    data = load_golden("paillier_512.json")
+    pk, keys = _keys(data)
+    n = pk["n"]
+    from cuhepy_b200._numbers import factors_from_phi
+
+    p, q = factors_from_phi(n, keys["sk"]["phi"])
+    ctx = PaillierDevice(n)
+    ctx.set_secret(keys["sk"]["phi"], keys["sk"]["inv"])
+    with pytest.raises(ValueError):
+        ctx.set_factors(p + 2, q)          # p * q != n
+    with pytest.raises(ValueError):
+        ctx.set_factors(1, n)              # unit factor
+    assert not ctx.has_factors
+    ctx.set_factors(q, p)                  # either order
+    assert ctx.has_factors
+    c = hx(data["encrypt"][1]["c"])
+    assert ctx.decrypt([c]) == [hx(data["encrypt"][1]["m"])]
+    ctx.set_factors(None, None)
+    assert not ctx.has_factors
+    assert ctx.decrypt([c]) == [hx(data["encrypt"][1]["m"])]
+    # unbalanced factors (p^2 wider than half of n^2) stay on the direct kernel
+    small, big = 1000003, (1 << 1000) + 1  # set_factors checks the product, not primality
+    lop = PaillierDevice(small * big)
+    with pytest.raises(ValueError):
+        lop.set_factors(small, big)
+    assert not lop.has_factors
+
+
+def test_reference_facing_apis_install_factors_from_phi():
+    from cuhepy_b200.paillier import lookup, scheme
+    from cuhepy_b200.paillier.gpu import device_for
+
+    data = load_golden("paillier_512.json")
+    _, keys = _keys(data)
+    c, m = hx(data["encrypt"][0]["c"]), hx(data["encrypt"][0]["m"])
+    assert scheme.Paillier.decrypt(c, keys) == m
+    sk = keys["sk"]
+    assert device_for(keys["pk"]["n"], (sk["phi"], sk["inv"]), phi=sk["phi"]).has_factors
+    data = load_golden("lookup_512.json")
+    _, keys = _keys(data)
+    c, m = hx(data["encrypt"][0]["c"]), hx(data["encrypt"][0]["m"])
+    assert lookup.PaillierLookup.decrypt(c, keys) == m
+    sk = keys["sk"]
+    assert device_for(keys["pk"]["n"], (sk["a"], sk["g_a_inv"]), phi=sk["phi"]).has_factors
+
+
+def test_static_decode_with_factors_matches_allocating_decode():
+    import torch
+
+    from cuhepy_b200 import _native
+
+    data = load_golden("lookup_512.json")
+    pk, keys = _keys(data)
+    direct, crt, _, _ = _pair(pk["n"], (keys["sk"]["a"], keys["sk"]["g_a_inv"]), keys["sk"]["phi"])
+    rng = random.Random(12)
+    vectors, chunk_num, chunk_len = 200, 3, 2 * data["key_len"]
+    vals = [rng.randrange(pk["n_squared"]) for _ in range(vectors * chunk_num)]
+    c = torch.from_numpy(crt.limbs(vals).view(np.int32)).cuda()
+    a = torch.zeros(vectors, dtype=torch.int64, device="cuda")
+    b = torch.zeros_like(a)
+    crt.decode_array(c, vectors, chunk_num, chunk_len, a)
+    lib = _native.paillier_lib()
+    rc = lib.cuhe_paillier_decode_hamming_static(crt._ctx, c.data_ptr(), vectors, chunk_num, chunk_len, b.data_ptr())
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    rows = [vals[chunk_num * i:chunk_num * i + chunk_num] for i in range(vectors)]
+    want = np.array(direct.decode_hamming(rows, chunk_num, chunk_len))
+    assert np.array_equal(a.cpu().numpy(), want)

@@ -31,7 +31,20 @@ def _device(n, secret=None):
 
 
 def _tunings(words):
-    return {64: [(8, 4), (16, 4)], 128: [(8, 4), (16, 4), (16, 5), (32, 4)], 256: [(16, 4), (32, 4), (32, 5)]}[words]
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    return PaillierDevice.VARIANTS[words]
+
+
+def test_autotune_picks_a_compiled_variant_and_keeps_results():
+    data = load_golden("paillier_1024.json")
+    pk, keys = _keys(data)
+    ctx = _device(pk["n"], (keys["sk"]["phi"], keys["sk"]["inv"]))
+    report = ctx.autotune(exponent_bits=280, count=2048, reps=1)
+    assert report["best"] in _tunings(ctx.words) and ctx.tuning() == report["best"]
+    ms = [hx(c["m"]) for c in data["encrypt"]]
+    rs = [hx(c["r"]) for c in data["encrypt"]]
+    assert ctx.encrypt(ms, rs) == [hx(c["c"]) for c in data["encrypt"]]
 
 
 @pytest.mark.parametrize("name", ["paillier_512.json", "paillier_1024.json"])
