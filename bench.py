@@ -386,6 +386,10 @@ def run_gpu(args) -> dict | None:
     }
     if not args.no_bfv:
         result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
+    if not args.no_serving and world == 1:
+        del prod, dist_out, index_ct, flush  # the serving section needs the HBM
+        torch.cuda.empty_cache()
+        result["serving"] = run_serving()
     if not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if dist:
@@ -397,7 +401,7 @@ BFV_N, BFV_Q_BITS, BFV_GADGET, BFV_T, BFV_EMBED = 8192, 180, 30, 65537, 512
 BFV_VECTORS = 16384
 
 
-def bfv_setup(seed: int = 8192):
+def bfv_setup(seed: int = 8192, embed: int = BFV_EMBED):
     """N=8192, Q = 3 x 60-bit NTT primes, 30-bit gadget, t=65537, embed 512
     (16 vectors per ciphertext, 1,024 index ciphertexts for 16,384 vectors).
     Keys and ciphertexts are uniform residues from a seeded generator: the
@@ -408,7 +412,7 @@ def bfv_setup(seed: int = 8192):
     q = 1
     for p in ob.rns_primes(BFV_N, BFV_Q_BITS):
         q *= p
-    layout = ob.Layout(BFV_N, BFV_EMBED)
+    layout = ob.Layout(BFV_N, embed)
     exps = sorted(set(layout.left()) | set(layout.right()))
     rng = np.random.default_rng(seed)
     width = (q.bit_length() + 7) // 8
@@ -683,6 +687,165 @@ def run_reference(args) -> dict | None:
     }
 
 
+SERVE_VECTORS = 1 << 20
+SERVE_REQUESTS = 48
+SERVE_EMBEDS = (256, 512, 1024)
+
+
+def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
+    """Serving: 1,048,576 Paillier-Lookup-encrypted 512-bit vectors plus three
+    BFV indexes (16,384 vectors each at embed_len 256 / 512 / 1024, their key
+    sets) resident in HBM.  Poisson arrivals of requests, half Paillier
+    (batch of 1-64 encrypted queries, answer = encode_hamming_server against
+    the whole index, kept on the device) and half BFV (one packed query,
+    embed_len drawn from the three).  The same arrival trace runs through
+    the served evaluator (continuous batching: one Paillier lane fed back to
+    back, three high-priority BFV lanes; admission by free HBM) and through
+    the plain path (one request at a time, one launch per
+    query).  Rates are set for about 80% offered load from single-query
+    timings taken first."""
+    import torch
+
+    from cuhepy_b200.bfv import _bfv_rns as m
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+    from cuhepy_b200.serving import KnnEvaluator
+
+    keys = seeded_lookup_keys(0)
+    pk, sk = keys["pk"], keys["sk"]
+    ctx = PaillierDevice(pk["n"])
+    ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
+    K = ctx.words
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    index = torch.empty((SERVE_VECTORS, K), dtype=torch.int32, device="cuda")
+    step = 1 << 16
+    for v0 in range(0, SERVE_VECTORS, step):
+        bits = torch.randint(0, 2, (step, EMBED_LEN), dtype=torch.uint8, device="cuda", generator=gen)
+        nidx = torch.randint(0, 256, (step, 14), dtype=torch.uint8, device="cuda", generator=gen)
+        ctx.lookup_encrypt_bits_array(bits, step, EMBED_LEN, 2 * KEY_LEN, 1, nidx, index[v0:v0 + step])
+    qbits = torch.randint(0, 2, (64 * 8, EMBED_LEN), dtype=torch.uint8, device="cuda", generator=gen)
+    qidx = torch.randint(0, 256, (64 * 8, 14), dtype=torch.uint8, device="cuda", generator=gen)
+    qpool = torch.empty((64 * 8, K), dtype=torch.int32, device="cuda")
+    ctx.lookup_encrypt_bits_array(qbits, 64 * 8, EMBED_LEN, 2 * KEY_LEN, 1, qidx, qpool)
+    torch.cuda.synchronize()
+    qpool = qpool.cpu()  # queries arrive from the host
+
+    ev = KnnEvaluator(paillier_lanes=1, bfv_lanes=3, max_batch=64)
+    ev.add_paillier_index("paillier", pk["n"], index.view(SERVE_VECTORS, 1, K))
+    bfv_queries = {}
+    for e in SERVE_EMBEDS:
+        q, layout, exps, bkeys, query, bindex, target = bfv_setup(8192 + e, embed=e)
+        ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+        relin = m.compile_key(ring, bkeys[0])
+        galois = tuple((g, m.compile_key(ring, bkeys[1 + i])) for i, g in enumerate(exps))
+        server = m.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
+        tiles = BFV_VECTORS // layout.capacity
+        resident = m.upload_index(server, bindex)
+        assert resident.tiles == tiles
+        ev.add_bfv_index(f"bfv{e}", server, resident, BFV_VECTORS, compact=True)
+        bfv_queries[e] = query
+
+    # single-query costs (warm), for the arrival rate
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ev.run_plain("paillier", "paillier", qpool[:1].view(1, 1, K))
+        t_p1 = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ev.run_plain("bfv", "bfv512", bfv_queries[512])
+        t_b = time.perf_counter() - t0
+    rng = random.Random(seed)
+    trace = []
+    for i in range(requests):
+        if i % 2 == 0:
+            b = rng.randint(1, 64)
+            start = rng.randrange(0, 64 * 8 - b)
+            trace.append(("paillier", "paillier", b, qpool[start:start + b].view(b, 1, K)))
+        else:
+            e = rng.choice(SERVE_EMBEDS)
+            trace.append(("bfv", f"bfv{e}", 1, bfv_queries[e]))
+    mean_cost = 0.5 * 32.5 * t_p1 + 0.5 * t_b
+    rate = 0.8 / mean_cost
+    arrivals, t = [], 0.0
+    for _ in trace:
+        t += rng.expovariate(rate)
+        arrivals.append(t)
+
+    def summarize(lat, t_end, label):
+        queries = sum(r[2] for r in trace)
+        lat_ms = [x * 1e3 for x in lat]
+        by_kind = {}
+        for kind in ("paillier", "bfv"):
+            k_lat = [l for l, r in zip(lat_ms, trace) if r[0] == kind]
+            by_kind[kind] = {"p50_ms": statistics.median(k_lat), "p99_ms": float(np.percentile(k_lat, 99)),
+                             "queries": sum(r[2] for r in trace if r[0] == kind)}
+        return {"queries_per_s": queries / t_end, "requests_per_s": len(trace) / t_end,
+                "p50_ms": statistics.median(lat_ms), "p99_ms": float(np.percentile(lat_ms, 99)),
+                "makespan_s": t_end, "by_kind": by_kind, "path": label}
+
+    def served_run(arr):
+        ev.start()
+        lat = [0.0] * len(trace)
+        done_at = [0.0] * len(trace)
+        t_start = time.perf_counter()
+        futs = []
+        for i, (kind, name, b, payload) in enumerate(trace):
+            delay = t_start + arr[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            f = ev.submit_paillier(name, payload) if kind == "paillier" else ev.submit_bfv(name, payload)
+
+            def finish(fut, i=i, kind=kind):
+                done_at[i] = time.perf_counter()
+                lat[i] = done_at[i] - (t_start + arr[i])
+                if kind == "paillier" and fut.exception() is None:
+                    fut.result().release()
+
+            f.add_done_callback(finish)
+            futs.append(f)
+        for f in futs:
+            f.result(600)
+        out = summarize(lat, max(done_at) - t_start,
+                        "served: continuous batching; 1 Paillier lane fed back to back, 3 high-priority BFV lanes; "
+                        "admission by free HBM")
+        sched = ev.scheduler
+        out.update({"launches": sched.launches, "max_concurrent": sched.max_concurrent,
+                    "peak_answer_bytes": sched.peak_in_use, "budget_bytes": sched.budget})
+        ev.stop()
+        return out
+
+    def plain_run(arr):
+        lat = [0.0] * len(trace)
+        t_start = time.perf_counter()
+        free_at = 0.0
+        for i, (kind, name, b, payload) in enumerate(trace):
+            now = time.perf_counter() - t_start
+            if now < arr[i]:
+                time.sleep(arr[i] - now)
+            out = ev.run_plain(kind, name, payload)
+            del out
+            free_at = time.perf_counter() - t_start
+            lat[i] = free_at - arr[i]
+        return summarize(lat, free_at, "plain: one request at a time, one launch per query")
+
+    served = served_run(arrivals)
+    plain = plain_run(arrivals)
+    burst = [0.0] * len(trace)  # every request waiting at once: the throughput bound
+    served_burst = served_run(burst)
+    plain_burst = plain_run(burst)
+    return {
+        "metric": "encrypted kNN queries/s and p50/p99 latency, served vs plain",
+        "workload": "serving_knn",
+        "index": {"paillier_vectors": SERVE_VECTORS, "paillier_key_len": KEY_LEN,
+                  "bfv_vectors_per_embed": BFV_VECTORS, "bfv_embeds": list(SERVE_EMBEDS), "bfv_n": BFV_N},
+        "requests": len(trace), "arrival_rate_per_s": rate,
+        "single_query_ms": {"paillier_1_query_x_1M": t_p1 * 1e3, "bfv_embed512": t_b * 1e3},
+        "served": served, "plain": plain,
+        "burst": {"served": served_burst, "plain": plain_burst,
+                  "note": "the same requests all arriving at t=0 (closed backlog)"},
+        "answers": "Paillier answers stay on the device (B x 1,048,576 x 512 B) and are released on completion",
+    }
+
+
 def profile_case(which: str) -> None:
     """Small cases of the dominant kernels, sized for ncu captures (inputs
     larger than L2 where the kernel streams memory, a few GB at most)."""
@@ -734,11 +897,16 @@ def main() -> None:
     parser.add_argument("--cpu-seconds", type=float, default=20.0)
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-bfv", action="store_true", help="skip the BFV kNN section")
+    parser.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    parser.add_argument("--serving-only", action="store_true", help="run only the serving section")
     parser.add_argument("--profile-case", choices=["paillier", "bfv"],
                         help="run one small step of a hot kernel (for ncu captures) and exit")
     args = parser.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)
+        return
+    if args.serving_only:
+        print(json.dumps(run_serving()))
         return
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -53,6 +53,9 @@ BFV_SIGNATURES: dict[str, tuple] = {
     "cuhe_bfv_index_release": (None, [_vp]),
     "cuhe_bfv_search_index": (ctypes.c_int, [_vp, _vp, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, _vp,
                                              ctypes.c_uint64, _u64p]),
+    "cuhe_bfv_set_lanes": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cuhe_bfv_get_lanes": (ctypes.c_int, [_vp]),
+    "cuhe_bfv_search_workspace": (ctypes.c_uint64, [_vp, ctypes.c_uint64, ctypes.c_int]),
 }
 
 BFV_LIB = "libcuhe_bfv_b200.so"
@@ -364,6 +367,21 @@ def search_index(server: Server, index: ResidentIndex, query: Any, count: int,
     raw = out.raw
     return [(raw[(2 * i) * size:(2 * i + 1) * size], raw[(2 * i + 1) * size:(2 * i + 2) * size])
             for i in range(responses.value)]
+
+
+def set_lanes(ring: Ring, lanes: int) -> None:
+    """Execution lanes of a ring (1..8): concurrent searches from several host
+    threads take free lanes and overlap on the GPU (not in the reference API)."""
+    _check(lib().cuhe_bfv_set_lanes(_get(ring, Ring).ptr, int(lanes)))
+
+
+def get_lanes(ring: Ring) -> int:
+    return int(lib().cuhe_bfv_get_lanes(_get(ring, Ring).ptr))
+
+
+def search_workspace(server: Server, tiles: int, compact: bool = True) -> int:
+    """Device bytes one lane holds for a search over `tiles` tiles."""
+    return int(lib().cuhe_bfv_search_workspace(_get(server, Server).ptr, int(tiles), int(bool(compact))))
 
 
 def _profile(fn, *args) -> tuple[Any, dict[str, Any]]:

@@ -80,6 +80,18 @@ struct Arena {
   }
 };
 
+// One execution lane of a ring: a stream, its device workspace and the lock
+// that serialises calls on it.  Lane 0 serves every call except searches,
+// which take a free lane among the active ones, so that searches issued from
+// several host threads overlap on the GPU.
+struct Lane {
+  cudaStream_t stream = nullptr;
+  Arena arena;
+  std::mutex mu;
+};
+
+constexpr int kMaxLanes = 8;
+
 #define BFV_ARENA(arena)                                                                  \
   do {                                                                                    \
     if ((arena).overflow) return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted"); \
@@ -100,16 +112,20 @@ struct cuhe_bfv_ring {
   size_t table_bytes = 0;
   RingDev host_dev{};
   std::map<u64, RingDev*> dev_for_t;  // t == 0: no scale constants
-  cudaStream_t stream = nullptr;
-  std::mutex mu;
-  Arena arena;
+  std::mutex mu;  // guards dev_for_t
+  std::vector<std::unique_ptr<Lane>> lanes;  // kMaxLanes, created with the ring
+  std::atomic<int> active_lanes{1};
+  std::atomic<unsigned> next_lane{0};
 
   ~cuhe_bfv_ring() {
     DeviceGuard g(device);
-    if (stream) cudaStreamSynchronize(stream);
+    for (auto& ln : lanes)
+      if (ln->stream) cudaStreamSynchronize(ln->stream);
     for (auto& kv : dev_for_t) cudaFree(kv.second);
     if (d_tables) cudaFree(d_tables);
-    if (stream) cudaStreamDestroy(stream);
+    for (auto& ln : lanes)
+      if (ln->stream) cudaStreamDestroy(ln->stream);
+    lanes.clear();  // workspaces are freed while this device is current
   }
 };
 
@@ -142,6 +158,7 @@ struct cuhe_bfv_server {
   u64* d_target = nullptr;
   std::map<size_t, u64*> partial_masks;
   RingDev* d_ring = nullptr;
+  std::mutex mu;  // guards partial_masks and profile_ms
   double profile_ms[6] = {0, 0, 0, 0, 0, 0};
   ~cuhe_bfv_server() {
     {
@@ -166,6 +183,7 @@ unsigned log2u(size_t n) {
 
 // Device copy of the ring constants; t != 0 adds the exact scale constants.
 int device_ring(cuhe_bfv_ring* r, u64 t, RingDev** out) {
+  std::lock_guard<std::mutex> lock(r->mu);
   auto it = r->dev_for_t.find(t);
   if (it != r->dev_for_t.end()) { *out = it->second; return CUHE_OK; }
   RingDev dev = r->host_dev;
@@ -246,30 +264,30 @@ unsigned blocks_for(long long items, int threads) { return unsigned((items + thr
 
 size_t ntt_smem(const cuhe_bfv_ring* r) { return plane_smem_words(int(r->plan.n)) * sizeof(u64); }
 
-cudaError_t launch_ntt(cuhe_bfv_ring* r, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
+cudaError_t launch_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
                        int prime_block, int inverse) {
   if (planes <= 0) return cudaSuccess;
   const size_t smem = ntt_smem(r);
   cudaError_t e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   const int threads = int(std::min<size_t>(1024, std::max<size_t>(32, r->plan.n / 16)));
-  k_ntt<<<unsigned(planes), threads, smem, r->stream>>>(data, d, prime_base, prime_mod, prime_block, inverse);
+  k_ntt<<<unsigned(planes), threads, smem, ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse);
   return cudaGetLastError();
 }
 
 // Compose ops then key-switch ops (one launch each).
-int run_switch(cuhe_bfv_ring* r, RingDev* d, const std::vector<ComposeOp>& cops, const std::vector<SwitchOp>& sops,
+int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<ComposeOp>& cops, const std::vector<SwitchOp>& sops,
                ComposeOp* d_cops, SwitchOp* d_sops) {
   const auto& P = r->plan;
   if (!cops.empty()) {
-    BFV_CUDA(cudaMemcpyAsync(d_cops, cops.data(), cops.size() * sizeof(ComposeOp), cudaMemcpyHostToDevice, r->stream),
+    BFV_CUDA(cudaMemcpyAsync(d_cops, cops.data(), cops.size() * sizeof(ComposeOp), cudaMemcpyHostToDevice, ln.stream),
              "compose ops");
     dim3 grid(blocks_for((long long)(P.n), 256), unsigned(cops.size()));
-    k_compose<<<grid, 256, 0, r->stream>>>(d_cops, d);
+    k_compose<<<grid, 256, 0, ln.stream>>>(d_cops, d);
     BFV_CUDA(cudaGetLastError(), "compose launch");
   }
   if (!sops.empty()) {
-    BFV_CUDA(cudaMemcpyAsync(d_sops, sops.data(), sops.size() * sizeof(SwitchOp), cudaMemcpyHostToDevice, r->stream),
+    BFV_CUDA(cudaMemcpyAsync(d_sops, sops.data(), sops.size() * sizeof(SwitchOp), cudaMemcpyHostToDevice, ln.stream),
              "switch ops");
     const size_t smem = ntt_smem(r);
     dim3 grid(unsigned(sops.size()), unsigned(P.residue_count));
@@ -277,15 +295,15 @@ int run_switch(cuhe_bfv_ring* r, RingDev* d, const std::vector<ComposeOp>& cops,
       const size_t smem_acc = smem + 2 * P.n * sizeof(u64);  // accumulators after the plane
       BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_acc)),
                "smem");
-      k_keyswitch<0><<<grid, kSwitchThreads, smem_acc, r->stream>>>(d_sops, d);
+      k_keyswitch<0><<<grid, kSwitchThreads, smem_acc, ln.stream>>>(d_sops, d);
     } else {
       BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
-      k_keyswitch<32><<<grid, kSwitchThreads, smem, r->stream>>>(d_sops, d);
+      k_keyswitch<32><<<grid, kSwitchThreads, smem, ln.stream>>>(d_sops, d);
     }
     BFV_CUDA(cudaGetLastError(), "keyswitch launch");
   }
   // op tables are reused by the next call; keep host order
-  BFV_CUDA(cudaStreamSynchronize(r->stream), "switch synchronize");
+  BFV_CUDA(cudaStreamSynchronize(ln.stream), "switch synchronize");
   return CUHE_OK;
 }
 
@@ -297,10 +315,10 @@ unsigned inverse_mod_2n(u64 g, size_t n) {
 }
 
 // host words of a composed result (after k_compose) -> bytes
-int download_words(cuhe_bfv_ring* r, const u64* d_words, size_t polys, uint8_t* out) {
+int download_words(cuhe_bfv_ring* r, Lane& ln, const u64* d_words, size_t polys, uint8_t* out) {
   std::vector<u64> words(polys * r->plan.n * size_t(r->host_dev.words));
-  BFV_CUDA(cudaMemcpyAsync(words.data(), d_words, words.size() * 8, cudaMemcpyDeviceToHost, r->stream), "download");
-  BFV_CUDA(cudaStreamSynchronize(r->stream), "download");
+  BFV_CUDA(cudaMemcpyAsync(words.data(), d_words, words.size() * 8, cudaMemcpyDeviceToHost, ln.stream), "download");
+  BFV_CUDA(cudaStreamSynchronize(ln.stream), "download");
   words_to_bytes(r, words, polys, out);
   return CUHE_OK;
 }
@@ -339,18 +357,18 @@ std::vector<u64> hamming_mask(size_t n, u64 t, size_t lanes, size_t count) {
 }
 
 // residues mod the first L primes of a small nonnegative polynomial, NTT'd
-int upload_plain_ntt(cuhe_bfv_ring* r, RingDev* d, const std::vector<u64>& coeffs_words, u64** out) {
+int upload_plain_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<u64>& coeffs_words, u64** out) {
   const auto& P = r->plan;
   const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
   u64* d_words = nullptr;
   u64* d_res = nullptr;
   BFV_CUDA(cudaMalloc(&d_words, n * W * 8), "plain alloc");
   BFV_CUDA(cudaMalloc(&d_res, L * n * 8), "plain alloc");
-  BFV_CUDA(cudaMemcpyAsync(d_words, coeffs_words.data(), n * W * 8, cudaMemcpyHostToDevice, r->stream), "plain");
-  k_words_to_residues<<<blocks_for((long long)(n), 256), 256, 0, r->stream>>>(d_words, 1, int(L), d_res, d);
+  BFV_CUDA(cudaMemcpyAsync(d_words, coeffs_words.data(), n * W * 8, cudaMemcpyHostToDevice, ln.stream), "plain");
+  k_words_to_residues<<<blocks_for((long long)(n), 256), 256, 0, ln.stream>>>(d_words, 1, int(L), d_res, d);
   BFV_CUDA(cudaGetLastError(), "plain residues");
-  BFV_CUDA(launch_ntt(r, d, d_res, (long long)(L), 0, int(L), 1, 0), "plain ntt");
-  BFV_CUDA(cudaStreamSynchronize(r->stream), "plain");
+  BFV_CUDA(launch_ntt(r, ln, d, d_res, (long long)(L), 0, int(L), 1, 0), "plain ntt");
+  BFV_CUDA(cudaStreamSynchronize(ln.stream), "plain");
   cudaFree(d_words);
   *out = d_res;
   return CUHE_OK;
@@ -375,11 +393,11 @@ struct TileArgs {
   std::vector<const u64*> masks;         // per tile mask NTT [L][N]
 };
 
-int tile_circuit(cuhe_bfv_ring* r, RingDev* d, const TileArgs& a, u64* dist, double* ms) {
+int tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const TileArgs& a, u64* dist, double* ms) {
   const auto& P = r->plan;
   const size_t n = P.n, L = P.residue_count, T = P.tensor_count, W = size_t(r->host_dev.words);
   const size_t ct = a.ct;
-  Arena& ar = r->arena;
+  Arena& ar = ln.arena;
   u64* diff = ar.take<u64>(ct * 2 * T * n);
   u64* tens = ar.take<u64>(ct * 3 * T * n);
   u64* scaled = ar.take<u64>(ct * 3 * L * n);
@@ -390,17 +408,17 @@ int tile_circuit(cuhe_bfv_ring* r, RingDev* d, const TileArgs& a, u64* dist, dou
   BFV_ARENA(ar);
   cudaEvent_t ev[5];
   for (auto& e : ev) cudaEventCreate(&e);
-  cudaEventRecord(ev[0], r->stream);
-  k_diff_residues<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, r->stream>>>(a.q_words, a.t_words, int(ct), int(T),
+  cudaEventRecord(ev[0], ln.stream);
+  k_diff_residues<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(a.q_words, a.t_words, int(ct), int(T),
                                                                                     diff, d);
   BFV_CUDA(cudaGetLastError(), "diff residues");
-  BFV_CUDA(launch_ntt(r, d, diff, (long long)(ct * 2 * T), 0, int(T), 1, 0), "tensor ntt");
-  k_tensor_square<<<blocks_for((long long)(ct * T * n), 256), 256, 0, r->stream>>>(diff, int(ct), int(T), tens, d);
+  BFV_CUDA(launch_ntt(r, ln, d, diff, (long long)(ct * 2 * T), 0, int(T), 1, 0), "tensor ntt");
+  k_tensor_square<<<blocks_for((long long)(ct * T * n), 256), 256, 0, ln.stream>>>(diff, int(ct), int(T), tens, d);
   BFV_CUDA(cudaGetLastError(), "tensor");
-  BFV_CUDA(launch_ntt(r, d, tens, (long long)(ct * 3 * T), 0, int(T), 1, 1), "tensor intt");
-  k_rns_scale<<<blocks_for((long long)(ct * 3 * n), 128), 128, 0, r->stream>>>(tens, (long long)(ct * 3), scaled, d);
+  BFV_CUDA(launch_ntt(r, ln, d, tens, (long long)(ct * 3 * T), 0, int(T), 1, 1), "tensor intt");
+  k_rns_scale<<<blocks_for((long long)(ct * 3 * n), 128), 128, 0, ln.stream>>>(tens, (long long)(ct * 3), scaled, d);
   BFV_CUDA(cudaGetLastError(), "rns scale");
-  cudaEventRecord(ev[1], r->stream);
+  cudaEventRecord(ev[1], ln.stream);
   // relinearize: dist = (c0, c1) + KS(c2)
   std::vector<ComposeOp> cops(ct);
   std::vector<SwitchOp> sops(ct);
@@ -408,15 +426,15 @@ int tile_circuit(cuhe_bfv_ring* r, RingDev* d, const TileArgs& a, u64* dist, dou
     cops[t] = ComposeOp{scaled + (t * 3 + 2) * L * n, words + t * n * W, 1u, 0u};
     sops[t] = SwitchOp{scaled + t * 3 * L * n, nullptr, words + t * n * W, a.relin->d_key, dist + t * 2 * L * n, 1u, 0u};
   }
-  if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
-  cudaEventRecord(ev[2], r->stream);
+  if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
+  cudaEventRecord(ev[2], ln.stream);
   // rotations: dist += rotate(dist, g)
   u64* cur = dist;
   u64* nxt = other;
   for (size_t k = 0; k < a.exps.size(); ++k) {
     const u64 g = a.exps[k];
     if (g == 1) {
-      k_add<<<blocks_for((long long)(ct * 2 * L * n), 256), 256, 0, r->stream>>>(cur, cur, nxt, (long long)(ct * 2 * L), int(L), d);
+      k_add<<<blocks_for((long long)(ct * 2 * L * n), 256), 256, 0, ln.stream>>>(cur, cur, nxt, (long long)(ct * 2 * L), int(L), d);
       BFV_CUDA(cudaGetLastError(), "double");
     } else {
       const unsigned ginv = inverse_mod_2n(g, n);
@@ -425,27 +443,27 @@ int tile_circuit(cuhe_bfv_ring* r, RingDev* d, const TileArgs& a, u64* dist, dou
         sops[t] = SwitchOp{cur + t * 2 * L * n, cur + t * 2 * L * n, words + t * n * W, a.keys[k]->d_key,
                            nxt + t * 2 * L * n, ginv, 0u};
       }
-      if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
+      if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
     }
     std::swap(cur, nxt);
   }
-  cudaEventRecord(ev[3], r->stream);
+  cudaEventRecord(ev[3], ln.stream);
   // masks in the NTT domain
-  BFV_CUDA(launch_ntt(r, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 0), "mask ntt");
+  BFV_CUDA(launch_ntt(r, ln, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 0), "mask ntt");
   for (size_t t = 0; t < ct; ++t) {
     const u64* m = a.masks[t];
     size_t run = 1;
     while (t + run < ct && a.masks[t + run] == m) ++run;
-    k_mul_plain<<<blocks_for((long long)(run * 2 * L * n), 256), 256, 0, r->stream>>>(cur + t * 2 * L * n,
+    k_mul_plain<<<blocks_for((long long)(run * 2 * L * n), 256), 256, 0, ln.stream>>>(cur + t * 2 * L * n,
                                                                                       (long long)(run * 2 * L), int(L), m, d);
     BFV_CUDA(cudaGetLastError(), "mask");
     t += run - 1;
   }
-  BFV_CUDA(launch_ntt(r, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 1), "mask intt");
+  BFV_CUDA(launch_ntt(r, ln, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 1), "mask intt");
   if (cur != dist)
-    BFV_CUDA(cudaMemcpyAsync(dist, cur, ct * 2 * L * n * 8, cudaMemcpyDeviceToDevice, r->stream), "dist copy");
-  cudaEventRecord(ev[4], r->stream);
-  BFV_CUDA(cudaStreamSynchronize(r->stream), "tile circuit");
+    BFV_CUDA(cudaMemcpyAsync(dist, cur, ct * 2 * L * n * 8, cudaMemcpyDeviceToDevice, ln.stream), "dist copy");
+  cudaEventRecord(ev[4], ln.stream);
+  BFV_CUDA(cudaStreamSynchronize(ln.stream), "tile circuit");
   if (ms) {
     float x;
     cudaEventElapsedTime(&x, ev[0], ev[1]); ms[0] += x;
@@ -522,7 +540,15 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
     std::memcpy(&tables[(j * 4 + 2) * N], P.ntt[j].inv.data(), N * 8);
     std::memcpy(&tables[(j * 4 + 3) * N], P.ntt[j].inv_q.data(), N * 8);
   }
-  cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
+  // Lane streams take the device's highest priority: a search is a chain of
+  // short dependent kernels, and its blocks should be scheduled ahead of the
+  // queued blocks of bulk work (Paillier batches) on default-priority streams.
+  int least_priority = 0, greatest_priority = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least_priority, &greatest_priority);
+  for (int k = 0; k < kMaxLanes && e == cudaSuccess; ++k) {
+    r->lanes.push_back(std::make_unique<Lane>());
+    e = cudaStreamCreateWithPriority(&r->lanes.back()->stream, cudaStreamNonBlocking, greatest_priority);
+  }
   if (e == cudaSuccess) e = cudaMalloc(&r->d_tables, r->table_bytes);
   if (e == cudaSuccess) e = cudaMemcpy(r->d_tables, tables.data(), r->table_bytes, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -596,7 +622,8 @@ int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t
   *out = nullptr;
   const auto& P = ring->plan;
   if (digits != P.digits) return fail(CUHE_INVALID_ARGUMENT, "Incorrect gadget digit count");
-  std::lock_guard<std::mutex> lock(ring->mu);
+  Lane& ln = *ring->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(ring->device);
   std::vector<u64> words;
   if (int rc = parse_polys(ring, key_polys, size_t(2 * digits), words)) return rc;
@@ -613,15 +640,15 @@ int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t
   if (!rc) e = cudaMalloc(&key->d_key, key->bytes);
   if (!rc && e == cudaSuccess) e = cudaMalloc(&d_words, words.size() * 8);
   if (!rc && e == cudaSuccess)
-    e = cudaMemcpyAsync(d_words, words.data(), words.size() * 8, cudaMemcpyHostToDevice, ring->stream);
+    e = cudaMemcpyAsync(d_words, words.data(), words.size() * 8, cudaMemcpyHostToDevice, ln.stream);
   if (!rc && e == cudaSuccess) {
     // layout: [digit][component][prime][N] == residues of polys in order b_0, a_0, b_1, ...
-    k_words_to_residues<<<blocks_for((long long)(2 * digits * n), 256), 256, 0, ring->stream>>>(
+    k_words_to_residues<<<blocks_for((long long)(2 * digits * n), 256), 256, 0, ln.stream>>>(
         d_words, (long long)(2 * digits), int(L), key->d_key, d);
     e = cudaGetLastError();
   }
-  if (!rc && e == cudaSuccess) e = launch_ntt(ring, d, key->d_key, (long long)(2 * digits * L), 0, int(L), 1, 0);
-  if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ring->stream);
+  if (!rc && e == cudaSuccess) e = launch_ntt(ring, ln, d, key->d_key, (long long)(2 * digits * L), 0, int(L), 1, 0);
+  if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ln.stream);
   if (d_words) cudaFree(d_words);
   if (rc || e != cudaSuccess) {
     cuhe_bfv_key_release(key);
@@ -640,34 +667,34 @@ uint64_t cuhe_bfv_key_bytes(const cuhe_bfv_key* key) { return key ? key->bytes :
 namespace {
 
 // upload fixed-width polys as words and residues (mod the first `primes` primes)
-int upload_polys(cuhe_bfv_ring* r, RingDev* d, const uint8_t* data, size_t polys, size_t primes, u64** d_words,
+int upload_polys(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const uint8_t* data, size_t polys, size_t primes, u64** d_words,
                  u64** d_res) {
   std::vector<u64> words;
   if (int rc = parse_polys(r, data, polys, words)) return rc;
   const size_t n = r->plan.n;
-  *d_words = r->arena.take<u64>(words.size());
-  BFV_ARENA(r->arena);
-  BFV_CUDA(cudaMemcpyAsync(*d_words, words.data(), words.size() * 8, cudaMemcpyHostToDevice, r->stream), "upload");
+  *d_words = ln.arena.take<u64>(words.size());
+  BFV_ARENA(ln.arena);
+  BFV_CUDA(cudaMemcpyAsync(*d_words, words.data(), words.size() * 8, cudaMemcpyHostToDevice, ln.stream), "upload");
   if (d_res) {
-    *d_res = r->arena.take<u64>(polys * primes * n);
-    BFV_ARENA(r->arena);
-    k_words_to_residues<<<blocks_for((long long)(polys * n), 256), 256, 0, r->stream>>>(*d_words, (long long)(polys),
+    *d_res = ln.arena.take<u64>(polys * primes * n);
+    BFV_ARENA(ln.arena);
+    k_words_to_residues<<<blocks_for((long long)(polys * n), 256), 256, 0, ln.stream>>>(*d_words, (long long)(polys),
                                                                                         int(primes), *d_res, d);
     BFV_CUDA(cudaGetLastError(), "residues");
   }
-  BFV_CUDA(cudaStreamSynchronize(r->stream), "upload");
+  BFV_CUDA(cudaStreamSynchronize(ln.stream), "upload");
   return CUHE_OK;
 }
 
-int compose_out(cuhe_bfv_ring* r, RingDev* d, const u64* res, size_t polys, uint8_t* out) {
+int compose_out(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* res, size_t polys, uint8_t* out) {
   const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
-  u64* words = r->arena.take<u64>(polys * n * W);
-  ComposeOp* d_cops = r->arena.take<ComposeOp>(polys);
-  BFV_ARENA(r->arena);
+  u64* words = ln.arena.take<u64>(polys * n * W);
+  ComposeOp* d_cops = ln.arena.take<ComposeOp>(polys);
+  BFV_ARENA(ln.arena);
   std::vector<ComposeOp> cops(polys);
   for (size_t k = 0; k < polys; ++k) cops[k] = ComposeOp{res + k * L * n, words + k * n * W, 1u, 0u};
-  if (int rc = run_switch(r, d, cops, {}, d_cops, nullptr)) return rc;
-  return download_words(r, words, polys, out);
+  if (int rc = run_switch(r, ln, d, cops, {}, d_cops, nullptr)) return rc;
+  return download_words(r, ln, words, polys, out);
 }
 
 }  // namespace
@@ -675,21 +702,22 @@ int compose_out(cuhe_bfv_ring* r, RingDev* d, const u64* res, size_t polys, uint
 int cuhe_bfv_apply_key(cuhe_bfv_key* key, const uint8_t* poly, uint8_t* out) {
   if (!key || !poly || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
   cuhe_bfv_ring* r = key->ring;
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
   const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
-  BFV_CUDA(r->arena.reserve(slice(n * W * 8) * 3 + slice(2 * L * n * 8) * 2 + 4096), "workspace");
-  r->arena.reset();
+  BFV_CUDA(ln.arena.reserve(slice(n * W * 8) * 3 + slice(2 * L * n * 8) * 2 + 4096), "workspace");
+  ln.arena.reset();
   u64* words = nullptr;
-  if (int rc = upload_polys(r, d, poly, 1, L, &words, nullptr)) return rc;
-  u64* res = r->arena.take<u64>(2 * L * n);
-  SwitchOp* d_sops = r->arena.take<SwitchOp>(1);
-  BFV_ARENA(r->arena);
+  if (int rc = upload_polys(r, ln, d, poly, 1, L, &words, nullptr)) return rc;
+  u64* res = ln.arena.take<u64>(2 * L * n);
+  SwitchOp* d_sops = ln.arena.take<SwitchOp>(1);
+  BFV_ARENA(ln.arena);
   std::vector<SwitchOp> sops{SwitchOp{nullptr, nullptr, words, key->d_key, res, 1u, 0u}};
-  if (int rc = run_switch(r, d, {}, sops, nullptr, d_sops)) return rc;
-  return compose_out(r, d, res, 2, out);
+  if (int rc = run_switch(r, ln, d, {}, sops, nullptr, d_sops)) return rc;
+  return compose_out(r, ln, d, res, 2, out);
 }
 
 int cuhe_bfv_rotate_rows(cuhe_bfv_key* key, const uint8_t* ct, uint64_t exponent, uint8_t* out) {
@@ -703,74 +731,77 @@ int cuhe_bfv_rotate_rows(cuhe_bfv_key* key, const uint8_t* ct, uint64_t exponent
     std::memcpy(out, ct, 2 * n * r->plan.coefficient_bytes);
     return CUHE_OK;
   }
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
-  BFV_CUDA(r->arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * L * n * 8) * 3 + slice(n * W * 8) + 8192), "workspace");
-  r->arena.reset();
+  BFV_CUDA(ln.arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * L * n * 8) * 3 + slice(n * W * 8) + 8192), "workspace");
+  ln.arena.reset();
   u64 *words = nullptr, *res = nullptr;
-  if (int rc = upload_polys(r, d, ct, 2, L, &words, &res)) return rc;
-  u64* sw = r->arena.take<u64>(n * W);
-  u64* outres = r->arena.take<u64>(2 * L * n);
-  ComposeOp* d_cops = r->arena.take<ComposeOp>(1);
-  SwitchOp* d_sops = r->arena.take<SwitchOp>(1);
-  BFV_ARENA(r->arena);
+  if (int rc = upload_polys(r, ln, d, ct, 2, L, &words, &res)) return rc;
+  u64* sw = ln.arena.take<u64>(n * W);
+  u64* outres = ln.arena.take<u64>(2 * L * n);
+  ComposeOp* d_cops = ln.arena.take<ComposeOp>(1);
+  SwitchOp* d_sops = ln.arena.take<SwitchOp>(1);
+  BFV_ARENA(ln.arena);
   std::vector<ComposeOp> cops{ComposeOp{res + L * n, sw, unsigned(exponent), 0u}};
   std::vector<SwitchOp> sops{SwitchOp{nullptr, res, sw, key->d_key, outres, inverse_mod_2n(exponent, n), 0u}};
-  if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
-  return compose_out(r, d, outres, 2, out);
+  if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
+  return compose_out(r, ln, d, outres, 2, out);
 }
 
 int cuhe_bfv_ring_product(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* rhs, uint8_t* out) {
   if (!r || !lhs || !rhs || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
   const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
-  BFV_CUDA(r->arena.reserve(slice(n * W * 8) * 4 + slice(L * n * 8) * 3 + 8192), "workspace");
-  r->arena.reset();
+  BFV_CUDA(ln.arena.reserve(slice(n * W * 8) * 4 + slice(L * n * 8) * 3 + 8192), "workspace");
+  ln.arena.reset();
   u64 *wa, *wb, *ra, *rb;
-  if (int rc = upload_polys(r, d, lhs, 1, L, &wa, &ra)) return rc;
-  if (int rc = upload_polys(r, d, rhs, 1, L, &wb, &rb)) return rc;
-  BFV_CUDA(launch_ntt(r, d, ra, (long long)(L), 0, int(L), 1, 0), "ntt");
-  BFV_CUDA(launch_ntt(r, d, rb, (long long)(L), 0, int(L), 1, 0), "ntt");
-  k_mul_plain<<<blocks_for((long long)(L * n), 256), 256, 0, r->stream>>>(ra, (long long)(L), int(L), rb, d);
+  if (int rc = upload_polys(r, ln, d, lhs, 1, L, &wa, &ra)) return rc;
+  if (int rc = upload_polys(r, ln, d, rhs, 1, L, &wb, &rb)) return rc;
+  BFV_CUDA(launch_ntt(r, ln, d, ra, (long long)(L), 0, int(L), 1, 0), "ntt");
+  BFV_CUDA(launch_ntt(r, ln, d, rb, (long long)(L), 0, int(L), 1, 0), "ntt");
+  k_mul_plain<<<blocks_for((long long)(L * n), 256), 256, 0, ln.stream>>>(ra, (long long)(L), int(L), rb, d);
   BFV_CUDA(cudaGetLastError(), "product");
-  BFV_CUDA(launch_ntt(r, d, ra, (long long)(L), 0, int(L), 1, 1), "intt");
-  return compose_out(r, d, ra, 1, out);
+  BFV_CUDA(launch_ntt(r, ln, d, ra, (long long)(L), 0, int(L), 1, 1), "intt");
+  return compose_out(r, ln, d, ra, 1, out);
 }
 
 int cuhe_bfv_multiply(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* rhs, uint64_t t, uint8_t* out) {
   if (!r || !lhs || !out) return fail(CUHE_INVALID_ARGUMENT, "null argument");
   if (t < 2 || t >= (u64(1) << 60) || H::cmp(H::Big(t), r->plan.q) >= 0)
     return fail(CUHE_INVALID_ARGUMENT, "Invalid plaintext modulus");
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, t, &d)) return rc;
   const size_t n = r->plan.n, L = r->plan.residue_count, T = r->plan.tensor_count, W = size_t(r->host_dev.words);
-  BFV_CUDA(r->arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * T * n * 8) * 2 + slice(3 * T * n * 8) +
+  BFV_CUDA(ln.arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * T * n * 8) * 2 + slice(3 * T * n * 8) +
                             slice(3 * L * n * 8) + slice(3 * n * W * 8) + 8192),
            "workspace");
-  r->arena.reset();
+  ln.arena.reset();
   u64 *wa, *ra, *wb = nullptr, *rb = nullptr;
-  if (int rc = upload_polys(r, d, lhs, 2, T, &wa, &ra)) return rc;
+  if (int rc = upload_polys(r, ln, d, lhs, 2, T, &wa, &ra)) return rc;
   if (rhs) {
-    if (int rc = upload_polys(r, d, rhs, 2, T, &wb, &rb)) return rc;
+    if (int rc = upload_polys(r, ln, d, rhs, 2, T, &wb, &rb)) return rc;
   }
-  u64* tens = r->arena.take<u64>(3 * T * n);
-  u64* scaled = r->arena.take<u64>(3 * L * n);
-  BFV_ARENA(r->arena);
-  BFV_CUDA(launch_ntt(r, d, ra, (long long)(2 * T), 0, int(T), 1, 0), "ntt");
-  if (rb) BFV_CUDA(launch_ntt(r, d, rb, (long long)(2 * T), 0, int(T), 1, 0), "ntt");
-  k_tensor<<<blocks_for((long long)(T * n), 256), 256, 0, r->stream>>>(ra, rb ? rb : ra, 1, int(T), tens, d);
+  u64* tens = ln.arena.take<u64>(3 * T * n);
+  u64* scaled = ln.arena.take<u64>(3 * L * n);
+  BFV_ARENA(ln.arena);
+  BFV_CUDA(launch_ntt(r, ln, d, ra, (long long)(2 * T), 0, int(T), 1, 0), "ntt");
+  if (rb) BFV_CUDA(launch_ntt(r, ln, d, rb, (long long)(2 * T), 0, int(T), 1, 0), "ntt");
+  k_tensor<<<blocks_for((long long)(T * n), 256), 256, 0, ln.stream>>>(ra, rb ? rb : ra, 1, int(T), tens, d);
   BFV_CUDA(cudaGetLastError(), "tensor");
-  BFV_CUDA(launch_ntt(r, d, tens, (long long)(3 * T), 0, int(T), 1, 1), "intt");
-  k_rns_scale<<<blocks_for((long long)(3 * n), 128), 128, 0, r->stream>>>(tens, 3, scaled, d);
+  BFV_CUDA(launch_ntt(r, ln, d, tens, (long long)(3 * T), 0, int(T), 1, 1), "intt");
+  k_rns_scale<<<blocks_for((long long)(3 * n), 128), 128, 0, ln.stream>>>(tens, 3, scaled, d);
   BFV_CUDA(cudaGetLastError(), "scale");
-  return compose_out(r, d, scaled, 3, out);
+  return compose_out(r, ln, d, scaled, 3, out);
 }
 
 int cuhe_bfv_hamming_tile(cuhe_bfv_key* relin, const uint8_t* query, const uint8_t* tile, const uint64_t* exponents,
@@ -786,21 +817,22 @@ int cuhe_bfv_hamming_tile(cuhe_bfv_key* relin, const uint8_t* query, const uint8
     if (!(exponents[k] & 1) || exponents[k] >= 2 * n) return fail(CUHE_INVALID_ARGUMENT, "Invalid Galois exponent");
     if (!keys[k] || keys[k]->ring != r) return fail(CUHE_INVALID_ARGUMENT, "Rotation key belongs to another native ring");
   }
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, t, &d)) return rc;
-  BFV_CUDA(r->arena.reserve(tile_arena_bytes(r, 1) + slice(2 * n * W * 8) * 2 + slice(n * W * 8) + slice(L * n * 8) * 2 +
+  BFV_CUDA(ln.arena.reserve(tile_arena_bytes(r, 1) + slice(2 * n * W * 8) * 2 + slice(n * W * 8) + slice(L * n * 8) * 2 +
                             slice(2 * L * n * 8) + slice(2 * n * W * 8) + 16384),
            "workspace");
-  r->arena.reset();
+  ln.arena.reset();
   u64 *qw, *tw, *mw, *mres;
-  if (int rc = upload_polys(r, d, query, 2, 0, &qw, nullptr)) return rc;
-  if (int rc = upload_polys(r, d, tile, 2, 0, &tw, nullptr)) return rc;
-  if (int rc = upload_polys(r, d, mask, 1, L, &mw, &mres)) return rc;
-  BFV_CUDA(launch_ntt(r, d, mres, (long long)(L), 0, int(L), 1, 0), "mask ntt");
-  u64* dist = r->arena.take<u64>(2 * L * n);
-  BFV_ARENA(r->arena);
+  if (int rc = upload_polys(r, ln, d, query, 2, 0, &qw, nullptr)) return rc;
+  if (int rc = upload_polys(r, ln, d, tile, 2, 0, &tw, nullptr)) return rc;
+  if (int rc = upload_polys(r, ln, d, mask, 1, L, &mw, &mres)) return rc;
+  BFV_CUDA(launch_ntt(r, ln, d, mres, (long long)(L), 0, int(L), 1, 0), "mask ntt");
+  u64* dist = ln.arena.take<u64>(2 * L * n);
+  BFV_ARENA(ln.arena);
   TileArgs a;
   a.q_words = qw;
   a.t_words = tw;
@@ -811,8 +843,8 @@ int cuhe_bfv_hamming_tile(cuhe_bfv_key* relin, const uint8_t* query, const uint8
     a.keys.push_back(keys[k]);
   }
   a.masks = {mres};
-  if (int rc = tile_circuit(r, d, a, dist, nullptr)) return rc;
-  return compose_out(r, d, dist, 2, out);
+  if (int rc = tile_circuit(r, ln, d, a, dist, nullptr)) return rc;
+  return compose_out(r, ln, d, dist, 2, out);
 }
 
 int cuhe_bfv_create_server(cuhe_bfv_key* relin, const uint64_t* exponents, cuhe_bfv_key* const* keys, uint64_t count,
@@ -854,7 +886,8 @@ int cuhe_bfv_create_server(cuhe_bfv_key* relin, const uint64_t* exponents, cuhe_
     if (!keymap.count(left.back()) || !keymap.count(right.back()))
       return fail(CUHE_INVALID_ARGUMENT, "Missing native server rotation key");
   }
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, t, &d)) return rc;
@@ -879,7 +912,7 @@ int cuhe_bfv_create_server(cuhe_bfv_key* relin, const uint64_t* exponents, cuhe_
   s->right = right;
   s->d_ring = d;
   const size_t W = size_t(r->host_dev.words);
-  int rc = upload_plain_ntt(r, d, small_to_words(hamming_mask(n, t, lanes, s->capacity), W), &s->d_full_mask);
+  int rc = upload_plain_ntt(r, ln, d, small_to_words(hamming_mask(n, t, lanes, s->capacity), W), &s->d_full_mask);
   cudaError_t e = cudaSuccess;
   if (!rc) e = cudaMalloc(&s->d_target, 8 * std::max<size_t>(1, target.w.size()));
   if (!rc && e == cudaSuccess)
@@ -916,9 +949,20 @@ int cuhe_bfv_server_layout(const cuhe_bfv_server* s, uint64_t* capacity, uint64_
 
 int cuhe_bfv_last_profile(const cuhe_bfv_server* s, double* ms, int capacity) {
   if (!s || !ms) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lock(const_cast<cuhe_bfv_server*>(s)->mu);
   for (int i = 0; i < capacity && i < 6; ++i) ms[i] = s->profile_ms[i];
   return CUHE_OK;
 }
+
+int cuhe_bfv_set_lanes(cuhe_bfv_ring* ring, int lanes) {
+  if (!ring) return fail(CUHE_INVALID_ARGUMENT, "null ring");
+  if (lanes < 1 || lanes > kMaxLanes)
+    return fail(CUHE_INVALID_ARGUMENT, "lane count must be 1.." + std::to_string(kMaxLanes));
+  ring->active_lanes = lanes;
+  return CUHE_OK;
+}
+
+int cuhe_bfv_get_lanes(const cuhe_bfv_ring* ring) { return ring ? ring->active_lanes.load() : 0; }
 
 }  // extern "C"
 
@@ -939,6 +983,43 @@ namespace {
 
 // The Hamming search over tiles given either as packed host bytes (index) or
 // as composed words already resident in HBM (resident).
+// Workspace of one search chunk of ct tiles (whole response groups).
+size_t search_chunk_bytes(const cuhe_bfv_server* s, size_t ct, unsigned out_bits) {
+  const cuhe_bfv_ring* r = s->ring;
+  const auto& P = r->plan;
+  const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
+  const size_t in_bytes = (n * P.q_bits + 7) / 8;
+  const size_t out_words = (n * out_bits + 63) / 64;
+  const size_t gc = (ct + s->padded - 1) / s->padded;
+  return tile_arena_bytes(r, ct) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) + slice(2 * n * W * 8) +
+         slice(ct * 2 * n * W * 8) + slice(ct * 2 * L * n * 8) + slice(gc * 2 * n * W * 8) +
+         slice(gc * 2 * out_words * 8) + slice(sizeof(int)) + slice(ct * n * W * 8) + slice(ct * sizeof(ComposeOp)) +
+         slice(ct * sizeof(SwitchOp)) + 65536;
+}
+
+// Tiles per search chunk: whole response groups, about 1024 tiles.
+size_t search_chunk_tiles(const cuhe_bfv_server* s) {
+  return std::max<size_t>(s->padded, 1024 / s->padded * s->padded);
+}
+
+// A free lane among the active ones (round robin from a rotating start), or
+// else the start lane once it frees up.
+Lane& acquire_lane(cuhe_bfv_ring* r, std::unique_lock<std::mutex>& lock) {
+  const unsigned count = unsigned(std::max(1, std::min(kMaxLanes, r->active_lanes.load())));
+  const unsigned start = r->next_lane++ % count;
+  for (unsigned k = 0; k < count; ++k) {
+    Lane& ln = *r->lanes[(start + k) % count];
+    std::unique_lock<std::mutex> attempt(ln.mu, std::try_to_lock);
+    if (attempt.owns_lock()) {
+      lock = std::move(attempt);
+      return ln;
+    }
+  }
+  Lane& ln = *r->lanes[start];
+  lock = std::unique_lock<std::mutex>(ln.mu);
+  return ln;
+}
+
 int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, const u64* resident,
                 uint64_t tiles, uint64_t count, int compact, uint8_t* out, uint64_t out_capacity,
                 uint64_t* responses) {
@@ -954,17 +1035,19 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
   const size_t groups = (size_t(tiles) + s->padded - 1) / s->padded;
   *responses = 0;
   if (groups * 2 * out_bytes > out_capacity) return fail(CUHE_INVALID_ARGUMENT, "output buffer too small");
-  std::lock_guard<std::mutex> lock(r->mu);
+  std::unique_lock<std::mutex> lock;
+  Lane& ln = acquire_lane(r, lock);
   DeviceGuard guard(r->device);
   RingDev* d = s->d_ring;
-  for (double& v : s->profile_ms) v = 0;
+  double prof[6] = {0, 0, 0, 0, 0, 0};
   // partial mask for the last tile
   const u64* partial = nullptr;
   if (count % s->capacity) {
+    std::lock_guard<std::mutex> masks_lock(s->mu);
     auto it = s->partial_masks.find(size_t(count % s->capacity));
     if (it == s->partial_masks.end()) {
       u64* m = nullptr;
-      if (int rc = upload_plain_ntt(r, d, small_to_words(hamming_mask(n, s->t, s->lanes, size_t(count % s->capacity)), W), &m))
+      if (int rc = upload_plain_ntt(r, ln, d, small_to_words(hamming_mask(n, s->t, s->lanes, size_t(count % s->capacity)), W), &m))
         return rc;
       it = s->partial_masks.emplace(size_t(count % s->capacity), m).first;
     }
@@ -972,43 +1055,39 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
   }
   if (tiles == 0) return CUHE_OK;
   // chunks of whole groups, at most ~1024 tiles each
-  const size_t max_tiles = std::max<size_t>(s->padded, 1024 / s->padded * s->padded);
+  const size_t max_tiles = search_chunk_tiles(s);
   const size_t out_words = (n * out_bits + 63) / 64;
   for (size_t g0 = 0; g0 < groups;) {
     const size_t first = g0 * s->padded;
     size_t ct = std::min<size_t>(size_t(tiles) - first, max_tiles);
     const size_t gc = (ct + s->padded - 1) / s->padded;
     ct = std::min<size_t>(size_t(tiles) - first, gc * s->padded);
-    const size_t need = tile_arena_bytes(r, ct) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) +
-                        slice(2 * n * W * 8) + slice(ct * 2 * n * W * 8) + slice(ct * 2 * L * n * 8) +
-                        slice(gc * 2 * n * W * 8) + slice(gc * 2 * out_words * 8) + slice(sizeof(int)) +
-                        slice(ct * n * W * 8) + slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp)) + 65536;
-    BFV_CUDA(r->arena.reserve(need), "workspace");
-    r->arena.reset();
-    uint8_t* d_qb = r->arena.take<uint8_t>(2 * in_bytes);
-    uint8_t* d_ib = resident ? nullptr : r->arena.take<uint8_t>(ct * 2 * in_bytes);
-    u64* qw = r->arena.take<u64>(2 * n * W);
-    u64* tw = resident ? const_cast<u64*>(resident) + first * 2 * n * W : r->arena.take<u64>(ct * 2 * n * W);
-    u64* dist = r->arena.take<u64>(ct * 2 * L * n);
-    u64* ow = r->arena.take<u64>(gc * 2 * n * W);
-    u64* packed = r->arena.take<u64>(gc * 2 * out_words);
-    int* d_status = r->arena.take<int>(1);
-    BFV_ARENA(r->arena);
-    BFV_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), r->stream), "status");
-    BFV_CUDA(cudaMemcpyAsync(d_qb, query, 2 * in_bytes, cudaMemcpyHostToDevice, r->stream), "query upload");
-    k_unpack<<<blocks_for((long long)(2 * n), 256), 256, 0, r->stream>>>(d_qb, (long long)(in_bytes), int(P.q_bits), 2, qw, d,
+    BFV_CUDA(ln.arena.reserve(search_chunk_bytes(s, ct, out_bits)), "workspace");
+    ln.arena.reset();
+    uint8_t* d_qb = ln.arena.take<uint8_t>(2 * in_bytes);
+    uint8_t* d_ib = resident ? nullptr : ln.arena.take<uint8_t>(ct * 2 * in_bytes);
+    u64* qw = ln.arena.take<u64>(2 * n * W);
+    u64* tw = resident ? const_cast<u64*>(resident) + first * 2 * n * W : ln.arena.take<u64>(ct * 2 * n * W);
+    u64* dist = ln.arena.take<u64>(ct * 2 * L * n);
+    u64* ow = ln.arena.take<u64>(gc * 2 * n * W);
+    u64* packed = ln.arena.take<u64>(gc * 2 * out_words);
+    int* d_status = ln.arena.take<int>(1);
+    BFV_ARENA(ln.arena);
+    BFV_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), ln.stream), "status");
+    BFV_CUDA(cudaMemcpyAsync(d_qb, query, 2 * in_bytes, cudaMemcpyHostToDevice, ln.stream), "query upload");
+    k_unpack<<<blocks_for((long long)(2 * n), 256), 256, 0, ln.stream>>>(d_qb, (long long)(in_bytes), int(P.q_bits), 2, qw, d,
                                                                          d_status);
     if (!resident) {
       BFV_CUDA(cudaMemcpyAsync(d_ib, index + first * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice,
-                               r->stream),
+                               ln.stream),
                "index upload");
-      k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, r->stream>>>(
+      k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(
           d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), tw, d, d_status);
     }
     BFV_CUDA(cudaGetLastError(), "unpack");
     int status = 0;
-    BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, r->stream), "status");
-    BFV_CUDA(cudaStreamSynchronize(r->stream), "unpack");
+    BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
+    BFV_CUDA(cudaStreamSynchronize(ln.stream), "unpack");
     if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
     TileArgs a;
     a.q_words = qw;
@@ -1021,12 +1100,12 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
     }
     a.masks.assign(ct, s->d_full_mask);
     if (partial && first + ct == size_t(tiles)) a.masks[ct - 1] = partial;
-    if (int rc = tile_circuit(r, d, a, dist, s->profile_ms)) return rc;
+    if (int rc = tile_circuit(r, ln, d, a, dist, prof)) return rc;
     // merge tree (bfv_server.h:15-45), executed in waves of independent merges
     cudaEvent_t m0, m1;
     cudaEventCreate(&m0);
     cudaEventCreate(&m1);
-    cudaEventRecord(m0, r->stream);
+    cudaEventRecord(m0, ln.stream);
     struct Merge { size_t left, right; size_t level; size_t wave; };
     std::vector<Merge> merges;
     std::vector<size_t> result_slot;
@@ -1064,10 +1143,10 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
     }
     size_t waves = 0;
     for (const auto& m : merges) waves = std::max(waves, m.wave + 1);
-    u64* mwords = r->arena.take<u64>(std::max<size_t>(1, ct) * n * W);
-    ComposeOp* d_cops = r->arena.take<ComposeOp>(std::max<size_t>(1, ct));
-    SwitchOp* d_sops = r->arena.take<SwitchOp>(std::max<size_t>(1, ct));
-    BFV_ARENA(r->arena);
+    u64* mwords = ln.arena.take<u64>(std::max<size_t>(1, ct) * n * W);
+    ComposeOp* d_cops = ln.arena.take<ComposeOp>(std::max<size_t>(1, ct));
+    SwitchOp* d_sops = ln.arena.take<SwitchOp>(std::max<size_t>(1, ct));
+    BFV_ARENA(ln.arena);
     for (size_t w = 0; w < waves; ++w) {
       std::vector<ComposeOp> cops;
       std::vector<SwitchOp> sops;
@@ -1079,34 +1158,34 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
         sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, s->keys.at(g)->d_key,
                                 dist + m.left * 2 * L * n, inverse_mod_2n(g, n), 0u});
       }
-      if (int rc = run_switch(r, d, cops, sops, d_cops, d_sops)) return rc;
+      if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
     }
-    cudaEventRecord(m1, r->stream);
+    cudaEventRecord(m1, ln.stream);
     // outputs: compose, optional compaction, packing
     std::vector<ComposeOp> cops;
     for (size_t gi = 0; gi < gc; ++gi)
       for (size_t comp = 0; comp < 2; ++comp)
         cops.push_back(ComposeOp{dist + (result_slot[gi] * 2 + comp) * L * n, ow + (gi * 2 + comp) * n * W, 1u, 0u});
-    if (int rc = run_switch(r, d, cops, {}, d_cops, nullptr)) return rc;
+    if (int rc = run_switch(r, ln, d, cops, {}, d_cops, nullptr)) return rc;
     if (compact) {
-      k_compact<<<blocks_for((long long)(gc * 2 * n), 128), 128, 0, r->stream>>>(ow, (long long)(gc * 2 * n), s->d_target,
+      k_compact<<<blocks_for((long long)(gc * 2 * n), 128), 128, 0, ln.stream>>>(ow, (long long)(gc * 2 * n), s->d_target,
                                                                                  int(s->target_words.size()), d);
       BFV_CUDA(cudaGetLastError(), "compact");
     }
-    k_pack<<<blocks_for((long long)(gc * 2 * out_words), 256), 256, 0, r->stream>>>(ow, int(W), int(n), int(out_bits),
+    k_pack<<<blocks_for((long long)(gc * 2 * out_words), 256), 256, 0, ln.stream>>>(ow, int(W), int(n), int(out_bits),
                                                                                    int(gc * 2), packed, (long long)(out_words));
     BFV_CUDA(cudaGetLastError(), "pack");
     std::vector<u64> host(gc * 2 * out_words);
-    BFV_CUDA(cudaMemcpyAsync(host.data(), packed, host.size() * 8, cudaMemcpyDeviceToHost, r->stream), "download");
+    BFV_CUDA(cudaMemcpyAsync(host.data(), packed, host.size() * 8, cudaMemcpyDeviceToHost, ln.stream), "download");
     cudaEvent_t o1;
     cudaEventCreate(&o1);
-    cudaEventRecord(o1, r->stream);
-    BFV_CUDA(cudaStreamSynchronize(r->stream), "search");
+    cudaEventRecord(o1, ln.stream);
+    BFV_CUDA(cudaStreamSynchronize(ln.stream), "search");
     float x = 0;
     cudaEventElapsedTime(&x, m0, m1);
-    s->profile_ms[4] += x;
+    prof[4] += x;
     cudaEventElapsedTime(&x, m1, o1);
-    s->profile_ms[5] += x;
+    prof[5] += x;
     cudaEventDestroy(m0);
     cudaEventDestroy(m1);
     cudaEventDestroy(o1);
@@ -1116,6 +1195,8 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
     g0 += gc;
   }
   *responses = groups;
+  std::lock_guard<std::mutex> profile_lock(s->mu);
+  std::copy(prof, prof + 6, s->profile_ms);
   return CUHE_OK;
 }
 
@@ -1135,7 +1216,8 @@ int cuhe_bfv_upload_index(cuhe_bfv_server* s, const uint8_t* index, uint64_t til
   const auto& P = r->plan;
   const size_t n = P.n, W = size_t(r->host_dev.words);
   const size_t in_bytes = (n * P.q_bits + 7) / 8;
-  std::lock_guard<std::mutex> lock(r->mu);
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
   DeviceGuard guard(r->device);
   auto* idx = new (std::nothrow) cuhe_bfv_index();
   if (!idx) return fail(CUHE_OUT_OF_MEMORY, "index allocation");
@@ -1150,21 +1232,21 @@ int cuhe_bfv_upload_index(cuhe_bfv_server* s, const uint8_t* index, uint64_t til
       return fail(CUHE_OUT_OF_MEMORY, "index does not fit in device memory");
     }
     const size_t need = slice(chunk * 2 * in_bytes) + slice(sizeof(int));
-    if (r->arena.reserve(need) != cudaSuccess) {
+    if (ln.arena.reserve(need) != cudaSuccess) {
       delete idx;
       return fail(CUHE_OUT_OF_MEMORY, "workspace");
     }
-    r->arena.reset();
-    uint8_t* d_ib = r->arena.take<uint8_t>(chunk * 2 * in_bytes);
-    int* d_status = r->arena.take<int>(1);
-    if (r->arena.overflow) { delete idx; return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted"); }
-    cudaMemsetAsync(d_status, 0, sizeof(int), r->stream);
+    ln.arena.reset();
+    uint8_t* d_ib = ln.arena.take<uint8_t>(chunk * 2 * in_bytes);
+    int* d_status = ln.arena.take<int>(1);
+    if (ln.arena.overflow) { delete idx; return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted"); }
+    cudaMemsetAsync(d_status, 0, sizeof(int), ln.stream);
     for (size_t t0 = 0; t0 < tiles; t0 += chunk) {
       const size_t ct = std::min<size_t>(chunk, size_t(tiles) - t0);
-      cudaMemcpyAsync(d_ib, index + t0 * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice, r->stream);
-      k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, r->stream>>>(
+      cudaMemcpyAsync(d_ib, index + t0 * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice, ln.stream);
+      k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(
           d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), idx->d_words + t0 * 2 * n * W, s->d_ring, d_status);
-      cudaStreamSynchronize(r->stream);  // the staging slice is reused by the next chunk
+      cudaStreamSynchronize(ln.stream);  // the staging slice is reused by the next chunk
     }
     int status = 0;
     cudaError_t e = cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
@@ -1181,6 +1263,12 @@ int cuhe_bfv_search_index(cuhe_bfv_server* s, cuhe_bfv_index* index, const uint8
                           int compact, uint8_t* out, uint64_t out_capacity, uint64_t* responses) {
   if (!index || index->server != s) return fail(CUHE_INVALID_ARGUMENT, "index belongs to another server");
   return search_impl(s, query, nullptr, index->d_words, index->tiles, count, compact, out, out_capacity, responses);
+}
+
+uint64_t cuhe_bfv_search_workspace(const cuhe_bfv_server* s, uint64_t tiles, int compact) {
+  if (!s || !tiles) return 0;
+  const size_t ct = std::min<size_t>(size_t(tiles), search_chunk_tiles(s));
+  return search_chunk_bytes(s, ct, compact ? s->target_bits : unsigned(s->ring->plan.q_bits));
 }
 
 }  // extern "C"

@@ -98,6 +98,24 @@ int cuhe_bfv_search_index(cuhe_bfv_server* server, cuhe_bfv_index* index, const 
  * output.  No counterpart in the reference; it feeds the profile_* calls. */
 int cuhe_bfv_last_profile(const cuhe_bfv_server* server, double* ms, int capacity);
 
+/* Execution lanes of a ring (1..8; 1 after create_ring).  Each lane is a
+ * CUDA stream with its own device workspace.  packed_search / search_index
+ * calls issued concurrently from several host threads take free lanes and
+ * overlap on the GPU; every other call runs on lane 0.  Lane streams have
+ * the device's highest stream priority, so a search's short dependent
+ * kernels are scheduled ahead of queued blocks of bulk work on
+ * default-priority streams.  Each lane keeps the workspace of the largest
+ * search it ran until the ring is released.  No
+ * counterpart in the reference, whose calls release the GIL but run on the
+ * host (src/cuhepy/bfv/_cpu_ext/bindings.cpp:20-23). */
+int cuhe_bfv_set_lanes(cuhe_bfv_ring* ring, int lanes);
+int cuhe_bfv_get_lanes(const cuhe_bfv_ring* ring);
+/* Device workspace (bytes) one lane holds for a search over `tiles` tiles:
+ * searches run in chunks of about 1024 tiles, so this is the size of the
+ * largest chunk (about 4.4 GB at N = 8192, L = 3, K = 7 for 1024 tiles).
+ * Serving code admits a search when this fits in free device memory. */
+uint64_t cuhe_bfv_search_workspace(const cuhe_bfv_server* server, uint64_t tiles, int compact);
+
 #ifdef __cplusplus
 }
 #endif
