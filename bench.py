@@ -386,6 +386,8 @@ def run_gpu(args) -> dict | None:
     }
     if not args.no_bfv:
         result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
+    if not args.no_mixed and world == 1:
+        result["mixed"] = run_mixed()
     if not args.no_serving and world == 1:
         del prod, dist_out, index_ct, flush  # the serving section needs the HBM
         torch.cuda.empty_cache()
@@ -687,6 +689,89 @@ def run_reference(args) -> dict | None:
     }
 
 
+def run_mixed(steps: int = 5, seed: int = 5) -> dict:
+    """Batched uneven mix: Paillier fixed-exponent exponentiations r^n at two
+    widths (n^2 2048-bit and 4096-bit, four keys each) with 1,000-50,000
+    bases per key drawn log-uniform, plus BFV NTT / INTT batches at
+    N = 4096 / 8192 / 16384 with 2-8 RNS limbs, in one CUDA-graph launch
+    (persistent work-stealing Paillier kernels, NTTs on a forked stream)
+    against one launch per operation; both with the autotuned variants."""
+    import torch
+
+    from cuhepy_b200.batch import MixedBatch
+    from cuhepy_b200.bfv import _bfv_rns as m
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+    from oracle import bfv as ob
+
+    rng = random.Random(seed)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    mb = MixedBatch()
+    modexps, ntts = 0, 0
+    keys = []
+    for bits in (1024, 2048):  # n bits: n^2 2048 and 4096
+        for k in range(4):
+            p = (1 << (bits // 2 - 1)) + 2 * rng.getrandbits(bits // 2 - 3) + 1
+            q = (1 << (bits // 2 - 1)) + 2 * rng.getrandbits(bits // 2 - 3) + 1
+            n = p * q | 1  # odd modulus of the width; primality does not change the work
+            ctx = PaillierDevice(n)
+            count = int(round(math.exp(rng.uniform(math.log(1000), math.log(50000)))))
+            # uniform bases below n^2, drawn on the device
+            words = ctx.words
+            raw = torch.randint(0, 1 << 31, (count, words), dtype=torch.int32, device="cuda", generator=gen)
+            raw[:, words - 1] = 0  # below 2^(32(K-1)) < n^2
+            mb.add_modexp(ctx, raw, n)
+            keys.append({"n_squared_bits": (n * n).bit_length(), "count": count})
+            modexps += count
+    ntt_batches = []
+    for k, n in enumerate((4096, 8192, 16384) * 2):
+        limbs = rng.randint(2, 8)
+        qm = 1
+        for pr in ob.rns_primes(n, 60 * limbs):
+            qm *= pr
+        ring = m.create_ring(n, format(qm, "x"), 30, True, True, 2)
+        primes = m.ring_info(ring)["primes"][:limbs]
+        planes = torch.randint(0, 1 << 59, (64 * limbs, n), dtype=torch.int64, device="cuda", generator=gen)
+        inverse = k >= 3
+        mb.add_ntt(ring, planes, limbs, inverse=inverse)
+        ntt_batches.append({"n": n, "limbs": limbs, "planes": 64 * limbs, "inverse": inverse})
+        ntts += 64 * limbs
+    tune = mb.autotune(reps=1)
+    mb.capture()
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        mb.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        mb.replay()
+    b.record(stream)
+    b.synchronize()
+    graph_ms = a.elapsed_time(b) / steps
+    mb.check()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        mb.run_plain()
+    plain_ms = (time.perf_counter() - t0) * 1e3 / steps
+    widths = mb.widths()
+    mb.close()
+    return {
+        "workload": "mixed_uneven_batch",
+        "metric": "modexp/s (r^n mod n^2) and NTT planes/s of the mix, one graph launch vs one launch per op",
+        "graph_ms": graph_ms, "plain_ms": plain_ms, "speedup": plain_ms / graph_ms,
+        "modexps": modexps, "ntt_planes": ntts,
+        "graph_modexp_per_s": modexps / (graph_ms / 1e3), "plain_modexp_per_s": modexps / (plain_ms / 1e3),
+        "keys": keys, "ntt_batches": ntt_batches,
+        "paillier_widths": widths,
+        "autotune": {"paillier": {str(k): v["best"] for k, v in tune["paillier"].items()},
+                     "ntt": {str(k): {"threads": v["best"][0], "radix": 1 << v["best"][1]}
+                             for k, v in tune["ntt"].items()}},
+        "note": "graph time: CUDA events around replays; plain: host wall clock around per-op launches, "
+                "each waited for",
+    }
+
+
 SERVE_VECTORS = 1 << 20
 SERVE_REQUESTS = 48
 SERVE_EMBEDS = (256, 512, 1024)
@@ -899,6 +984,8 @@ def main() -> None:
     parser.add_argument("--no-bfv", action="store_true", help="skip the BFV kNN section")
     parser.add_argument("--no-serving", action="store_true", help="skip the serving section")
     parser.add_argument("--serving-only", action="store_true", help="run only the serving section")
+    parser.add_argument("--mixed-only", action="store_true", help="run only the mixed-batch section")
+    parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
     parser.add_argument("--profile-case", choices=["paillier", "bfv"],
                         help="run one small step of a hot kernel (for ncu captures) and exit")
     args = parser.parse_args()
@@ -907,6 +994,9 @@ def main() -> None:
         return
     if args.serving_only:
         print(json.dumps(run_serving()))
+        return
+    if args.mixed_only:
+        print(json.dumps(run_mixed()))
         return
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -71,6 +71,20 @@ PAILLIER_SIGNATURES: dict[str, tuple] = {
     "cuhe_window_schedule": (ctypes.c_int, [c_u32_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.c_int]),
     "cuhe_paillier_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "cuhe_mix_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "cuhe_mix_destroy": (None, [ctypes.c_void_p]),
+    "cuhe_mix_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "cuhe_mix_add_modexp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_int64, c_u32_p, ctypes.c_int]),
+    "cuhe_mix_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "cuhe_mix_plan": (ctypes.c_int, [ctypes.c_void_p]),
+    "cuhe_mix_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cuhe_mix_check": (ctypes.c_int, [ctypes.c_void_p]),
+    "cuhe_mix_widths": (ctypes.c_int, [ctypes.c_void_p]),
+    "cuhe_mix_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
+                                     ctypes.POINTER(ctypes.c_int)]),
     "cuhe_paillier_get_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
                                                 ctypes.POINTER(ctypes.c_int)]),
 }

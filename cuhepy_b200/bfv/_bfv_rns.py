@@ -54,6 +54,8 @@ BFV_SIGNATURES: dict[str, tuple] = {
     "cuhe_bfv_search_index": (ctypes.c_int, [_vp, _vp, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, _vp,
                                              ctypes.c_uint64, _u64p]),
     "cuhe_bfv_set_lanes": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cuhe_bfv_ntt": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, _vp]),
     "cuhe_bfv_get_lanes": (ctypes.c_int, [_vp]),
     "cuhe_bfv_search_workspace": (ctypes.c_uint64, [_vp, ctypes.c_uint64, ctypes.c_int]),
 }
@@ -367,6 +369,25 @@ def search_index(server: Server, index: ResidentIndex, query: Any, count: int,
     raw = out.raw
     return [(raw[(2 * i) * size:(2 * i + 1) * size], raw[(2 * i + 1) * size:(2 * i + 2) * size])
             for i in range(responses.value)]
+
+
+def ntt(ring: Ring, planes, primes: int, inverse: bool = False, threads: int = 0, radix_log: int = 0,
+        stream: int | None = None) -> None:
+    """In-place batched NTT of device planes ([count, N] 64-bit residues, a
+    torch CUDA tensor; plane b mod the ring's prime b % primes), enqueued on
+    `stream` (a cudaStream_t as int; None: the current torch stream) without
+    synchronising, so it can be captured in a CUDA graph (not in the
+    reference API)."""
+    import torch
+
+    ring = _get(ring, Ring)
+    if not (isinstance(planes, torch.Tensor) and planes.is_cuda and planes.dim() == 2
+            and planes.shape[1] == ring.n and planes.element_size() == 8 and planes.is_contiguous()):
+        raise ValueError("planes must be a contiguous CUDA tensor [count, N] of 64-bit words")
+    if stream is None:
+        stream = torch.cuda.current_stream(planes.device).cuda_stream
+    _check(lib().cuhe_bfv_ntt(ring.ptr, planes.data_ptr(), planes.shape[0], int(primes), int(bool(inverse)),
+                              int(threads), int(radix_log), _vp(stream)))
 
 
 def set_lanes(ring: Ring, lanes: int) -> None:

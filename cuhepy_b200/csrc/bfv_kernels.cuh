@@ -145,11 +145,12 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
 }
 
 // Whole transforms over a padded shared-memory plane (all threads of the CTA).
-__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j) {
+// max_p (1..4) caps the stages per register pass (radix 2^max_p).
+__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4) {
   const int logn = R.logn;
   const u64 p = R.prime[j].p;
-  for (int s0 = 0; s0 < logn; s0 += 4) {
-    const int P = logn - s0 < 4 ? logn - s0 : 4;
+  for (int s0 = 0; s0 < logn; s0 += max_p) {
+    const int P = logn - s0 < max_p ? logn - s0 : max_p;
     const bool last = s0 + P == logn;
     switch (P) {
       case 4: ntt_forward_pass<4>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
@@ -161,11 +162,11 @@ __device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j
   }
 }
 
-__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j) {
+__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j, int max_p = 4) {
   const int logn = R.logn;
   const u64 p = R.prime[j].p;
-  for (int u0 = 0; u0 < logn; u0 += 4) {
-    const int P = logn - u0 < 4 ? logn - u0 : 4;
+  for (int u0 = 0; u0 < logn; u0 += max_p) {
+    const int P = logn - u0 < max_p ? logn - u0 : max_p;
     switch (P) {
       case 4: ntt_inverse_pass<4>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
       case 3: ntt_inverse_pass<3>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
@@ -238,7 +239,7 @@ __device__ __forceinline__ void ntt_inverse_smem(u64* a, const RingDev& R, int j
 // Batched transform: plane b of `data` (stride n) uses prime prime_of(b).
 // prime = (b / prime_block) % prime_mod + prime_base.
 __global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block,
-                      int inverse) {
+                      int inverse, int max_p = 4) {
   extern __shared__ __align__(16) u64 s_plane[];
   const RingDev& R = *ring;
   const int n = R.n;
@@ -247,8 +248,8 @@ __global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_bas
   u64* plane = data + b * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[sp(i)] = plane[i];
   __syncthreads();
-  if (inverse) ntt_inverse_fast(s_plane, R, j);
-  else ntt_forward_fast(s_plane, R, j);
+  if (inverse) ntt_inverse_fast(s_plane, R, j, max_p);
+  else ntt_forward_fast(s_plane, R, j, max_p);
   for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[sp(i)];
 }
 

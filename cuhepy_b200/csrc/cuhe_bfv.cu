@@ -264,13 +264,29 @@ unsigned blocks_for(long long items, int threads) { return unsigned((items + thr
 
 size_t ntt_smem(const cuhe_bfv_ring* r) { return plane_smem_words(int(r->plan.n)) * sizeof(u64); }
 
+// Largest CTA k_ntt can launch with (its register use bounds it below 1024).
+int ntt_max_threads() {
+  static int cached = 0;
+  if (!cached) {
+    cudaFuncAttributes attr{};
+    cached = cudaFuncGetAttributes(&attr, k_ntt) == cudaSuccess ? attr.maxThreadsPerBlock : 256;
+  }
+  return cached;
+}
+
+// Default CTA size of an N-point transform: one radix-16 block per thread.
+int ntt_default_threads(size_t n) {
+  const int want = int(std::min<size_t>(1024, std::max<size_t>(32, n / 16)));
+  return std::min(want, ntt_max_threads() / 32 * 32);
+}
+
 cudaError_t launch_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
                        int prime_block, int inverse) {
   if (planes <= 0) return cudaSuccess;
   const size_t smem = ntt_smem(r);
   cudaError_t e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
-  const int threads = int(std::min<size_t>(1024, std::max<size_t>(32, r->plan.n / 16)));
+  const int threads = ntt_default_threads(r->plan.n);
   k_ntt<<<unsigned(planes), threads, smem, ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse);
   return cudaGetLastError();
 }
@@ -593,7 +609,37 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
     delete r;
     return rc;
   }
+  // k_ntt's shared-memory size for the largest supported plane, once, so
+  // that cuhe_bfv_ntt needs no attribute call (it may run under capture)
+  e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(plane_smem_words(16384) * sizeof(u64)));
+  if (e != cudaSuccess) {
+    delete r;
+    return fail(CUHE_CUDA_ERROR, std::string("ring setup: ") + cudaGetErrorString(e));
+  }
   *out = r;
+  return CUHE_OK;
+}
+
+int cuhe_bfv_ntt(cuhe_bfv_ring* r, uint64_t* planes_dev, uint64_t planes, int primes, int inverse, int threads,
+                 int radix_log, void* stream) {
+  if (!r || (planes && !planes_dev)) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  const auto& P = r->plan;
+  if (primes < 1 || size_t(primes) > P.primes.size())
+    return fail(CUHE_INVALID_ARGUMENT, "prime count outside the ring's primes");
+  if (threads == 0) threads = ntt_default_threads(P.n);
+  if (radix_log == 0) radix_log = 4;
+  if (threads < 32 || threads > ntt_max_threads() || threads % 32 || radix_log < 1 || radix_log > 4)
+    return fail(CUHE_INVALID_ARGUMENT, "threads must be a multiple of 32 from 32 to " +
+                                           std::to_string(ntt_max_threads()) + ", radix_log 1..4");
+  if (planes == 0) return CUHE_OK;
+  if (planes > (uint64_t(1) << 31) - 1) return fail(CUHE_INVALID_ARGUMENT, "too many planes for one launch");
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, 0, &d)) return rc;
+  k_ntt<<<unsigned(planes), threads, ntt_smem(r), static_cast<cudaStream_t>(stream)>>>(
+      reinterpret_cast<u64*>(planes_dev), d, 0, primes, 1, inverse ? 1 : 0, radix_log);
+  BFV_CUDA(cudaGetLastError(), "ntt launch");
   return CUHE_OK;
 }
 

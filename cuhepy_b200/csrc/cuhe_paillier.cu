@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -248,6 +249,32 @@ cudaError_t launch_table_rows(cuhe_paillier* ctx, const uint32_t* bases, int row
   return cudaGetLastError();
 }
 
+// Persistent mixed launch: shared memory attribute and a grid of one wave of
+// resident CTAs (SMs x CTAs per SM).
+template <int K, int TPI, int W>
+cudaError_t prepare_tasks(int device, int* grid) {
+  const size_t smem = modexp_smem<K, TPI, W>();
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp_tasks<K, TPI, W>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cuhe::k_modexp_tasks<K, TPI, W>, cuhe::kBlockThreads,
+                                                    smem);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  *grid = std::max(1, per_sm) * sms;
+  return cudaSuccess;
+}
+
+template <int K, int TPI, int W>
+cudaError_t launch_tasks(const cuhe::ModexpTask* tasks, int ntasks, long long units, unsigned long long* counter,
+                         int* status, int grid, cudaStream_t stream) {
+  cuhe::k_modexp_tasks<K, TPI, W><<<grid, cuhe::kBlockThreads, modexp_smem<K, TPI, W>(), stream>>>(
+      tasks, ntasks, units, counter, status);
+  return cudaGetLastError();
+}
+
 // Runtime dispatch over the compiled variants.
 struct Dispatch {
   cudaError_t (*modexp)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long, const int32_t*,
@@ -260,6 +287,9 @@ struct Dispatch {
   cudaError_t (*lookup)(cuhe_paillier*, const uint8_t*, int, int, int, const uint32_t*, long long, const uint8_t*,
                         uint32_t*) = nullptr;
   cudaError_t (*table_rows)(cuhe_paillier*, const uint32_t*, int, uint32_t*) = nullptr;
+  cudaError_t (*prepare_tasks)(int, int*) = nullptr;
+  cudaError_t (*launch_tasks)(const cuhe::ModexpTask*, int, long long, unsigned long long*, int*, int,
+                              cudaStream_t) = nullptr;
 };
 
 bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
@@ -273,6 +303,8 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
     d->outer = &launch_outer<k, t>;                                \
     d->lookup = &launch_lookup<k, t>;                              \
     d->table_rows = &launch_table_rows<k, t>;                      \
+    d->prepare_tasks = &prepare_tasks<k, t, w>;                    \
+    d->launch_tasks = &launch_tasks<k, t, w>;                      \
     return true;                                                   \
   }
   CUHE_VARIANTS(CUHE_MATCH)
@@ -1084,5 +1116,224 @@ int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t coun
   if (int rc = st.finish()) return rc;
   return check_status(ctx, st.staged());
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Mixed batches: many (key, exponent, bases) exponentiations of uneven sizes
+// and widths in one persistent launch per width.
+// ---------------------------------------------------------------------------
+struct cuhe_mix {
+  struct Entry {
+    cuhe_paillier* ctx;
+    const uint32_t* base;
+    uint32_t* out;
+    long long count;
+    Limbs exponent;
+  };
+  struct Width {
+    int K = 0, tpi = 0, window = 0, grid = 0, ntasks = 0;
+    long long units = 0;
+    cuhe::ModexpTask* d_tasks = nullptr;
+    std::vector<int32_t*> d_ops;
+    Dispatch d;
+  };
+  int device = 0;
+  std::vector<Entry> entries;
+  std::map<int, std::pair<int, int>> tuning;  // K -> (tpi, window)
+  std::vector<Width> widths;
+  unsigned long long* d_counters = nullptr;
+  int* d_status = nullptr;
+  bool planned = false;
+  std::string error;
+
+  void release_plan() {
+    for (auto& w : widths) {
+      cudaFree(w.d_tasks);
+      for (int32_t* p : w.d_ops) cudaFree(p);
+    }
+    widths.clear();
+    cudaFree(d_counters);
+    d_counters = nullptr;
+    planned = false;
+  }
+};
+
+namespace {
+int mix_fail(cuhe_mix* mix, int code, const std::string& msg) {
+  if (mix) mix->error = msg; else g_create_error = msg;
+  return code;
+}
+}  // namespace
+
+extern "C" {
+
+const char* cuhe_mix_last_error(const cuhe_mix* mix) { return mix ? mix->error.c_str() : g_create_error.c_str(); }
+
+int cuhe_mix_create(int device, cuhe_mix** out) {
+  if (!out) return mix_fail(nullptr, CUHE_INVALID_ARGUMENT, "null output");
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    return mix_fail(nullptr, CUHE_INVALID_ARGUMENT, "invalid device ordinal");
+  }
+  auto* mix = new (std::nothrow) cuhe_mix();
+  if (!mix) return mix_fail(nullptr, CUHE_OUT_OF_MEMORY, "mix allocation");
+  mix->device = device;
+  DeviceGuard guard(device);
+  if (cudaMalloc(&mix->d_status, sizeof(int)) != cudaSuccess || cudaMemset(mix->d_status, 0, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    delete mix;
+    return mix_fail(nullptr, CUHE_OUT_OF_MEMORY, "mix status allocation");
+  }
+  *out = mix;
+  return CUHE_OK;
+}
+
+void cuhe_mix_destroy(cuhe_mix* mix) {
+  if (!mix) return;
+  DeviceGuard guard(mix->device);
+  cudaDeviceSynchronize();
+  mix->release_plan();
+  cudaFree(mix->d_status);
+  delete mix;
+}
+
+int cuhe_mix_add_modexp(cuhe_mix* mix, cuhe_paillier* ctx, const uint32_t* base, uint32_t* out, int64_t count,
+                        const uint32_t* exponent, int exponent_words) {
+  if (!mix || !ctx || !exponent || exponent_words <= 0 || count < 0)
+    return mix_fail(mix, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (ctx->device != mix->device) return mix_fail(mix, CUHE_INVALID_ARGUMENT, "context on another device");
+  if (count == 0) return CUHE_OK;
+  DeviceGuard guard(mix->device);
+  if (!is_device_pointer(base) || !is_device_pointer(out))
+    return mix_fail(mix, CUHE_INVALID_ARGUMENT, "mixed batches take device buffers");
+  if (!cuhe::host::fits(exponent, size_t(exponent_words), size_t(ctx->K)))
+    return mix_fail(mix, CUHE_INVALID_ARGUMENT, "exponent wider than n^2");
+  mix->entries.push_back({ctx, base, out, count, cuhe::host::resized(exponent, size_t(exponent_words), size_t(ctx->K))});
+  mix->planned = false;
+  return CUHE_OK;
+}
+
+int cuhe_mix_set_tuning(cuhe_mix* mix, int words, int tpi, int window) {
+  if (!mix) return CUHE_INVALID_ARGUMENT;
+  Dispatch d;
+  if (!find_dispatch(words, tpi, window, &d))
+    return mix_fail(mix, CUHE_INVALID_ARGUMENT, "tuning (threads per instance, window) not compiled for this width");
+  mix->tuning[words] = {tpi, window};
+  mix->planned = false;
+  return CUHE_OK;
+}
+
+int cuhe_mix_plan(cuhe_mix* mix) {
+  if (!mix) return CUHE_INVALID_ARGUMENT;
+  DeviceGuard guard(mix->device);
+  cudaDeviceSynchronize();
+  mix->release_plan();
+  std::map<int, std::vector<size_t>> by_width;
+  for (size_t i = 0; i < mix->entries.size(); ++i) by_width[mix->entries[i].ctx->K].push_back(i);
+  for (auto& kv : by_width) {
+    cuhe_mix::Width w;
+    w.K = kv.first;
+    auto it = mix->tuning.find(w.K);
+    if (it != mix->tuning.end()) {
+      w.tpi = it->second.first;
+      w.window = it->second.second;
+    } else {
+      default_tuning(w.K, &w.tpi, &w.window);
+    }
+    if (!find_dispatch(w.K, w.tpi, w.window, &w.d)) return mix_fail(mix, CUHE_INVALID_ARGUMENT, "no compiled variant");
+    const long long ipb = cuhe::kBlockThreads / w.tpi;
+    std::vector<cuhe::ModexpTask> tasks;
+    for (size_t i : kv.second) {
+      const auto& e = mix->entries[i];
+      std::vector<int32_t> ops = cuhe::host::window_schedule(e.exponent, w.window);
+      int32_t* d_ops = nullptr;
+      if (!ops.empty()) {
+        if (cudaMalloc(&d_ops, ops.size() * 4) != cudaSuccess ||
+            cudaMemcpy(d_ops, ops.data(), ops.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+          cudaGetLastError();
+          cudaFree(d_ops);
+          return mix_fail(mix, CUHE_OUT_OF_MEMORY, "schedule upload");
+        }
+        w.d_ops.push_back(d_ops);
+      }
+      cuhe::ModexpTask t{};
+      t.base = e.base;
+      t.out = e.out;
+      t.count = e.count;
+      t.consts = e.ctx->d_consts;
+      t.ops = d_ops;
+      t.first_unit = w.units;
+      t.ks = e.ctx->ks;
+      t.nops = int(ops.size());
+      t.mode = cuhe::EXP_POW;
+      tasks.push_back(t);
+      w.units += (e.count + ipb - 1) / ipb;
+    }
+    w.ntasks = int(tasks.size());
+    if (cudaMalloc(&w.d_tasks, tasks.size() * sizeof(cuhe::ModexpTask)) != cudaSuccess ||
+        cudaMemcpy(w.d_tasks, tasks.data(), tasks.size() * sizeof(cuhe::ModexpTask), cudaMemcpyHostToDevice) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      return mix_fail(mix, CUHE_OUT_OF_MEMORY, "task table upload");
+    }
+    cudaError_t e = w.d.prepare_tasks(mix->device, &w.grid);
+    if (e != cudaSuccess) return mix_fail(mix, CUHE_CUDA_ERROR, std::string("mixed launch setup: ") + cudaGetErrorString(e));
+    mix->widths.push_back(std::move(w));
+  }
+  if (!mix->widths.empty() &&
+      cudaMalloc(&mix->d_counters, mix->widths.size() * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return mix_fail(mix, CUHE_OUT_OF_MEMORY, "counter allocation");
+  }
+  mix->planned = true;
+  return CUHE_OK;
+}
+
+int cuhe_mix_launch(cuhe_mix* mix, void* stream) {
+  if (!mix) return CUHE_INVALID_ARGUMENT;
+  if (!mix->planned) return mix_fail(mix, CUHE_NOT_READY, "mixed batch not planned");
+  if (mix->widths.empty()) return CUHE_OK;
+  DeviceGuard guard(mix->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(mix->d_counters, 0, mix->widths.size() * sizeof(unsigned long long), s);
+  for (size_t i = 0; i < mix->widths.size() && e == cudaSuccess; ++i) {
+    const auto& w = mix->widths[i];
+    e = w.d.launch_tasks(w.d_tasks, w.ntasks, w.units, mix->d_counters + i, mix->d_status, w.grid, s);
+  }
+  if (e != cudaSuccess) return mix_fail(mix, CUHE_CUDA_ERROR, std::string("mixed launch: ") + cudaGetErrorString(e));
+  return CUHE_OK;
+}
+
+int cuhe_mix_check(cuhe_mix* mix) {
+  if (!mix) return CUHE_INVALID_ARGUMENT;
+  DeviceGuard guard(mix->device);
+  int status = 0;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&status, mix->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return mix_fail(mix, CUHE_CUDA_ERROR, std::string("mixed batch: ") + cudaGetErrorString(e));
+  if (status) {
+    cudaMemset(mix->d_status, 0, sizeof(int));
+    return mix_fail(mix, CUHE_RANGE, "input outside its valid range (base >= n^2)");
+  }
+  return CUHE_OK;
+}
+
+int cuhe_mix_info(const cuhe_mix* mix, int index, int* words, int* tpi, int* window, int* grid, int64_t* units,
+                  int* tasks) {
+  if (!mix || index < 0 || size_t(index) >= mix->widths.size()) return CUHE_INVALID_ARGUMENT;
+  const auto& w = mix->widths[size_t(index)];
+  if (words) *words = w.K;
+  if (tpi) *tpi = w.tpi;
+  if (window) *window = w.window;
+  if (grid) *grid = w.grid;
+  if (units) *units = w.units;
+  if (tasks) *tasks = w.ntasks;
+  return CUHE_OK;
+}
+
+int cuhe_mix_widths(const cuhe_mix* mix) { return mix ? int(mix->widths.size()) : 0; }
 
 }  // extern "C"

@@ -219,11 +219,15 @@ __device__ __forceinline__ void decrypt_epilogue(const Group<K, TPI>& g, uint32_
 //   EXP_DECODE  out32 = popcount of the even bits of the EXP_DECRYPT value
 // The exponent is a host-built sliding-window schedule (host_bigint.h).
 // ---------------------------------------------------------------------------
+// One CTA's share of a modexp launch: instances [block*IPB, block*IPB + IPB).
+// Every thread of the CTA calls it (it synchronises the CTA once, after
+// staging the key rows in shared memory).
 template <int K, int TPI, int W>
-__global__ void __launch_bounds__(kBlockThreads)
-k_modexp(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, int aux_words,
-         uint32_t* __restrict__ out, long long count, const uint32_t* __restrict__ consts, KeyScalars ks,
-         const int32_t* __restrict__ ops, int nops, int mode, int pop_words, int* status) {
+__device__ __forceinline__ void modexp_unit(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux,
+                                            int aux_words, uint32_t* __restrict__ out, long long count,
+                                            const uint32_t* __restrict__ consts, const KeyScalars& ks,
+                                            const int32_t* __restrict__ ops, int nops, int mode, int pop_words,
+                                            int* status, long long block) {
   constexpr int L = K / TPI;
   constexpr int T = 1 << (W - 1);
   constexpr int IPB = kBlockThreads / TPI;
@@ -243,7 +247,7 @@ k_modexp(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, in
 
   Group<K, TPI> g;
   const int slot = threadIdx.x / TPI;
-  const long long inst = (long long)blockIdx.x * IPB + slot;
+  const long long inst = block * IPB + slot;
   if (inst >= count) return;  // whole groups leave together
   uint32_t* s_inst = smem + 5 * K + slot * STRIDE;
   uint32_t* s_x = s_inst;               // current value (b operand of squarings)
@@ -322,6 +326,56 @@ k_modexp(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, in
   // decrypt / decode
   g.mont_mul(x, acc, s_one, n2, ks.ninv2);
   decrypt_epilogue<K, TPI>(g, x, out, inst, consts, ks, s_one, s_r2n, s_multr, mode, pop_words);
+}
+
+template <int K, int TPI, int W>
+__global__ void __launch_bounds__(kBlockThreads)
+k_modexp(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, int aux_words,
+         uint32_t* __restrict__ out, long long count, const uint32_t* __restrict__ consts, KeyScalars ks,
+         const int32_t* __restrict__ ops, int nops, int mode, int pop_words, int* status) {
+  modexp_unit<K, TPI, W>(base, aux, aux_words, out, count, consts, ks, ops, nops, mode, pop_words, status,
+                         (long long)blockIdx.x);
+}
+
+// One fixed-exponent exponentiation batch of a mixed launch: `count` bases of
+// one key (its constant block and Montgomery scalars) raised to one exponent
+// (its window schedule).  first_unit = CTA units of the tasks before it.
+struct ModexpTask {
+  const uint32_t* base;
+  uint32_t* out;
+  long long count;
+  const uint32_t* consts;
+  const int32_t* ops;
+  long long first_unit;
+  KeyScalars ks;
+  int nops;
+  int mode;
+};
+
+// Persistent mixed launch: CTAs take units (IPB instances of one task) from
+// a global counter until every unit of every task is done, so batches of
+// uneven sizes and different keys share one launch without tail waves per
+// batch.  tasks[] is ordered by first_unit.
+template <int K, int TPI, int W>
+__global__ void __launch_bounds__(kBlockThreads)
+k_modexp_tasks(const ModexpTask* __restrict__ tasks, int ntasks, long long total_units,
+               unsigned long long* __restrict__ counter, int* status) {
+  __shared__ long long s_unit;
+  while (true) {
+    if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
+    __syncthreads();
+    const long long unit = s_unit;
+    if (unit >= total_units) break;
+    int lo = 0, hi = ntasks - 1;  // last task with first_unit <= unit
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tasks[mid].first_unit <= unit) lo = mid; else hi = mid - 1;
+    }
+    const ModexpTask& t = tasks[lo];
+    modexp_unit<K, TPI, W>(t.base, nullptr, K, t.out, t.count, t.consts, t.ks, t.ops, t.nops, t.mode, 0, status,
+                           unit - t.first_unit);
+    __syncthreads();  // shared rows and tables are restaged by the next unit
+  }
 }
 
 // ---------------------------------------------------------------------------

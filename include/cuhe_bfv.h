@@ -98,6 +98,19 @@ int cuhe_bfv_search_index(cuhe_bfv_server* server, cuhe_bfv_index* index, const 
  * output.  No counterpart in the reference; it feeds the profile_* calls. */
 int cuhe_bfv_last_profile(const cuhe_bfv_server* server, double* ms, int capacity);
 
+/* Batched negacyclic NTT of device-resident residue planes ([planes][N]
+ * u64, plane b reduced mod the ring's prime b % primes, canonical in and
+ * out): forward (bit-reversed output) or inverse (bit-reversed input,
+ * 1/N folded in), in place.  Enqueued on `stream` (a cudaStream_t) with no
+ * allocation or synchronisation, so it can be captured in a CUDA graph.
+ * threads: CTA size (0: N/16, at most the kernel's register-bound CTA
+ * limit, which a larger request exceeds with an error); radix_log: register
+ * pass width, 1..4 stages
+ * (0: 4).  These two are the knobs of the autotuner.  The transform the
+ * reference runs per prime (rns_ntt.h:178-255), batched. */
+int cuhe_bfv_ntt(cuhe_bfv_ring* ring, uint64_t* planes, uint64_t count, int primes, int inverse, int threads,
+                 int radix_log, void* stream);
+
 /* Execution lanes of a ring (1..8; 1 after create_ring).  Each lane is a
  * CUDA stream with its own device workspace.  packed_search / search_index
  * calls issued concurrently from several host threads take free lanes and

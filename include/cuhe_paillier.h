@@ -202,6 +202,36 @@ int cuhe_window_schedule(const uint32_t* exponent, int exponent_words, int windo
 int cuhe_paillier_set_tuning(cuhe_paillier* ctx, int threads_per_instance, int window);
 int cuhe_paillier_get_tuning(const cuhe_paillier* ctx, int* threads_per_instance, int* window);
 
+/* Mixed batches.  A cuhe_mix collects fixed-exponent exponentiations
+ * out[i] = base[i]^e mod n^2 of uneven sizes over several keys and widths
+ * (each added with its context and device buffers), and runs them as one
+ * persistent launch per width: CTAs take units of a few instances from a
+ * global counter until every batch is done, so small batches do not leave
+ * the GPU idle between launches.  cuhe_mix_launch only enqueues work on the
+ * given stream (no allocation, no synchronisation), so it can be captured
+ * in a CUDA graph; cuhe_mix_plan (after the last add or tuning change)
+ * builds the schedules and task tables and must run outside capture.
+ * cuhe_mix_check waits for the device and reports range errors (a base not
+ * below n^2).  Contexts and buffers must outlive the mix.  No counterpart in
+ * the reference, which launches one kernel per call
+ * (paillier_GPU_client.cu:873-974). */
+typedef struct cuhe_mix cuhe_mix;
+int cuhe_mix_create(int device, cuhe_mix** out);
+void cuhe_mix_destroy(cuhe_mix* mix);
+const char* cuhe_mix_last_error(const cuhe_mix* mix);
+int cuhe_mix_add_modexp(cuhe_mix* mix, cuhe_paillier* ctx, const uint32_t* base, uint32_t* out, int64_t count,
+                        const uint32_t* exponent, int exponent_words);
+/* (threads per instance, window) of the persistent launch for one width. */
+int cuhe_mix_set_tuning(cuhe_mix* mix, int words, int threads_per_instance, int window);
+int cuhe_mix_plan(cuhe_mix* mix);
+int cuhe_mix_launch(cuhe_mix* mix, void* stream);
+int cuhe_mix_check(cuhe_mix* mix);
+/* Planned widths (ascending words) and, per width, its tuning, grid, CTA
+ * units and batch count. */
+int cuhe_mix_widths(const cuhe_mix* mix);
+int cuhe_mix_info(const cuhe_mix* mix, int index, int* words, int* threads_per_instance, int* window, int* grid,
+                  int64_t* units, int* tasks);
+
 #ifdef __cplusplus
 }
 #endif
