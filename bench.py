@@ -386,6 +386,8 @@ def run_gpu(args) -> dict | None:
     }
     if not args.no_bfv:
         result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
+    if not args.no_textbook and world == 1:
+        result["textbook"] = [run_textbook(512), run_textbook(1024)]
     if not args.no_mixed and world == 1:
         result["mixed"] = run_mixed()
     if not args.no_serving and world == 1:
@@ -689,6 +691,119 @@ def run_reference(args) -> dict | None:
     }
 
 
+def run_textbook(key_len: int, count: int = 4096, plain_sample: int = 32, cpu_sample: int = 8) -> dict:
+    """Plain Paillier at one key_len: keys from seed 0 (the reference's
+    key_gen with seeded primes), 4096 plaintexts uniform in [0, 2^32)
+    (seed 1), r uniform in Z_n* (seed 2); encrypt all, add 2048 pairs,
+    decrypt all (c^phi, by CRT).  Batched = one launch per batch; plain = one
+    launch per ciphertext (timed on a sample, host-synchronised); the oracle
+    (GMP powmod, one core) timed on a few operations beside it."""
+    import torch
+
+    from cuhepy_b200 import _numbers
+    from cuhepy_b200._limbs import from_limbs
+    from cuhepy_b200.paillier import scheme
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+    from oracle import paillier as oracle
+
+    fake = SeededSecrets(0)
+    saved = (_numbers.secrets, scheme.secrets)
+    _numbers.secrets = scheme.secrets = fake
+    try:
+        keys = scheme.Paillier.key_gen(key_len)
+    finally:
+        _numbers.secrets, scheme.secrets = saved
+    pk, sk = keys["pk"], keys["sk"]
+    n, n2 = pk["n"], pk["n_squared"]
+    r1, r2 = random.Random(1), random.Random(2)
+    ms = [r1.getrandbits(32) for _ in range(count)]
+    rs = []
+    while len(rs) < count:
+        r = r2.randrange(1, n)
+        if math.gcd(r, n) == 1:
+            rs.append(r)
+    ctx = PaillierDevice(n)
+    ctx.set_secret(sk["phi"], sk["inv"])
+    ctx.set_factors(*factors_from_phi(n, sk["phi"]))
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    K = ctx.words
+    half = count // 2
+
+    def dev(a):
+        return torch.from_numpy(a.view(np.int32)).cuda()
+
+    m_d, r_d = dev(ctx.limbs(ms)), dev(ctx.limbs(rs))
+    c_d = torch.empty((count, K), dtype=torch.int32, device="cuda")
+    s_d = torch.empty((half, K), dtype=torch.int32, device="cuda")
+    p_d = torch.empty((count, K), dtype=torch.int32, device="cuda")
+    left = torch.empty((half, K), dtype=torch.int32, device="cuda")
+    right = torch.empty((half, K), dtype=torch.int32, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def batched():
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            ctx.encrypt_array(m_d, r_d, c_d, count)
+            ev[1].record(stream)
+            left.copy_(c_d[0::2])
+            right.copy_(c_d[1::2])
+            ctx.mulmod_array(left, right, s_d, half)
+            ev[2].record(stream)
+            ctx.decrypt_array(c_d, p_d, count)
+            ev[3].record(stream)
+        ev[3].synchronize()
+        return [ev[i].elapsed_time(ev[i + 1]) for i in range(3)]
+
+    for _ in range(3):
+        batched()
+    runs = [batched() for _ in range(3)]
+    enc_ms, add_ms, dec_ms = (statistics.mean(r[i] for r in runs) for i in range(3))
+    cs = from_limbs(c_d.cpu().numpy().view(np.uint32))
+    back = from_limbs(p_d.cpu().numpy().view(np.uint32))
+    sums = from_limbs(s_d.cpu().numpy().view(np.uint32))
+    if back != ms:
+        raise RuntimeError("decrypt(encrypt(m)) != m")
+    keys_o = {"pk": pk, "sk": sk}
+    rng = random.Random(3)
+    for i in rng.sample(range(count), 8):
+        if cs[i] != oracle.encrypt(ms[i], rs[i], pk):
+            raise RuntimeError("ciphertexts differ from the oracle")
+    for i in rng.sample(range(half), 4):
+        if oracle.decrypt(sums[i], keys_o) != (ms[2 * i] + ms[2 * i + 1]) % n:
+            raise RuntimeError("homomorphic sums differ from the oracle")
+    # plain: one launch per ciphertext, host-synchronised
+    t0 = time.perf_counter()
+    for i in range(plain_sample):
+        ctx.encrypt_array(m_d[i:i + 1], r_d[i:i + 1], c_d[i:i + 1], 1)
+        stream.synchronize()
+    plain_enc = plain_sample / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for i in range(plain_sample):
+        ctx.decrypt_array(c_d[i:i + 1], p_d[i:i + 1], 1)
+        stream.synchronize()
+    plain_dec = plain_sample / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for i in range(cpu_sample):
+        oracle.encrypt(ms[i], rs[i], pk)
+    cpu_enc = cpu_sample / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for i in range(cpu_sample):
+        oracle.decrypt(cs[i], keys_o)
+    cpu_dec = cpu_sample / (time.perf_counter() - t0)
+    return {
+        "key_len": key_len, "n_squared_bits": n2.bit_length(), "count": count,
+        "encrypt_ms": enc_ms, "add_ms": add_ms, "decrypt_ms": dec_ms,
+        "encrypt_per_s": count / (enc_ms / 1e3), "decrypt_per_s": count / (dec_ms / 1e3),
+        "add_per_s": half / (add_ms / 1e3),
+        "plain_encrypt_per_s": plain_enc, "plain_decrypt_per_s": plain_dec,
+        "cpu_encrypt_per_s_1core": cpu_enc, "cpu_decrypt_per_s_1core": cpu_dec,
+        "decrypt": "c^phi by CRT (factors from phi)",
+        "plain": f"one launch per ciphertext, host-synchronised, {plain_sample}-op sample",
+        "cpu": f"oracle (GMP powmod), one core, {cpu_sample}-op sample",
+    }
+
+
 def run_mixed(steps: int = 5, seed: int = 5) -> dict:
     """Batched uneven mix: Paillier fixed-exponent exponentiations r^n at two
     widths (n^2 2048-bit and 4096-bit, four keys each) with 1,000-50,000
@@ -985,6 +1100,8 @@ def main() -> None:
     parser.add_argument("--no-serving", action="store_true", help="skip the serving section")
     parser.add_argument("--serving-only", action="store_true", help="run only the serving section")
     parser.add_argument("--mixed-only", action="store_true", help="run only the mixed-batch section")
+    parser.add_argument("--textbook-only", action="store_true", help="run only the plain Paillier section")
+    parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
     parser.add_argument("--profile-case", choices=["paillier", "bfv"],
                         help="run one small step of a hot kernel (for ncu captures) and exit")
@@ -994,6 +1111,9 @@ def main() -> None:
         return
     if args.serving_only:
         print(json.dumps(run_serving()))
+        return
+    if args.textbook_only:
+        print(json.dumps({"textbook": [run_textbook(512), run_textbook(1024)]}))
         return
     if args.mixed_only:
         print(json.dumps(run_mixed()))

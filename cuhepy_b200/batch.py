@@ -254,8 +254,9 @@ class MixedBatch:
             n = items[0].ring.n
             candidates = []
             for threads in (n // 32, n // 16, n // 8):
-                if 32 <= threads <= 512:
-                    for radix in (2, 3, 4):
+                for radix in (2, 3, 4):
+                    # radix 16 runs the register-heavy kernel: at most 512 threads
+                    if 32 <= threads <= (512 if radix == 4 else 1024):
                         candidates.append((threads, radix))
             timings = {}
             for cand in candidates:

@@ -29,10 +29,9 @@ struct BaseDev {
 struct RingDev {
   int n, logn, primes, residue, tensor, digits, digit_bits, words;
   Prime prime[kMaxPrimes];
-  const u64* fwd[kMaxPrimes];
-  const u64* fwd_q[kMaxPrimes];
-  const u64* inv[kMaxPrimes];
-  const u64* inv_q[kMaxPrimes];
+  // twiddles as (w, floor(w 2^64 / p)) pairs, one 16-byte load each
+  const ulonglong2* fwd2[kMaxPrimes];
+  const ulonglong2* inv2[kMaxPrimes];
   u64 n_inv[kMaxPrimes], n_inv_q[kMaxPrimes], last[kMaxPrimes], last_q[kMaxPrimes];
   u64 garner[kMaxResidue][kMaxResidue], garner_q[kMaxResidue][kMaxResidue];
   u64 q_words[kMaxWords];       // Q
@@ -57,8 +56,8 @@ __host__ __device__ constexpr size_t plane_smem_words(int n) { return size_t(n) 
 // memory.  Stage s has 2^s groups of gap N/2^(s+1); inside a block the group
 // of element k at stage s0+t is G*2^t + (k >> (P-t)).
 template <int P>
-__device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const u64* __restrict__ w,
-                                                 const u64* __restrict__ wq, u64 p, bool last) {
+__device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const ulonglong2* __restrict__ w2,
+                                                 u64 p, bool last) {
   constexpr int E = 1 << P;
   const int n = 1 << logn;
   const u64 two_p = 2 * p;
@@ -80,7 +79,8 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
       for (int k = 0; k < E; ++k) {
         if (k & half) continue;
         const int idx = m + (G << t) + (k >> (P - t));
-        const u64 root = __ldg(w + idx), rq = __ldg(wq + idx);
+        const ulonglong2 tw = __ldg(w2 + idx);
+        const u64 root = tw.x, rq = tw.y;
         u64 u = x[k];
         if (u >= two_p) u -= two_p;
         const u64 v = shoup_lazy(x[k + half], root, rq, p);
@@ -103,9 +103,8 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
 // Inverse (decimation in time) passes: stage u has gap 2^u and N/2^(u+1)
 // groups; the final stage (gap N/2) folds in 1/N and the inverse twist.
 template <int P>
-__device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const u64* __restrict__ w,
-                                                 const u64* __restrict__ wq, u64 p, u64 n_inv, u64 n_inv_q,
-                                                 u64 last_w, u64 last_q) {
+__device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const ulonglong2* __restrict__ w2,
+                                                 u64 p, u64 n_inv, u64 n_inv_q, u64 last_w, u64 last_q) {
   constexpr int E = 1 << P;
   const int n = 1 << logn;
   const u64 two_p = 2 * p;
@@ -132,7 +131,8 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
           x[k + half] = shoup(u + two_p - v, last_w, last_q, p);
         } else {
           const int idx = m + (G << (P - t - 1)) + (k >> (t + 1));
-          const u64 root = __ldg(w + idx), rq = __ldg(wq + idx);
+          const ulonglong2 tw = __ldg(w2 + idx);
+          const u64 root = tw.x, rq = tw.y;
           const u64 s = u + v;
           x[k] = s >= two_p ? s - two_p : s;
           x[k + half] = shoup_lazy(u + two_p - v, root, rq, p);
@@ -153,10 +153,10 @@ __device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j
     const int P = logn - s0 < max_p ? logn - s0 : max_p;
     const bool last = s0 + P == logn;
     switch (P) {
-      case 4: ntt_forward_pass<4>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
-      case 3: ntt_forward_pass<3>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
-      case 2: ntt_forward_pass<2>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
-      default: ntt_forward_pass<1>(a, s0, logn, R.fwd[j], R.fwd_q[j], p, last); break;
+      case 4: ntt_forward_pass<4>(a, s0, logn, R.fwd2[j], p, last); break;
+      case 3: ntt_forward_pass<3>(a, s0, logn, R.fwd2[j], p, last); break;
+      case 2: ntt_forward_pass<2>(a, s0, logn, R.fwd2[j], p, last); break;
+      default: ntt_forward_pass<1>(a, s0, logn, R.fwd2[j], p, last); break;
     }
     __syncthreads();
   }
@@ -168,78 +168,23 @@ __device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j
   for (int u0 = 0; u0 < logn; u0 += max_p) {
     const int P = logn - u0 < max_p ? logn - u0 : max_p;
     switch (P) {
-      case 4: ntt_inverse_pass<4>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
-      case 3: ntt_inverse_pass<3>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
-      case 2: ntt_inverse_pass<2>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
-      default: ntt_inverse_pass<1>(a, u0, logn, R.inv[j], R.inv_q[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      case 4: ntt_inverse_pass<4>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      case 3: ntt_inverse_pass<3>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      case 2: ntt_inverse_pass<2>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+      default: ntt_inverse_pass<1>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
     }
     __syncthreads();
   }
-}
-
-// Forward: decimation in frequency with psi^bitrev twiddles; output bit-reversed.
-__device__ __forceinline__ void ntt_forward_smem(u64* a, const RingDev& R, int j) {
-  const int n = R.n;
-  const u64 p = R.prime[j].p, two_p = 2 * p;
-  const u64* __restrict__ w = R.fwd[j];
-  const u64* __restrict__ wq = R.fwd_q[j];
-  int shift = R.logn - 1;  // log2(gap)
-  for (int m = 1; m < n; m <<= 1, --shift) {
-    const int gap = 1 << shift;
-    for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
-      const int group = b >> shift, jj = b & (gap - 1);
-      const int i0 = (group << (shift + 1)) + jj, i1 = i0 + gap;
-      const u64 root = __ldg(w + m + group), rq = __ldg(wq + m + group);
-      u64 u = a[i0];
-      if (u >= two_p) u -= two_p;
-      const u64 v = shoup_lazy(a[i1], root, rq, p);
-      a[i0] = u + v;
-      a[i1] = u + two_p - v;
-    }
-    __syncthreads();
-  }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    u64 x = a[i];
-    if (x >= two_p) x -= two_p;
-    if (x >= p) x -= p;
-    a[i] = x;
-  }
-  __syncthreads();
-}
-
-// Inverse: decimation in time, 1/N fused into the last stage; canonical output.
-__device__ __forceinline__ void ntt_inverse_smem(u64* a, const RingDev& R, int j) {
-  const int n = R.n;
-  const u64 p = R.prime[j].p, two_p = 2 * p;
-  const u64* __restrict__ w = R.inv[j];
-  const u64* __restrict__ wq = R.inv_q[j];
-  int shift = 0;
-  for (int m = n / 2; m > 1; m >>= 1, ++shift) {
-    const int gap = 1 << shift;
-    for (int b = threadIdx.x; b < n / 2; b += blockDim.x) {
-      const int group = b >> shift, jj = b & (gap - 1);
-      const int i0 = (group << (shift + 1)) + jj, i1 = i0 + gap;
-      const u64 root = __ldg(w + m + group), rq = __ldg(wq + m + group);
-      const u64 u = a[i0], v = a[i1];
-      const u64 s = u + v;
-      a[i0] = s >= two_p ? s - two_p : s;
-      a[i1] = shoup_lazy(u + two_p - v, root, rq, p);
-    }
-    __syncthreads();
-  }
-  const int half = n / 2;
-  for (int b = threadIdx.x; b < half; b += blockDim.x) {
-    const u64 u = a[b], v = a[b + half];
-    a[b] = shoup(u + v, R.n_inv[j], R.n_inv_q[j], p);
-    a[b + half] = shoup(u + two_p - v, R.last[j], R.last_q[j], p);
-  }
-  __syncthreads();
 }
 
 // Batched transform: plane b of `data` (stride n) uses prime prime_of(b).
-// prime = (b / prime_block) % prime_mod + prime_base.
-__global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block,
-                      int inverse, int max_p = 4) {
+// prime = (b / prime_block) % prime_mod + prime_base.  MAXP bounds the
+// register pass width at compile time: radix-8 passes fit 64 registers, so
+// the <3> kernel runs 1024-thread CTAs; the <4> kernel (radix 16) needs more
+// registers per thread and runs smaller CTAs.
+template <int MAXP>
+__device__ __forceinline__ void ntt_plane(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod,
+                                          int prime_block, int inverse, int max_p) {
   extern __shared__ __align__(16) u64 s_plane[];
   const RingDev& R = *ring;
   const int n = R.n;
@@ -248,9 +193,21 @@ __global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_bas
   u64* plane = data + b * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[sp(i)] = plane[i];
   __syncthreads();
+  max_p = max_p < MAXP ? max_p : MAXP;
   if (inverse) ntt_inverse_fast(s_plane, R, j, max_p);
   else ntt_forward_fast(s_plane, R, j, max_p);
   for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[sp(i)];
+}
+
+__global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block,
+                      int inverse, int max_p = 4) {
+  ntt_plane<4>(data, ring, prime_base, prime_mod, prime_block, inverse, max_p);
+}
+
+__global__ void __launch_bounds__(1024, 1)
+k_ntt8(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block, int inverse,
+       int max_p = 3) {
+  ntt_plane<3>(data, ring, prime_base, prime_mod, prime_block, inverse, max_p);
 }
 
 // ---- wire unpacking ---------------------------------------------------------
@@ -605,12 +562,13 @@ __device__ __forceinline__ u64 gadget_digit(const u64* w, int W, int d, const Ri
   return r;
 }
 
-constexpr int kSwitchThreads = 512;
-
 // CTA per (op, prime j < L): D forward NTTs of the digits, multiply-accumulate
 // with the key in the NTT domain, two inverse NTTs, epilogue additions.
-template <int kSwitchPer>  // coefficients per thread: N / kSwitchThreads (rounded up)
-__global__ void __launch_bounds__(kSwitchThreads)
+// kSwitchThreads threads per CTA; MAXP stages per register pass (radix
+// 2^MAXP): 1024 threads with radix-8 passes keeps a thread within 64
+// registers, so a whole CTA of 32 warps is resident beside the accumulators.
+template <int kSwitchPer, int kSwitchThreads, int MAXP>  // kSwitchPer: coefficients per thread, 0 = shared accumulators
+__global__ void __launch_bounds__(kSwitchThreads, 1)
 k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) {
   extern __shared__ __align__(16) u64 s_plane[];
   const RingDev& R = *ring;
@@ -633,7 +591,7 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
     for (int i = threadIdx.x; i < n; i += kSwitchThreads)
       s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
     __syncthreads();
-    ntt_forward_fast(s_plane, R, j);
+    ntt_forward_fast(s_plane, R, j, MAXP);
     const u64* k0 = op.key + ((long long)(d * 2 + 0) * L + j) * n;
     const u64* k1 = op.key + ((long long)(d * 2 + 1) * L + j) * n;
     if (kSmemAcc) {
@@ -664,7 +622,7 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
         if (k < per) s_plane[sp(threadIdx.x + k * kSwitchThreads)] = comp ? acc1[k] : acc0[k];
     }
     __syncthreads();
-    ntt_inverse_fast(s_plane, R, j);
+    ntt_inverse_fast(s_plane, R, j, MAXP);
     u64* out = op.out + ((long long)comp * L + j) * n;
     const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
     for (int i = threadIdx.x; i < n; i += kSwitchThreads) {

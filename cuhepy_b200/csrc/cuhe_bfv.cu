@@ -264,30 +264,29 @@ unsigned blocks_for(long long items, int threads) { return unsigned((items + thr
 
 size_t ntt_smem(const cuhe_bfv_ring* r) { return plane_smem_words(int(r->plan.n)) * sizeof(u64); }
 
-// Largest CTA k_ntt can launch with (its register use bounds it below 1024).
-int ntt_max_threads() {
+// Largest CTA of an NTT launch at this radix: the radix-8 kernel k_ntt8 is
+// compiled for 1024 threads; the radix-16 kernel k_ntt is bounded below 1024
+// by its register use.
+int ntt_max_threads(int radix_log = 4) {
+  if (radix_log <= 3) return 1024;
   static int cached = 0;
   if (!cached) {
     cudaFuncAttributes attr{};
-    cached = cudaFuncGetAttributes(&attr, k_ntt) == cudaSuccess ? attr.maxThreadsPerBlock : 256;
+    cached = cudaFuncGetAttributes(&attr, k_ntt) == cudaSuccess ? attr.maxThreadsPerBlock / 32 * 32 : 256;
   }
   return cached;
 }
 
-// Default CTA size of an N-point transform: one radix-16 block per thread.
-int ntt_default_threads(size_t n) {
-  const int want = int(std::min<size_t>(1024, std::max<size_t>(32, n / 16)));
-  return std::min(want, ntt_max_threads() / 32 * 32);
-}
+// Default launch of an N-point transform: radix-8 passes, one block of eight
+// per thread (at most 1024 threads).
+int ntt_default_threads(size_t n) { return int(std::min<size_t>(1024, std::max<size_t>(32, n / 8))); }
 
 cudaError_t launch_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
                        int prime_block, int inverse) {
   if (planes <= 0) return cudaSuccess;
-  const size_t smem = ntt_smem(r);
-  cudaError_t e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return e;
+  const size_t smem = ntt_smem(r);  // within the attribute set at ring creation
   const int threads = ntt_default_threads(r->plan.n);
-  k_ntt<<<unsigned(planes), threads, smem, ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse);
+  k_ntt8<<<unsigned(planes), threads, smem, ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse, 3);
   return cudaGetLastError();
 }
 
@@ -309,12 +308,14 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
     dim3 grid(unsigned(sops.size()), unsigned(P.residue_count));
     if (P.n <= 8192) {
       const size_t smem_acc = smem + 2 * P.n * sizeof(u64);  // accumulators after the plane
-      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_acc)),
+      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<0, 1024, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(smem_acc)),
                "smem");
-      k_keyswitch<0><<<grid, kSwitchThreads, smem_acc, ln.stream>>>(d_sops, d);
+      k_keyswitch<0, 1024, 3><<<grid, 1024, smem_acc, ln.stream>>>(d_sops, d);
     } else {
-      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "smem");
-      k_keyswitch<32><<<grid, kSwitchThreads, smem, ln.stream>>>(d_sops, d);
+      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32, 512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+               "smem");
+      k_keyswitch<32, 512, 4><<<grid, 512, smem, ln.stream>>>(d_sops, d);
     }
     BFV_CUDA(cudaGetLastError(), "keyswitch launch");
   }
@@ -549,12 +550,17 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   const auto& P = r->plan;
   const size_t K = P.primes.size(), N = P.n;
   r->table_bytes = K * 4 * N * 8;
+  // per prime: forward (w, w_shoup) pairs, then inverse pairs
   std::vector<u64> tables(K * 4 * N);
   for (size_t j = 0; j < K; ++j) {
-    std::memcpy(&tables[(j * 4 + 0) * N], P.ntt[j].fwd.data(), N * 8);
-    std::memcpy(&tables[(j * 4 + 1) * N], P.ntt[j].fwd_q.data(), N * 8);
-    std::memcpy(&tables[(j * 4 + 2) * N], P.ntt[j].inv.data(), N * 8);
-    std::memcpy(&tables[(j * 4 + 3) * N], P.ntt[j].inv_q.data(), N * 8);
+    u64* f = &tables[(j * 4 + 0) * N];
+    u64* v = &tables[(j * 4 + 2) * N];
+    for (size_t i = 0; i < N; ++i) {
+      f[2 * i] = P.ntt[j].fwd[i];
+      f[2 * i + 1] = P.ntt[j].fwd_q[i];
+      v[2 * i] = P.ntt[j].inv[i];
+      v[2 * i + 1] = P.ntt[j].inv_q[i];
+    }
   }
   // Lane streams take the device's highest priority: a search is a chain of
   // short dependent kernels, and its blocks should be scheduled ahead of the
@@ -583,10 +589,8 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   dev.words = int((P.q_bits + 63) / 64);
   for (size_t j = 0; j < K; ++j) {
     dev.prime[j] = H::make_prime(P.primes[j]);
-    dev.fwd[j] = r->d_tables + (j * 4 + 0) * N;
-    dev.fwd_q[j] = r->d_tables + (j * 4 + 1) * N;
-    dev.inv[j] = r->d_tables + (j * 4 + 2) * N;
-    dev.inv_q[j] = r->d_tables + (j * 4 + 3) * N;
+    dev.fwd2[j] = reinterpret_cast<const ulonglong2*>(r->d_tables + (j * 4 + 0) * N);
+    dev.inv2[j] = reinterpret_cast<const ulonglong2*>(r->d_tables + (j * 4 + 2) * N);
     dev.n_inv[j] = P.ntt[j].n_inv;
     dev.n_inv_q[j] = P.ntt[j].n_inv_q;
     dev.last[j] = P.ntt[j].last;
@@ -609,10 +613,14 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
     delete r;
     return rc;
   }
-  // k_ntt's shared-memory size for the largest supported plane, once, so
-  // that cuhe_bfv_ntt needs no attribute call (it may run under capture)
+  // the NTT kernels' shared-memory size for the largest supported plane,
+  // once, so that later launches need no attribute call (they may run under
+  // stream capture)
   e = cudaFuncSetAttribute(k_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            int(plane_smem_words(16384) * sizeof(u64)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ntt8, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(plane_smem_words(16384) * sizeof(u64)));
   if (e != cudaSuccess) {
     delete r;
     return fail(CUHE_CUDA_ERROR, std::string("ring setup: ") + cudaGetErrorString(e));
@@ -627,18 +635,23 @@ int cuhe_bfv_ntt(cuhe_bfv_ring* r, uint64_t* planes_dev, uint64_t planes, int pr
   const auto& P = r->plan;
   if (primes < 1 || size_t(primes) > P.primes.size())
     return fail(CUHE_INVALID_ARGUMENT, "prime count outside the ring's primes");
-  if (threads == 0) threads = ntt_default_threads(P.n);
-  if (radix_log == 0) radix_log = 4;
-  if (threads < 32 || threads > ntt_max_threads() || threads % 32 || radix_log < 1 || radix_log > 4)
+  if (radix_log == 0) radix_log = 3;
+  if (radix_log < 1 || radix_log > 4) return fail(CUHE_INVALID_ARGUMENT, "radix_log must be 1..4");
+  if (threads == 0) threads = std::min(ntt_default_threads(P.n), ntt_max_threads(radix_log));
+  if (threads < 32 || threads > ntt_max_threads(radix_log) || threads % 32)
     return fail(CUHE_INVALID_ARGUMENT, "threads must be a multiple of 32 from 32 to " +
-                                           std::to_string(ntt_max_threads()) + ", radix_log 1..4");
+                                           std::to_string(ntt_max_threads(radix_log)) + " at this radix");
   if (planes == 0) return CUHE_OK;
   if (planes > (uint64_t(1) << 31) - 1) return fail(CUHE_INVALID_ARGUMENT, "too many planes for one launch");
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
-  k_ntt<<<unsigned(planes), threads, ntt_smem(r), static_cast<cudaStream_t>(stream)>>>(
-      reinterpret_cast<u64*>(planes_dev), d, 0, primes, 1, inverse ? 1 : 0, radix_log);
+  if (radix_log <= 3)
+    k_ntt8<<<unsigned(planes), threads, ntt_smem(r), static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<u64*>(planes_dev), d, 0, primes, 1, inverse ? 1 : 0, radix_log);
+  else
+    k_ntt<<<unsigned(planes), threads, ntt_smem(r), static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<u64*>(planes_dev), d, 0, primes, 1, inverse ? 1 : 0, radix_log);
   BFV_CUDA(cudaGetLastError(), "ntt launch");
   return CUHE_OK;
 }

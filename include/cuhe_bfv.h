@@ -103,11 +103,11 @@ int cuhe_bfv_last_profile(const cuhe_bfv_server* server, double* ms, int capacit
  * out): forward (bit-reversed output) or inverse (bit-reversed input,
  * 1/N folded in), in place.  Enqueued on `stream` (a cudaStream_t) with no
  * allocation or synchronisation, so it can be captured in a CUDA graph.
- * threads: CTA size (0: N/16, at most the kernel's register-bound CTA
- * limit, which a larger request exceeds with an error); radix_log: register
- * pass width, 1..4 stages
- * (0: 4).  These two are the knobs of the autotuner.  The transform the
- * reference runs per prime (rns_ntt.h:178-255), batched. */
+ * threads: CTA size (0: N/8, at most 1024; radix 16 has a smaller,
+ * register-bound limit that a larger request exceeds with an error);
+ * radix_log: register pass width, 1..4 stages (0: 3).  These two are the
+ * knobs of the autotuner.  The transform the reference runs per prime
+ * (rns_ntt.h:178-255), batched. */
 int cuhe_bfv_ntt(cuhe_bfv_ring* ring, uint64_t* planes, uint64_t count, int primes, int inverse, int threads,
                  int radix_log, void* stream);
 

@@ -115,19 +115,19 @@ def test_fifo_head_is_not_overtaken():
     try:
         s.submit(_req(index="a", nbytes=50, payload=0))
         gate.wait_groups(1)
-        big = s.submit(_req(index="b", nbytes=80, payload=1))      # does not fit yet
-        small = s.submit(_req(index="c", nbytes=10, payload=2))    # would fit, must wait behind
+        big_req = _req(index="b", nbytes=80, payload=1)      # does not fit yet
+        small_req = _req(index="c", nbytes=10, payload=2)    # would fit, must wait behind
+        big, small = s.submit(big_req), s.submit(small_req)
         time.sleep(0.05)
         assert len(gate.groups) == 1
         gate.open(0)
         s.release(50)
-        gate.wait_groups(2)
-        assert gate.groups[1][0] == [1]
+        gate.wait_groups(3)            # 80 + 10 <= 100: both run once the head fits
+        assert sorted(g for g, _ in gate.groups[1:]) == [[1], [2]]
+        assert big_req.admitted <= small_req.admitted
         gate.open(1)
-        big.result(5)
-        gate.wait_groups(3)                    # 80 + 10 <= 100: the small one follows at once
         gate.open(2)
-        assert small.result(5) == ("answer", 2)
+        assert big.result(5) == ("answer", 1) and small.result(5) == ("answer", 2)
     finally:
         for e in gate.events:
             e.set()
