@@ -1101,6 +1101,7 @@ def main() -> None:
     parser.add_argument("--serving-only", action="store_true", help="run only the serving section")
     parser.add_argument("--mixed-only", action="store_true", help="run only the mixed-batch section")
     parser.add_argument("--textbook-only", action="store_true", help="run only the plain Paillier section")
+    parser.add_argument("--bfv-only", action="store_true", help="run only the BFV kNN section")
     parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
     parser.add_argument("--profile-case", choices=["paillier", "bfv"],
@@ -1111,6 +1112,9 @@ def main() -> None:
         return
     if args.serving_only:
         print(json.dumps(run_serving()))
+        return
+    if args.bfv_only:
+        print(json.dumps({"bfv": run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)}))
         return
     if args.textbook_only:
         print(json.dumps({"textbook": [run_textbook(512), run_textbook(1024)]}))

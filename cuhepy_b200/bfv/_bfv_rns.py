@@ -54,6 +54,11 @@ BFV_SIGNATURES: dict[str, tuple] = {
     "cuhe_bfv_search_index": (ctypes.c_int, [_vp, _vp, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, _vp,
                                              ctypes.c_uint64, _u64p]),
     "cuhe_bfv_set_lanes": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cuhe_bfv_packed_search_parts": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p),
+                                                    ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _vp,
+                                                    ctypes.c_uint64, _u64p]),
+    "cuhe_bfv_upload_index_parts": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint64,
+                                                   ctypes.POINTER(_vp)]),
     "cuhe_bfv_ntt": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.c_int, _vp]),
     "cuhe_bfv_get_lanes": (ctypes.c_int, [_vp]),
@@ -308,6 +313,24 @@ def _packed(value: Any, server: Server) -> bytes:
     return value[0] + value[1]
 
 
+def _poly_pointers(index: Any, server: Server):
+    """One pointer per packed polynomial of the index tuple, into the bytes
+    objects themselves (validated, not copied); None for an empty index."""
+    if not isinstance(index, tuple):
+        raise ValueError("index must be a tuple of packed ciphertexts")
+    parts = []
+    for value in index:
+        if not isinstance(value, tuple) or len(value) != 2:
+            raise ValueError("Expected two packed components")
+        for part in value:
+            if not isinstance(part, bytes) or len(part) != server.input_bytes:
+                raise ValueError("Incorrect packed polynomial bytes")
+            parts.append(part)
+    if not parts:
+        return None
+    return (ctypes.c_char_p * len(parts))(*parts)
+
+
 def packed_search(server: Server, query: Any, index: Any, count: int, compact: bool) -> list[tuple[bytes, bytes]]:
     server = _get(server, Server)
     count = _u64(count, "count")
@@ -315,14 +338,13 @@ def packed_search(server: Server, query: Any, index: Any, count: int, compact: b
             (count + server.capacity - 1) // server.capacity != len(index):
         raise ValueError("vector_count does not match the packed ciphertext count")
     q = _packed(query, server)
-    blob = b"".join(_packed(v, server) for v in index)
+    polys = _poly_pointers(index, server)
     groups = (len(index) + server.padded - 1) // server.padded
     size = server.compact_bytes if compact else server.output_bytes
     out = ctypes.create_string_buffer(max(1, groups * 2 * size))
     responses = ctypes.c_uint64()
-    src = ctypes.create_string_buffer(blob, len(blob)) if blob else None
-    _check(lib().cuhe_bfv_packed_search(server.ptr, q, src, len(index), count, int(bool(compact)), out,
-                                        len(out), ctypes.byref(responses)))
+    _check(lib().cuhe_bfv_packed_search_parts(server.ptr, q, polys, len(index), count, int(bool(compact)), out,
+                                              len(out), ctypes.byref(responses)))
     raw = out.raw
     return [(raw[(2 * i) * size:(2 * i + 1) * size], raw[(2 * i + 1) * size:(2 * i + 2) * size])
             for i in range(responses.value)]
@@ -342,12 +364,9 @@ class ResidentIndex(_Handle):
 def upload_index(server: Server, index: Any) -> ResidentIndex:
     """Serving form: keep the packed index resident (not in the reference API)."""
     server = _get(server, Server)
-    if not isinstance(index, tuple):
-        raise ValueError("index must be a tuple of packed ciphertexts")
-    blob = b"".join(_packed(v, server) for v in index)
-    src = ctypes.create_string_buffer(blob, len(blob)) if blob else None
+    polys = _poly_pointers(index, server)
     handle = _vp()
-    _check(lib().cuhe_bfv_upload_index(server.ptr, src, len(index), ctypes.byref(handle)))
+    _check(lib().cuhe_bfv_upload_index_parts(server.ptr, polys, len(index), ctypes.byref(handle)))
     return ResidentIndex(handle.value, server, len(index))
 
 

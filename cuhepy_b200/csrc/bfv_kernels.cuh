@@ -472,6 +472,7 @@ struct SwitchOp {
   const u64* x0;     // [L][N] or null
   const u64* words;  // composed sigma_g(x1): [N][W]
   const u64* key;    // [D][2][L][N] NTT domain
+  const u64* key_q;  // Shoup quotients floor(key * 2^64 / p), same layout
   u64* out;          // [2][L][N]
   unsigned g_inv;    // inverse of g mod 2N (gather for x0)
   unsigned pad;
@@ -592,13 +593,17 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
       s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
     __syncthreads();
     ntt_forward_fast(s_plane, R, j, MAXP);
-    const u64* k0 = op.key + ((long long)(d * 2 + 0) * L + j) * n;
-    const u64* k1 = op.key + ((long long)(d * 2 + 1) * L + j) * n;
+    // key products by Shoup with the precomputed quotients; accumulators
+    // stay in [0, 2p) and are made canonical before the inverse transforms
+    const long long k0o = ((long long)(d * 2 + 0) * L + j) * n, k1o = ((long long)(d * 2 + 1) * L + j) * n;
+    const u64 two_p = 2 * m.p;
     if (kSmemAcc) {
       for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
         const u64 v = s_plane[sp(i)];
-        s_acc[i] = addmod(s_acc[i], reduce128(u128(v) * __ldg(k0 + i), m), m.p);
-        s_acc[n + i] = addmod(s_acc[n + i], reduce128(u128(v) * __ldg(k1 + i), m), m.p);
+        u64 a0 = s_acc[i] + shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), m.p);
+        u64 a1 = s_acc[n + i] + shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), m.p);
+        s_acc[i] = a0 >= two_p ? a0 - two_p : a0;
+        s_acc[n + i] = a1 >= two_p ? a1 - two_p : a1;
       }
     } else {
 #pragma unroll
@@ -606,8 +611,10 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
         if (k < per) {
           const int i = threadIdx.x + k * kSwitchThreads;
           const u64 v = s_plane[sp(i)];
-          acc0[k] = addmod(acc0[k], reduce128(u128(v) * __ldg(k0 + i), m), m.p);
-          acc1[k] = addmod(acc1[k], reduce128(u128(v) * __ldg(k1 + i), m), m.p);
+          const u64 a0 = acc0[k] + shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), m.p);
+          const u64 a1 = acc1[k] + shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), m.p);
+          acc0[k] = a0 >= two_p ? a0 - two_p : a0;
+          acc1[k] = a1 >= two_p ? a1 - two_p : a1;
         }
       }
     }
@@ -615,11 +622,17 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
   }
   for (int comp = 0; comp < 2; ++comp) {
     if (kSmemAcc) {
-      for (int i = threadIdx.x; i < n; i += kSwitchThreads) s_plane[sp(i)] = s_acc[comp * n + i];
+      for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
+        const u64 a = s_acc[comp * n + i];
+        s_plane[sp(i)] = a >= m.p ? a - m.p : a;
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < kRegs; ++k)
-        if (k < per) s_plane[sp(threadIdx.x + k * kSwitchThreads)] = comp ? acc1[k] : acc0[k];
+        if (k < per) {
+          const u64 a = comp ? acc1[k] : acc0[k];
+          s_plane[sp(threadIdx.x + k * kSwitchThreads)] = a >= m.p ? a - m.p : a;
+        }
     }
     __syncthreads();
     ntt_inverse_fast(s_plane, R, j, MAXP);
@@ -651,6 +664,17 @@ __global__ void k_mul_plain(u64* __restrict__ data, long long planes, int L, con
   const int i = int(idx % R.n);
   const int j = int(plane % L);
   data[idx] = reduce128(u128(data[idx]) * plain[(long long)j * R.n + i], R.prime[j]);
+}
+
+// q[b][i] = floor(x[b][i] * 2^64 / p_j), j = b % L: Shoup quotients of fixed
+// multipliers (compiled keys).
+__global__ void k_shoup_quotients(const u64* __restrict__ x, u64* __restrict__ q, long long planes, int L,
+                                  const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= planes * R.n) return;
+  const int j = int((idx / R.n) % L);
+  q[idx] = fraction64(x[idx], R.prime[j]);
 }
 
 // out = a + b elementwise over planes of L primes

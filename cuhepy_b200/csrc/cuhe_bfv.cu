@@ -10,6 +10,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/cuhe_bfv.h"
@@ -88,7 +89,54 @@ struct Lane {
   cudaStream_t stream = nullptr;
   Arena arena;
   std::mutex mu;
+  uint8_t* host_stage = nullptr;  // pinned staging of host polynomials (grow-only)
+  size_t host_cap = 0;
+  ~Lane() {
+    if (host_stage) cudaFreeHost(host_stage);
+  }
 };
+
+// Packed host polynomials of an index: one contiguous buffer, or one pointer
+// per polynomial (two per tile), each poly_bytes long.
+struct PolySource {
+  const uint8_t* contiguous = nullptr;
+  const uint8_t* const* parts = nullptr;
+  size_t poly_bytes = 0;
+  const uint8_t* poly(size_t k) const { return parts ? parts[k] : contiguous + k * poly_bytes; }
+};
+
+// Copy polys [first, first + count) of src into the lane's pinned staging
+// buffer (several host threads for large copies) and enqueue one
+// host-to-device copy to d_dst on the lane's stream.  The caller
+// synchronises the stream before the lane stages again.
+cudaError_t stage_polys(Lane& ln, const PolySource& src, size_t first, size_t count, uint8_t* d_dst) {
+  const size_t bytes = count * src.poly_bytes;
+  if (bytes == 0) return cudaSuccess;
+  if (bytes > ln.host_cap) {
+    if (ln.host_stage) cudaFreeHost(ln.host_stage);
+    ln.host_stage = nullptr;
+    ln.host_cap = 0;
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&ln.host_stage), bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    ln.host_cap = bytes;
+  }
+  const size_t workers = std::min<size_t>(std::max<size_t>(1, bytes >> 24), 8);  // one per 16 MiB, at most 8
+  auto copy = [&](size_t lo, size_t hi) {
+    for (size_t k = lo; k < hi; ++k) std::memcpy(ln.host_stage + k * src.poly_bytes, src.poly(first + k), src.poly_bytes);
+  };
+  if (workers == 1) {
+    copy(0, count);
+  } else {
+    std::vector<std::thread> pool;
+    const size_t per = (count + workers - 1) / workers;
+    for (size_t w = 0; w < workers; ++w) {
+      const size_t lo = w * per, hi = std::min(count, lo + per);
+      if (lo < hi) pool.emplace_back(copy, lo, hi);
+    }
+    for (auto& t : pool) t.join();
+  }
+  return cudaMemcpyAsync(d_dst, ln.host_stage, bytes, cudaMemcpyHostToDevice, ln.stream);
+}
 
 constexpr int kMaxLanes = 8;
 
@@ -132,7 +180,8 @@ struct cuhe_bfv_ring {
 struct cuhe_bfv_key {
   std::atomic<int> refs{1};
   cuhe_bfv_ring* ring = nullptr;
-  u64* d_key = nullptr;  // [D][2][L][N] NTT domain
+  u64* d_key = nullptr;  // [D][2][L][N] NTT domain, then as many Shoup quotients
+  u64* d_key_q = nullptr;
   size_t bytes = 0;
   ~cuhe_bfv_key() {
     if (d_key) {
@@ -441,7 +490,8 @@ int tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const TileArgs& a, u64*
   std::vector<SwitchOp> sops(ct);
   for (size_t t = 0; t < ct; ++t) {
     cops[t] = ComposeOp{scaled + (t * 3 + 2) * L * n, words + t * n * W, 1u, 0u};
-    sops[t] = SwitchOp{scaled + t * 3 * L * n, nullptr, words + t * n * W, a.relin->d_key, dist + t * 2 * L * n, 1u, 0u};
+    sops[t] = SwitchOp{scaled + t * 3 * L * n, nullptr, words + t * n * W, a.relin->d_key, a.relin->d_key_q,
+                       dist + t * 2 * L * n, 1u, 0u};
   }
   if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
   cudaEventRecord(ev[2], ln.stream);
@@ -458,7 +508,7 @@ int tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const TileArgs& a, u64*
       for (size_t t = 0; t < ct; ++t) {
         cops[t] = ComposeOp{cur + (t * 2 + 1) * L * n, words + t * n * W, unsigned(g), 0u};
         sops[t] = SwitchOp{cur + t * 2 * L * n, cur + t * 2 * L * n, words + t * n * W, a.keys[k]->d_key,
-                           nxt + t * 2 * L * n, ginv, 0u};
+                           a.keys[k]->d_key_q, nxt + t * 2 * L * n, ginv, 0u};
       }
       if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
     }
@@ -691,7 +741,7 @@ int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t
   if (!key) return fail(CUHE_OUT_OF_MEMORY, "key allocation");
   key->ring = ring;
   ++ring->refs;
-  key->bytes = size_t(digits) * 2 * L * n * 8;
+  key->bytes = 2 * size_t(digits) * 2 * L * n * 8;  // residues + Shoup quotients
   RingDev* d = nullptr;
   int rc = device_ring(ring, 0, &d);
   u64* d_words = nullptr;
@@ -707,6 +757,12 @@ int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t
     e = cudaGetLastError();
   }
   if (!rc && e == cudaSuccess) e = launch_ntt(ring, ln, d, key->d_key, (long long)(2 * digits * L), 0, int(L), 1, 0);
+  if (!rc && e == cudaSuccess) {
+    key->d_key_q = key->d_key + size_t(digits) * 2 * L * n;
+    k_shoup_quotients<<<blocks_for((long long)(2 * digits * L * n), 256), 256, 0, ln.stream>>>(
+        key->d_key, key->d_key_q, (long long)(2 * digits * L), int(L), d);
+    e = cudaGetLastError();
+  }
   if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ln.stream);
   if (d_words) cudaFree(d_words);
   if (rc || e != cudaSuccess) {
@@ -774,7 +830,7 @@ int cuhe_bfv_apply_key(cuhe_bfv_key* key, const uint8_t* poly, uint8_t* out) {
   u64* res = ln.arena.take<u64>(2 * L * n);
   SwitchOp* d_sops = ln.arena.take<SwitchOp>(1);
   BFV_ARENA(ln.arena);
-  std::vector<SwitchOp> sops{SwitchOp{nullptr, nullptr, words, key->d_key, res, 1u, 0u}};
+  std::vector<SwitchOp> sops{SwitchOp{nullptr, nullptr, words, key->d_key, key->d_key_q, res, 1u, 0u}};
   if (int rc = run_switch(r, ln, d, {}, sops, nullptr, d_sops)) return rc;
   return compose_out(r, ln, d, res, 2, out);
 }
@@ -805,7 +861,7 @@ int cuhe_bfv_rotate_rows(cuhe_bfv_key* key, const uint8_t* ct, uint64_t exponent
   SwitchOp* d_sops = ln.arena.take<SwitchOp>(1);
   BFV_ARENA(ln.arena);
   std::vector<ComposeOp> cops{ComposeOp{res + L * n, sw, unsigned(exponent), 0u}};
-  std::vector<SwitchOp> sops{SwitchOp{nullptr, res, sw, key->d_key, outres, inverse_mod_2n(exponent, n), 0u}};
+  std::vector<SwitchOp> sops{SwitchOp{nullptr, res, sw, key->d_key, key->d_key_q, outres, inverse_mod_2n(exponent, n), 0u}};
   if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
   return compose_out(r, ln, d, outres, 2, out);
 }
@@ -1079,7 +1135,7 @@ Lane& acquire_lane(cuhe_bfv_ring* r, std::unique_lock<std::mutex>& lock) {
   return ln;
 }
 
-int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, const u64* resident,
+int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* index, const u64* resident,
                 uint64_t tiles, uint64_t count, int compact, uint8_t* out, uint64_t out_capacity,
                 uint64_t* responses) {
   if (!s || !query || (tiles && !index && !resident) || !responses) return fail(CUHE_INVALID_ARGUMENT, "null argument");
@@ -1137,9 +1193,7 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
     k_unpack<<<blocks_for((long long)(2 * n), 256), 256, 0, ln.stream>>>(d_qb, (long long)(in_bytes), int(P.q_bits), 2, qw, d,
                                                                          d_status);
     if (!resident) {
-      BFV_CUDA(cudaMemcpyAsync(d_ib, index + first * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice,
-                               ln.stream),
-               "index upload");
+      BFV_CUDA(stage_polys(ln, *index, first * 2, ct * 2, d_ib), "index upload");
       k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(
           d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), tw, d, d_status);
     }
@@ -1214,7 +1268,8 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, 
         const u64 g = s->right.at(m.level);
         u64* words = mwords + cops.size() * n * W;
         cops.push_back(ComposeOp{dist + (m.right * 2 + 1) * L * n, words, unsigned(g), 0u});
-        sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, s->keys.at(g)->d_key,
+        const cuhe_bfv_key* key = s->keys.at(g);
+        sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, key->d_key, key->d_key_q,
                                 dist + m.left * 2 * L * n, inverse_mod_2n(g, n), 0u});
       }
       if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
@@ -1265,10 +1320,53 @@ extern "C" {
 
 int cuhe_bfv_packed_search(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* index, uint64_t tiles,
                            uint64_t count, int compact, uint8_t* out, uint64_t out_capacity, uint64_t* responses) {
-  return search_impl(s, query, index, nullptr, tiles, count, compact, out, out_capacity, responses);
+  if (!s) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  PolySource src;
+  src.contiguous = index;
+  src.poly_bytes = (s->ring->plan.n * s->ring->plan.q_bits + 7) / 8;
+  return search_impl(s, query, index ? &src : nullptr, nullptr, tiles, count, compact, out, out_capacity, responses);
+}
+
+int cuhe_bfv_packed_search_parts(cuhe_bfv_server* s, const uint8_t* query, const uint8_t* const* polys,
+                                 uint64_t tiles, uint64_t count, int compact, uint8_t* out, uint64_t out_capacity,
+                                 uint64_t* responses) {
+  if (!s) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  for (uint64_t k = 0; polys && k < 2 * tiles; ++k)
+    if (!polys[k]) return fail(CUHE_INVALID_ARGUMENT, "null polynomial pointer");
+  PolySource src;
+  src.parts = polys;
+  src.poly_bytes = (s->ring->plan.n * s->ring->plan.q_bits + 7) / 8;
+  return search_impl(s, query, polys ? &src : nullptr, nullptr, tiles, count, compact, out, out_capacity, responses);
+}
+
+namespace {
+int upload_index_impl(cuhe_bfv_server* s, const PolySource* index, uint64_t tiles, cuhe_bfv_index** out);
 }
 
 int cuhe_bfv_upload_index(cuhe_bfv_server* s, const uint8_t* index, uint64_t tiles, cuhe_bfv_index** out) {
+  if (!s) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  PolySource src;
+  src.contiguous = index;
+  src.poly_bytes = (s->ring->plan.n * s->ring->plan.q_bits + 7) / 8;
+  return upload_index_impl(s, index ? &src : nullptr, tiles, out);
+}
+
+int cuhe_bfv_upload_index_parts(cuhe_bfv_server* s, const uint8_t* const* polys, uint64_t tiles,
+                                cuhe_bfv_index** out) {
+  if (!s) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  for (uint64_t k = 0; polys && k < 2 * tiles; ++k)
+    if (!polys[k]) return fail(CUHE_INVALID_ARGUMENT, "null polynomial pointer");
+  PolySource src;
+  src.parts = polys;
+  src.poly_bytes = (s->ring->plan.n * s->ring->plan.q_bits + 7) / 8;
+  return upload_index_impl(s, polys ? &src : nullptr, tiles, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+int upload_index_impl(cuhe_bfv_server* s, const PolySource* index, uint64_t tiles, cuhe_bfv_index** out) {
   if (!s || !out || (tiles && !index)) return fail(CUHE_INVALID_ARGUMENT, "null argument");
   *out = nullptr;
   cuhe_bfv_ring* r = s->ring;
@@ -1302,7 +1400,11 @@ int cuhe_bfv_upload_index(cuhe_bfv_server* s, const uint8_t* index, uint64_t til
     cudaMemsetAsync(d_status, 0, sizeof(int), ln.stream);
     for (size_t t0 = 0; t0 < tiles; t0 += chunk) {
       const size_t ct = std::min<size_t>(chunk, size_t(tiles) - t0);
-      cudaMemcpyAsync(d_ib, index + t0 * 2 * in_bytes, ct * 2 * in_bytes, cudaMemcpyHostToDevice, ln.stream);
+      if (stage_polys(ln, *index, t0 * 2, ct * 2, d_ib) != cudaSuccess) {
+        cudaGetLastError();
+        delete idx;
+        return fail(CUHE_CUDA_ERROR, "index upload");
+      }
       k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(
           d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), idx->d_words + t0 * 2 * n * W, s->d_ring, d_status);
       cudaStreamSynchronize(ln.stream);  // the staging slice is reused by the next chunk
@@ -1315,6 +1417,10 @@ int cuhe_bfv_upload_index(cuhe_bfv_server* s, const uint8_t* index, uint64_t til
   *out = idx;
   return CUHE_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 void cuhe_bfv_index_release(cuhe_bfv_index* index) { delete index; }
 

@@ -89,6 +89,19 @@ int cuhe_bfv_packed_search(cuhe_bfv_server* server, const uint8_t* query, const 
  * every call (bindings.cpp:340-351). */
 typedef struct cuhe_bfv_index cuhe_bfv_index;
 int cuhe_bfv_upload_index(cuhe_bfv_server* server, const uint8_t* index, uint64_t tiles, cuhe_bfv_index** out);
+
+/* packed_search and upload_index with the index given as 2 * tiles
+ * pointers, one per packed polynomial (b_0, a_0, b_1, a_1, ...), so that a
+ * caller holding the polynomials in separate buffers (the reference API's
+ * tuple of bytes pairs) need not join them first.  The library gathers them
+ * into pinned staging memory with several host threads and copies each
+ * chunk to the device in one transfer.  Same results as the contiguous
+ * forms. */
+int cuhe_bfv_packed_search_parts(cuhe_bfv_server* server, const uint8_t* query, const uint8_t* const* polys,
+                                 uint64_t tiles, uint64_t count, int compact, uint8_t* out, uint64_t out_capacity,
+                                 uint64_t* responses);
+int cuhe_bfv_upload_index_parts(cuhe_bfv_server* server, const uint8_t* const* polys, uint64_t tiles,
+                                cuhe_bfv_index** out);
 void cuhe_bfv_index_release(cuhe_bfv_index* index);
 int cuhe_bfv_search_index(cuhe_bfv_server* server, cuhe_bfv_index* index, const uint8_t* query, uint64_t count,
                           int compact, uint8_t* out, uint64_t out_capacity, uint64_t* responses);
