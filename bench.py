@@ -40,6 +40,7 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 from cuhepy_b200._numbers import factors_from_phi  # noqa: E402
+from cuhepy_b200.sharding import max_over_ranks  # noqa: E402
 
 KEY_LEN = 1024
 ALPHA_LEN = 280
@@ -242,11 +243,7 @@ def run_gpu(args) -> dict | None:
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), dist, dev)
     units = modexp_count(INDEX_VECTORS, QUERY_BATCH) * args.steps * world
     value = units / (total_ms / 1e3)
 
@@ -284,11 +281,7 @@ def run_gpu(args) -> dict | None:
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         e2e_step()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
     if not np.array_equal(dist_p, dist_out.cpu().numpy()):
         raise RuntimeError("e2e distances differ from the device-resident run")
     h2d = bits_h.nbytes + qbits_h.nbytes + idx_h.nbytes + qidx_h.nbytes + index_p.nbytes + query_p.nbytes + prod_p.nbytes
@@ -492,8 +485,43 @@ def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
         m.hamming_tile(relin, qf, qf, rot, mask, BFV_T)
     per_tile = (time.perf_counter() - t0) / plain_tiles
     tiles = len(index)
+    # algorithmic work per query (the counts of bfv_server.h's circuit, which
+    # this implementation follows transform for transform): per tile 200
+    # forward and 87 inverse N-point transforms, per merge 18 and 6
+    groups = (tiles + layout.padded - 1) // layout.padded
+    merges = tiles - groups
+    fwd, inv = 200 * tiles + 18 * merges, 87 * tiles + 6 * merges
+    butterflies = (fwd + inv) * (BFV_N // 2) * int(math.log2(BFV_N))
+    step_s = statistics.mean(times)
+    from cuhepy_b200 import _native
+
+    imad = ctypes_imad_peak(_native, 0)
+    hbm_peak = 6456.5
+    try:
+        hbm_peak = float(json.loads((REPO / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+        hbm_src = "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError, KeyError):
+        hbm_src = "fallback"
+    L = 3
+    switches = tiles * 10 + merges
+    ntt_bytes = (fwd + inv) * 16 * BFV_N                               # u64 read + write per transform
+    mac_bytes = switches * (6 * L * BFV_N * 8 + 2 * 6 * L * BFV_N * 8 + 2 * L * BFV_N * 8)
+    out_roofline = {
+        "bound": "imad",
+        "kernel": "whole search (k_keyswitch<0,1024,3> ~75% of device time)",
+        "transforms_per_query": fwd + inv, "butterflies_per_query": butterflies,
+        "achieved": butterflies * 10 / step_s / 1e12, "peak": imad / 1e12, "unit": "Twp/s",
+        "frac": butterflies * 10 / step_s / imad,
+        "work_per_unit": "10 word products per 60-bit Shoup butterfly, (N/2) log2 N butterflies per transform",
+        "hbm_effective_gbs": (ntt_bytes + mac_bytes) / step_s / 1e9,
+        "hbm_frac_of_measured": (ntt_bytes + mac_bytes) / step_s / 1e9 / hbm_peak,
+        "hbm_note": ("bytes if every transform and key-switch operand streamed from HBM (16 N per transform, "
+                     "digits + keys + outputs per switch); the fused kernels keep planes on chip, so this "
+                     f"effective figure exceeds what DRAM carries; peak {hbm_peak} GB/s from {hbm_src}"),
+    }
     out = {
         "metric": "BFV kNN queries/s (N=8192, Q=3x60-bit, 16,384 x 512-bit index resident, compacted responses)",
+        "roofline": out_roofline,
         "value": 1.0 / statistics.mean(times), "unit": "queries/s",
         "p50_ms": 1e3 * statistics.median(times), "p99_ms": 1e3 * float(np.percentile(times, 99)),
         "phase_ms": {k: 1e3 * v["seconds"] for k, v in prof.items() if k != "other"},
