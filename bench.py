@@ -379,6 +379,8 @@ def run_gpu(args) -> dict | None:
     }
     if not args.no_bfv:
         result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
+    if not args.no_client and world == 1:
+        result["client"] = run_client()
     if not args.no_textbook and world == 1:
         result["textbook"] = [run_textbook(512), run_textbook(1024)]
     if not args.no_mixed and world == 1:
@@ -404,12 +406,10 @@ def bfv_setup(seed: int = 8192, embed: int = BFV_EMBED):
     Keys and ciphertexts are uniform residues from a seeded generator: the
     evaluator's work is independent of the values, and bit-exactness on real
     encryptions is covered by the parity tests."""
-    from oracle import bfv as ob
+    from cuhepy_b200.bfv import layout as lay
 
-    q = 1
-    for p in ob.rns_primes(BFV_N, BFV_Q_BITS):
-        q *= p
-    layout = ob.Layout(BFV_N, embed)
+    q = lay.rns_modulus(BFV_N, BFV_Q_BITS)
+    layout = lay.Layout(BFV_N, embed)
     exps = sorted(set(layout.left()) | set(layout.right()))
     rng = np.random.default_rng(seed)
     width = (q.bit_length() + 7) // 8
@@ -432,14 +432,14 @@ def bfv_setup(seed: int = 8192, embed: int = BFV_EMBED):
         for _ in range(2):
             vals = [int(x) for x in rng.integers(0, 1 << 62, size=(BFV_N, 3), dtype=np.int64).reshape(-1)]
             coeffs = [((vals[3 * i] << 124) | (vals[3 * i + 1] << 62) | vals[3 * i + 2]) % q for i in range(BFV_N)]
-            out.append(ob.pack_poly(coeffs, bits))
+            out.append(lay.pack_poly(coeffs, bits))
         return tuple(out)
 
     query = packed_ct()
     base_tiles = [packed_ct() for _ in range(8)]
     tiles = BFV_VECTORS // layout.capacity
     index = tuple(base_tiles[i % len(base_tiles)] for i in range(tiles))
-    target = ob.coefficient_modulus(50)
+    target = lay.coefficient_modulus(50)
     return q, layout, exps, keys, query, index, target
 
 
@@ -470,12 +470,10 @@ def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
     if resp2 != resp:
         raise RuntimeError("BFV resident and packed searches differ")
     # per-operation form: one hamming_tile call per tile (no batching across tiles)
-    width = (q.bit_length() + 7) // 8
-    from oracle import bfv as ob
-    unpack = [ob.unpack_poly(c, q.bit_length(), BFV_N) for c in query]
-    qf = tuple(b"".join(int(v).to_bytes(width, "little") for v in poly) for poly in unpack)
-    mask = b"".join(int(v).to_bytes(width, "little")
-                    for v in ob.batch_encode(layout.mask_slots(layout.capacity), BFV_N, BFV_T))
+    from cuhepy_b200.bfv import layout as lay
+
+    qf = tuple(lay.fixed_poly(lay.unpack_poly(c, q.bit_length(), BFV_N), q) for c in query)
+    mask = lay.fixed_poly(m.batch_encode(ring, BFV_T, layout.mask_slots(layout.capacity))[0], q)
     rot = tuple((g, k) for g, k in galois if g in layout.left())
     rot = tuple(sorted(rot, key=lambda e: layout.left().index(e[0])))
     m.hamming_tile(relin, qf, qf, rot, mask, BFV_T)
@@ -724,15 +722,14 @@ def run_textbook(key_len: int, count: int = 4096, plain_sample: int = 32, cpu_sa
     key_gen with seeded primes), 4096 plaintexts uniform in [0, 2^32)
     (seed 1), r uniform in Z_n* (seed 2); encrypt all, add 2048 pairs,
     decrypt all (c^phi, by CRT).  Batched = one launch per batch; plain = one
-    launch per ciphertext (timed on a sample, host-synchronised); the oracle
-    (GMP powmod, one core) timed on a few operations beside it."""
+    launch per ciphertext (timed on a sample, host-synchronised); the CPU
+    baseline (textbook_cpu_baseline) timed on a few operations beside it."""
     import torch
 
     from cuhepy_b200 import _numbers
     from cuhepy_b200._limbs import from_limbs
     from cuhepy_b200.paillier import scheme
     from cuhepy_b200.paillier.gpu import PaillierDevice
-    from oracle import paillier as oracle
 
     fake = SeededSecrets(0)
     saved = (_numbers.secrets, scheme.secrets)
@@ -792,14 +789,12 @@ def run_textbook(key_len: int, count: int = 4096, plain_sample: int = 32, cpu_sa
     sums = from_limbs(s_d.cpu().numpy().view(np.uint32))
     if back != ms:
         raise RuntimeError("decrypt(encrypt(m)) != m")
-    keys_o = {"pk": pk, "sk": sk}
-    rng = random.Random(3)
-    for i in rng.sample(range(count), 8):
-        if cs[i] != oracle.encrypt(ms[i], rs[i], pk):
-            raise RuntimeError("ciphertexts differ from the oracle")
-    for i in rng.sample(range(half), 4):
-        if oracle.decrypt(sums[i], keys_o) != (ms[2 * i] + ms[2 * i + 1]) % n:
-            raise RuntimeError("homomorphic sums differ from the oracle")
+    sp_d = torch.empty_like(s_d)
+    ctx.decrypt_array(s_d, sp_d, half)
+    torch.cuda.synchronize()
+    if from_limbs(sp_d.cpu().numpy().view(np.uint32)) != [(ms[2 * i] + ms[2 * i + 1]) % n for i in range(half)]:
+        raise RuntimeError("decrypted homomorphic sums differ from the plaintext sums")
+    del sums
     # plain: one launch per ciphertext, host-synchronised
     t0 = time.perf_counter()
     for i in range(plain_sample):
@@ -811,14 +806,7 @@ def run_textbook(key_len: int, count: int = 4096, plain_sample: int = 32, cpu_sa
         ctx.decrypt_array(c_d[i:i + 1], p_d[i:i + 1], 1)
         stream.synchronize()
     plain_dec = plain_sample / (time.perf_counter() - t0)
-    t0 = time.perf_counter()
-    for i in range(cpu_sample):
-        oracle.encrypt(ms[i], rs[i], pk)
-    cpu_enc = cpu_sample / (time.perf_counter() - t0)
-    t0 = time.perf_counter()
-    for i in range(cpu_sample):
-        oracle.decrypt(cs[i], keys_o)
-    cpu_dec = cpu_sample / (time.perf_counter() - t0)
+    cpu_enc, cpu_dec = textbook_cpu_baseline(keys, ms[:cpu_sample], rs[:cpu_sample], cs[:cpu_sample])
     return {
         "key_len": key_len, "n_squared_bits": n2.bit_length(), "count": count,
         "encrypt_ms": enc_ms, "add_ms": add_ms, "decrypt_ms": dec_ms,
@@ -832,6 +820,95 @@ def run_textbook(key_len: int, count: int = 4096, plain_sample: int = 32, cpu_sa
     }
 
 
+def run_client(vectors: int = 8192, reps: int = 3) -> dict:
+    """Client-side BFV encryption of an index: `vectors` Bernoulli(0.5)
+    512-bit vectors (seed 1337) in the packed layout (16 per ciphertext at
+    N = 8192), batch-encoded and encrypted on the device; noise drawn on the
+    host from the OS CSPRNG; public key uniform (the work is value-
+    independent).  The reference's client runs the same on the CPU one
+    ciphertext at a time (54.6 s for 8,192 vectors, docs/research/native-bfv.md:481)."""
+    from cuhepy_b200.bfv import _bfv_rns as m
+    from cuhepy_b200.bfv import layout as lay
+    from cuhepy_b200.bfv.client import draw_noise
+
+    q = lay.rns_modulus(BFV_N, BFV_Q_BITS)
+    layout = lay.Layout(BFV_N, BFV_EMBED)
+    ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+    rng = np.random.default_rng(1337)
+    bits = rng.integers(0, 2, size=(vectors, BFV_EMBED), dtype=np.uint8)
+    slots = layout.index_slots(bits)
+    width = (q.bit_length() + 7) // 8
+    prng = random.Random(99)
+    pk = tuple(b"".join(prng.randrange(q).to_bytes(width, "little") for _ in range(BFV_N)) for _ in range(2))
+    u, e = draw_noise(len(slots), BFV_N, 21)
+    m.encrypt_packed(ring, pk, BFV_T, slots, u, e)  # warm
+    device_s, total_s = [], []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        u, e = draw_noise(len(slots), BFV_N, 21)
+        t1 = time.perf_counter()
+        cts = m.encrypt_packed(ring, pk, BFV_T, slots, u, e)
+        t2 = time.perf_counter()
+        device_s.append(t2 - t1)
+        total_s.append(t2 - t0)
+    cpu = client_cpu_baseline(q, pk, slots[0])
+    return {
+        "workload": "bfv_client_encrypt",
+        "metric": "BFV ciphertexts encrypted per second (N=8192, Q=3x60-bit, t=65537, 16 vectors per ciphertext)",
+        "ciphertexts": len(cts), "vectors": vectors,
+        "ciphertexts_per_s": len(cts) / statistics.mean(total_s),
+        "call_ms": 1e3 * statistics.mean(device_s), "with_noise_ms": 1e3 * statistics.mean(total_s),
+        "vectors_per_s": vectors / statistics.mean(total_s),
+        "cpu_baseline": cpu,
+        "reference_published": {"seconds_for_8192_vectors": 54.6, "hardware": "Ryzen 7 5800X, one thread",
+                                "source": "docs/research/native-bfv.md:481"},
+        "path": "cuhe_bfv_encrypt: batch encode (NTT mod t), NTT(u) x NTT(pk), inverse NTT, noise + delta m, "
+                "compose, pack; H2D of slots/u/e and D2H of the packed wire inside the call",
+    }
+
+
+def client_cpu_baseline(q: int, pk: tuple, slots) -> dict:
+    """The oracle's encrypt (GMP products, one core) of one ciphertext."""
+    from oracle import bfv as ob
+
+    width = (q.bit_length() + 7) // 8
+    keys = {"params": ob.Params(BFV_N, BFV_T, BFV_Q_BITS, BFV_GADGET, 21), "q": q,
+            "b": [int.from_bytes(pk[0][i * width:(i + 1) * width], "little") for i in range(BFV_N)],
+            "a": [int.from_bytes(pk[1][i * width:(i + 1) * width], "little") for i in range(BFV_N)]}
+
+    class Rng:
+        def __init__(self):
+            self.r = random.Random(5)
+
+        def randbelow(self, k):
+            return self.r.randrange(k)
+
+        def randbits(self, k):
+            return self.r.getrandbits(k)
+
+    t0 = time.perf_counter()
+    ob.encrypt(ob.batch_encode([int(v) for v in slots], BFV_N, BFV_T), keys, Rng())
+    secs = time.perf_counter() - t0
+    return {"value": 1.0 / secs, "unit": "ciphertexts/s", "cores": 1, "kind": "port",
+            "sample": "one ciphertext: oracle/bfv.py batch_encode + encrypt over GMP products, one core"}
+
+
+def textbook_cpu_baseline(keys: dict, ms: list, rs: list, cs: list) -> tuple[float, float]:
+    """CPU baseline of the plain Paillier section: the oracle (GMP powm, one
+    core) encrypting and decrypting a few of the same operands."""
+    from oracle import paillier as oracle
+
+    t0 = time.perf_counter()
+    for m, r in zip(ms, rs):
+        oracle.encrypt(m, r, keys["pk"])
+    enc = len(ms) / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for c in cs:
+        oracle.decrypt(c, keys)
+    dec = len(cs) / (time.perf_counter() - t0)
+    return enc, dec
+
+
 def run_mixed(steps: int = 5, seed: int = 5) -> dict:
     """Batched uneven mix: Paillier fixed-exponent exponentiations r^n at two
     widths (n^2 2048-bit and 4096-bit, four keys each) with 1,000-50,000
@@ -843,8 +920,8 @@ def run_mixed(steps: int = 5, seed: int = 5) -> dict:
 
     from cuhepy_b200.batch import MixedBatch
     from cuhepy_b200.bfv import _bfv_rns as m
+    from cuhepy_b200.bfv import layout as lay
     from cuhepy_b200.paillier.gpu import PaillierDevice
-    from oracle import bfv as ob
 
     rng = random.Random(seed)
     gen = torch.Generator(device="cuda")
@@ -869,9 +946,7 @@ def run_mixed(steps: int = 5, seed: int = 5) -> dict:
     ntt_batches = []
     for k, n in enumerate((4096, 8192, 16384) * 2):
         limbs = rng.randint(2, 8)
-        qm = 1
-        for pr in ob.rns_primes(n, 60 * limbs):
-            qm *= pr
+        qm = lay.rns_modulus(n, 60 * limbs)
         ring = m.create_ring(n, format(qm, "x"), 30, True, True, 2)
         primes = m.ring_info(ring)["primes"][:limbs]
         planes = torch.randint(0, 1 << 59, (64 * limbs, n), dtype=torch.int64, device="cuda", generator=gen)
@@ -1082,7 +1157,7 @@ def profile_case(which: str) -> None:
     if which == "paillier":
         from cuhepy_b200.paillier.gpu import PaillierDevice
 
-        keys = seeded_lookup_keys_cpu(0)  # host-built keys: the only k_modexp launches are the decodes
+        keys = seeded_lookup_keys(0)  # k_modexp_crt serves only the decodes
         pk, sk = keys["pk"], keys["sk"]
         ctx = PaillierDevice(pk["n"])
         ctx.set_secret(sk["a"], sk["g_a_inv"])
@@ -1130,6 +1205,8 @@ def main() -> None:
     parser.add_argument("--mixed-only", action="store_true", help="run only the mixed-batch section")
     parser.add_argument("--textbook-only", action="store_true", help="run only the plain Paillier section")
     parser.add_argument("--bfv-only", action="store_true", help="run only the BFV kNN section")
+    parser.add_argument("--client-only", action="store_true", help="run only the BFV client encryption section")
+    parser.add_argument("--no-client", action="store_true", help="skip the BFV client encryption section")
     parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
     parser.add_argument("--profile-case", choices=["paillier", "bfv"],
@@ -1140,6 +1217,9 @@ def main() -> None:
         return
     if args.serving_only:
         print(json.dumps(run_serving()))
+        return
+    if args.client_only:
+        print(json.dumps({"client": run_client()}))
         return
     if args.bfv_only:
         print(json.dumps({"bfv": run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)}))

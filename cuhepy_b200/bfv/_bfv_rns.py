@@ -54,6 +54,9 @@ BFV_SIGNATURES: dict[str, tuple] = {
     "cuhe_bfv_search_index": (ctypes.c_int, [_vp, _vp, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, _vp,
                                              ctypes.c_uint64, _u64p]),
     "cuhe_bfv_set_lanes": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "cuhe_bfv_batch_encode": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp, ctypes.c_uint64, _vp]),
+    "cuhe_bfv_encrypt": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint64, _vp, _vp, _vp, ctypes.c_uint64,
+                                        _vp]),
     "cuhe_bfv_packed_search_parts": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p),
                                                     ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _vp,
                                                     ctypes.c_uint64, _u64p]),
@@ -109,10 +112,11 @@ class _Handle:
 class Ring(_Handle):
     _release = "cuhe_bfv_ring_release"
 
-    def __init__(self, ptr: int, n: int, coefficient_bytes: int) -> None:
+    def __init__(self, ptr: int, n: int, coefficient_bytes: int, q_bits: int = 0) -> None:
         super().__init__(ptr)
         self.n = n
         self.coefficient_bytes = coefficient_bytes
+        self.q_bits = q_bits
 
 
 class Key(_Handle):
@@ -182,7 +186,7 @@ def create_ring(n: int, q_hex: str, digit_bits: int, fast: bool = False, residue
     _check(lib().cuhe_bfv_create_ring(n, q_hex.encode(), digit_bits, int(bool(fast)), int(bool(residue)),
                                       kernel_level, 0, ctypes.byref(handle)))
     q_bits = int(q_hex, 16).bit_length()
-    return Ring(handle.value, n, (q_bits + 7) // 8)
+    return Ring(handle.value, n, (q_bits + 7) // 8, q_bits)
 
 
 def ring_info(ring: Ring) -> dict[str, Any]:
@@ -407,6 +411,47 @@ def ntt(ring: Ring, planes, primes: int, inverse: bool = False, threads: int = 0
         stream = torch.cuda.current_stream(planes.device).cuda_stream
     _check(lib().cuhe_bfv_ntt(ring.ptr, planes.data_ptr(), planes.shape[0], int(primes), int(bool(inverse)),
                               int(threads), int(radix_log), _vp(stream)))
+
+
+def batch_encode(ring: Ring, t: int, slots):
+    """Batch encoding on the device (not in the reference ABI): slots
+    [count, N] below t -> [count, N] plaintext coefficients (numpy uint64)."""
+    import numpy as np
+
+    ring = _get(ring, Ring)
+    slots = np.ascontiguousarray(slots, dtype=np.uint32)
+    if slots.ndim == 1:
+        slots = slots.reshape(1, -1)
+    if slots.ndim != 2 or slots.shape[1] != ring.n:
+        raise ValueError("slots must be [count, N]")
+    out = np.empty(slots.shape, dtype=np.uint64)
+    _check(lib().cuhe_bfv_batch_encode(ring.ptr, int(t), slots.ctypes.data, slots.shape[0], out.ctypes.data))
+    return out
+
+
+def encrypt_packed(ring: Ring, public_key: Any, t: int, slots, u, e) -> list[tuple[bytes, bytes]]:
+    """Batched client encryption on the device (not in the reference ABI):
+    public_key = (b, a) fixed-width polys; slots [count, N] (< t), u
+    [count, N] ternary, e [count, 2, N] signed small noise (numpy arrays).
+    Returns packed (c0, c1) per plaintext, the packed_search wire."""
+    import numpy as np
+
+    ring = _get(ring, Ring)
+    if not isinstance(public_key, tuple) or len(public_key) != 2:
+        raise ValueError("public key must be (b, a)")
+    pk = b"".join(_poly(p, ring) for p in public_key)
+    slots = np.ascontiguousarray(slots, dtype=np.uint32)
+    u = np.ascontiguousarray(u, dtype=np.int8)
+    e = np.ascontiguousarray(e, dtype=np.int8)
+    count = slots.shape[0] if slots.ndim == 2 else -1
+    if slots.shape != (count, ring.n) or u.shape != (count, ring.n) or e.shape != (count, 2, ring.n):
+        raise ValueError("slots, u and e must be [count, N], [count, N] and [count, 2, N]")
+    size = (ring.n * ring.q_bits + 7) // 8
+    out = ctypes.create_string_buffer(max(1, count * 2 * size))
+    _check(lib().cuhe_bfv_encrypt(ring.ptr, pk, int(t), slots.ctypes.data, u.ctypes.data, e.ctypes.data, count,
+                                  out))
+    raw = out.raw
+    return [(raw[2 * i * size:(2 * i + 1) * size], raw[(2 * i + 1) * size:(2 * i + 2) * size]) for i in range(count)]
 
 
 def set_lanes(ring: Ring, lanes: int) -> None:

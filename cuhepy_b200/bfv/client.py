@@ -1,0 +1,66 @@
+"""Client-side BFV encryption on the device (batched).
+
+The reference's client encrypts one plaintext at a time in Python
+(``BFV.encrypt``, src/cuhepy/bfv/scheme.py:426-444, with the batch encoding
+of scheme.py:371-394): u ternary, e0 and e1 centred binomial with ``eta``
+bits per side, c0 = b u + e0 + floor(Q/t) m and c1 = a u + e1.  Here the
+noise is drawn on the host and every ring product, the batch encoding and
+the wire packing run on the GPU for the whole batch (``cuhe_bfv_encrypt``).
+Given the same draws, the ciphertexts are the reference's.
+"""
+
+from __future__ import annotations
+
+import secrets
+from typing import Any
+
+import numpy as np
+
+from cuhepy_b200.bfv import _bfv_rns
+
+
+def draw_noise(count: int, n: int, eta: int = 21, rng: Any = None) -> tuple[np.ndarray, np.ndarray]:
+    """(u [count, n] ternary, e [count, 2, n]) as int8.
+
+    With ``rng`` (an object with ``randbelow``/``randbits``, like
+    ``secrets``) the draws are made one value at a time in the reference's
+    order per ciphertext (u, then e0, then e1; scheme.py:236-246, 438-439),
+    so a seeded ``rng`` reproduces the reference's ciphertexts.  Without it,
+    the same distributions are drawn in bulk from the operating system's
+    CSPRNG."""
+    if not 1 <= eta <= 63:
+        raise ValueError("eta must be 1..63")
+    if rng is not None:
+        u = np.empty((count, n), dtype=np.int8)
+        e = np.empty((count, 2, n), dtype=np.int8)
+        for c in range(count):
+            u[c] = [rng.randbelow(3) - 1 for _ in range(n)]
+            for k in range(2):
+                e[c, k] = [rng.randbits(eta).bit_count() - rng.randbits(eta).bit_count() for _ in range(n)]
+        return u, e
+    gen = np.random.Generator(np.random.PCG64DXSM(secrets.randbits(128)))
+    # ternary by rejection on bytes (0..254 are uniform mod 3)
+    u = np.empty(count * n, dtype=np.int8)
+    filled = 0
+    while filled < u.size:
+        raw = np.frombuffer(secrets.token_bytes(2 * (u.size - filled) + 64), dtype=np.uint8)
+        raw = raw[raw < 255][: u.size - filled]
+        u[filled:filled + raw.size] = (raw % 3).astype(np.int8) - 1
+        filled += raw.size
+    mask = (1 << eta) - 1
+    pos = gen.integers(0, 1 << 63, size=(count, 2, n), dtype=np.int64) & mask
+    neg = gen.integers(0, 1 << 63, size=(count, 2, n), dtype=np.int64) & mask
+    popcount = np.vectorize(int.bit_count, otypes=[np.int64]) if not hasattr(np, "bitwise_count") else np.bitwise_count
+    e = (popcount(pos).astype(np.int16) - popcount(neg).astype(np.int16)).astype(np.int8)
+    return u.reshape(count, n), e
+
+
+def encrypt_batch(ring, public_key: tuple, t: int, slots, eta: int = 21, rng: Any = None) -> list[tuple[bytes, bytes]]:
+    """Encrypt every row of ``slots`` ([count, N] slot values below t) under
+    ``public_key`` = (b, a) fixed-width polys; returns packed (c0, c1)
+    ciphertexts (the packed_search input wire)."""
+    slots = np.ascontiguousarray(slots, dtype=np.uint32)
+    if slots.ndim != 2:
+        raise ValueError("slots must be [count, N]")
+    u, e = draw_noise(slots.shape[0], slots.shape[1], eta, rng)
+    return _bfv_rns.encrypt_packed(ring, public_key, t, slots, u, e)

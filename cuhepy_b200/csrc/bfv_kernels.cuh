@@ -666,6 +666,75 @@ __global__ void k_mul_plain(u64* __restrict__ data, long long planes, int L, con
   data[idx] = reduce128(u128(data[idx]) * plain[(long long)j * R.n + i], R.prime[j]);
 }
 
+// ---- client-side encryption (bfv/scheme.py:371-394, 426-444) -------------------
+// Batch encoding: plane c position perm[j] receives slot j of plaintext c, so
+// that the inverse negacyclic NTT mod t of the plane is the encoded
+// polynomial (slot j is the value at the evaluation point of order[j]).
+__global__ void k_scatter_slots(const uint32_t* __restrict__ slots, const int32_t* __restrict__ perm,
+                                long long count, int n, uint32_t t, u64* __restrict__ planes, int* status) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= count * n) return;
+  const long long c = idx / n;
+  const int j = int(idx % n);
+  const uint32_t v = slots[idx];
+  if (v >= t) {
+    atomicOr(status, 1);
+    return;
+  }
+  planes[c * n + perm[j]] = v;
+}
+
+// out[poly][j][i] = v mod p_j for signed small v (u, e): residues mod the
+// first L primes.
+__global__ void k_small_residues(const int8_t* __restrict__ v, long long polys, int L, u64* __restrict__ out,
+                                 const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const int x = v[idx];
+  for (int j = 0; j < L; ++j) {
+    const u64 p = R.prime[j].p;
+    out[(poly * L + j) * R.n + i] = x >= 0 ? u64(x) : p - u64(-x);
+  }
+}
+
+// prod[c][comp][j][i] = u_ntt[c][j][i] * pk_ntt[comp][j][i] mod p_j
+__global__ void k_mul_public(const u64* __restrict__ u_ntt, const u64* __restrict__ pk_ntt, long long count, int L,
+                             u64* __restrict__ prod, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = 2LL * L * R.n;
+  if (idx >= count * per) return;
+  const long long c = idx / per;
+  const long long rest = idx % per;
+  const int comp = int(rest / ((long long)L * R.n));
+  const int j = int((rest / R.n) % L);
+  const int i = int(rest % R.n);
+  prod[idx] = mulmod(u_ntt[(c * L + j) * R.n + i], pk_ntt[((long long)comp * L + j) * R.n + i], R.prime[j]);
+}
+
+// ct[c][0] += e[c][0] + delta * m[c], ct[c][1] += e[c][1]  (mod p_j); m < t
+__global__ void k_add_noise_message(u64* __restrict__ ct, const int8_t* __restrict__ e, const u64* __restrict__ m,
+                                    const u64* __restrict__ delta, long long count, int L,
+                                    const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = 2LL * L * R.n;
+  if (idx >= count * per) return;
+  const long long c = idx / per;
+  const long long rest = idx % per;
+  const int comp = int(rest / ((long long)L * R.n));
+  const int j = int((rest / R.n) % L);
+  const int i = int(rest % R.n);
+  const u64 p = R.prime[j].p;
+  const int x = e[(c * 2 + comp) * R.n + i];
+  u64 v = addmod(ct[idx], x >= 0 ? u64(x) : p - u64(-x), p);
+  if (comp == 0) v = addmod(v, mulmod(delta[j], m[c * R.n + i], R.prime[j]), p);
+  ct[idx] = v;
+}
+
 // q[b][i] = floor(x[b][i] * 2^64 / p_j), j = b % L: Shoup quotients of fixed
 // multipliers (compiled keys).
 __global__ void k_shoup_quotients(const u64* __restrict__ x, u64* __restrict__ q, long long planes, int L,

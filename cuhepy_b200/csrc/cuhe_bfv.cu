@@ -160,6 +160,12 @@ struct cuhe_bfv_ring {
   size_t table_bytes = 0;
   RingDev host_dev{};
   std::map<u64, RingDev*> dev_for_t;  // t == 0: no scale constants
+  struct PlainRing {             // batch encoding mod t: NTT tables and slot permutation
+    RingDev* d = nullptr;
+    u64* d_tables = nullptr;
+    int32_t* d_perm = nullptr;
+  };
+  std::map<u64, PlainRing> plain_for_t;  // guarded by mu
   std::mutex mu;  // guards dev_for_t
   std::vector<std::unique_ptr<Lane>> lanes;  // kMaxLanes, created with the ring
   std::atomic<int> active_lanes{1};
@@ -170,6 +176,11 @@ struct cuhe_bfv_ring {
     for (auto& ln : lanes)
       if (ln->stream) cudaStreamSynchronize(ln->stream);
     for (auto& kv : dev_for_t) cudaFree(kv.second);
+    for (auto& kv : plain_for_t) {
+      cudaFree(kv.second.d);
+      cudaFree(kv.second.d_tables);
+      cudaFree(kv.second.d_perm);
+    }
     if (d_tables) cudaFree(d_tables);
     for (auto& ln : lanes)
       if (ln->stream) cudaStreamDestroy(ln->stream);
@@ -278,6 +289,67 @@ int device_ring(cuhe_bfv_ring* r, u64 t, RingDev** out) {
   BFV_CUDA(cudaMemcpy(d, &dev, sizeof(RingDev), cudaMemcpyHostToDevice), "ring constants");
   r->dev_for_t[t] = d;
   *out = d;
+  return CUHE_OK;
+}
+
+// Batch-encoding tables for plaintext modulus t (prime, t = 1 mod 2N): the
+// NTT tables of t in RingDev form (one prime) and the permutation taking
+// slot j to the inverse transform's input position bitrev(order[j]), where
+// order lists the evaluation points psi^(3^j) then psi^(-3^j) (the
+// reference's batch layout, bfv/scheme.py:139-183).
+int plain_ring(cuhe_bfv_ring* r, u64 t, cuhe_bfv_ring::PlainRing* out) {
+  std::lock_guard<std::mutex> lock(r->mu);
+  auto it = r->plain_for_t.find(t);
+  if (it != r->plain_for_t.end()) { *out = it->second; return CUHE_OK; }
+  const size_t n = r->plan.n;
+  if (t < 3 || t >= (u64(1) << 32) || t % (2 * n) != 1 || !H::is_prime64(t))
+    return fail(CUHE_INVALID_ARGUMENT, "plaintext modulus must be a prime below 2^32 with t = 1 mod 2N");
+  const H::NTTTable tab = H::build_ntt(n, t);
+  std::vector<u64> tables(4 * n);
+  for (size_t i = 0; i < n; ++i) {
+    tables[2 * i] = tab.fwd[i];
+    tables[2 * i + 1] = tab.fwd_q[i];
+    tables[2 * n + 2 * i] = tab.inv[i];
+    tables[2 * n + 2 * i + 1] = tab.inv_q[i];
+  }
+  const unsigned logn = H::log2_exact(n);
+  std::vector<int32_t> perm(n);
+  u64 g = 1;
+  for (size_t j = 0; j < n / 2; ++j) {
+    const u64 e = g, e_neg = (2 * n - g) % (2 * n);
+    perm[j] = int32_t(H::bitrev(size_t((e - 1) / 2), logn));
+    perm[n / 2 + j] = int32_t(H::bitrev(size_t((e_neg - 1) / 2), logn));
+    g = g * 3 % (2 * n);
+  }
+  RingDev dev;
+  std::memset(&dev, 0, sizeof(dev));
+  dev.n = int(n);
+  dev.logn = int(logn);
+  dev.primes = dev.residue = dev.tensor = 1;
+  dev.prime[0] = H::make_prime(t);
+  dev.n_inv[0] = tab.n_inv;
+  dev.n_inv_q[0] = tab.n_inv_q;
+  dev.last[0] = tab.last;
+  dev.last_q[0] = tab.last_q;
+  cuhe_bfv_ring::PlainRing pr;
+  cudaError_t e = cudaMalloc(&pr.d_tables, tables.size() * 8);
+  if (e == cudaSuccess) e = cudaMemcpy(pr.d_tables, tables.data(), tables.size() * 8, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    dev.fwd2[0] = reinterpret_cast<const ulonglong2*>(pr.d_tables);
+    dev.inv2[0] = reinterpret_cast<const ulonglong2*>(pr.d_tables + 2 * n);
+    e = cudaMalloc(&pr.d, sizeof(RingDev));
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(pr.d, &dev, sizeof(RingDev), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&pr.d_perm, n * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMemcpy(pr.d_perm, perm.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(pr.d);
+    cudaFree(pr.d_tables);
+    cudaFree(pr.d_perm);
+    return fail(CUHE_CUDA_ERROR, std::string("plaintext tables: ") + cudaGetErrorString(e));
+  }
+  r->plain_for_t[t] = pr;
+  *out = pr;
   return CUHE_OK;
 }
 
@@ -1435,6 +1507,137 @@ uint64_t cuhe_bfv_search_workspace(const cuhe_bfv_server* s, uint64_t tiles, int
   if (!s || !tiles) return 0;
   const size_t ct = std::min<size_t>(size_t(tiles), search_chunk_tiles(s));
   return search_chunk_bytes(s, ct, compact ? s->target_bits : unsigned(s->ring->plan.q_bits));
+}
+
+int cuhe_bfv_batch_encode(cuhe_bfv_ring* r, uint64_t t, const uint32_t* slots, uint64_t count, uint64_t* out) {
+  if (!r || (count && (!slots || !out))) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  if (count == 0) return CUHE_OK;
+  const size_t n = r->plan.n;
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
+  DeviceGuard guard(r->device);
+  cuhe_bfv_ring::PlainRing pr;
+  if (int rc = plain_ring(r, t, &pr)) return rc;
+  const size_t chunk = std::min<size_t>(size_t(count), 1024);
+  BFV_CUDA(ln.arena.reserve(slice(chunk * n * 4) + slice(chunk * n * 8) + slice(sizeof(int)) + 4096), "workspace");
+  ln.arena.reset();
+  uint32_t* d_slots = ln.arena.take<uint32_t>(chunk * n);
+  u64* m = ln.arena.take<u64>(chunk * n);
+  int* d_status = ln.arena.take<int>(1);
+  BFV_ARENA(ln.arena);
+  BFV_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), ln.stream), "status");
+  for (size_t c0 = 0; c0 < size_t(count); c0 += chunk) {
+    const size_t cc = std::min(chunk, size_t(count) - c0);
+    BFV_CUDA(cudaMemcpyAsync(d_slots, slots + c0 * n, cc * n * 4, cudaMemcpyHostToDevice, ln.stream), "slots");
+    k_scatter_slots<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_slots, pr.d_perm, (long long)cc,
+                                                                                 int(n), uint32_t(t), m, d_status);
+    BFV_CUDA(cudaGetLastError(), "scatter");
+    k_ntt8<<<unsigned(cc), ntt_default_threads(n), ntt_smem(r), ln.stream>>>(m, pr.d, 0, 1, 1, 1, 3);
+    BFV_CUDA(cudaGetLastError(), "batch encode");
+    int status = 0;
+    BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
+    BFV_CUDA(cudaMemcpyAsync(out + c0 * n, m, cc * n * 8, cudaMemcpyDeviceToHost, ln.stream), "download");
+    BFV_CUDA(cudaStreamSynchronize(ln.stream), "batch encode");
+    if (status) return fail(CUHE_INVALID_ARGUMENT, "slot value not below the plaintext modulus");
+  }
+  return CUHE_OK;
+}
+
+int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
+                     const int8_t* e, uint64_t count, uint8_t* out) {
+  if (!r || !pk || (count && (!slots || !u || !e || !out))) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  if (!r->residue) return fail(CUHE_INVALID_ARGUMENT, "client encryption needs a residue ring");
+  if (count == 0) return CUHE_OK;
+  const auto& P = r->plan;
+  const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
+  const size_t in_bytes = (n * P.q_bits + 7) / 8;
+  for (uint64_t k = 0; k < count * n; ++k)
+    if (u[k] < -1 || u[k] > 1) return fail(CUHE_INVALID_ARGUMENT, "u must be ternary");
+  std::vector<u64> pk_words;
+  if (int rc = parse_polys(r, pk, 2, pk_words)) return rc;
+  Lane& ln = *r->lanes[0];
+  std::lock_guard<std::mutex> lock(ln.mu);
+  DeviceGuard guard(r->device);
+  RingDev* d = nullptr;
+  if (int rc = device_ring(r, 0, &d)) return rc;
+  cuhe_bfv_ring::PlainRing pr;
+  if (int rc = plain_ring(r, t, &pr)) return rc;
+  // delta = floor(Q / t) mod p_j = -(Q mod t) * t^-1 mod p_j (p_j divides Q)
+  const u64 q_mod_t = H::mod_small(P.q, t);
+  std::vector<u64> delta(L);
+  for (size_t j = 0; j < L; ++j) {
+    const u64 p = P.primes[j];
+    const u64 t_inv = H::powmod(t % p, p - 2, p);
+    delta[j] = u64(u128((p - q_mod_t % p) % p) * t_inv % p);
+  }
+  const size_t chunk = std::min<size_t>(size_t(count), 512);
+  const size_t out_words = (n * P.q_bits + 63) / 64;
+  const size_t need = slice(2 * n * W * 8) + slice(2 * L * n * 8) + slice(L * 8) + slice(sizeof(int)) +
+                      slice(chunk * n * 4) + slice(chunk * n) + slice(chunk * 2 * n) + slice(chunk * n * 8) +
+                      slice(chunk * L * n * 8) + slice(chunk * 2 * L * n * 8) + slice(chunk * 2 * n * W * 8) +
+                      slice(chunk * 2 * out_words * 8) + slice(chunk * 2 * sizeof(ComposeOp)) + 65536;
+  BFV_CUDA(ln.arena.reserve(need), "workspace");
+  ln.arena.reset();
+  u64* pk_w = ln.arena.take<u64>(2 * n * W);
+  u64* pk_ntt = ln.arena.take<u64>(2 * L * n);
+  u64* d_delta = ln.arena.take<u64>(L);
+  int* d_status = ln.arena.take<int>(1);
+  uint32_t* d_slots = ln.arena.take<uint32_t>(chunk * n);
+  int8_t* d_u = ln.arena.take<int8_t>(chunk * n);
+  int8_t* d_e = ln.arena.take<int8_t>(chunk * 2 * n);
+  u64* m = ln.arena.take<u64>(chunk * n);
+  u64* u_ntt = ln.arena.take<u64>(chunk * L * n);
+  u64* ct = ln.arena.take<u64>(chunk * 2 * L * n);
+  u64* words = ln.arena.take<u64>(chunk * 2 * n * W);
+  u64* packed = ln.arena.take<u64>(chunk * 2 * out_words);
+  ComposeOp* d_cops = ln.arena.take<ComposeOp>(chunk * 2);
+  BFV_ARENA(ln.arena);
+  BFV_CUDA(cudaMemcpyAsync(pk_w, pk_words.data(), pk_words.size() * 8, cudaMemcpyHostToDevice, ln.stream), "pk");
+  BFV_CUDA(cudaMemcpyAsync(d_delta, delta.data(), L * 8, cudaMemcpyHostToDevice, ln.stream), "delta");
+  BFV_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), ln.stream), "status");
+  k_words_to_residues<<<blocks_for((long long)(2 * n), 256), 256, 0, ln.stream>>>(pk_w, 2, int(L), pk_ntt, d);
+  BFV_CUDA(cudaGetLastError(), "pk residues");
+  BFV_CUDA(launch_ntt(r, ln, d, pk_ntt, (long long)(2 * L), 0, int(L), 1, 0), "pk ntt");
+  std::vector<u64> host(chunk * 2 * out_words);
+  for (size_t c0 = 0; c0 < size_t(count); c0 += chunk) {
+    const size_t cc = std::min(chunk, size_t(count) - c0);
+    BFV_CUDA(cudaMemcpyAsync(d_slots, slots + c0 * n, cc * n * 4, cudaMemcpyHostToDevice, ln.stream), "slots");
+    BFV_CUDA(cudaMemcpyAsync(d_u, u + c0 * n, cc * n, cudaMemcpyHostToDevice, ln.stream), "u");
+    BFV_CUDA(cudaMemcpyAsync(d_e, e + c0 * 2 * n, cc * 2 * n, cudaMemcpyHostToDevice, ln.stream), "e");
+    // batch encoding: m = INTT_t(scattered slots)
+    k_scatter_slots<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_slots, pr.d_perm, (long long)cc,
+                                                                                 int(n), uint32_t(t), m, d_status);
+    BFV_CUDA(cudaGetLastError(), "scatter");
+    k_ntt8<<<unsigned(cc), ntt_default_threads(n), ntt_smem(r), ln.stream>>>(m, pr.d, 0, 1, 1, 1, 3);
+    BFV_CUDA(cudaGetLastError(), "batch encode");
+    // (b, a) * u + (e0 + delta m, e1)
+    k_small_residues<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_u, (long long)cc, int(L), u_ntt, d);
+    BFV_CUDA(cudaGetLastError(), "u residues");
+    BFV_CUDA(launch_ntt(r, ln, d, u_ntt, (long long)(cc * L), 0, int(L), 1, 0), "u ntt");
+    k_mul_public<<<blocks_for((long long)(cc * 2 * L * n), 256), 256, 0, ln.stream>>>(u_ntt, pk_ntt, (long long)cc,
+                                                                                     int(L), ct, d);
+    BFV_CUDA(cudaGetLastError(), "products");
+    BFV_CUDA(launch_ntt(r, ln, d, ct, (long long)(cc * 2 * L), 0, int(L), 1, 1), "intt");
+    k_add_noise_message<<<blocks_for((long long)(cc * 2 * L * n), 256), 256, 0, ln.stream>>>(
+        ct, d_e, m, d_delta, (long long)cc, int(L), d);
+    BFV_CUDA(cudaGetLastError(), "noise");
+    std::vector<ComposeOp> cops(cc * 2);
+    for (size_t k = 0; k < cc * 2; ++k) cops[k] = ComposeOp{ct + k * L * n, words + k * n * W, 1u, 0u};
+    if (int rc = run_switch(r, ln, d, cops, {}, d_cops, nullptr)) return rc;
+    k_pack<<<blocks_for((long long)(cc * 2 * out_words), 256), 256, 0, ln.stream>>>(
+        words, int(W), int(n), int(P.q_bits), int(cc * 2), packed, (long long)(out_words));
+    BFV_CUDA(cudaGetLastError(), "pack");
+    int status = 0;
+    BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
+    BFV_CUDA(cudaMemcpyAsync(host.data(), packed, cc * 2 * out_words * 8, cudaMemcpyDeviceToHost, ln.stream),
+             "download");
+    BFV_CUDA(cudaStreamSynchronize(ln.stream), "encrypt");
+    if (status) return fail(CUHE_INVALID_ARGUMENT, "slot value not below the plaintext modulus");
+    for (size_t k = 0; k < cc * 2; ++k)
+      std::memcpy(out + (c0 * 2 + k) * in_bytes, reinterpret_cast<const uint8_t*>(host.data() + k * out_words),
+                  in_bytes);
+  }
+  return CUHE_OK;
 }
 
 }  // extern "C"

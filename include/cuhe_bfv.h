@@ -124,6 +124,23 @@ int cuhe_bfv_last_profile(const cuhe_bfv_server* server, double* ms, int capacit
 int cuhe_bfv_ntt(cuhe_bfv_ring* ring, uint64_t* planes, uint64_t count, int primes, int inverse, int threads,
                  int radix_log, void* stream);
 
+/* Batch encoding mod t of `count` slot vectors ([count][N], < t, in the
+ * reference's slot order; bfv/scheme.py:371-394): out receives the
+ * [count][N] plaintext coefficients.  t prime with t = 1 mod 2N. */
+int cuhe_bfv_batch_encode(cuhe_bfv_ring* ring, uint64_t t, const uint32_t* slots, uint64_t count, uint64_t* out);
+
+/* Client-side public-key encryption of `count` batched plaintexts
+ * (bfv/scheme.py:426-444 with the batch encoding of 371-394): for each c,
+ *   m  = batch_encode(slots[c])                    (mod t)
+ *   c0 = b u + e0 + floor(Q/t) m,  c1 = a u + e1   (mod Q)
+ * with pk = (b, a) as two fixed-width polys, slots [count][N] (< t, in the
+ * reference's slot order), u [count][N] ternary and e [count][2][N] signed
+ * small noise drawn by the caller.  out receives count * 2 packed polys
+ * (bits(Q) bits per coefficient, the packed_search wire), c0 then c1.
+ * Residue rings only; t prime with t = 1 mod 2N. */
+int cuhe_bfv_encrypt(cuhe_bfv_ring* ring, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
+                     const int8_t* e, uint64_t count, uint8_t* out);
+
 /* Execution lanes of a ring (1..8; 1 after create_ring).  Each lane is a
  * CUDA stream with its own device workspace.  packed_search / search_index
  * calls issued concurrently from several host threads take free lanes and
