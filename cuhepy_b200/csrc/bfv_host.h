@@ -342,7 +342,7 @@ inline size_t prime_count_for(const std::vector<u64>& primes, const Big& bound) 
   throw std::invalid_argument("Insufficient auxiliary CRT modulus for exact reconstruction");
 }
 
-inline RingPlan build_ring(size_t n, const Big& q, unsigned bits) {
+inline RingPlan build_ring(size_t n, const Big& q, unsigned bits, bool residue = true) {
   RingPlan r;
   const size_t qb = q.bits();
   if (n < 8 || n > 32768 || (n & (n - 1)) || cmp(q, Big(3)) < 0 || qb > 512 || bits < 1 || bits > qb)
@@ -376,13 +376,18 @@ inline RingPlan build_ring(size_t n, const Big& q, unsigned bits) {
     prefix = mul_small(prefix, r.primes[c - 1]);
     if (cmp(prefix, q) == 0) r.residue_count = c;
   }
-  if (!r.residue_count || r.residue_count > 8)
+  if (residue && (!r.residue_count || r.residue_count > 8))
     throw std::invalid_argument("Residue backend requires Q to be a product of the first 60-bit NTT primes");
+  if (!residue) r.residue_count = 0;
   r.tensor_count = prime_count_for(r.primes, tensor_bound);
   for (u64 p : r.primes) r.ntt.push_back(build_ntt(n, p));
-  r.garner_inv.assign(r.residue_count, {});
-  r.garner_inv_q.assign(r.residue_count, {});
-  for (size_t j = 0; j < r.residue_count; ++j) {
+  // Garner constants: over the residue primes, or over every auxiliary
+  // prime of a native (prime q) ring, whose results are composed from up to
+  // all of them
+  const size_t garner = residue ? r.residue_count : r.primes.size();
+  r.garner_inv.assign(garner, {});
+  r.garner_inv_q.assign(garner, {});
+  for (size_t j = 0; j < garner; ++j) {
     const u64 p = r.primes[j];
     for (size_t k = 0; k < j; ++k) {
       const u64 inv = powmod(r.primes[k] % p, p - 2, p);

@@ -12,7 +12,7 @@
 namespace cuhe {
 namespace bfv {
 
-constexpr int kMaxPrimes = 17;
+constexpr int kMaxPrimes = 18;
 constexpr int kMaxResidue = 8;
 constexpr int kCrtWordsDev = 18;
 constexpr int kMaxWords = 8;  // composed coefficient words (Q <= 512 bits)
@@ -33,7 +33,7 @@ struct RingDev {
   const ulonglong2* fwd2[kMaxPrimes];
   const ulonglong2* inv2[kMaxPrimes];
   u64 n_inv[kMaxPrimes], n_inv_q[kMaxPrimes], last[kMaxPrimes], last_q[kMaxPrimes];
-  u64 garner[kMaxResidue][kMaxResidue], garner_q[kMaxResidue][kMaxResidue];
+  u64 garner[kMaxPrimes][kMaxPrimes], garner_q[kMaxPrimes][kMaxPrimes];
   u64 q_words[kMaxWords];       // Q
   u64 pow64_mod[kMaxPrimes][kMaxWords];  // 2^(64i) mod p_j
   // exact scale-and-round (valid when has_scale)
@@ -664,6 +664,391 @@ __global__ void k_mul_plain(u64* __restrict__ data, long long planes, int L, con
   const int i = int(idx % R.n);
   const int j = int(plane % L);
   data[idx] = reduce128(u128(data[idx]) * plain[(long long)j * R.n + i], R.prime[j]);
+}
+
+// ---- native rings: coefficients are integers mod a prime q ----------------------
+// (rns_ntt.h:394-513, bfv_server.h:123-151 of the reference).  Products are
+// exact integers recovered by Garner from enough auxiliary primes, then
+// reduced mod q or scaled; the multiword division is Knuth's algorithm D on
+// 32-bit limbs.  Exact products fit kNarrowWords words up to 8 auxiliary
+// primes (moduli up to about 220 bits); larger moduli use the wide variant.
+constexpr int kNarrowWords = kMaxWords;
+constexpr int kWideWords = 18;  // 18 primes x 60 bits
+
+// u (nu limbs) = quo (nu - nv + 1 limbs) * v (nv limbs, top limb nonzero) + rem (nv limbs)
+template <int LIMBS>
+__device__ __forceinline__ void divmod_limbs(const uint32_t* u, int nu, const uint32_t* v, int nv, uint32_t* quo,
+                                             uint32_t* rem) {
+  if (nu < nv) {
+    for (int i = 0; i < nv; ++i) rem[i] = i < nu ? u[i] : 0u;
+    return;
+  }
+  if (nv == 1) {
+    u64 r = 0;
+    for (int i = nu - 1; i >= 0; --i) {
+      const u64 cur = (r << 32) | u[i];
+      quo[i] = uint32_t(cur / v[0]);
+      r = cur % v[0];
+    }
+    rem[0] = uint32_t(r);
+    return;
+  }
+  const int sh = __clz(v[nv - 1]);
+  uint32_t vn[LIMBS], un[LIMBS + 1];
+  for (int i = nv - 1; i > 0; --i) vn[i] = sh ? (v[i] << sh) | (v[i - 1] >> (32 - sh)) : v[i];
+  vn[0] = v[0] << sh;
+  un[nu] = sh ? u[nu - 1] >> (32 - sh) : 0u;
+  for (int i = nu - 1; i > 0; --i) un[i] = sh ? (u[i] << sh) | (u[i - 1] >> (32 - sh)) : u[i];
+  un[0] = u[0] << sh;
+  for (int j = nu - nv; j >= 0; --j) {
+    const u64 num = (u64(un[j + nv]) << 32) | un[j + nv - 1];
+    u64 qhat = num / vn[nv - 1];
+    u64 rhat = num % vn[nv - 1];
+    while (qhat >> 32 || qhat * vn[nv - 2] > ((rhat << 32) | un[j + nv - 2])) {
+      --qhat;
+      rhat += vn[nv - 1];
+      if (rhat >> 32) break;
+    }
+    long long borrow = 0;
+    for (int i = 0; i < nv; ++i) {
+      const u64 prod = qhat * vn[i];
+      const long long t = (long long)un[i + j] - borrow - (long long)(prod & 0xffffffffu);
+      un[i + j] = uint32_t(t);
+      borrow = (long long)(prod >> 32) - (t >> 32);
+    }
+    const long long t = (long long)un[j + nv] - borrow;
+    un[j + nv] = uint32_t(t);
+    quo[j] = uint32_t(qhat);
+    if (t < 0) {
+      --quo[j];
+      u64 carry = 0;
+      for (int i = 0; i < nv; ++i) {
+        const u64 sum = u64(un[i + j]) + vn[i] + carry;
+        un[i + j] = uint32_t(sum);
+        carry = sum >> 32;
+      }
+      un[j + nv] += uint32_t(carry);
+    }
+  }
+  for (int i = 0; i < nv; ++i) rem[i] = sh ? (un[i] >> sh) | (un[i + 1] << (32 - sh)) : un[i];
+}
+
+// significant 32-bit limbs of W words (at least one)
+__device__ __forceinline__ int words_to_limbs(const u64* w, int W, uint32_t* l) {
+  int n = 0;
+  for (int k = 0; k < W; ++k) {
+    l[2 * k] = uint32_t(w[k]);
+    l[2 * k + 1] = uint32_t(w[k] >> 32);
+  }
+  n = 2 * W;
+  while (n > 1 && l[n - 1] == 0) --n;
+  return n;
+}
+
+// Garner composition of `count` residues (stride apart) into the centred
+// integer x in (-P/2, P/2), P = prod p_j (the reference's decode:
+// value %= product; if value > half, value -= product).  Writes |x| as words,
+// sets *negative, returns the number of words written.
+//
+// The mixed-radix digits d_j (x mod P = d_0 + p_0 (d_1 + p_1 (d_2 + ...)))
+// decide the sign without composing P: as every p_j is odd, x mod P exceeds
+// (P - 1) / 2 exactly when (d_{c-1}, ..., d_0) exceeds ((p_{c-1} - 1) / 2,
+// ..., (p_0 - 1) / 2) lexicographically.  The digits of P - x are then
+// (p_j - 1 - d_j) plus one, carried upward.
+template <int MAXW>
+__device__ __forceinline__ int garner_words(const u64* res, long long stride, int count, const RingDev& R,
+                                            u64 (&w)[MAXW], bool* negative) {
+  u64 digit[kMaxPrimes];
+  for (int j = 0; j < count; ++j) {
+    const u64 p = R.prime[j].p;
+    u64 value = res[(long long)j * stride];
+    for (int k = 0; k < j; ++k) {
+      const u64 d = digit[k] >= p ? digit[k] - p : digit[k];
+      value = shoup(value + p - d, R.garner[j][k], R.garner_q[j][k], p);
+    }
+    digit[j] = value;
+  }
+  bool neg = false;
+  for (int j = count - 1; j >= 0; --j) {
+    const u64 half = (R.prime[j].p - 1) >> 1;
+    if (digit[j] != half) {
+      neg = digit[j] > half;
+      break;
+    }
+  }
+  if (neg) {
+    u64 carry = 1;
+    for (int j = 0; j < count; ++j) {
+      const u64 p = R.prime[j].p;
+      u64 e = p - 1 - digit[j] + carry;
+      carry = e == p ? 1 : 0;
+      digit[j] = carry ? 0 : e;
+    }
+  }
+  *negative = neg;
+  for (int k = 0; k < MAXW; ++k) w[k] = 0;
+  w[0] = digit[count - 1];
+  int used = 1;
+  for (int j = count - 1; j > 0; --j) {
+    u64 carry = digit[j - 1];
+    const u64 p = R.prime[j - 1].p;
+    for (int k = 0; k < used; ++k) {
+      const u128 prod = u128(w[k]) * p + carry;
+      w[k] = u64(prod);
+      carry = u64(prod >> 64);
+    }
+    if (carry && used < MAXW) w[used++] = carry;
+  }
+  return used;
+}
+
+// res: [polys][count][N] coefficient residues of exact integers x with
+// |x| < prod p_j / 2 (negacyclic products are signed).  mode 0: out = x mod q;
+// mode 1: out = floor((2 t x + q) / (2 q)) mod q, the signed BFV
+// scale-and-round of rns_ntt.h:500-510 (floor division).  out: [polys][N][W]
+// words.  MAXW: words of |x| (at least ceil(60 count / 64)).
+//
+// For x = -m < 0: x mod q = (q - m mod q) mod q, and
+// floor((q - 2 t m) / (2 q)) = -floor((2 t m + q - 1) / (2 q)).
+template <int MAXW>
+__global__ void k_native_reduce(const u64* __restrict__ res, long long polys, int count, u64* __restrict__ out,
+                                int mode, u64 t, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const int W = R.words;
+  constexpr int kLimbs = 2 * MAXW + 4;
+  u64 x[MAXW];
+  bool neg = false;
+  int xw = garner_words<MAXW>(res + poly * count * R.n + i, R.n, count, R, x, &neg);
+  uint32_t ql[kLimbs], xl[kLimbs], quo[kLimbs], rem[kLimbs];
+  const int qn = words_to_limbs(R.q_words, W, ql);
+  if (mode == 1) {
+    // y = 2 t |x| + q (- 1 when x < 0), then its quotient by 2 q
+    u64 y[MAXW + 2];
+    const int yw = (xw + 1 > W ? xw + 1 : W) + 1;
+    u64 carry = 0;
+    for (int k = 0; k < yw; ++k) {
+      const u128 prod = u128(k < xw ? x[k] : 0) * (2 * t) + carry;
+      y[k] = u64(prod);
+      carry = u64(prod >> 64);
+    }
+    u64 c2 = 0;
+    for (int k = 0; k < yw; ++k) {
+      const u128 sum = u128(y[k]) + (k < W ? R.q_words[k] : 0) + c2;
+      y[k] = u64(sum);
+      c2 = u64(sum >> 64);
+    }
+    if (neg)
+      for (int k = 0; k < yw; ++k)
+        if (y[k]--) break;  // y >= q >= 1: the borrow stops inside y
+    uint32_t yl[2 * (MAXW + 2)], dl[kLimbs];
+    const int yn = words_to_limbs(y, yw, yl);
+    u64 q2[kMaxWords + 1];
+    u64 c3 = 0;
+    for (int k = 0; k < W; ++k) {
+      q2[k] = (R.q_words[k] << 1) | c3;
+      c3 = R.q_words[k] >> 63;
+    }
+    q2[W] = c3;
+    const int dn = words_to_limbs(q2, W + 1, dl);
+    for (int k = 0; k < kLimbs; ++k) quo[k] = 0;
+    divmod_limbs<kLimbs>(yl, yn, dl, dn, quo, rem);
+    const int qlen = yn >= dn ? yn - dn + 1 : 1;
+    if (yn < dn) quo[0] = 0;
+    for (int k = 0; k < qlen; ++k) xl[k] = quo[k];
+    int xn = qlen;
+    while (xn > 1 && xl[xn - 1] == 0) --xn;
+    divmod_limbs<kLimbs>(xl, xn, ql, qn, quo, rem);
+  } else {
+    const int xn = words_to_limbs(x, xw, xl);
+    divmod_limbs<kLimbs>(xl, xn, ql, qn, quo, rem);
+  }
+  u64 r[kMaxWords];
+  bool nonzero = false;
+  for (int k = 0; k < W; ++k) {
+    const uint32_t lo = 2 * k < qn ? rem[2 * k] : 0u, hi = 2 * k + 1 < qn ? rem[2 * k + 1] : 0u;
+    r[k] = u64(lo) | (u64(hi) << 32);
+    nonzero |= r[k] != 0;
+  }
+  if (neg && nonzero) {  // r <- q - r
+    u64 borrow = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 d = u128(R.q_words[k]) - r[k] - borrow;
+      r[k] = u64(d);
+      borrow = u64(d >> 64) ? 1 : 0;
+    }
+  }
+  u64* o = out + (poly * R.n + i) * W;
+  for (int k = 0; k < W; ++k) o[k] = r[k];
+}
+
+// out = a +- b mod q over `units` polys of words; poly u of a / b / out
+// starts at u * stride coefficients (stride 0 repeats one poly).
+__global__ void k_words_addsub(const u64* __restrict__ a, long long a_stride, const u64* __restrict__ b,
+                               long long b_stride, u64* __restrict__ out, long long out_stride, long long units,
+                               int subtract, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= units * R.n) return;
+  const long long u = idx / R.n;
+  const int i = int(idx % R.n);
+  const int W = R.words;
+  const u64* x = a + (u * a_stride + i) * W;
+  const u64* y = b + (u * b_stride + i) * W;
+  u64 r[kMaxWords];
+  if (subtract) {
+    u64 borrow = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 d = u128(x[k]) - y[k] - borrow;
+      r[k] = u64(d);
+      borrow = u64(d >> 64) ? 1 : 0;
+    }
+    if (borrow) {
+      u64 carry = 0;
+      for (int k = 0; k < W; ++k) {
+        const u128 sum = u128(r[k]) + R.q_words[k] + carry;
+        r[k] = u64(sum);
+        carry = u64(sum >> 64);
+      }
+    }
+  } else {
+    u64 carry = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 sum = u128(x[k]) + y[k] + carry;
+      r[k] = u64(sum);
+      carry = u64(sum >> 64);
+    }
+    // subtract q when the sum is at least q (a carry out means it is)
+    bool ge = carry != 0;
+    if (!ge) {
+      ge = true;
+      for (int k = W - 1; k >= 0; --k)
+        if (r[k] != R.q_words[k]) { ge = r[k] > R.q_words[k]; break; }
+    }
+    if (ge) {
+      u64 borrow = 0;
+      for (int k = 0; k < W; ++k) {
+        const u128 d = u128(r[k]) - R.q_words[k] - borrow;
+        r[k] = u64(d);
+        borrow = u64(d >> 64) ? 1 : 0;
+      }
+    }
+  }
+  u64* o = out + (u * out_stride + i) * W;
+  for (int k = 0; k < W; ++k) o[k] = r[k];
+}
+
+// out[poly] = sigma_g(in[poly]) on words mod q: coefficient i moves to
+// g i mod 2N, negated when that wraps past N (rns_ntt.h:656-664).
+__global__ void k_words_automorphism(const u64* __restrict__ in, u64* __restrict__ out, long long polys, unsigned g,
+                                     const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const int W = R.words;
+  const unsigned at = unsigned((unsigned long long)i * g % (2u * unsigned(R.n)));
+  const u64* x = in + idx * W;
+  u64* o = out + (poly * R.n + (at % unsigned(R.n))) * W;
+  bool nonzero = false;
+  for (int k = 0; k < W; ++k) nonzero |= x[k] != 0;
+  if (at >= unsigned(R.n) && nonzero) {
+    u64 borrow = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 d = u128(R.q_words[k]) - x[k] - borrow;
+      o[k] = u64(d);
+      borrow = u64(d >> 64) ? 1 : 0;
+    }
+  } else {
+    for (int k = 0; k < W; ++k) o[k] = x[k];
+  }
+}
+
+// Per-ciphertext descriptors of the native rotate / add steps (two word polys
+// each): permute writes perm = sigma_g(in); finish writes out = (ks0 + perm0,
+// ks1); add writes out = in + perm.
+struct NativeOp {
+  const u64* in;
+  u64* perm;
+  u64* out;
+  const u64* ks;
+};
+
+__device__ __forceinline__ void words_add_modq(const u64* x, const u64* y, u64* o, const RingDev& R) {
+  const int W = R.words;
+  u64 r[kMaxWords];
+  u64 carry = 0;
+  for (int k = 0; k < W; ++k) {
+    const u128 sum = u128(x[k]) + y[k] + carry;
+    r[k] = u64(sum);
+    carry = u64(sum >> 64);
+  }
+  bool ge = carry != 0;
+  if (!ge) {
+    ge = true;
+    for (int k = W - 1; k >= 0; --k)
+      if (r[k] != R.q_words[k]) { ge = r[k] > R.q_words[k]; break; }
+  }
+  if (ge) {
+    u64 borrow = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 d = u128(r[k]) - R.q_words[k] - borrow;
+      r[k] = u64(d);
+      borrow = u64(d >> 64) ? 1 : 0;
+    }
+  }
+  for (int k = 0; k < W; ++k) o[k] = r[k];
+}
+
+// grid: (blocks over 2N coefficients, ops)
+__global__ void k_native_permute(const NativeOp* __restrict__ ops, unsigned g, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const NativeOp op = ops[blockIdx.y];
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 2 * R.n) return;
+  const int c = idx / R.n, i = idx % R.n, W = R.words;
+  const unsigned at = unsigned((unsigned long long)i * g % (2u * unsigned(R.n)));
+  const u64* x = op.in + ((long long)c * R.n + i) * W;
+  u64* o = op.perm + ((long long)c * R.n + (at % unsigned(R.n))) * W;
+  bool nonzero = false;
+  for (int k = 0; k < W; ++k) nonzero |= x[k] != 0;
+  if (at >= unsigned(R.n) && nonzero) {
+    u64 borrow = 0;
+    for (int k = 0; k < W; ++k) {
+      const u128 d = u128(R.q_words[k]) - x[k] - borrow;
+      o[k] = u64(d);
+      borrow = u64(d >> 64) ? 1 : 0;
+    }
+  } else {
+    for (int k = 0; k < W; ++k) o[k] = x[k];
+  }
+}
+
+__global__ void k_native_finish(const NativeOp* __restrict__ ops, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const NativeOp op = ops[blockIdx.y];
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 2 * R.n) return;
+  const int W = R.words;
+  const long long off = (long long)idx * W;
+  if (idx < R.n) {
+    words_add_modq(op.ks + off, op.perm + off, op.out + off, R);
+  } else {
+    for (int k = 0; k < W; ++k) op.out[off + k] = op.ks[off + k];
+  }
+}
+
+__global__ void k_native_add(const NativeOp* __restrict__ ops, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const NativeOp op = ops[blockIdx.y];
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 2 * R.n) return;
+  const long long off = (long long)idx * R.words;
+  words_add_modq(op.in + off, op.perm + off, op.out + off, R);
 }
 
 // ---- client-side encryption (bfv/scheme.py:371-394, 426-444) -------------------

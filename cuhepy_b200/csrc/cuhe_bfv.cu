@@ -217,6 +217,7 @@ struct cuhe_bfv_server {
   u64* d_full_mask = nullptr;  // [L][N] NTT domain
   u64* d_target = nullptr;
   std::map<size_t, u64*> partial_masks;
+  size_t mask_primes = 0;  // primes of the prepared masks (L, or enough for N (q-1)(t-1) on native rings)
   RingDev* d_ring = nullptr;
   std::mutex mu;  // guards partial_masks and profile_ms
   double profile_ms[6] = {0, 0, 0, 0, 0, 0};
@@ -247,7 +248,7 @@ int device_ring(cuhe_bfv_ring* r, u64 t, RingDev** out) {
   auto it = r->dev_for_t.find(t);
   if (it != r->dev_for_t.end()) { *out = it->second; return CUHE_OK; }
   RingDev dev = r->host_dev;
-  if (t) {
+  if (t && r->residue) {  // native rings scale with multiword arithmetic instead
     H::RingPlan plan = r->plan;
     try {
       H::build_scale(plan, t);
@@ -426,7 +427,7 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
     BFV_CUDA(cudaMemcpyAsync(d_sops, sops.data(), sops.size() * sizeof(SwitchOp), cudaMemcpyHostToDevice, ln.stream),
              "switch ops");
     const size_t smem = ntt_smem(r);
-    dim3 grid(unsigned(sops.size()), unsigned(P.residue_count));
+    dim3 grid(unsigned(sops.size()), unsigned(r->residue ? P.residue_count : r->switch_prime_count));
     if (P.n <= 8192) {
       const size_t smem_acc = smem + 2 * P.n * sizeof(u64);  // accumulators after the plane
       BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<0, 1024, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -496,9 +497,10 @@ std::vector<u64> hamming_mask(size_t n, u64 t, size_t lanes, size_t count) {
 }
 
 // residues mod the first L primes of a small nonnegative polynomial, NTT'd
-int upload_plain_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<u64>& coeffs_words, u64** out) {
+int upload_plain_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<u64>& coeffs_words, u64** out,
+                     size_t primes = 0) {
   const auto& P = r->plan;
-  const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
+  const size_t n = P.n, L = primes ? primes : P.residue_count, W = size_t(r->host_dev.words);
   u64* d_words = nullptr;
   u64* d_res = nullptr;
   BFV_CUDA(cudaMalloc(&d_words, n * W * 8), "plain alloc");
@@ -622,6 +624,198 @@ size_t tile_arena_bytes(const cuhe_bfv_ring* r, size_t ct) {
          slice(ct * 2 * L * n * 8) + slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp));
 }
 
+// ---- native (prime q) rings: ciphertexts as words mod q --------------------------
+
+size_t native_mask_primes(const cuhe_bfv_ring* r, u64 t) {
+  // exact ct x pt product bound N (q - 1)(t - 1) (PreparedPlain, bfv_server.h:47-64)
+  const auto& P = r->plan;
+  const H::Big bound = H::mul_small(H::mul_small(H::sub(P.q, H::Big(1)), u64(P.n)), t - 1);
+  return H::prime_count_for(P.primes, bound);
+}
+
+int native_reduce(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* res, size_t polys, size_t count, u64* out,
+                  int mode, u64 t) {
+  if (!polys) return CUHE_OK;
+  const unsigned blocks = blocks_for((long long)(polys * r->plan.n), 128);
+  if (count <= size_t(kNarrowWords))
+    k_native_reduce<kNarrowWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, mode, t, d);
+  else
+    k_native_reduce<kWideWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, mode, t, d);
+  BFV_CUDA(cudaGetLastError(), "native reduce");
+  return CUHE_OK;
+}
+
+int words_addsub(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* a, size_t a_stride, const u64* b,
+                 size_t b_stride, u64* out, size_t out_stride, size_t units, int subtract) {
+  if (!units) return CUHE_OK;
+  k_words_addsub<<<blocks_for((long long)(units * r->plan.n), 256), 256, 0, ln.stream>>>(
+      a, (long long)a_stride, b, (long long)b_stride, out, (long long)out_stride, (long long)units, subtract, d);
+  BFV_CUDA(cudaGetLastError(), "words add/sub");
+  return CUHE_OK;
+}
+
+// exact products of `polys` word polys with NTT-domain plains (`count`
+// primes; masks[k] for poly k), reduced mod q into out (may alias words)
+int native_mul_plain(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* words, size_t polys,
+                     const std::vector<const u64*>& masks, size_t count, u64* res, u64* out) {
+  const size_t n = r->plan.n;
+  k_words_to_residues<<<blocks_for((long long)(polys * n), 256), 256, 0, ln.stream>>>(words, (long long)polys,
+                                                                                   int(count), res, d);
+  BFV_CUDA(cudaGetLastError(), "residues");
+  BFV_CUDA(launch_ntt(r, ln, d, res, (long long)(polys * count), 0, int(count), 1, 0), "ntt");
+  for (size_t k = 0; k < polys;) {
+    size_t run = 1;
+    while (k + run < polys && masks[k + run] == masks[k]) ++run;
+    k_mul_plain<<<blocks_for((long long)(run * count * n), 256), 256, 0, ln.stream>>>(
+        res + k * count * n, (long long)(run * count), int(count), masks[k], d);
+    BFV_CUDA(cudaGetLastError(), "product");
+    k += run;
+  }
+  BFV_CUDA(launch_ntt(r, ln, d, res, (long long)(polys * count), 0, int(count), 1, 1), "intt");
+  return native_reduce(r, ln, d, res, polys, count, out, 0, 0);
+}
+
+// key switches: out[k] = (key_k . digits(in[k])) mod q as two word polys
+// ([ops][2][N][W]); res: [ops][2][S][N] scratch
+int native_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<const u64*>& in,
+                  const std::vector<const cuhe_bfv_key*>& keys, u64* res, u64* out, SwitchOp* d_sops) {
+  const size_t n = r->plan.n, S = r->switch_prime_count;
+  std::vector<SwitchOp> sops(in.size());
+  for (size_t k = 0; k < in.size(); ++k)
+    sops[k] = SwitchOp{nullptr, nullptr, in[k], keys[k]->d_key, keys[k]->d_key_q, res + k * 2 * S * n, 1u, 0u};
+  if (int rc = run_switch(r, ln, d, {}, sops, nullptr, d_sops)) return rc;
+  return native_reduce(r, ln, d, res, in.size() * 2, S, out, 0, 0);
+}
+
+// rotations of word ciphertexts by g: ops[k].out = (sigma(c0) + KS(sigma(c1))_0,
+// KS(sigma(c1))_1) for ops[k].in, with ops[k].perm and ops[k].ks as
+// per-ciphertext scratch (two word polys each); d_ops, res and ks_all sized
+// for ops.size()
+int native_rotate(cuhe_bfv_ring* r, Lane& ln, RingDev* d, std::vector<NativeOp> ops, unsigned g,
+                  const cuhe_bfv_key* key, NativeOp* d_ops, u64* res, u64* ks_all, SwitchOp* d_sops) {
+  const size_t n = r->plan.n, W = size_t(r->host_dev.words);
+  if (ops.empty()) return CUHE_OK;
+  for (size_t k = 0; k < ops.size(); ++k) ops[k].ks = ks_all + k * 2 * n * W;
+  BFV_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(NativeOp), cudaMemcpyHostToDevice, ln.stream),
+           "rotation ops");
+  dim3 grid(blocks_for((long long)(2 * n), 256), unsigned(ops.size()));
+  k_native_permute<<<grid, 256, 0, ln.stream>>>(d_ops, g, d);
+  BFV_CUDA(cudaGetLastError(), "automorphism");
+  std::vector<const u64*> c1(ops.size());
+  std::vector<const cuhe_bfv_key*> keys(ops.size(), key);
+  for (size_t k = 0; k < ops.size(); ++k) c1[k] = ops[k].perm + n * W;
+  if (int rc = native_switch(r, ln, d, c1, keys, res, ks_all, d_sops)) return rc;
+  k_native_finish<<<grid, 256, 0, ln.stream>>>(d_ops, d);
+  BFV_CUDA(cudaGetLastError(), "rotation finish");
+  return CUHE_OK;
+}
+
+int native_add_ops(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<NativeOp>& ops, NativeOp* d_ops) {
+  if (ops.empty()) return CUHE_OK;
+  BFV_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(NativeOp), cudaMemcpyHostToDevice, ln.stream),
+           "add ops");
+  dim3 grid(blocks_for((long long)(2 * r->plan.n), 256), unsigned(ops.size()));
+  k_native_add<<<grid, 256, 0, ln.stream>>>(d_ops, d);
+  BFV_CUDA(cudaGetLastError(), "add");
+  return CUHE_OK;
+}
+
+// The Hamming tile circuit on word ciphertexts (distance_tile,
+// rns_ntt.h:672-700): (q - t)^2 scaled, relinearised, rotated and summed,
+// masked.  dist: [ct][2][N][W].
+struct NativeScratch {
+  u64 *diff, *dres, *tens, *words3, *ksres, *ksw, *perm, *tmp, *mres;
+  SwitchOp* d_sops;
+  NativeOp* d_nops;
+};
+
+size_t native_tile_bytes(const cuhe_bfv_ring* r, size_t ct, size_t mask_primes) {
+  const auto& P = r->plan;
+  const size_t n = P.n, T = P.tensor_count, S = r->switch_prime_count, W = size_t(r->host_dev.words);
+  return slice(ct * 2 * n * W * 8) + slice(ct * 2 * T * n * 8) + slice(ct * 3 * T * n * 8) +
+         slice(ct * 3 * n * W * 8) + slice(ct * 2 * S * n * 8) + 3 * slice(ct * 2 * n * W * 8) +
+         slice(ct * 2 * mask_primes * n * 8) + slice(ct * sizeof(SwitchOp)) + slice(ct * sizeof(NativeOp)) + 4096;
+}
+
+int native_scratch(Arena& ar, const cuhe_bfv_ring* r, size_t ct, size_t mask_primes, NativeScratch* s) {
+  const auto& P = r->plan;
+  const size_t n = P.n, T = P.tensor_count, S = r->switch_prime_count, W = size_t(r->host_dev.words);
+  s->diff = ar.take<u64>(ct * 2 * n * W);
+  s->dres = ar.take<u64>(ct * 2 * T * n);
+  s->tens = ar.take<u64>(ct * 3 * T * n);
+  s->words3 = ar.take<u64>(ct * 3 * n * W);
+  s->ksres = ar.take<u64>(ct * 2 * S * n);
+  s->ksw = ar.take<u64>(ct * 2 * n * W);
+  s->perm = ar.take<u64>(ct * 2 * n * W);
+  s->tmp = ar.take<u64>(ct * 2 * n * W);
+  s->mres = ar.take<u64>(ct * 2 * mask_primes * n);
+  s->d_sops = ar.take<SwitchOp>(std::max<size_t>(1, ct));
+  s->d_nops = ar.take<NativeOp>(std::max<size_t>(1, ct));
+  BFV_ARENA(ar);
+  return CUHE_OK;
+}
+
+int native_tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* qw, const u64* tw, size_t ct, u64 t,
+                        const cuhe_bfv_key* relin, const std::vector<u64>& exps,
+                        const std::vector<const cuhe_bfv_key*>& keys, const std::vector<const u64*>& masks,
+                        size_t mask_primes, const NativeScratch& s, u64* dist, double* ms) {
+  const auto& P = r->plan;
+  const size_t n = P.n, T = P.tensor_count, W = size_t(r->host_dev.words);
+  cudaEvent_t ev[5];
+  for (auto& e : ev) cudaEventCreate(&e);
+  cudaEventRecord(ev[0], ln.stream);
+  for (size_t c = 0; c < 2; ++c)
+    if (int rc = words_addsub(r, ln, d, qw + c * n * W, 0, tw + c * n * W, 2 * n, s.diff + c * n * W, 2 * n, ct, 1))
+      return rc;
+  k_words_to_residues<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(s.diff, (long long)(ct * 2),
+                                                                                       int(T), s.dres, d);
+  BFV_CUDA(cudaGetLastError(), "tensor residues");
+  BFV_CUDA(launch_ntt(r, ln, d, s.dres, (long long)(ct * 2 * T), 0, int(T), 1, 0), "tensor ntt");
+  k_tensor_square<<<blocks_for((long long)(ct * T * n), 256), 256, 0, ln.stream>>>(s.dres, int(ct), int(T), s.tens, d);
+  BFV_CUDA(cudaGetLastError(), "tensor");
+  BFV_CUDA(launch_ntt(r, ln, d, s.tens, (long long)(ct * 3 * T), 0, int(T), 1, 1), "tensor intt");
+  if (int rc = native_reduce(r, ln, d, s.tens, ct * 3, T, s.words3, 1, t)) return rc;
+  cudaEventRecord(ev[1], ln.stream);
+  // relinearise: dist = KS(p2) + (p0, p1)
+  std::vector<const u64*> p2(ct);
+  std::vector<const cuhe_bfv_key*> rk(ct, relin);
+  for (size_t k = 0; k < ct; ++k) p2[k] = s.words3 + (k * 3 + 2) * n * W;
+  if (int rc = native_switch(r, ln, d, p2, rk, s.ksres, s.ksw, s.d_sops)) return rc;
+  for (size_t c = 0; c < 2; ++c)
+    if (int rc = words_addsub(r, ln, d, s.ksw + c * n * W, 2 * n, s.words3 + c * n * W, 3 * n, dist + c * n * W,
+                              2 * n, ct, 0))
+      return rc;
+  cudaEventRecord(ev[2], ln.stream);
+  // rotations: dist += rotate(dist, g)
+  for (size_t e = 0; e < exps.size(); ++e) {
+    if (exps[e] == 1) {
+      if (int rc = words_addsub(r, ln, d, dist, n, dist, n, dist, n, ct * 2, 0)) return rc;
+      continue;
+    }
+    std::vector<NativeOp> ops(ct);
+    for (size_t k = 0; k < ct; ++k)
+      ops[k] = NativeOp{dist + k * 2 * n * W, s.perm + k * 2 * n * W, s.tmp + k * 2 * n * W, nullptr};
+    if (int rc = native_rotate(r, ln, d, ops, unsigned(exps[e]), keys[e], s.d_nops, s.ksres, s.ksw, s.d_sops))
+      return rc;
+    if (int rc = words_addsub(r, ln, d, dist, n, s.tmp, n, dist, n, ct * 2, 0)) return rc;
+  }
+  cudaEventRecord(ev[3], ln.stream);
+  std::vector<const u64*> pm(ct * 2);
+  for (size_t k = 0; k < ct * 2; ++k) pm[k] = masks[k / 2];
+  if (int rc = native_mul_plain(r, ln, d, dist, ct * 2, pm, mask_primes, s.mres, dist)) return rc;
+  cudaEventRecord(ev[4], ln.stream);
+  BFV_CUDA(cudaStreamSynchronize(ln.stream), "native tile circuit");
+  if (ms) {
+    float x;
+    cudaEventElapsedTime(&x, ev[0], ev[1]); ms[0] += x;
+    cudaEventElapsedTime(&x, ev[1], ev[2]); ms[1] += x;
+    cudaEventElapsedTime(&x, ev[2], ev[3]); ms[2] += x;
+    cudaEventElapsedTime(&x, ev[3], ev[4]); ms[3] += x;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return CUHE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -650,7 +844,7 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   if (!r) return fail(CUHE_OUT_OF_MEMORY, "ring allocation");
   try {
     const H::Big q = H::from_hex(q_hex);
-    r->plan = H::build_ring(size_t(n), q, unsigned(digit_bits));
+    r->plan = H::build_ring(size_t(n), q, unsigned(digit_bits), residue != 0);
     if (r->plan.n > 16384) throw std::invalid_argument("the B200 evaluator supports N <= 16384");
     if (r->plan.primes.size() > size_t(kMaxPrimes)) throw std::invalid_argument("too many auxiliary primes");
     if (!residue) {
@@ -658,6 +852,8 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
       const H::Big sb = H::mul(H::mul_small(H::Big(u64(n)), u64(r->plan.digits)),
                                H::mul(H::sub(H::shl(H::Big(1), size_t(digit_bits)), H::Big(1)), qm1));
       r->switch_prime_count = H::prime_count_for(r->plan.primes, sb);
+      if (r->plan.tensor_count > size_t(kMaxPrimes) || r->switch_prime_count > size_t(kMaxPrimes))
+        throw std::invalid_argument("native ring needs more auxiliary primes than the B200 evaluator holds");
     } else {
       r->switch_prime_count = r->plan.residue_count;
     }
@@ -725,11 +921,13 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
       pw = u64(u128(pw) * two64 % P.primes[j]);
     }
   }
-  for (size_t j = 0; j < P.residue_count; ++j)
+  for (size_t j = 0; j < P.garner_inv.size() && j < size_t(kMaxPrimes); ++j)
     for (size_t k = 0; k < j; ++k) {
       dev.garner[j][k] = P.garner_inv[j][k];
       dev.garner_q[j][k] = P.garner_inv_q[j][k];
     }
+  // native rings: key switches run over the switch primes
+  if (!r->residue) dev.residue = int(r->switch_prime_count);
   for (size_t w = 0; w < P.q.w.size() && w < size_t(kMaxWords); ++w) dev.q_words[w] = P.q.w[w];
   RingDev* dummy = nullptr;
   if (int rc = device_ring(r, 0, &dummy)) {
@@ -809,7 +1007,8 @@ int cuhe_bfv_compile_key(cuhe_bfv_ring* ring, const uint8_t* key_polys, uint64_t
   DeviceGuard guard(ring->device);
   std::vector<u64> words;
   if (int rc = parse_polys(ring, key_polys, size_t(2 * digits), words)) return rc;
-  const size_t n = P.n, L = P.residue_count, W = size_t(ring->host_dev.words);
+  // residue rings: keys over the L primes of Q; native rings: over the switch primes
+  const size_t n = P.n, L = ring->residue ? P.residue_count : ring->switch_prime_count;
   auto* key = new (std::nothrow) cuhe_bfv_key();
   if (!key) return fail(CUHE_OUT_OF_MEMORY, "key allocation");
   key->ring = ring;
@@ -896,6 +1095,19 @@ int cuhe_bfv_apply_key(cuhe_bfv_key* key, const uint8_t* poly, uint8_t* out) {
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
   const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  if (!r->residue) {
+    const size_t S = r->switch_prime_count;
+    BFV_CUDA(ln.arena.reserve(slice(n * W * 8) * 4 + slice(2 * S * n * 8) + 4096), "workspace");
+    ln.arena.reset();
+    u64* words = nullptr;
+    if (int rc = upload_polys(r, ln, d, poly, 1, 0, &words, nullptr)) return rc;
+    u64* res = ln.arena.take<u64>(2 * S * n);
+    u64* outw = ln.arena.take<u64>(2 * n * W);
+    SwitchOp* d_sops = ln.arena.take<SwitchOp>(1);
+    BFV_ARENA(ln.arena);
+    if (int rc = native_switch(r, ln, d, {words}, {key}, res, outw, d_sops)) return rc;
+    return download_words(r, ln, outw, 2, out);
+  }
   BFV_CUDA(ln.arena.reserve(slice(n * W * 8) * 3 + slice(2 * L * n * 8) * 2 + 4096), "workspace");
   ln.arena.reset();
   u64* words = nullptr;
@@ -924,6 +1136,24 @@ int cuhe_bfv_rotate_rows(cuhe_bfv_key* key, const uint8_t* ct, uint64_t exponent
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
+  if (!r->residue) {
+    const size_t S = r->switch_prime_count;
+    BFV_CUDA(ln.arena.reserve(slice(2 * n * W * 8) * 5 + slice(2 * S * n * 8) + 8192), "workspace");
+    ln.arena.reset();
+    u64* words = nullptr;
+    if (int rc = upload_polys(r, ln, d, ct, 2, 0, &words, nullptr)) return rc;
+    u64* perm = ln.arena.take<u64>(2 * n * W);
+    u64* outw = ln.arena.take<u64>(2 * n * W);
+    u64* ks = ln.arena.take<u64>(2 * n * W);
+    u64* res = ln.arena.take<u64>(2 * S * n);
+    SwitchOp* d_sops = ln.arena.take<SwitchOp>(1);
+    NativeOp* d_nops = ln.arena.take<NativeOp>(1);
+    BFV_ARENA(ln.arena);
+    if (int rc = native_rotate(r, ln, d, {NativeOp{words, perm, outw, nullptr}}, unsigned(exponent), key, d_nops, res,
+                               ks, d_sops))
+      return rc;
+    return download_words(r, ln, outw, 2, out);
+  }
   BFV_CUDA(ln.arena.reserve(slice(2 * n * W * 8) * 2 + slice(2 * L * n * 8) * 3 + slice(n * W * 8) + 8192), "workspace");
   ln.arena.reset();
   u64 *words = nullptr, *res = nullptr;
@@ -946,7 +1176,10 @@ int cuhe_bfv_ring_product(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* r
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
-  const size_t n = r->plan.n, L = r->plan.residue_count, W = size_t(r->host_dev.words);
+  const size_t n = r->plan.n, W = size_t(r->host_dev.words);
+  // residue rings multiply mod Q over its L primes; native rings take the
+  // exact product over the tensor primes and reduce it mod q
+  const size_t L = r->residue ? r->plan.residue_count : r->plan.tensor_count;
   BFV_CUDA(ln.arena.reserve(slice(n * W * 8) * 4 + slice(L * n * 8) * 3 + 8192), "workspace");
   ln.arena.reset();
   u64 *wa, *wb, *ra, *rb;
@@ -957,6 +1190,12 @@ int cuhe_bfv_ring_product(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* r
   k_mul_plain<<<blocks_for((long long)(L * n), 256), 256, 0, ln.stream>>>(ra, (long long)(L), int(L), rb, d);
   BFV_CUDA(cudaGetLastError(), "product");
   BFV_CUDA(launch_ntt(r, ln, d, ra, (long long)(L), 0, int(L), 1, 1), "intt");
+  if (!r->residue) {
+    u64* outw = ln.arena.take<u64>(n * W);
+    BFV_ARENA(ln.arena);
+    if (int rc = native_reduce(r, ln, d, ra, 1, L, outw, 0, 0)) return rc;
+    return download_words(r, ln, outw, 1, out);
+  }
   return compose_out(r, ln, d, ra, 1, out);
 }
 
@@ -987,6 +1226,12 @@ int cuhe_bfv_multiply(cuhe_bfv_ring* r, const uint8_t* lhs, const uint8_t* rhs, 
   k_tensor<<<blocks_for((long long)(T * n), 256), 256, 0, ln.stream>>>(ra, rb ? rb : ra, 1, int(T), tens, d);
   BFV_CUDA(cudaGetLastError(), "tensor");
   BFV_CUDA(launch_ntt(r, ln, d, tens, (long long)(3 * T), 0, int(T), 1, 1), "intt");
+  if (!r->residue) {
+    u64* outw = ln.arena.take<u64>(3 * n * W);
+    BFV_ARENA(ln.arena);
+    if (int rc = native_reduce(r, ln, d, tens, 3, T, outw, 1, t)) return rc;
+    return download_words(r, ln, outw, 3, out);
+  }
   k_rns_scale<<<blocks_for((long long)(3 * n), 128), 128, 0, ln.stream>>>(tens, 3, scaled, d);
   BFV_CUDA(cudaGetLastError(), "scale");
   return compose_out(r, ln, d, scaled, 3, out);
@@ -1010,6 +1255,28 @@ int cuhe_bfv_hamming_tile(cuhe_bfv_key* relin, const uint8_t* query, const uint8
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, t, &d)) return rc;
+  if (!r->residue) {
+    // the caller's mask may be any poly below q: take its exact product over
+    // the tensor primes (they cover N (q - 1)^2)
+    const size_t T = r->plan.tensor_count;
+    BFV_CUDA(ln.arena.reserve(native_tile_bytes(r, 1, T) + slice(2 * n * W * 8) * 3 + slice(n * W * 8) +
+                              slice(T * n * 8) + 16384),
+             "workspace");
+    ln.arena.reset();
+    u64 *qw, *tw, *mw, *mres;
+    if (int rc = upload_polys(r, ln, d, query, 2, 0, &qw, nullptr)) return rc;
+    if (int rc = upload_polys(r, ln, d, tile, 2, 0, &tw, nullptr)) return rc;
+    if (int rc = upload_polys(r, ln, d, mask, 1, T, &mw, &mres)) return rc;
+    BFV_CUDA(launch_ntt(r, ln, d, mres, (long long)(T), 0, int(T), 1, 0), "mask ntt");
+    u64* dist = ln.arena.take<u64>(2 * n * W);
+    NativeScratch sc;
+    if (int rc = native_scratch(ln.arena, r, 1, T, &sc)) return rc;
+    std::vector<u64> exps(exponents, exponents + rotations);
+    std::vector<const cuhe_bfv_key*> rkeys(keys, keys + rotations);
+    if (int rc = native_tile_circuit(r, ln, d, qw, tw, 1, t, relin, exps, rkeys, {mres}, T, sc, dist, nullptr))
+      return rc;
+    return download_words(r, ln, dist, 2, out);
+  }
   BFV_CUDA(ln.arena.reserve(tile_arena_bytes(r, 1) + slice(2 * n * W * 8) * 2 + slice(n * W * 8) + slice(L * n * 8) * 2 +
                             slice(2 * L * n * 8) + slice(2 * n * W * 8) + 16384),
            "workspace");
@@ -1100,7 +1367,9 @@ int cuhe_bfv_create_server(cuhe_bfv_key* relin, const uint64_t* exponents, cuhe_
   s->right = right;
   s->d_ring = d;
   const size_t W = size_t(r->host_dev.words);
-  int rc = upload_plain_ntt(r, ln, d, small_to_words(hamming_mask(n, t, lanes, s->capacity), W), &s->d_full_mask);
+  s->mask_primes = r->residue ? P.residue_count : native_mask_primes(r, t);
+  int rc = upload_plain_ntt(r, ln, d, small_to_words(hamming_mask(n, t, lanes, s->capacity), W), &s->d_full_mask,
+                            s->mask_primes);
   cudaError_t e = cudaSuccess;
   if (!rc) e = cudaMalloc(&s->d_target, 8 * std::max<size_t>(1, target.w.size()));
   if (!rc && e == cudaSuccess)
@@ -1179,6 +1448,11 @@ size_t search_chunk_bytes(const cuhe_bfv_server* s, size_t ct, unsigned out_bits
   const size_t in_bytes = (n * P.q_bits + 7) / 8;
   const size_t out_words = (n * out_bits + 63) / 64;
   const size_t gc = (ct + s->padded - 1) / s->padded;
+  if (!r->residue)
+    return native_tile_bytes(r, ct, s->mask_primes) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) +
+           slice(2 * n * W * 8) + slice(ct * 2 * n * W * 8) * 2 + slice(gc * 2 * n * W * 8) +
+           slice(gc * 2 * out_words * 8) + slice(sizeof(int)) + slice(ct * n * W * 8) +
+           slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp)) + 65536;
   return tile_arena_bytes(r, ct) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) + slice(2 * n * W * 8) +
          slice(ct * 2 * n * W * 8) + slice(ct * 2 * L * n * 8) + slice(gc * 2 * n * W * 8) +
          slice(gc * 2 * out_words * 8) + slice(sizeof(int)) + slice(ct * n * W * 8) + slice(ct * sizeof(ComposeOp)) +
@@ -1235,7 +1509,9 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     auto it = s->partial_masks.find(size_t(count % s->capacity));
     if (it == s->partial_masks.end()) {
       u64* m = nullptr;
-      if (int rc = upload_plain_ntt(r, ln, d, small_to_words(hamming_mask(n, s->t, s->lanes, size_t(count % s->capacity)), W), &m))
+      if (int rc = upload_plain_ntt(r, ln, d,
+                                    small_to_words(hamming_mask(n, s->t, s->lanes, size_t(count % s->capacity)), W),
+                                    &m, s->mask_primes))
         return rc;
       it = s->partial_masks.emplace(size_t(count % s->capacity), m).first;
     }
@@ -1256,7 +1532,7 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     uint8_t* d_ib = resident ? nullptr : ln.arena.take<uint8_t>(ct * 2 * in_bytes);
     u64* qw = ln.arena.take<u64>(2 * n * W);
     u64* tw = resident ? const_cast<u64*>(resident) + first * 2 * n * W : ln.arena.take<u64>(ct * 2 * n * W);
-    u64* dist = ln.arena.take<u64>(ct * 2 * L * n);
+    u64* dist = ln.arena.take<u64>(r->residue ? ct * 2 * L * n : ct * 2 * n * W);
     u64* ow = ln.arena.take<u64>(gc * 2 * n * W);
     u64* packed = ln.arena.take<u64>(gc * 2 * out_words);
     int* d_status = ln.arena.take<int>(1);
@@ -1275,18 +1551,31 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
     BFV_CUDA(cudaStreamSynchronize(ln.stream), "unpack");
     if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
-    TileArgs a;
-    a.q_words = qw;
-    a.t_words = tw;
-    a.ct = ct;
-    a.relin = s->relin;
-    for (u64 g : s->left) {
-      a.exps.push_back(g);
-      a.keys.push_back(s->keys.at(g));
+    NativeScratch sc{};
+    if (r->residue) {
+      TileArgs a;
+      a.q_words = qw;
+      a.t_words = tw;
+      a.ct = ct;
+      a.relin = s->relin;
+      for (u64 g : s->left) {
+        a.exps.push_back(g);
+        a.keys.push_back(s->keys.at(g));
+      }
+      a.masks.assign(ct, s->d_full_mask);
+      if (partial && first + ct == size_t(tiles)) a.masks[ct - 1] = partial;
+      if (int rc = tile_circuit(r, ln, d, a, dist, prof)) return rc;
+    } else {
+      if (int rc = native_scratch(ln.arena, r, ct, s->mask_primes, &sc)) return rc;
+      std::vector<u64> exps(s->left.begin(), s->left.end());
+      std::vector<const cuhe_bfv_key*> rkeys;
+      for (u64 g : s->left) rkeys.push_back(s->keys.at(g));
+      std::vector<const u64*> masks(ct, s->d_full_mask);
+      if (partial && first + ct == size_t(tiles)) masks[ct - 1] = partial;
+      if (int rc = native_tile_circuit(r, ln, d, qw, tw, ct, s->t, s->relin, exps, rkeys, masks, s->mask_primes, sc,
+                                       dist, prof))
+        return rc;
     }
-    a.masks.assign(ct, s->d_full_mask);
-    if (partial && first + ct == size_t(tiles)) a.masks[ct - 1] = partial;
-    if (int rc = tile_circuit(r, ln, d, a, dist, prof)) return rc;
     // merge tree (bfv_server.h:15-45), executed in waves of independent merges
     cudaEvent_t m0, m1;
     cudaEventCreate(&m0);
@@ -1329,6 +1618,33 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     }
     size_t waves = 0;
     for (const auto& m : merges) waves = std::max(waves, m.wave + 1);
+    if (!r->residue) {
+      // native: rotate each right operand (grouped by level, one key each),
+      // then add it into its left operand
+      for (size_t w = 0; w < waves; ++w) {
+        std::vector<NativeOp> adds;
+        size_t used = 0;
+        for (size_t level = 0; level < s->right.size(); ++level) {
+          std::vector<NativeOp> rots;
+          for (const auto& m : merges) {
+            if (m.wave != w || m.level != level) continue;
+            const size_t k = used + rots.size();
+            rots.push_back(NativeOp{dist + m.right * 2 * n * W, sc.perm + k * 2 * n * W, sc.tmp + k * 2 * n * W,
+                                    nullptr});
+            adds.push_back(NativeOp{dist + m.left * 2 * n * W, sc.tmp + k * 2 * n * W, dist + m.left * 2 * n * W,
+                                    nullptr});
+          }
+          if (rots.empty()) continue;
+          const u64 g = s->right.at(level);
+          if (int rc = native_rotate(r, ln, d, rots, unsigned(g), s->keys.at(g), sc.d_nops, sc.ksres,
+                                     sc.ksw + used * 2 * n * W, sc.d_sops))
+            return rc;
+          used += rots.size();
+        }
+        if (int rc = native_add_ops(r, ln, d, adds, sc.d_nops)) return rc;
+      }
+      waves = 0;  // the residue waves below are skipped
+    }
     u64* mwords = ln.arena.take<u64>(std::max<size_t>(1, ct) * n * W);
     ComposeOp* d_cops = ln.arena.take<ComposeOp>(std::max<size_t>(1, ct));
     SwitchOp* d_sops = ln.arena.take<SwitchOp>(std::max<size_t>(1, ct));
@@ -1349,11 +1665,18 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     }
     cudaEventRecord(m1, ln.stream);
     // outputs: compose, optional compaction, packing
-    std::vector<ComposeOp> cops;
-    for (size_t gi = 0; gi < gc; ++gi)
-      for (size_t comp = 0; comp < 2; ++comp)
-        cops.push_back(ComposeOp{dist + (result_slot[gi] * 2 + comp) * L * n, ow + (gi * 2 + comp) * n * W, 1u, 0u});
-    if (int rc = run_switch(r, ln, d, cops, {}, d_cops, nullptr)) return rc;
+    if (r->residue) {
+      std::vector<ComposeOp> cops;
+      for (size_t gi = 0; gi < gc; ++gi)
+        for (size_t comp = 0; comp < 2; ++comp)
+          cops.push_back(ComposeOp{dist + (result_slot[gi] * 2 + comp) * L * n, ow + (gi * 2 + comp) * n * W, 1u, 0u});
+      if (int rc = run_switch(r, ln, d, cops, {}, d_cops, nullptr)) return rc;
+    } else {
+      for (size_t gi = 0; gi < gc; ++gi)
+        BFV_CUDA(cudaMemcpyAsync(ow + gi * 2 * n * W, dist + result_slot[gi] * 2 * n * W, 2 * n * W * 8,
+                                 cudaMemcpyDeviceToDevice, ln.stream),
+                 "result copy");
+    }
     if (compact) {
       k_compact<<<blocks_for((long long)(gc * 2 * n), 128), 128, 0, ln.stream>>>(ow, (long long)(gc * 2 * n), s->d_target,
                                                                                  int(s->target_words.size()), d);

@@ -146,7 +146,7 @@ def test_boundary_errors():
     with pytest.raises(ValueError):
         m.rotate_rows(k, (fixed([0] * 16, q), fixed([0] * 16, q)), 4)
     with pytest.raises(ValueError, match="(?i)residue"):
-        m.create_ring(16, format(ob.coefficient_modulus(100), "x"), 15, True, False)
+        m.create_ring(16, format(ob.coefficient_modulus(100), "x"), 15, True, False, 2)
     layout = ob.Layout(16, 3)
     with pytest.raises(ValueError, match="rotation key"):
         m.create_server(k, (), layout.padded, 97, format(ob.coefficient_modulus(40), "x"))
