@@ -379,6 +379,9 @@ def run_gpu(args) -> dict | None:
     }
     if not args.no_bfv:
         result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
+        if world == 1:
+            result["bfv_native"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline,
+                                           native=True)
     if not args.no_client and world == 1:
         result["client"] = run_client()
     if not args.no_textbook and world == 1:
@@ -400,15 +403,16 @@ BFV_N, BFV_Q_BITS, BFV_GADGET, BFV_T, BFV_EMBED = 8192, 180, 30, 65537, 512
 BFV_VECTORS = 16384
 
 
-def bfv_setup(seed: int = 8192, embed: int = BFV_EMBED):
-    """N=8192, Q = 3 x 60-bit NTT primes, 30-bit gadget, t=65537, embed 512
-    (16 vectors per ciphertext, 1,024 index ciphertexts for 16,384 vectors).
-    Keys and ciphertexts are uniform residues from a seeded generator: the
-    evaluator's work is independent of the values, and bit-exactness on real
-    encryptions is covered by the parity tests."""
+def bfv_setup(seed: int = 8192, embed: int = BFV_EMBED, native: bool = False):
+    """N=8192, Q = 3 x 60-bit NTT primes (native: the largest prime below
+    2^180), 30-bit gadget, t=65537, embed 512 (16 vectors per ciphertext,
+    1,024 index ciphertexts for 16,384 vectors).  Keys and ciphertexts are
+    uniform residues from a seeded generator: the evaluator's work is
+    independent of the values, and bit-exactness on real encryptions is
+    covered by the parity tests."""
     from cuhepy_b200.bfv import layout as lay
 
-    q = lay.rns_modulus(BFV_N, BFV_Q_BITS)
+    q = lay.coefficient_modulus(BFV_Q_BITS) if native else lay.rns_modulus(BFV_N, BFV_Q_BITS)
     layout = lay.Layout(BFV_N, embed)
     exps = sorted(set(layout.left()) | set(layout.right()))
     rng = np.random.default_rng(seed)
@@ -443,13 +447,15 @@ def bfv_setup(seed: int = 8192, embed: int = BFV_EMBED):
     return q, layout, exps, keys, query, index, target
 
 
-def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
+def run_bfv(steps: int, warmup: int, cpu: bool, native: bool = False) -> dict:
     """BFV packed Hamming kNN: one step = one encrypted query against the
-    resident 16,384-vector index (1,024 tiles, 2 compacted responses)."""
+    resident 16,384-vector index (1,024 tiles, 2 compacted responses).
+    native: the ring of the reference's default client (a 180-bit prime q,
+    residue=False), whose products go through auxiliary primes."""
     from cuhepy_b200.bfv import _bfv_rns as m
 
-    q, layout, exps, keys, query, index, target = bfv_setup()
-    ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+    q, layout, exps, keys, query, index, target = bfv_setup(native=native)
+    ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, not native, 0 if native else 2)
     relin = m.compile_key(ring, keys[0])
     galois = tuple((g, m.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
     server = m.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
@@ -485,10 +491,19 @@ def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
     tiles = len(index)
     # algorithmic work per query (the counts of bfv_server.h's circuit, which
     # this implementation follows transform for transform): per tile 200
-    # forward and 87 inverse N-point transforms, per merge 18 and 6
+    # forward and 87 inverse N-point transforms, per merge 18 and 6.  Native
+    # rings: T tensor, S switch and M mask primes, D digits, R rotations per
+    # tile: forward 2T + (1 + R) D S + 2M, inverse 3T + (1 + R) 2S + 2M;
+    # per merge D S and 2S.
     groups = (tiles + layout.padded - 1) // layout.padded
     merges = tiles - groups
     fwd, inv = 200 * tiles + 18 * merges, 87 * tiles + 6 * merges
+    info = m.ring_info(ring)
+    if native:
+        T, S, D, R = len(info["primes"]), info["switch_prime_count"], 6, len(layout.left())
+        M = native_mask_primes(info["primes"], q, BFV_N, BFV_T)
+        fwd = (2 * T + (1 + R) * D * S + 2 * M) * tiles + D * S * merges
+        inv = (3 * T + (1 + R) * 2 * S + 2 * M) * tiles + 2 * S * merges
     butterflies = (fwd + inv) * (BFV_N // 2) * int(math.log2(BFV_N))
     step_s = statistics.mean(times)
     from cuhepy_b200 import _native
@@ -500,7 +515,7 @@ def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
         hbm_src = "MEASURED_PEAKS.json hbm_gbs"
     except (OSError, ValueError, KeyError):
         hbm_src = "fallback"
-    L = 3
+    L = info["switch_prime_count"]
     switches = tiles * 10 + merges
     ntt_bytes = (fwd + inv) * 16 * BFV_N                               # u64 read + write per transform
     mac_bytes = switches * (6 * L * BFV_N * 8 + 2 * 6 * L * BFV_N * 8 + 2 * L * BFV_N * 8)
@@ -517,8 +532,9 @@ def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
                      "digits + keys + outputs per switch); the fused kernels keep planes on chip, so this "
                      f"effective figure exceeds what DRAM carries; peak {hbm_peak} GB/s from {hbm_src}"),
     }
+    modulus = "q = largest prime below 2^180 (native ring)" if native else "Q=3x60-bit"
     out = {
-        "metric": "BFV kNN queries/s (N=8192, Q=3x60-bit, 16,384 x 512-bit index resident, compacted responses)",
+        "metric": f"BFV kNN queries/s (N=8192, {modulus}, 16,384 x 512-bit index resident, compacted responses)",
         "roofline": out_roofline,
         "value": 1.0 / statistics.mean(times), "unit": "queries/s",
         "p50_ms": 1e3 * statistics.median(times), "p99_ms": 1e3 * float(np.percentile(times, 99)),
@@ -532,12 +548,27 @@ def run_bfv(steps: int, warmup: int, cpu: bool) -> dict:
         "tiles": tiles,
         "data": "seeded uniform keys and ciphertexts (evaluation work is value-independent)",
     }
+    if native:
+        out["roofline"]["kernel"] = "whole search (key switches, transforms and Garner reductions)"
+        out["primes"] = {"tensor": len(info["primes"]), "switch": info["switch_prime_count"]}
     if cpu:
-        out["cpu_baseline"] = bfv_cpu_baseline(q, layout, exps, keys, query, index, target)
+        out["cpu_baseline"] = bfv_cpu_baseline(q, layout, exps, keys, query, index, target, native=native)
     return out
 
 
-def bfv_cpu_baseline(q, layout, exps, keys, query, index, target, sample_tiles: int = 2) -> dict:
+def native_mask_primes(primes, q: int, n: int, t: int) -> int:
+    """Auxiliary primes of the exact ct x pt mask product: the first c whose
+    product exceeds 2 N (q - 1)(t - 1)."""
+    bound, product = 2 * n * (q - 1) * (t - 1), 1
+    for c, p in enumerate(primes, 1):
+        product *= p
+        if product > bound:
+            return c
+    raise ValueError("not enough auxiliary primes")
+
+
+def bfv_cpu_baseline(q, layout, exps, keys, query, index, target, sample_tiles: int = 2,
+                     native: bool = False) -> dict:
     """The reference's own compiled _bfv_rns (oracle/_ref) on the host cores:
     one search of `sample_tiles` tiles per thread (the module releases the GIL),
     extrapolated linearly to the 1,024-tile query."""
@@ -550,7 +581,7 @@ def bfv_cpu_baseline(q, layout, exps, keys, query, index, target, sample_tiles: 
     if ref is None:
         return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
                 "sample": "oracle/_ref not built on this machine"}
-    ring = ref.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+    ring = ref.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, not native, 0 if native else 2)
     relin = ref.compile_key(ring, keys[0])
     galois = tuple((g, ref.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
     server = ref.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
@@ -1205,6 +1236,8 @@ def main() -> None:
     parser.add_argument("--mixed-only", action="store_true", help="run only the mixed-batch section")
     parser.add_argument("--textbook-only", action="store_true", help="run only the plain Paillier section")
     parser.add_argument("--bfv-only", action="store_true", help="run only the BFV kNN section")
+    parser.add_argument("--bfv-native-only", action="store_true",
+                        help="run only the BFV kNN section on the prime-q (native) ring")
     parser.add_argument("--client-only", action="store_true", help="run only the BFV client encryption section")
     parser.add_argument("--no-client", action="store_true", help="skip the BFV client encryption section")
     parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
@@ -1223,6 +1256,10 @@ def main() -> None:
         return
     if args.bfv_only:
         print(json.dumps({"bfv": run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)}))
+        return
+    if args.bfv_native_only:
+        print(json.dumps({"bfv_native": run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline,
+                                                native=True)}))
         return
     if args.textbook_only:
         print(json.dumps({"textbook": [run_textbook(512), run_textbook(1024)]}))

@@ -3,8 +3,9 @@
 Same function names, argument meanings, buffer formats and error mapping as
 src/cuhepy/bfv/_cpu_ext/bindings.cpp:405-433 (``ValueError`` for invalid
 arguments, ``TypeError`` for non-bytes buffers, ``RuntimeError`` otherwise);
-the arithmetic runs on the B200 through libcuhe_bfv_b200.so.  Rings must be
-residue rings (Q a product of the first 60-bit NTT primes).  The C ABI
+the arithmetic runs on the B200 through libcuhe_bfv_b200.so.  Rings are
+residue rings (Q a product of the first 60-bit NTT primes) or native rings
+(residue=False: any odd q up to 512 bits, exact products).  The C ABI
 releases no Python state, so the GIL is dropped during every call (ctypes
 releases it for foreign calls).
 """

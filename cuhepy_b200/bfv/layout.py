@@ -17,11 +17,14 @@ from __future__ import annotations
 import numpy as np
 
 _SMALL = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+_MORE = _SMALL + (41, 43, 47, 53, 59, 61, 67, 71, 73, 79, 83, 89, 97)
 
 
 def is_prime(x: int) -> bool:
-    """Miller-Rabin with the first twelve prime bases: deterministic below
-    3.3e24, which covers every modulus here (at most 64 bits per prime)."""
+    """Miller-Rabin with the first twelve prime bases, deterministic below
+    3.3e24 (every NTT prime); above that the first 25 prime bases, a
+    probable-prime test like the reference's gmpy2.is_prime (error below
+    4^-25 for any composite)."""
     if x < 2:
         return False
     for p in _SMALL:
@@ -31,7 +34,7 @@ def is_prime(x: int) -> bool:
     while not d & 1:
         d >>= 1
         r += 1
-    for a in _SMALL:
+    for a in (_SMALL if x < 3_317_044_064_679_887_385_961_981 else _MORE):
         y = pow(a, d, x)
         if y in (1, x - 1):
             continue
@@ -64,9 +67,10 @@ def rns_modulus(n: int, bits: int) -> int:
 
 
 def coefficient_modulus(bits: int) -> int:
-    """Largest prime below 2^bits (bits <= 80)."""
-    if not 2 <= bits <= 80:
-        raise ValueError("coefficient modulus bits must be 2..80")
+    """Largest prime below 2^bits (scheme.py:186-193): the response modulus
+    of a compacted search, and the ciphertext modulus of a native ring."""
+    if not 2 <= bits <= 512:
+        raise ValueError("coefficient modulus bits must be 2..512")
     c = (1 << bits) - 1
     while not is_prime(c):
         c -= 2

@@ -1,9 +1,10 @@
-/* C ABI of the B200 BFV residue evaluator (libcuhe_bfv_b200.so).
+/* C ABI of the B200 BFV evaluator (libcuhe_bfv_b200.so).
  *
  * Replaces the CPython module _bfv_rns (ABI_VERSION 4) of the reference,
- * src/cuhepy/bfv/_cpu_ext/bindings.cpp:405-433, for rings whose ciphertext
+ * src/cuhepy/bfv/_cpu_ext/bindings.cpp:405-433: rings whose ciphertext
  * modulus Q is a product of the first 60-bit NTT primes (the reference's
- * "residue" backend).  Handles are reference counted: a key keeps its ring
+ * "residue" backend) and rings with any odd modulus q up to 512 bits (its
+ * "native" backend).  Handles are reference counted: a key keeps its ring
  * alive and a server keeps its keys alive (bindings.cpp:25-38).
  *
  * Buffers: a "poly" is N coefficients of coefficient_bytes little-endian
@@ -30,7 +31,10 @@ typedef struct cuhe_bfv_server cuhe_bfv_server;
 const char* cuhe_bfv_last_error(void);
 
 /* create_ring(n, q_hex, digit_bits, fast, residue, kernel_level)
- * (bindings.cpp:120-136).  Only residue rings are served by the device. */
+ * (bindings.cpp:120-136).  residue != 0: q must be a product of the first
+ * 60-bit NTT primes (the reference's residue backend); residue == 0: any odd
+ * q of at most 512 bits (the native backend; exact products over auxiliary
+ * primes), kernel_level 0. */
 int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int fast, int residue,
                          uint64_t kernel_level, int device, cuhe_bfv_ring** out);
 void cuhe_bfv_ring_release(cuhe_bfv_ring* ring);

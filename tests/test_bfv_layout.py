@@ -15,7 +15,7 @@ def test_primes_match(n, bits):
 
 
 def test_coefficient_modulus_matches():
-    for bits in (20, 40, 50, 61, 64):
+    for bits in (20, 40, 50, 61, 64, 100, 180, 300, 512):
         assert lay.coefficient_modulus(bits) == ob.coefficient_modulus(bits)
 
 

@@ -200,3 +200,63 @@ def test_native_ring_errors():
         m.apply_key(k, fixed([q] + [0] * 15, q))
     with pytest.raises(ValueError):
         m.rotate_rows(k, (fixed([0] * 16, q), fixed([0] * 16, q)), 4)
+
+
+class _PrimeParams(ob.Params):
+    """The reference's default BFVClient() ring: q is the largest prime below
+    2^q_bits (scheme.py:186-193) instead of a product of NTT primes."""
+
+    @property
+    def q(self):
+        return ob.coefficient_modulus(self.q_bits)
+
+
+def test_default_parameters_search_decrypts_to_hamming_distances():
+    """The reference's test_default_parameters_match_gmp (test_bfv_rns.py:178-194)
+    on the device: N=8192, 180-bit prime q, 30-bit gadget, t=65537, embed 512,
+    33 vectors with the query and its complement among them.  Real keys and
+    encryptions (the oracle's client, seeded); the uncompacted responses equal
+    the reference checker's, and the compacted ones decrypt to the plaintext
+    Hamming distances."""
+    from bfv_helpers import Seeded
+
+    params = _PrimeParams(8192, 65537, 180, 30, 21)
+    n, t, q = params.n, params.t, params.q
+    layout = ob.Layout(n, 512)
+    rng = Seeded(1337)
+    keys = ob.key_gen(params, layout.rotation_steps(), rng)
+    bits_rng = random.Random(1337)
+    query = [bits_rng.getrandbits(1) for _ in range(512)]
+    vectors = [[bits_rng.getrandbits(1) for _ in range(512)] for _ in range(33)]
+    vectors[0] = query[:]
+    vectors[1] = [1 - b for b in query]
+    qct = ob.encrypt(ob.batch_encode(layout.query_slots(query), n, t), keys, rng)
+    index = [ob.encrypt(ob.batch_encode(s, n, t), keys, rng) for s in layout.index_slots(vectors)]
+    m = native()
+    ring = m.create_ring(n, format(q, "x"), params.gadget_bits, True, False)
+    relin = m.compile_key(ring, key_bytes(keys["relin"], q))
+    exps = sorted(set(layout.left()) | set(layout.right()))
+    galois = tuple((g, m.compile_key(ring, key_bytes(keys["galois"][g], q))) for g in exps)
+    target = ob.coefficient_modulus(50)
+    server = m.create_server(relin, galois, layout.padded, t, format(target, "x"))
+    bits = q.bit_length()
+    qp = (packed(qct[0], bits), packed(qct[1], bits))
+    ip = tuple((packed(c[0], bits), packed(c[1], bits)) for c in index)
+    full = m.packed_search(server, qp, ip, len(vectors), False)
+    ref = reference_native()
+    if ref is not None:
+        rring = ref.create_ring(n, format(q, "x"), params.gadget_bits, True, False)
+        rrelin = ref.compile_key(rring, key_bytes(keys["relin"], q))
+        rg = tuple((g, ref.compile_key(rring, key_bytes(keys["galois"][g], q))) for g in exps)
+        rserver = ref.create_server(rrelin, rg, layout.padded, t, format(target, "x"))
+        assert full == ref.packed_search(rserver, qp, ip, len(vectors), False)
+    (response,) = m.packed_search(server, qp, ip, len(vectors), True)
+    ct = tuple(ob.unpack_poly(c, target.bit_length(), n) for c in response)
+    slots = ob.batch_decode(ob.decrypt(ct, keys, target), n, t)
+    got = []
+    for pos in range(len(vectors)):
+        tile, lane = divmod(pos, layout.capacity)
+        row, col = divmod(lane, layout.lanes)
+        got.append(slots[row * (n // 2) + tile * layout.lanes + col])
+    assert got == [sum(x != y for x, y in zip(v, query)) for v in vectors]
+    assert got[0] == 0 and got[1] == 512
