@@ -1201,17 +1201,23 @@ def profile_case(which: str) -> None:
         nidx = torch.from_numpy(noise_indices(vectors, 3)).cuda()
         cts = torch.empty((vectors, ctx.words), dtype=torch.int32, device="cuda")
         dist = torch.empty(vectors, dtype=torch.int64, device="cuda")
+        queries = 16
+        prod = torch.empty((queries, vectors, ctx.words), dtype=torch.int32, device="cuda")
         with torch.cuda.stream(stream):
             for _ in range(2):  # launch 1-2: encrypt; decode follows each
                 ctx.lookup_encrypt_bits_array(bits, vectors, EMBED_LEN, 2 * KEY_LEN, 1, nidx, cts)
                 ctx.decode_array(cts, vectors, 1, 2 * KEY_LEN, dist)
+            # encode_hamming_server: 16 queries x 8,192 index ciphertexts (64 MB of products)
+            for _ in range(2):
+                ctx.mulmod_outer_array(cts[:queries], queries, cts, vectors, prod)
         torch.cuda.synchronize()
         print("paillier profile case done", int(dist[:4].sum()))
     else:
         from cuhepy_b200.bfv import _bfv_rns as m
 
-        q, layout, exps, keys, query, index, target = bfv_setup()
-        ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, True, 2)
+        native = which == "bfv_native"
+        q, layout, exps, keys, query, index, target = bfv_setup(native=native)
+        ring = m.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, not native, 0 if native else 2)
         relin = m.compile_key(ring, keys[0])
         galois = tuple((g, m.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
         server = m.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
@@ -1242,7 +1248,7 @@ def main() -> None:
     parser.add_argument("--no-client", action="store_true", help="skip the BFV client encryption section")
     parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
-    parser.add_argument("--profile-case", choices=["paillier", "bfv"],
+    parser.add_argument("--profile-case", choices=["paillier", "bfv", "bfv_native"],
                         help="run one small step of a hot kernel (for ncu captures) and exit")
     args = parser.parse_args()
     if args.profile_case:

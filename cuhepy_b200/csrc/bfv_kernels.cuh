@@ -55,7 +55,9 @@ __host__ __device__ constexpr size_t plane_smem_words(int n) { return size_t(n) 
 // elements at stride `stride` runs stages s0 .. s0+P-1 without touching shared
 // memory.  Stage s has 2^s groups of gap N/2^(s+1); inside a block the group
 // of element k at stage s0+t is G*2^t + (k >> (P-t)).
-template <int P>
+// kSharedTw: the twiddle table w2 lives in shared memory (staged by the
+// caller) instead of global memory read through the read-only cache.
+template <int P, bool kSharedTw = false>
 __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const ulonglong2* __restrict__ w2,
                                                  u64 p, bool last) {
   constexpr int E = 1 << P;
@@ -79,7 +81,7 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
       for (int k = 0; k < E; ++k) {
         if (k & half) continue;
         const int idx = m + (G << t) + (k >> (P - t));
-        const ulonglong2 tw = __ldg(w2 + idx);
+        const ulonglong2 tw = kSharedTw ? w2[idx] : __ldg(w2 + idx);
         const u64 root = tw.x, rq = tw.y;
         u64 u = x[k];
         if (u >= two_p) u -= two_p;
@@ -102,7 +104,7 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
 
 // Inverse (decimation in time) passes: stage u has gap 2^u and N/2^(u+1)
 // groups; the final stage (gap N/2) folds in 1/N and the inverse twist.
-template <int P>
+template <int P, bool kSharedTw = false, bool kFinal = false>
 __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const ulonglong2* __restrict__ w2,
                                                  u64 p, u64 n_inv, u64 n_inv_q, u64 last_w, u64 last_q) {
   constexpr int E = 1 << P;
@@ -120,7 +122,7 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
     for (int t = 0; t < P; ++t) {
       const int half = 1 << t;
       const int stage = u0 + t;
-      const bool final_stage = stage == logn - 1;
+      const bool final_stage = kFinal && t == P - 1;  // kFinal: this pass ends at stage logn - 1
       const int m = n >> (stage + 1);
 #pragma unroll
       for (int k = 0; k < E; ++k) {
@@ -131,7 +133,7 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
           x[k + half] = shoup(u + two_p - v, last_w, last_q, p);
         } else {
           const int idx = m + (G << (P - t - 1)) + (k >> (t + 1));
-          const ulonglong2 tw = __ldg(w2 + idx);
+          const ulonglong2 tw = kSharedTw ? w2[idx] : __ldg(w2 + idx);
           const u64 root = tw.x, rq = tw.y;
           const u64 s = u + v;
           x[k] = s >= two_p ? s - two_p : s;
@@ -146,33 +148,49 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
 
 // Whole transforms over a padded shared-memory plane (all threads of the CTA).
 // max_p (1..4) caps the stages per register pass (radix 2^max_p).
-__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4) {
+// tw: the prime's twiddle pairs staged in shared memory (kSharedTw), else
+// the ring's global tables are used.
+template <bool kSharedTw = false>
+__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4,
+                                                 const ulonglong2* tw = nullptr) {
   const int logn = R.logn;
   const u64 p = R.prime[j].p;
+  const ulonglong2* w2 = kSharedTw ? tw : R.fwd2[j];
   for (int s0 = 0; s0 < logn; s0 += max_p) {
     const int P = logn - s0 < max_p ? logn - s0 : max_p;
     const bool last = s0 + P == logn;
     switch (P) {
-      case 4: ntt_forward_pass<4>(a, s0, logn, R.fwd2[j], p, last); break;
-      case 3: ntt_forward_pass<3>(a, s0, logn, R.fwd2[j], p, last); break;
-      case 2: ntt_forward_pass<2>(a, s0, logn, R.fwd2[j], p, last); break;
-      default: ntt_forward_pass<1>(a, s0, logn, R.fwd2[j], p, last); break;
+      case 4: ntt_forward_pass<4, kSharedTw>(a, s0, logn, w2, p, last); break;
+      case 3: ntt_forward_pass<3, kSharedTw>(a, s0, logn, w2, p, last); break;
+      case 2: ntt_forward_pass<2, kSharedTw>(a, s0, logn, w2, p, last); break;
+      default: ntt_forward_pass<1, kSharedTw>(a, s0, logn, w2, p, last); break;
     }
     __syncthreads();
   }
 }
 
-__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j, int max_p = 4) {
+template <bool kSharedTw = false>
+__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j, int max_p = 4,
+                                                 const ulonglong2* tw = nullptr) {
   const int logn = R.logn;
   const u64 p = R.prime[j].p;
+  const ulonglong2* w2 = kSharedTw ? tw : R.inv2[j];
   for (int u0 = 0; u0 < logn; u0 += max_p) {
     const int P = logn - u0 < max_p ? logn - u0 : max_p;
-    switch (P) {
-      case 4: ntt_inverse_pass<4>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
-      case 3: ntt_inverse_pass<3>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
-      case 2: ntt_inverse_pass<2>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
-      default: ntt_inverse_pass<1>(a, u0, logn, R.inv2[j], p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j]); break;
+    const int key = P * 2 + (u0 + P == logn ? 1 : 0);
+#define CUHE_INV_PASS(PP, F) \
+  ntt_inverse_pass<PP, kSharedTw, F>(a, u0, logn, w2, p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j])
+    switch (key) {
+      case 9: CUHE_INV_PASS(4, true); break;
+      case 8: CUHE_INV_PASS(4, false); break;
+      case 7: CUHE_INV_PASS(3, true); break;
+      case 6: CUHE_INV_PASS(3, false); break;
+      case 5: CUHE_INV_PASS(2, true); break;
+      case 4: CUHE_INV_PASS(2, false); break;
+      case 3: CUHE_INV_PASS(1, true); break;
+      default: CUHE_INV_PASS(1, false); break;
     }
+#undef CUHE_INV_PASS
     __syncthreads();
   }
 }

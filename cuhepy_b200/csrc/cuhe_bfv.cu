@@ -401,14 +401,20 @@ int ntt_max_threads(int radix_log = 4) {
 
 // Default launch of an N-point transform: radix-8 passes, one block of eight
 // per thread (at most 1024 threads).
-int ntt_default_threads(size_t n) { return int(std::min<size_t>(1024, std::max<size_t>(32, n / 8))); }
+// radix-8 CTA size: one 8-point block per thread up to 512 threads; at N =
+// 8192 two 512-thread CTAs per SM (64 registers each) overlap one CTA's
+// plane loads and barriers with the other's butterflies, which beats one
+// 1024-thread CTA.  N = 16384 planes take a whole SM's shared memory alone.
+int ntt_default_threads(size_t n) {
+  return int(std::min<size_t>(n >= 16384 ? 1024 : 512, std::max<size_t>(32, n / 8)));
+}
 
 cudaError_t launch_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
                        int prime_block, int inverse) {
   if (planes <= 0) return cudaSuccess;
-  const size_t smem = ntt_smem(r);  // within the attribute set at ring creation
   const int threads = ntt_default_threads(r->plan.n);
-  k_ntt8<<<unsigned(planes), threads, smem, ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse, 3);
+  // the shared-memory size is within the attribute set at ring creation
+  k_ntt8<<<unsigned(planes), threads, ntt_smem(r), ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse, 3);
   return cudaGetLastError();
 }
 
@@ -942,6 +948,7 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_ntt8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(plane_smem_words(16384) * sizeof(u64)));
+
   if (e != cudaSuccess) {
     delete r;
     return fail(CUHE_CUDA_ERROR, std::string("ring setup: ") + cudaGetErrorString(e));
