@@ -206,15 +206,44 @@ __device__ __forceinline__ void ntt_plane(u64* data, const RingDev* __restrict__
   extern __shared__ __align__(16) u64 s_plane[];
   const RingDev& R = *ring;
   const int n = R.n;
-  const long long b = blockIdx.x;
+  long long b = blockIdx.x;
+  const long long group = (long long)prime_mod * prime_block;
+  if (prime_mod > 1 && gridDim.x % group == 0) {
+    // prime-major order: CTAs launched together transform planes of the
+    // same prime, so they share its twiddle table in L1 / L2 (a bijection:
+    // slot s, index k -> ((k / block) * mod + s) * block + k % block)
+    const long long per_slot = gridDim.x / prime_mod;
+    const long long slot = b / per_slot, k = b % per_slot;
+    b = ((k / prime_block) * prime_mod + slot) * prime_block + k % prime_block;
+  }
   const int j = prime_base + int((b / prime_block) % prime_mod);
   u64* plane = data + b * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[sp(i)] = plane[i];
+  // 16-byte global accesses when the plane allows them (pairs 2i, 2i + 1
+  // never straddle a padding gap of sp, which falls every 16 words)
+  const bool wide = (reinterpret_cast<uintptr_t>(plane) & 15) == 0;
+  if (wide) {
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(plane);
+    for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+      const ulonglong2 v = src[i];
+      s_plane[sp(2 * i)] = v.x;
+      s_plane[sp(2 * i) + 1] = v.y;
+    }
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[sp(i)] = plane[i];
+  }
   __syncthreads();
   max_p = max_p < MAXP ? max_p : MAXP;
   if (inverse) ntt_inverse_fast(s_plane, R, j, max_p);
   else ntt_forward_fast(s_plane, R, j, max_p);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[sp(i)];
+  if (wide) {
+    ulonglong2* dst = reinterpret_cast<ulonglong2*>(plane);
+    for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+      const int at = sp(2 * i);
+      dst[i] = make_ulonglong2(s_plane[at], s_plane[at + 1]);
+    }
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[sp(i)];
+  }
 }
 
 __global__ void k_ntt(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block,
@@ -669,6 +698,153 @@ k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) 
     }
     __syncthreads();
   }
+}
+
+// ---- tensor memory (TMEM) as accumulator storage ------------------------------
+// Each SM has 512 TMEM columns x 128 lanes of 32 bits.  A CTA allocates
+// columns with tcgen05.alloc (one warp; the address lands in shared memory),
+// and warp w may access lanes 32 (w % 4) .. 32 (w % 4) + 31 only.  The
+// 32x32b shapes move one lane per thread: thread t of the warp reads or
+// writes 16 consecutive columns of lane 32 (w % 4) + t.
+__device__ __forceinline__ uint32_t smem_addr_u32(const void* ptr) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(ptr));
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+               :: "r"(smem_addr_u32(dst)), "r"(cols) : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(cols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// load 16 columns of this thread's lane; the registers are valid on return
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n\t"
+               "tcgen05.wait::ld.sync.aligned;"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]) : "r"(taddr) : "memory");
+}
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+               :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]) : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// The key switch of k_keyswitch with its accumulators in TMEM instead of
+// shared memory: shared memory holds only the plane (70 KB at N = 8192), so
+// two 512-thread CTAs (64 registers each) are resident per SM and one CTA's
+// global loads and barriers overlap the other's butterflies.  Thread t owns
+// coefficients i = t + 512 k (k < 16) and keeps (acc0, acc1) of each as four
+// 32-bit columns: 64 columns per thread, lanes by warp quarter, 4 warps per
+// quarter -> 256 columns per CTA, 512 for the two CTAs of an SM (the whole
+// TMEM; a third co-resident CTA would wait in tcgen05.alloc until one of
+// them deallocates).  Every tcgen05 instruction is executed by whole warps
+// (the coefficient guard i < n covers only the arithmetic), and no thread
+// leaves before the final dealloc.
+template <int MAXP>
+__global__ void __launch_bounds__(512, 2)
+k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) {
+  constexpr int kThreads = 512, kChunks = 4, kCols = 256;  // 16 coefficients per thread, 4 per chunk
+  extern __shared__ __align__(16) u64 s_plane[];
+  __shared__ uint32_t s_tmem;
+  const RingDev& R = *ring;
+  const SwitchOp op = ops[blockIdx.x];
+  const int j = blockIdx.y;
+  const int n = R.n, L = R.residue, W = R.words;
+  const u64 p = R.prime[j].p, two_p = 2 * p;
+  const int warp = int(threadIdx.x >> 5);
+  if (warp == 0) {
+    tmem_alloc(&s_tmem, kCols);
+    tmem_relinquish();
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  const uint32_t tbase = s_tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t((warp >> 2) * 64);
+  for (int d = 0; d < R.digits; ++d) {
+    for (int i = threadIdx.x; i < n; i += kThreads)
+      s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
+    __syncthreads();
+    ntt_forward_fast(s_plane, R, j, MAXP);
+    const long long k0o = ((long long)(d * 2 + 0) * L + j) * n, k1o = ((long long)(d * 2 + 1) * L + j) * n;
+    const bool last = d + 1 == R.digits;
+#pragma unroll 1
+    for (int c = 0; c < kChunks; ++c) {
+      uint32_t acc[16];
+      if (d > 0) {
+        tmem_ld16(tbase + uint32_t(c * 16), acc);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc[k] = 0;
+      }
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
+        if (i < n) {
+          const u64 v = s_plane[sp(i)];
+          u64 a0 = shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), p);
+          u64 a1 = shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), p);
+          a0 += u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
+          a1 += u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+          a0 = a0 >= two_p ? a0 - two_p : a0;
+          a1 = a1 >= two_p ? a1 - two_p : a1;
+          if (last) {
+            a0 = a0 >= p ? a0 - p : a0;
+            a1 = a1 >= p ? a1 - p : a1;
+            s_plane[sp(i)] = a0;  // component 0 transforms first
+          }
+          acc[4 * kk] = uint32_t(a0);
+          acc[4 * kk + 1] = uint32_t(a0 >> 32);
+          acc[4 * kk + 2] = uint32_t(a1);
+          acc[4 * kk + 3] = uint32_t(a1 >> 32);
+        }
+      }
+      tmem_st16(tbase + uint32_t(c * 16), acc);
+    }
+    tmem_wait_st();
+    __syncthreads();
+  }
+  for (int comp = 0; comp < 2; ++comp) {
+    if (comp == 1) {
+#pragma unroll 1
+      for (int c = 0; c < kChunks; ++c) {
+        uint32_t acc[16];
+        tmem_ld16(tbase + uint32_t(c * 16), acc);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
+          if (i < n) s_plane[sp(i)] = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+        }
+      }
+      __syncthreads();
+    }
+    ntt_inverse_fast(s_plane, R, j, MAXP);
+    u64* out = op.out + ((long long)comp * L + j) * n;
+    const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
+    for (int i = threadIdx.x; i < n; i += kThreads) {
+      u64 v = s_plane[sp(i)];
+      if (base) v = addmod(v, base[i], p);
+      if (comp == 0 && op.x0) {
+        const unsigned sidx = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));
+        u64 x = sidx < unsigned(n) ? op.x0[(long long)j * n + sidx] : op.x0[(long long)j * n + (sidx - n)];
+        if (sidx >= unsigned(n) && x) x = p - x;
+        v = addmod(v, x, p);
+      }
+      out[i] = v;
+    }
+    __syncthreads();
+  }
+  tmem_fence_before_sync();
+  __syncthreads();
+  tmem_fence_after_sync();
+  if (warp == 0) tmem_dealloc(s_tmem, kCols);
 }
 
 // ---- elementwise ------------------------------------------------------------------

@@ -435,11 +435,9 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
     const size_t smem = ntt_smem(r);
     dim3 grid(unsigned(sops.size()), unsigned(r->residue ? P.residue_count : r->switch_prime_count));
     if (P.n <= 8192) {
-      const size_t smem_acc = smem + 2 * P.n * sizeof(u64);  // accumulators after the plane
-      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<0, 1024, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(smem_acc)),
-               "smem");
-      k_keyswitch<0, 1024, 3><<<grid, 1024, smem_acc, ln.stream>>>(d_sops, d);
+      // accumulators in tensor memory, two CTAs per SM (shared-memory size
+      // within the attribute set at ring creation)
+      k_keyswitch_tm<3><<<grid, 512, smem, ln.stream>>>(d_sops, d);
     } else {
       BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32, 512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "smem");
@@ -948,6 +946,9 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_ntt8, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(plane_smem_words(16384) * sizeof(u64)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_keyswitch_tm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(plane_smem_words(8192) * sizeof(u64)));
 
   if (e != cudaSuccess) {
     delete r;
