@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -91,8 +92,15 @@ struct Lane {
   std::mutex mu;
   uint8_t* host_stage = nullptr;  // pinned staging of host polynomials (grow-only)
   size_t host_cap = 0;
+  cudaStream_t copy = nullptr;      // uploads overlapped with the lane's compute
+  uint8_t* pin[2] = {nullptr, nullptr};  // their pinned double buffer
+  size_t pin_cap[2] = {0, 0};
   ~Lane() {
+    if (copy) cudaStreamSynchronize(copy);
     if (host_stage) cudaFreeHost(host_stage);
+    for (uint8_t* p : pin)
+      if (p) cudaFreeHost(p);
+    if (copy) cudaStreamDestroy(copy);
   }
 };
 
@@ -109,6 +117,27 @@ struct PolySource {
 // buffer (several host threads for large copies) and enqueue one
 // host-to-device copy to d_dst on the lane's stream.  The caller
 // synchronises the stream before the lane stages again.
+// Copy polys [first, first + count) of src to dst, with up to max_workers
+// host threads (one per 16 MiB).
+void copy_polys(const PolySource& src, size_t first, size_t count, uint8_t* dst, size_t max_workers) {
+  const size_t bytes = count * src.poly_bytes;
+  const size_t workers = std::min<size_t>(std::max<size_t>(1, bytes >> 24), max_workers);
+  auto copy = [&](size_t lo, size_t hi) {
+    for (size_t k = lo; k < hi; ++k) std::memcpy(dst + k * src.poly_bytes, src.poly(first + k), src.poly_bytes);
+  };
+  if (workers == 1) {
+    copy(0, count);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const size_t per = (count + workers - 1) / workers;
+  for (size_t w = 0; w < workers; ++w) {
+    const size_t lo = w * per, hi = std::min(count, lo + per);
+    if (lo < hi) pool.emplace_back(copy, lo, hi);
+  }
+  for (auto& t : pool) t.join();
+}
+
 cudaError_t stage_polys(Lane& ln, const PolySource& src, size_t first, size_t count, uint8_t* d_dst) {
   const size_t bytes = count * src.poly_bytes;
   if (bytes == 0) return cudaSuccess;
@@ -120,23 +149,12 @@ cudaError_t stage_polys(Lane& ln, const PolySource& src, size_t first, size_t co
     if (e != cudaSuccess) return e;
     ln.host_cap = bytes;
   }
-  const size_t workers = std::min<size_t>(std::max<size_t>(1, bytes >> 24), 8);  // one per 16 MiB, at most 8
-  auto copy = [&](size_t lo, size_t hi) {
-    for (size_t k = lo; k < hi; ++k) std::memcpy(ln.host_stage + k * src.poly_bytes, src.poly(first + k), src.poly_bytes);
-  };
-  if (workers == 1) {
-    copy(0, count);
-  } else {
-    std::vector<std::thread> pool;
-    const size_t per = (count + workers - 1) / workers;
-    for (size_t w = 0; w < workers; ++w) {
-      const size_t lo = w * per, hi = std::min(count, lo + per);
-      if (lo < hi) pool.emplace_back(copy, lo, hi);
-    }
-    for (auto& t : pool) t.join();
-  }
+  copy_polys(src, first, count, ln.host_stage, 8);
   return cudaMemcpyAsync(d_dst, ln.host_stage, bytes, cudaMemcpyHostToDevice, ln.stream);
 }
+
+// Index tiles per upload sub-batch of a search over a host-memory index.
+constexpr size_t kPipeTiles = 256;
 
 constexpr int kMaxLanes = 8;
 
@@ -1549,40 +1567,133 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     BFV_CUDA(cudaMemcpyAsync(d_qb, query, 2 * in_bytes, cudaMemcpyHostToDevice, ln.stream), "query upload");
     k_unpack<<<blocks_for((long long)(2 * n), 256), 256, 0, ln.stream>>>(d_qb, (long long)(in_bytes), int(P.q_bits), 2, qw, d,
                                                                          d_status);
-    if (!resident) {
+    // Host-memory indexes of at least two pieces of kPipeTiles tiles are
+    // uploaded piece by piece by a helper thread (pinned double buffer, the
+    // lane's copy stream) while the lane runs the tile circuits of the
+    // tiles already uploaded.
+    const bool piped = !resident && ct >= 2 * kPipeTiles;
+    if (!resident && !piped) {
       BFV_CUDA(stage_polys(ln, *index, first * 2, ct * 2, d_ib), "index upload");
       k_unpack<<<blocks_for((long long)(ct * 2 * n), 256), 256, 0, ln.stream>>>(
           d_ib, (long long)(in_bytes), int(P.q_bits), int(ct * 2), tw, d, d_status);
     }
     BFV_CUDA(cudaGetLastError(), "unpack");
     int status = 0;
-    BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
-    BFV_CUDA(cudaStreamSynchronize(ln.stream), "unpack");
-    if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
+    if (!piped) {
+      BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
+      BFV_CUDA(cudaStreamSynchronize(ln.stream), "unpack");
+      if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
+    }
     NativeScratch sc{};
-    if (r->residue) {
-      TileArgs a;
-      a.q_words = qw;
-      a.t_words = tw;
-      a.ct = ct;
-      a.relin = s->relin;
-      for (u64 g : s->left) {
-        a.exps.push_back(g);
-        a.keys.push_back(s->keys.at(g));
-      }
-      a.masks.assign(ct, s->d_full_mask);
-      if (partial && first + ct == size_t(tiles)) a.masks[ct - 1] = partial;
-      if (int rc = tile_circuit(r, ln, d, a, dist, prof)) return rc;
-    } else {
+    if (!r->residue)
       if (int rc = native_scratch(ln.arena, r, ct, s->mask_primes, &sc)) return rc;
-      std::vector<u64> exps(s->left.begin(), s->left.end());
-      std::vector<const cuhe_bfv_key*> rkeys;
-      for (u64 g : s->left) rkeys.push_back(s->keys.at(g));
-      std::vector<const u64*> masks(ct, s->d_full_mask);
-      if (partial && first + ct == size_t(tiles)) masks[ct - 1] = partial;
-      if (int rc = native_tile_circuit(r, ln, d, qw, tw, ct, s->t, s->relin, exps, rkeys, masks, s->mask_primes, sc,
-                                       dist, prof))
-        return rc;
+    // tile circuits of chunk tiles [t0, t0 + tc) into their dist slots
+    auto run_tiles = [&](size_t t0, size_t tc) -> int {
+      const size_t mark = ln.arena.used;  // the circuit's workspace is free again when it returns
+      int rc;
+      if (r->residue) {
+        TileArgs a;
+        a.q_words = qw;
+        a.t_words = tw + t0 * 2 * n * W;
+        a.ct = tc;
+        a.relin = s->relin;
+        for (u64 g : s->left) {
+          a.exps.push_back(g);
+          a.keys.push_back(s->keys.at(g));
+        }
+        a.masks.assign(tc, s->d_full_mask);
+        if (partial && first + t0 + tc == size_t(tiles)) a.masks[tc - 1] = partial;
+        rc = tile_circuit(r, ln, d, a, dist + t0 * 2 * L * n, prof);
+      } else {
+        std::vector<u64> exps(s->left.begin(), s->left.end());
+        std::vector<const cuhe_bfv_key*> rkeys;
+        for (u64 g : s->left) rkeys.push_back(s->keys.at(g));
+        std::vector<const u64*> masks(tc, s->d_full_mask);
+        if (partial && first + t0 + tc == size_t(tiles)) masks[tc - 1] = partial;
+        rc = native_tile_circuit(r, ln, d, qw, tw + t0 * 2 * n * W, tc, s->t, s->relin, exps, rkeys, masks,
+                                 s->mask_primes, sc, dist + t0 * 2 * n * W, prof);
+      }
+      ln.arena.used = mark;
+      return rc;
+    };
+    if (!piped) {
+      if (int rc = run_tiles(0, ct)) return rc;
+    } else {
+      const size_t subs = (ct + kPipeTiles - 1) / kPipeTiles;
+      const size_t sub_bytes = kPipeTiles * 2 * in_bytes;
+      if (!ln.copy) BFV_CUDA(cudaStreamCreateWithFlags(&ln.copy, cudaStreamNonBlocking), "copy stream");
+      for (int h = 0; h < 2; ++h)
+        if (ln.pin_cap[h] < sub_bytes) {
+          if (ln.pin[h]) cudaFreeHost(ln.pin[h]);
+          ln.pin[h] = nullptr;
+          ln.pin_cap[h] = 0;
+          BFV_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ln.pin[h]), sub_bytes, cudaHostAllocDefault), "pinned");
+          ln.pin_cap[h] = sub_bytes;
+        }
+      std::vector<cudaEvent_t> up(subs, nullptr);
+      for (auto& e : up) BFV_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      std::mutex mu;
+      std::condition_variable cv;
+      size_t issued = 0;
+      cudaError_t stage_error = cudaSuccess;
+      std::atomic<bool> stop{false};
+      const int device = r->device;
+      std::thread stager([&] {
+        cudaSetDevice(device);
+        for (size_t k = 0; k < subs && !stop.load(); ++k) {
+          const size_t t0 = k * kPipeTiles, tc = std::min(kPipeTiles, ct - t0);
+          uint8_t* pin = ln.pin[k % 2];
+          cudaError_t e = k >= 2 ? cudaEventSynchronize(up[k - 2]) : cudaSuccess;  // its half is free again
+          if (e == cudaSuccess) {
+            copy_polys(*index, (first + t0) * 2, tc * 2, pin, 4);
+            e = cudaMemcpyAsync(d_ib + t0 * 2 * in_bytes, pin, tc * 2 * in_bytes, cudaMemcpyHostToDevice, ln.copy);
+          }
+          if (e == cudaSuccess) e = cudaEventRecord(up[k], ln.copy);
+          {
+            std::lock_guard<std::mutex> g(mu);
+            if (e != cudaSuccess) stage_error = e;
+            else issued = k + 1;
+          }
+          cv.notify_one();
+          if (e != cudaSuccess) break;
+        }
+      });
+      // compute in two batches: the first piece, then all the others (their
+      // uploads hide under the first batch's circuits, and the large second
+      // batch keeps the key-switch launches many waves long)
+      int rc = CUHE_OK;
+      for (size_t batch = 0; batch < 2 && rc == CUHE_OK; ++batch) {
+        const size_t k = batch == 0 ? 0 : subs - 1;  // last piece of the batch
+        const size_t t0 = batch == 0 ? 0 : kPipeTiles, tc = batch == 0 ? kPipeTiles : ct - kPipeTiles;
+        {
+          std::unique_lock<std::mutex> g(mu);
+          cv.wait(g, [&] { return issued > k || stage_error != cudaSuccess; });
+          if (stage_error != cudaSuccess) {
+            rc = fail(CUHE_CUDA_ERROR, std::string("index upload: ") + cudaGetErrorString(stage_error));
+            break;
+          }
+        }
+        cudaError_t e = cudaStreamWaitEvent(ln.stream, up[k], 0);
+        if (e == cudaSuccess) {
+          k_unpack<<<blocks_for((long long)(tc * 2 * n), 256), 256, 0, ln.stream>>>(
+              d_ib + t0 * 2 * in_bytes, (long long)(in_bytes), int(P.q_bits), int(tc * 2), tw + t0 * 2 * n * W, d,
+              d_status);
+          e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) {
+          rc = fail(CUHE_CUDA_ERROR, std::string("unpack: ") + cudaGetErrorString(e));
+          break;
+        }
+        rc = run_tiles(t0, tc);
+      }
+      stop.store(true);
+      stager.join();
+      cudaStreamSynchronize(ln.copy);  // no upload still writes the workspace
+      for (auto& e : up) cudaEventDestroy(e);
+      if (rc) return rc;
+      BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
+      BFV_CUDA(cudaStreamSynchronize(ln.stream), "unpack");
+      if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
     }
     // merge tree (bfv_server.h:15-45), executed in waves of independent merges
     cudaEvent_t m0, m1;

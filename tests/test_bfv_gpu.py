@@ -173,3 +173,50 @@ def test_resident_index_search_matches_packed_search():
     bad = (packed([q] * n, bits), ip[0][1])
     with pytest.raises(ValueError, match="Noncanonical"):
         m.upload_index(server, (bad,) + ip[1:])
+
+
+@pytest.mark.parametrize("residue", [True, False])
+def test_pipelined_host_index_search_matches_reference_checker(residue):
+    """A host-memory index of 589 tiles is uploaded in sub-batches of 256
+    tiles overlapped with the tile circuits (three sub-batches, the last one
+    ragged, a partial last tile); the responses equal the reference
+    checker's and the resident-index search's, on residue and native rings."""
+    ref = reference_native()
+    if ref is None:
+        pytest.skip("reference checker oracle/_ref not built")
+    n, gadget, t, tiles = 16, 30, 97, 589
+    q = 1
+    for p in ob.rns_primes(n, 180):
+        q *= p
+    if not residue:
+        q = ob.coefficient_modulus(180)
+    m = native()
+    rring = ref.create_ring(n, format(q, "x"), gadget, True, residue, 2 if residue else 0)
+    ring = m.create_ring(n, format(q, "x"), gadget, True, residue, 2 if residue else 0)
+    layout = ob.Layout(n, 3)
+    exps = sorted(set(layout.left()) | set(layout.right()))
+    keys = random_keys(n, q, 6, 1 + len(exps), seed=589)
+    kb = [key_bytes(k, q) for k in keys]
+    rrelin, grelin = ref.compile_key(rring, kb[0]), m.compile_key(ring, kb[0])
+    rg = tuple((g, ref.compile_key(rring, kb[1 + i])) for i, g in enumerate(exps))
+    gg = tuple((g, m.compile_key(ring, kb[1 + i])) for i, g in enumerate(exps))
+    target = ob.coefficient_modulus(40)
+    rserver = ref.create_server(rrelin, rg, layout.padded, t, format(target, "x"))
+    gserver = m.create_server(grelin, gg, layout.padded, t, format(target, "x"))
+    rng = random.Random(589)
+    bits = q.bit_length()
+
+    def ct():
+        return tuple(packed([rng.randrange(q) for _ in range(n)], bits) for _ in range(2))
+
+    query = ct()
+    index = tuple(ct() for _ in range(tiles))
+    count = (tiles - 1) * layout.capacity + 3
+    resident = m.upload_index(gserver, index)
+    for compact in (True, False):
+        want = ref.packed_search(rserver, query, index, count, compact)
+        assert m.packed_search(gserver, query, index, count, compact) == want, compact
+        assert m.search_index(gserver, resident, query, count, compact) == want, compact
+    bad = index[:300] + ((packed([q] * n, bits), index[300][1]),) + index[301:]
+    with pytest.raises(ValueError, match="Noncanonical"):
+        m.packed_search(gserver, query, bad, count, True)
