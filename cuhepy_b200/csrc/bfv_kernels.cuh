@@ -26,8 +26,20 @@ struct BaseDev {
   u64 product_words[kCrtWordsDev];
 };
 
+// Native rings: constants of the first `count` auxiliary primes (P their
+// product) for reducing a centred CRT integer mod q without composing it
+// (k_native_reduce, mode 0); R2 = 2^128.
+struct NativeCrt {
+  u64 inv[kMaxPrimes], inv_q[kMaxPrimes];  // (P / p_j)^-1 mod p_j and its Shoup quotient
+  u64 c[kMaxPrimes][kMaxWords];            // (P / p_j) R2 mod q
+  u64 pq[kMaxWords];                       // P R2 mod q
+  u64 cq[kMaxWords + 1];                   // count q
+};
+
 struct RingDev {
   int n, logn, primes, residue, tensor, digits, digit_bits, words;
+  const NativeCrt* crt;  // native rings: [count - 1] for count = 1 .. primes; else null
+  u64 q_ninv;            // -q^-1 mod 2^64 (native rings)
   Prime prime[kMaxPrimes];
   // twiddles as (w, floor(w 2^64 / p)) pairs, one 16-byte load each
   const ulonglong2* fwd2[kMaxPrimes];
@@ -1004,19 +1016,15 @@ __device__ __forceinline__ int garner_words(const u64* res, long long stride, in
 //
 // For x = -m < 0: x mod q = (q - m mod q) mod q, and
 // floor((q - 2 t m) / (2 q)) = -floor((2 t m + q - 1) / (2 q)).
+// One coefficient: residues at res[j * stride] (j < count) -> out[0 .. W).
 template <int MAXW>
-__global__ void k_native_reduce(const u64* __restrict__ res, long long polys, int count, u64* __restrict__ out,
-                                int mode, u64 t, const RingDev* __restrict__ ring) {
-  const RingDev& R = *ring;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= polys * R.n) return;
-  const long long poly = idx / R.n;
-  const int i = int(idx % R.n);
+__device__ __forceinline__ void native_reduce_one(const u64* __restrict__ res, long long stride, int count,
+                                               u64* __restrict__ o, int mode, u64 t, const RingDev& R) {
   const int W = R.words;
   constexpr int kLimbs = 2 * MAXW + 4;
   u64 x[MAXW];
   bool neg = false;
-  int xw = garner_words<MAXW>(res + poly * count * R.n + i, R.n, count, R, x, &neg);
+  int xw = garner_words<MAXW>(res, stride, count, R, x, &neg);
   uint32_t ql[kLimbs], xl[kLimbs], quo[kLimbs], rem[kLimbs];
   const int qn = words_to_limbs(R.q_words, W, ql);
   if (mode == 1) {
@@ -1075,8 +1083,113 @@ __global__ void k_native_reduce(const u64* __restrict__ res, long long polys, in
       borrow = u64(d >> 64) ? 1 : 0;
     }
   }
-  u64* o = out + (poly * R.n + i) * W;
   for (int k = 0; k < W; ++k) o[k] = r[k];
+}
+
+template <int MAXW>
+__global__ void k_native_reduce(const u64* __restrict__ res, long long polys, int count, u64* __restrict__ out,
+                                int mode, u64 t, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  native_reduce_one<MAXW>(res + poly * count * R.n + i, R.n, count, out + (poly * R.n + i) * R.words, mode, t, R);
+}
+
+// Mode-0 reduction straight from the residues, after the reference's
+// certified CRT (rns_ntt.h:422-469): with y_j = r_j (P / p_j)^-1 mod p_j and
+// theta = sum y_j / p_j, the centred integer is x = sum y_j (P / p_j) - v P
+// with v = round(theta), so x = sum y_j c_j - v pq (mod q) for c_j = P / p_j
+// mod q, pq = P mod q.  theta is summed in 64-bit fixed point (each term
+// within 2 units of the last place below its true value); when a rounding
+// boundary falls inside that error interval the coefficient is decoded
+// exactly instead (native_reduce_one).  Otherwise A = sum y_j c'_j + count q
+// - v pq' (c', pq' carry an extra factor 2^128) lies in [0, 2^65 q), and two
+// Montgomery word steps give A 2^-128 mod q = x mod q in [0, 2q).  kW = the
+// ring's words, a compile-time constant so that A stays in registers.
+template <int kW, int MAXW>
+__global__ void k_native_mod_q(const u64* __restrict__ res, long long polys, int count, u64* __restrict__ out,
+                               const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const u64* z = res + poly * count * R.n + i;
+  u64* o = out + (poly * R.n + i) * kW;
+  const NativeCrt& C = R.crt[count - 1];
+  u64 a[kW + 2];
+#pragma unroll
+  for (int k = 0; k < kW + 2; ++k) a[k] = k <= kW ? C.cq[k] : 0;
+  u128 theta = 0;
+  for (int j = 0; j < count; ++j) {
+    const Prime& m = R.prime[j];
+    const u64 y = shoup(z[(long long)j * R.n], C.inv[j], C.inv_q[j], m.p);
+    theta += u128(y * m.mu_hi + mulhi(y, m.mu_lo));  // floor(y mu / 2^64), mu = floor(2^128 / p)
+    u64 carry = 0;
+#pragma unroll
+    for (int k = 0; k < kW; ++k) {
+      const u128 sum = u128(C.c[j][k]) * y + a[k] + carry;
+      a[k] = u64(sum);
+      carry = u64(sum >> 64);
+    }
+    const u128 s1 = u128(a[kW]) + carry;
+    a[kW] = u64(s1);
+    a[kW + 1] += u64(s1 >> 64);
+  }
+  const u128 half = u128(1) << 63;
+  const u64 v = u64((theta + half) >> 64);
+  if (v != u64((theta + u128(2 * count) + half) >> 64)) {
+    native_reduce_one<MAXW>(z, R.n, count, o, 0, 0, R);
+    return;
+  }
+  u64 borrow = 0;  // a -= v pq (stays >= 0: v <= count and pq < q)
+#pragma unroll
+  for (int k = 0; k < kW + 2; ++k) {
+    const u128 prod = k < kW ? u128(C.pq[k]) * v + borrow : u128(borrow);
+    const u64 lo = u64(prod);
+    borrow = u64(prod >> 64) + (a[k] < lo ? 1 : 0);
+    a[k] -= lo;
+  }
+#pragma unroll
+  for (int step = 0; step < 2; ++step) {  // a <- (a + m q) / 2^64
+    const u64 mq = a[0] * R.q_ninv;
+    u64 carry = 0;
+#pragma unroll
+    for (int k = 0; k < kW; ++k) {
+      const u128 sum = u128(R.q_words[k]) * mq + a[k] + carry;
+      a[k] = u64(sum);
+      carry = u64(sum >> 64);
+    }
+    const u128 s1 = u128(a[kW]) + carry;
+    a[kW] = u64(s1);
+    a[kW + 1] += u64(s1 >> 64);
+#pragma unroll
+    for (int k = 0; k < kW + 1; ++k) a[k] = a[k + 1];
+    a[kW + 1] = 0;
+  }
+  // a < 2q (a[kW] may hold the top bit): subtract q once if a >= q
+  bool ge = a[kW] != 0;
+  bool decided = ge;
+#pragma unroll
+  for (int k = kW - 1; k >= 0; --k)
+    if (!decided && a[k] != R.q_words[k]) {
+      ge = a[k] > R.q_words[k];
+      decided = true;
+    }
+  if (!decided) ge = true;  // a == q
+  if (ge) {
+    u64 b = 0;
+#pragma unroll
+    for (int k = 0; k < kW; ++k) {
+      const u128 d = u128(a[k]) - R.q_words[k] - b;
+      a[k] = u64(d);
+      b = u64(d >> 64) ? 1 : 0;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kW; ++k) o[k] = a[k];
 }
 
 // out = a +- b mod q over `units` polys of words; poly u of a / b / out

@@ -176,6 +176,7 @@ struct cuhe_bfv_ring {
   size_t switch_prime_count = 0;
   u64* d_tables = nullptr;
   size_t table_bytes = 0;
+  NativeCrt* d_crt = nullptr;  // native rings: CRT constants per prime count
   RingDev host_dev{};
   std::map<u64, RingDev*> dev_for_t;  // t == 0: no scale constants
   struct PlainRing {             // batch encoding mod t: NTT tables and slot permutation
@@ -200,6 +201,7 @@ struct cuhe_bfv_ring {
       cudaFree(kv.second.d_perm);
     }
     if (d_tables) cudaFree(d_tables);
+    if (d_crt) cudaFree(d_crt);
     for (auto& ln : lanes)
       if (ln->stream) cudaStreamDestroy(ln->stream);
     lanes.clear();  // workspaces are freed while this device is current
@@ -639,6 +641,35 @@ int tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const TileArgs& a, u64*
   return CUHE_OK;
 }
 
+// CRT constants of the native reduction (NativeCrt) for every prime count
+// 1 .. K of the ring's auxiliary primes.
+std::vector<NativeCrt> native_crt_constants(const H::RingPlan& P) {
+  const size_t K = P.primes.size(), W = (P.q_bits + 63) / 64;
+  if (W > size_t(kMaxWords) || K > size_t(kMaxPrimes)) throw std::invalid_argument("native constants exceed limits");
+  auto mod_q = [&](const H::Big& a) { return H::sub(a, H::mul(H::div(a, P.q), P.q)); };
+  auto words = [&](const H::Big& a, u64* out, size_t count) {
+    for (size_t k = 0; k < count; ++k) out[k] = k < a.w.size() ? a.w[k] : 0;
+  };
+  const H::Big r2 = H::shl(H::Big(1), 128);
+  std::vector<NativeCrt> crt(K);
+  H::Big prod(1);
+  for (size_t c = 1; c <= K; ++c) {
+    prod = H::mul_small(prod, P.primes[c - 1]);
+    NativeCrt& C = crt[c - 1];
+    std::memset(&C, 0, sizeof(C));
+    for (size_t j = 0; j < c; ++j) {
+      const u64 p = P.primes[j];
+      const H::Big pj = H::div_small(prod, p);
+      C.inv[j] = H::powmod(H::mod_small(pj, p), p - 2, p);
+      C.inv_q[j] = H::shoup_quotient(C.inv[j], p);
+      words(mod_q(H::mul(pj, r2)), C.c[j], W);
+    }
+    words(mod_q(H::mul(prod, r2)), C.pq, W);
+    words(H::mul_small(P.q, u64(c)), C.cq, W + 1);
+  }
+  return crt;
+}
+
 size_t tile_arena_bytes(const cuhe_bfv_ring* r, size_t ct) {
   const auto& P = r->plan;
   const size_t n = P.n, L = P.residue_count, T = P.tensor_count, W = size_t(r->host_dev.words);
@@ -659,6 +690,23 @@ int native_reduce(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* res, size_t
                   int mode, u64 t) {
   if (!polys) return CUHE_OK;
   const unsigned blocks = blocks_for((long long)(polys * r->plan.n), 128);
+  if (mode == 0 && r->d_crt) {
+    const bool narrow = count <= size_t(kNarrowWords);
+#define CUHE_MOD_Q(KW)                                                                                          \
+  case KW:                                                                                                      \
+    if (narrow)                                                                                                 \
+      k_native_mod_q<KW, kNarrowWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, d); \
+    else                                                                                                        \
+      k_native_mod_q<KW, kWideWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, d);   \
+    break;
+    switch (r->host_dev.words) {
+      CUHE_MOD_Q(1) CUHE_MOD_Q(2) CUHE_MOD_Q(3) CUHE_MOD_Q(4) CUHE_MOD_Q(5) CUHE_MOD_Q(6) CUHE_MOD_Q(7)
+      default: CUHE_MOD_Q(8)
+    }
+#undef CUHE_MOD_Q
+    BFV_CUDA(cudaGetLastError(), "native reduce");
+    return CUHE_OK;
+  }
   if (count <= size_t(kNarrowWords))
     k_native_reduce<kNarrowWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, mode, t, d);
   else
@@ -951,6 +999,26 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   // native rings: key switches run over the switch primes
   if (!r->residue) dev.residue = int(r->switch_prime_count);
   for (size_t w = 0; w < P.q.w.size() && w < size_t(kMaxWords); ++w) dev.q_words[w] = P.q.w[w];
+  if (!r->residue) {
+    std::vector<NativeCrt> crt;
+    try {
+      crt = native_crt_constants(P);
+    } catch (const std::invalid_argument& ex) {
+      delete r;
+      return fail(CUHE_INVALID_ARGUMENT, ex.what());
+    }
+    cudaError_t ce = cudaMalloc(&r->d_crt, crt.size() * sizeof(NativeCrt));
+    if (ce == cudaSuccess)
+      ce = cudaMemcpy(r->d_crt, crt.data(), crt.size() * sizeof(NativeCrt), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) {
+      delete r;
+      return fail(CUHE_CUDA_ERROR, std::string("native constants: ") + cudaGetErrorString(ce));
+    }
+    dev.crt = r->d_crt;
+    u64 inv = 1;  // q^-1 mod 2^64 by Newton's iteration (q odd)
+    for (int k = 0; k < 6; ++k) inv *= 2 - P.q.w[0] * inv;
+    dev.q_ninv = u64(0) - inv;
+  }
   RingDev* dummy = nullptr;
   if (int rc = device_ring(r, 0, &dummy)) {
     delete r;
