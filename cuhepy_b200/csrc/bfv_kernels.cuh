@@ -36,10 +36,22 @@ struct NativeCrt {
   u64 cq[kMaxWords + 1];                   // count q
 };
 
+// Native rings, plaintext modulus t: constants of the scale-and-round over
+// the tensor primes (P their product).  With t P / p_j = A_j q + B_j and
+// t P = A_P q + B_P: a = (A mod q) 2^128 mod q, f = floor(B 2^128 / q).
+struct NativeScale {
+  u64 a[kMaxPrimes][kMaxWords];
+  u64 ap[kMaxWords];
+  u64 f[kMaxPrimes][2];
+  u64 fp[2];
+};
+
 struct RingDev {
   int n, logn, primes, residue, tensor, digits, digit_bits, words;
   const NativeCrt* crt;  // native rings: [count - 1] for count = 1 .. primes; else null
   u64 q_ninv;            // -q^-1 mod 2^64 (native rings)
+  int has_nscale;        // nscale valid (native ring with t set, q of at least 68 bits)
+  NativeScale nscale;
   Prime prime[kMaxPrimes];
   // twiddles as (w, floor(w 2^64 / p)) pairs, one 16-byte load each
   const ulonglong2* fwd2[kMaxPrimes];
@@ -1190,6 +1202,193 @@ __global__ void k_native_mod_q(const u64* __restrict__ res, long long polys, int
   }
 #pragma unroll
   for (int k = 0; k < kW; ++k) o[k] = a[k];
+}
+
+// Mode-1 (scale-and-round) reduction from the residues of the tensor primes:
+// with x = sum y_j (P / p_j) - v P as in k_native_mod_q,
+//   floor((2 t x + q) / (2 q)) = I + floor(E / q + 1/2),
+//   I = sum y_j A_j - v A_P,  E = sum y_j B_j - v B_P,
+// so the result mod q is (I mod q) + round(E / q), the first by the same
+// Montgomery finish as k_native_mod_q and the second from 128-bit fixed-point
+// fractions f = B / q (error below 2^-60 in all).  A rounding boundary inside
+// the error interval, or q below 2^68 (then |round(E / q)| may reach q),
+// sends the coefficient to the exact path.
+template <int kW, int MAXW>
+__global__ void k_native_scale(const u64* __restrict__ res, long long polys, int count, u64* __restrict__ out, u64 t,
+                               const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= polys * R.n) return;
+  const long long poly = idx / R.n;
+  const int i = int(idx % R.n);
+  const u64* z = res + poly * count * R.n + i;
+  u64* o = out + (poly * R.n + i) * kW;
+  const NativeCrt& C = R.crt[count - 1];
+  const NativeScale& S = R.nscale;
+  u64 a[kW + 2];
+#pragma unroll
+  for (int k = 0; k < kW + 2; ++k) a[k] = k <= kW ? C.cq[k] : 0;
+  u64 e[4] = {0, 0, 0, 0};  // sum y_j f_j - v f_P: two's complement, 128 fraction bits
+  u128 theta = 0;
+  for (int j = 0; j < count; ++j) {
+    const Prime& m = R.prime[j];
+    const u64 y = shoup(z[(long long)j * R.n], C.inv[j], C.inv_q[j], m.p);
+    theta += u128(y * m.mu_hi + mulhi(y, m.mu_lo));
+    u64 carry = 0;
+#pragma unroll
+    for (int k = 0; k < kW; ++k) {
+      const u128 sum = u128(S.a[j][k]) * y + a[k] + carry;
+      a[k] = u64(sum);
+      carry = u64(sum >> 64);
+    }
+    const u128 s1 = u128(a[kW]) + carry;
+    a[kW] = u64(s1);
+    a[kW + 1] += u64(s1 >> 64);
+    const u128 p0 = u128(S.f[j][0]) * y + e[0];
+    e[0] = u64(p0);
+    const u128 p1 = u128(S.f[j][1]) * y + e[1] + u64(p0 >> 64);
+    e[1] = u64(p1);
+    const u128 p2 = u128(e[2]) + u64(p1 >> 64);
+    e[2] = u64(p2);
+    e[3] += u64(p2 >> 64);
+  }
+  const u128 half = u128(1) << 63;
+  const u64 v = u64((theta + half) >> 64);
+  if (v != u64((theta + u128(2 * count) + half) >> 64) || !R.has_nscale) {
+    native_reduce_one<MAXW>(z, R.n, count, o, 1, t, R);
+    return;
+  }
+  {
+    u64 borrow = 0;  // a -= v A_P
+#pragma unroll
+    for (int k = 0; k < kW + 2; ++k) {
+      const u128 prod = k < kW ? u128(S.ap[k]) * v + borrow : u128(borrow);
+      const u64 lo = u64(prod);
+      borrow = u64(prod >> 64) + (a[k] < lo ? 1 : 0);
+      a[k] -= lo;
+    }
+  }
+  {
+    u64 borrow = 0;  // e -= v f_P
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const u128 prod = k < 2 ? u128(S.fp[k]) * v + borrow : u128(borrow);
+      const u64 lo = u64(prod);
+      borrow = u64(prod >> 64) + (e[k] < lo ? 1 : 0);
+      e[k] -= lo;
+    }
+  }
+  // r = floor(E / q + 1/2): E 2^128 / q lies in (e - 32, e + 2^66), so r is
+  // certain when the top 128 bits of e - 32 + 2^127 and e + 2^66 + 2^127
+  // agree (256-bit two's complement)
+  u64 rlo[2], rhi[2];
+  {
+    u64 w[4] = {e[0], e[1], e[2], e[3]};
+    u64 c = w[0] < 32 ? 1 : 0;
+    w[0] -= 32;
+    for (int k = 1; k < 4; ++k) {
+      const u64 before = w[k];
+      w[k] -= c;
+      c = (c && before == 0) ? 1 : 0;
+    }
+    const u128 h1 = u128(w[1]) + (u64(1) << 63);
+    w[1] = u64(h1);
+    const u128 h2 = u128(w[2]) + u64(h1 >> 64);
+    w[2] = u64(h2);
+    w[3] += u64(h2 >> 64);
+    rlo[0] = w[2];
+    rlo[1] = w[3];
+  }
+  {
+    u64 w[4] = {e[0], e[1], e[2], e[3]};
+    const u128 h1 = u128(w[1]) + 4 + (u64(1) << 63);  // 2^66 + 2^127 in word 1
+    w[1] = u64(h1);
+    const u128 h2 = u128(w[2]) + u64(h1 >> 64);
+    w[2] = u64(h2);
+    w[3] += u64(h2 >> 64);
+    rhi[0] = w[2];
+    rhi[1] = w[3];
+  }
+  if (rlo[0] != rhi[0] || rlo[1] != rhi[1]) {
+    native_reduce_one<MAXW>(z, R.n, count, o, 1, t, R);
+    return;
+  }
+  // I mod q by two Montgomery word steps (a < 2^65 q)
+#pragma unroll
+  for (int step = 0; step < 2; ++step) {
+    const u64 mq = a[0] * R.q_ninv;
+    u64 carry = 0;
+#pragma unroll
+    for (int k = 0; k < kW; ++k) {
+      const u128 sum = u128(R.q_words[k]) * mq + a[k] + carry;
+      a[k] = u64(sum);
+      carry = u64(sum >> 64);
+    }
+    const u128 s1 = u128(a[kW]) + carry;
+    a[kW] = u64(s1);
+    a[kW + 1] += u64(s1 >> 64);
+#pragma unroll
+    for (int k = 0; k < kW + 1; ++k) a[k] = a[k + 1];
+    a[kW + 1] = 0;
+  }
+  // add r (signed 128-bit, |r| < 2^67 <= q): a in [0, 2q) -> a + r in (-q, 3q)
+  const bool rneg = (rlo[1] >> 63) != 0;
+  u64 rm[2] = {rlo[0], rlo[1]};
+  if (rneg) {  // |r|
+    rm[0] = ~rm[0] + 1;
+    rm[1] = ~rm[1] + (rm[0] == 0 ? 1 : 0);
+  }
+  u64 b[kW + 1];
+#pragma unroll
+  for (int k = 0; k < kW + 1; ++k) b[k] = a[k];
+  if (!rneg) {
+    u64 c = 0;
+#pragma unroll
+    for (int k = 0; k < kW + 1; ++k) {
+      const u128 sum = u128(b[k]) + (k < 2 ? rm[k] : 0) + c;
+      b[k] = u64(sum);
+      c = u64(sum >> 64);
+    }
+  } else {
+    u64 c = 0;  // b = a + q - |r| (>= 0 since |r| < q)
+#pragma unroll
+    for (int k = 0; k < kW + 1; ++k) {
+      const u128 sum = u128(b[k]) + (k < kW ? R.q_words[k] : 0) + c;
+      b[k] = u64(sum);
+      c = u64(sum >> 64);
+    }
+    u64 br = 0;
+#pragma unroll
+    for (int k = 0; k < kW + 1; ++k) {
+      const u128 d = u128(b[k]) - (k < 2 ? rm[k] : 0) - br;
+      b[k] = u64(d);
+      br = u64(d >> 64) ? 1 : 0;
+    }
+  }
+  // b in [0, 3q): subtract q while b >= q (at most twice)
+#pragma unroll
+  for (int pass = 0; pass < 2; ++pass) {
+    bool ge = b[kW] != 0;
+    bool decided = ge;
+#pragma unroll
+    for (int k = kW - 1; k >= 0; --k)
+      if (!decided && b[k] != R.q_words[k]) {
+        ge = b[k] > R.q_words[k];
+        decided = true;
+      }
+    if (!decided) ge = true;
+    if (ge) {
+      u64 br = 0;
+#pragma unroll
+      for (int k = 0; k < kW + 1; ++k) {
+        const u128 d = u128(b[k]) - (k < kW ? R.q_words[k] : 0) - br;
+        b[k] = u64(d);
+        br = u64(d >> 64) ? 1 : 0;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kW; ++k) o[k] = b[k];
 }
 
 // out = a +- b mod q over `units` polys of words; poly u of a / b / out

@@ -262,13 +262,44 @@ unsigned log2u(size_t n) {
   return l;
 }
 
+// Scale constants (NativeScale) of a native ring for plaintext modulus t over
+// its tensor primes.
+void native_scale_constants(const H::RingPlan& P, u64 t, NativeScale& S) {
+  const size_t T = P.tensor_count, W = (P.q_bits + 63) / 64;
+  std::memset(&S, 0, sizeof(S));
+  auto words = [&](const H::Big& a, u64* out, size_t count) {
+    for (size_t k = 0; k < count; ++k) out[k] = k < a.w.size() ? a.w[k] : 0;
+  };
+  auto mod_q = [&](const H::Big& a) { return H::sub(a, H::mul(H::div(a, P.q), P.q)); };
+  const H::Big r2 = H::shl(H::Big(1), 128);
+  // num = A q + B: a = (A mod q) 2^128 mod q, f = floor(B 2^128 / q)
+  auto split = [&](const H::Big& num, u64* a, u64* f) {
+    const H::Big A = H::div(num, P.q);
+    const H::Big B = H::sub(num, H::mul(A, P.q));
+    words(mod_q(H::mul(mod_q(A), r2)), a, W);
+    words(H::div(H::mul(B, r2), P.q), f, 2);
+  };
+  H::Big prod(1);
+  for (size_t j = 0; j < T; ++j) prod = H::mul_small(prod, P.primes[j]);
+  for (size_t j = 0; j < T; ++j) split(H::mul_small(H::div_small(prod, P.primes[j]), t), S.a[j], S.f[j]);
+  split(H::mul_small(prod, t), S.ap, S.fp);
+}
+
 // Device copy of the ring constants; t != 0 adds the exact scale constants.
 int device_ring(cuhe_bfv_ring* r, u64 t, RingDev** out) {
   std::lock_guard<std::mutex> lock(r->mu);
   auto it = r->dev_for_t.find(t);
   if (it != r->dev_for_t.end()) { *out = it->second; return CUHE_OK; }
   RingDev dev = r->host_dev;
-  if (t && r->residue) {  // native rings scale with multiword arithmetic instead
+  if (t && !r->residue && r->plan.q_bits >= 68) {
+    try {
+      native_scale_constants(r->plan, t, dev.nscale);
+      dev.has_nscale = 1;
+    } catch (const std::invalid_argument& e) {
+      return fail(CUHE_INVALID_ARGUMENT, e.what());
+    }
+  }
+  if (t && r->residue) {  // native rings scale with the CRT constants above
     H::RingPlan plan = r->plan;
     try {
       H::build_scale(plan, t);
@@ -690,6 +721,23 @@ int native_reduce(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* res, size_t
                   int mode, u64 t) {
   if (!polys) return CUHE_OK;
   const unsigned blocks = blocks_for((long long)(polys * r->plan.n), 128);
+  if (mode == 1 && r->d_crt && count == r->plan.tensor_count) {
+    const bool narrow = count <= size_t(kNarrowWords);
+#define CUHE_SCALE(KW)                                                                                         \
+  case KW:                                                                                                     \
+    if (narrow)                                                                                                \
+      k_native_scale<KW, kNarrowWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, t, d); \
+    else                                                                                                       \
+      k_native_scale<KW, kWideWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, t, d);   \
+    break;
+    switch (r->host_dev.words) {
+      CUHE_SCALE(1) CUHE_SCALE(2) CUHE_SCALE(3) CUHE_SCALE(4) CUHE_SCALE(5) CUHE_SCALE(6) CUHE_SCALE(7)
+      default: CUHE_SCALE(8)
+    }
+#undef CUHE_SCALE
+    BFV_CUDA(cudaGetLastError(), "native scale");
+    return CUHE_OK;
+  }
   if (mode == 0 && r->d_crt) {
     const bool narrow = count <= size_t(kNarrowWords);
 #define CUHE_MOD_Q(KW)                                                                                          \
