@@ -67,6 +67,7 @@ BFV_SIGNATURES: dict[str, tuple] = {
                                     ctypes.c_int, _vp]),
     "cuhe_bfv_get_lanes": (ctypes.c_int, [_vp]),
     "cuhe_bfv_search_workspace": (ctypes.c_uint64, [_vp, ctypes.c_uint64, ctypes.c_int]),
+    "cuhe_bfv_reserve_workspace": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_int]),
 }
 
 BFV_LIB = "libcuhe_bfv_b200.so"
@@ -468,6 +469,12 @@ def get_lanes(ring: Ring) -> int:
 def search_workspace(server: Server, tiles: int, compact: bool = True) -> int:
     """Device bytes one lane holds for a search over `tiles` tiles."""
     return int(lib().cuhe_bfv_search_workspace(_get(server, Server).ptr, int(tiles), int(bool(compact))))
+
+
+def reserve_workspace(server: Server, tiles: int, compact: bool = True) -> None:
+    """Allocate that workspace on every active lane of the server's ring now,
+    so later searches of up to `tiles` tiles allocate no device memory."""
+    _check(lib().cuhe_bfv_reserve_workspace(_get(server, Server).ptr, _u64(tiles, "tiles"), int(bool(compact))))
 
 
 def _profile(fn, *args) -> tuple[Any, dict[str, Any]]:

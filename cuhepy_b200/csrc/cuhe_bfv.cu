@@ -2067,6 +2067,22 @@ uint64_t cuhe_bfv_search_workspace(const cuhe_bfv_server* s, uint64_t tiles, int
   return search_chunk_bytes(s, ct, compact ? s->target_bits : unsigned(s->ring->plan.q_bits));
 }
 
+int cuhe_bfv_reserve_workspace(cuhe_bfv_server* s, uint64_t tiles, int compact) {
+  if (!s) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  if (!tiles) return CUHE_OK;
+  cuhe_bfv_ring* r = s->ring;
+  const uint64_t bytes = cuhe_bfv_search_workspace(s, tiles, compact);
+  const int lanes = std::max(1, std::min(kMaxLanes, r->active_lanes.load()));
+  DeviceGuard guard(r->device);
+  for (int k = 0; k < lanes; ++k) {
+    Lane& ln = *r->lanes[size_t(k)];
+    std::lock_guard<std::mutex> lock(ln.mu);
+    BFV_CUDA(cudaStreamSynchronize(ln.stream), "lane drain");
+    BFV_CUDA(ln.arena.reserve(size_t(bytes)), "workspace");
+  }
+  return CUHE_OK;
+}
+
 int cuhe_bfv_batch_encode(cuhe_bfv_ring* r, uint64_t t, const uint32_t* slots, uint64_t count, uint64_t* out) {
   if (!r || (count && (!slots || !out))) return fail(CUHE_INVALID_ARGUMENT, "null argument");
   if (count == 0) return CUHE_OK;

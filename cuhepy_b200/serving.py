@@ -353,6 +353,9 @@ class KnnEvaluator:
         from cuhepy_b200.bfv import _bfv_rns
 
         _bfv_rns.set_lanes(server.ring, self.lane_counts["bfv"])
+        # every lane's workspace now: an allocation inside a request would
+        # wait for whatever else runs on the GPU
+        _bfv_rns.reserve_workspace(server, index.tiles, compact)
         self._bfv[name] = {"server": server, "index": index, "count": int(count), "compact": bool(compact),
                            "workspace": _bfv_rns.search_workspace(server, index.tiles, compact)}
 

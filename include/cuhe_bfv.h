@@ -163,6 +163,13 @@ int cuhe_bfv_get_lanes(const cuhe_bfv_ring* ring);
  * Serving code admits a search when this fits in free device memory. */
 uint64_t cuhe_bfv_search_workspace(const cuhe_bfv_server* server, uint64_t tiles, int compact);
 
+/* Allocate that workspace now on every active lane of the server's ring
+ * (each lane's device arena grows to it), so that later searches of up to
+ * `tiles` tiles allocate nothing: a device allocation inside a search can
+ * wait for unrelated work running on the GPU.  No counterpart in the
+ * reference (serving addition). */
+int cuhe_bfv_reserve_workspace(cuhe_bfv_server* server, uint64_t tiles, int compact);
+
 #ifdef __cplusplus
 }
 #endif
