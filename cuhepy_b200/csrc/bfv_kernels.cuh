@@ -79,11 +79,13 @@ __host__ __device__ constexpr size_t plane_smem_words(int n) { return size_t(n) 
 // elements at stride `stride` runs stages s0 .. s0+P-1 without touching shared
 // memory.  Stage s has 2^s groups of gap N/2^(s+1); inside a block the group
 // of element k at stage s0+t is G*2^t + (k >> (P-t)).
-// kSharedTw: the twiddle table w2 lives in shared memory (staged by the
-// caller) instead of global memory read through the read-only cache.
-template <int P, bool kSharedTw = false>
+// kHalf: the plane is half `half` (0 or 1) of a transform of twice its
+// length whose first stage has already run; its stage s is the full
+// transform's stage s + 1, whose twiddles for this half start at m (2 + half)
+// instead of m.
+template <int P, bool kHalf = false>
 __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const ulonglong2* __restrict__ w2,
-                                                 u64 p, bool last) {
+                                                 u64 p, bool last, int half_id = 0) {
   constexpr int E = 1 << P;
   const int n = 1 << logn;
   const u64 two_p = 2 * p;
@@ -104,8 +106,8 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
 #pragma unroll
       for (int k = 0; k < E; ++k) {
         if (k & half) continue;
-        const int idx = m + (G << t) + (k >> (P - t));
-        const ulonglong2 tw = kSharedTw ? w2[idx] : __ldg(w2 + idx);
+        const int idx = (kHalf ? m * (2 + half_id) : m) + (G << t) + (k >> (P - t));
+        const ulonglong2 tw = __ldg(w2 + idx);
         const u64 root = tw.x, rq = tw.y;
         u64 u = x[k];
         if (u >= two_p) u -= two_p;
@@ -128,9 +130,10 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
 
 // Inverse (decimation in time) passes: stage u has gap 2^u and N/2^(u+1)
 // groups; the final stage (gap N/2) folds in 1/N and the inverse twist.
-template <int P, bool kSharedTw = false, bool kFinal = false>
+template <int P, bool kHalf = false, bool kFinal = false>
 __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const ulonglong2* __restrict__ w2,
-                                                 u64 p, u64 n_inv, u64 n_inv_q, u64 last_w, u64 last_q) {
+                                                 u64 p, u64 n_inv, u64 n_inv_q, u64 last_w, u64 last_q,
+                                                 int half_id = 0) {
   constexpr int E = 1 << P;
   const int n = 1 << logn;
   const u64 two_p = 2 * p;
@@ -157,7 +160,7 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
           x[k + half] = shoup(u + two_p - v, last_w, last_q, p);
         } else {
           const int idx = m + (G << (P - t - 1)) + (k >> (t + 1));
-          const ulonglong2 tw = kSharedTw ? w2[idx] : __ldg(w2 + idx);
+          const ulonglong2 tw = __ldg(w2 + (kHalf ? idx + m * (1 + half_id) : idx));
           const u64 root = tw.x, rq = tw.y;
           const u64 s = u + v;
           x[k] = s >= two_p ? s - two_p : s;
@@ -172,38 +175,37 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
 
 // Whole transforms over a padded shared-memory plane (all threads of the CTA).
 // max_p (1..4) caps the stages per register pass (radix 2^max_p).
-// tw: the prime's twiddle pairs staged in shared memory (kSharedTw), else
-// the ring's global tables are used.
-template <bool kSharedTw = false>
-__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4,
-                                                 const ulonglong2* tw = nullptr) {
-  const int logn = R.logn;
+// kHalf: the plane is half `half_id` of a transform of length 2^(logn + 1)
+// (logn = R.logn - 1): forward after that transform's first stage, inverse
+// before its last (whose 1/N and twist the caller applies).
+template <bool kHalf = false>
+__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4, int half_id = 0) {
+  const int logn = kHalf ? R.logn - 1 : R.logn;
   const u64 p = R.prime[j].p;
-  const ulonglong2* w2 = kSharedTw ? tw : R.fwd2[j];
+  const ulonglong2* w2 = R.fwd2[j];
   for (int s0 = 0; s0 < logn; s0 += max_p) {
     const int P = logn - s0 < max_p ? logn - s0 : max_p;
     const bool last = s0 + P == logn;
     switch (P) {
-      case 4: ntt_forward_pass<4, kSharedTw>(a, s0, logn, w2, p, last); break;
-      case 3: ntt_forward_pass<3, kSharedTw>(a, s0, logn, w2, p, last); break;
-      case 2: ntt_forward_pass<2, kSharedTw>(a, s0, logn, w2, p, last); break;
-      default: ntt_forward_pass<1, kSharedTw>(a, s0, logn, w2, p, last); break;
+      case 4: ntt_forward_pass<4, kHalf>(a, s0, logn, w2, p, last, half_id); break;
+      case 3: ntt_forward_pass<3, kHalf>(a, s0, logn, w2, p, last, half_id); break;
+      case 2: ntt_forward_pass<2, kHalf>(a, s0, logn, w2, p, last, half_id); break;
+      default: ntt_forward_pass<1, kHalf>(a, s0, logn, w2, p, last, half_id); break;
     }
     __syncthreads();
   }
 }
 
-template <bool kSharedTw = false>
-__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j, int max_p = 4,
-                                                 const ulonglong2* tw = nullptr) {
-  const int logn = R.logn;
+template <bool kHalf = false>
+__device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j, int max_p = 4, int half_id = 0) {
+  const int logn = kHalf ? R.logn - 1 : R.logn;
   const u64 p = R.prime[j].p;
-  const ulonglong2* w2 = kSharedTw ? tw : R.inv2[j];
+  const ulonglong2* w2 = R.inv2[j];
   for (int u0 = 0; u0 < logn; u0 += max_p) {
     const int P = logn - u0 < max_p ? logn - u0 : max_p;
-    const int key = P * 2 + (u0 + P == logn ? 1 : 0);
+    const int key = P * 2 + (!kHalf && u0 + P == logn ? 1 : 0);
 #define CUHE_INV_PASS(PP, F) \
-  ntt_inverse_pass<PP, kSharedTw, F>(a, u0, logn, w2, p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j])
+  ntt_inverse_pass<PP, kHalf, F>(a, u0, logn, w2, p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j], half_id)
     switch (key) {
       case 9: CUHE_INV_PASS(4, true); break;
       case 8: CUHE_INV_PASS(4, false); break;
@@ -279,6 +281,62 @@ __global__ void __launch_bounds__(1024, 1)
 k_ntt8(u64* data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block, int inverse,
        int max_p = 3) {
   ntt_plane<3>(data, ring, prime_base, prime_mod, prime_block, inverse, max_p);
+}
+
+// ---- transforms of N = 32768 (a plane exceeds one CTA's shared memory) ------
+// The first forward stage (gap N/2, one twiddle) and the last inverse stage
+// (1/N and the twist) pair the two halves of a plane and run as elementwise
+// kernels on global memory; every other stage stays within a half, which a
+// CTA transforms in shared memory (k_ntt_half).  Planes follow launch_ntt's
+// prime mapping: prime = (b / prime_block) % prime_mod + prime_base.
+__device__ __forceinline__ int plane_prime(long long b, int prime_base, int prime_mod, int prime_block) {
+  return prime_base + int((b / prime_block) % prime_mod);
+}
+
+// forward stage 0 (inputs canonical; outputs below 4p, as the passes take)
+// or, with kInverse, the final inverse stage (inputs below 2p, outputs
+// canonical); one thread per pair (i, i + N/2)
+template <bool kInverse>
+__global__ void k_ntt_cross(u64* __restrict__ data, long long planes, const RingDev* __restrict__ ring, int prime_base,
+                            int prime_mod, int prime_block) {
+  const RingDev& R = *ring;
+  const int hn = R.n >> 1;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= planes * hn) return;
+  const long long b = idx / hn;
+  const int i = int(idx % hn);
+  const int j = plane_prime(b, prime_base, prime_mod, prime_block);
+  const u64 p = R.prime[j].p, two_p = 2 * p;
+  u64* a = data + b * R.n;
+  const u64 u = a[i], v = a[i + hn];
+  if (kInverse) {
+    a[i] = shoup(u + v, R.n_inv[j], R.n_inv_q[j], p);
+    a[i + hn] = shoup(u + two_p - v, R.last[j], R.last_q[j], p);
+  } else {
+    const ulonglong2 tw = __ldg(R.fwd2[j] + 1);  // stage 0: one group
+    const u64 w = shoup_lazy(v, tw.x, tw.y, p);
+    a[i] = u + w;
+    a[i + hn] = u + two_p - w;
+  }
+}
+
+// stages 1 .. logN - 1 (forward) or 0 .. logN - 2 (inverse) of one half:
+// CTA b transforms half (b & 1) of plane b >> 1
+template <bool kInverse>
+__global__ void __launch_bounds__(1024, 1)
+k_ntt_half(u64* __restrict__ data, const RingDev* __restrict__ ring, int prime_base, int prime_mod, int prime_block) {
+  extern __shared__ __align__(16) u64 s_plane[];
+  const RingDev& R = *ring;
+  const int hn = R.n >> 1;
+  const long long b = blockIdx.x >> 1;
+  const int h = int(blockIdx.x & 1);
+  const int j = plane_prime(b, prime_base, prime_mod, prime_block);
+  u64* a = data + b * R.n + (long long)h * hn;
+  for (int i = threadIdx.x; i < hn; i += blockDim.x) s_plane[sp(i)] = a[i];
+  __syncthreads();
+  if (kInverse) ntt_inverse_fast<true>(s_plane, R, j, 3, h);
+  else ntt_forward_fast<true>(s_plane, R, j, 3, h);
+  for (int i = threadIdx.x; i < hn; i += blockDim.x) a[i] = s_plane[sp(i)];
 }
 
 // ---- wire unpacking ---------------------------------------------------------
@@ -869,6 +927,60 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
   __syncthreads();
   tmem_fence_after_sync();
   if (warp == 0) tmem_dealloc(s_tmem, kCols);
+}
+
+// ---- unfused key switch (N = 32768) --------------------------------------------
+// digits[op][prime][d][N] = digit d of op's composed words, mod the prime
+__global__ void k_ks_digits(const SwitchOp* __restrict__ ops, int L, u64* __restrict__ digits,
+                            const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R.n) return;
+  const int plane = blockIdx.y;  // (op * L + j) * D + d
+  const int d = plane % R.digits, j = (plane / R.digits) % L, op = plane / (R.digits * L);
+  const SwitchOp& o = ops[op];
+  digits[(long long)plane * R.n + i] = gadget_digit(o.words + (long long)i * R.words, R.words, d, R, j);
+}
+
+// acc[op][c][prime][N] = sum_d digits[op][prime][d] * key[d][c][prime] (NTT domain)
+__global__ void k_ks_mac(const SwitchOp* __restrict__ ops, int L, const u64* __restrict__ digits,
+                         u64* __restrict__ acc, const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R.n) return;
+  const int plane = blockIdx.y;  // (op * 2 + c) * L + j
+  const int j = plane % L, c = (plane / L) % 2, op = plane / (2 * L);
+  const SwitchOp& o = ops[op];
+  const u64 p = R.prime[j].p;
+  u64 sum = 0;
+  for (int d = 0; d < R.digits; ++d) {
+    const u64 v = digits[(((long long)op * L + j) * R.digits + d) * R.n + i];
+    const long long ko = ((long long)(d * 2 + c) * L + j) * R.n + i;
+    sum = addmod(sum, shoup(v, __ldg(o.key + ko), __ldg(o.key_q + ko), p), p);
+  }
+  acc[(long long)plane * R.n + i] = sum;
+}
+
+// out = acc + base + [c == 0] sigma(x0), as k_keyswitch's epilogue
+__global__ void k_ks_finish(const SwitchOp* __restrict__ ops, int L, const u64* __restrict__ acc,
+                            const RingDev* __restrict__ ring) {
+  const RingDev& R = *ring;
+  const int n = R.n;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int plane = blockIdx.y;  // (op * 2 + c) * L + j
+  const int j = plane % L, c = (plane / L) % 2, op = plane / (2 * L);
+  const SwitchOp& o = ops[op];
+  const u64 p = R.prime[j].p;
+  u64 v = acc[(long long)plane * n + i];
+  if (o.base) v = addmod(v, o.base[((long long)c * L + j) * n + i], p);
+  if (c == 0 && o.x0) {
+    const unsigned sidx = unsigned((unsigned long long)i * o.g_inv % (2u * unsigned(n)));
+    u64 x = sidx < unsigned(n) ? o.x0[(long long)j * n + sidx] : o.x0[(long long)j * n + (sidx - n)];
+    if (sidx >= unsigned(n) && x) x = p - x;
+    v = addmod(v, x, p);
+  }
+  o.out[((long long)c * L + j) * n + i] = v;
 }
 
 // ---- elementwise ------------------------------------------------------------------

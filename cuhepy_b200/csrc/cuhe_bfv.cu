@@ -95,8 +95,11 @@ struct Lane {
   cudaStream_t copy = nullptr;      // uploads overlapped with the lane's compute
   uint8_t* pin[2] = {nullptr, nullptr};  // their pinned double buffer
   size_t pin_cap[2] = {0, 0};
+  u64* ks_scratch = nullptr;  // N = 32768 key switches: digit and accumulator planes (grow-only)
+  size_t ks_scratch_bytes = 0;
   ~Lane() {
     if (copy) cudaStreamSynchronize(copy);
+    if (ks_scratch) cudaFree(ks_scratch);
     if (host_stage) cudaFreeHost(host_stage);
     for (uint8_t* p : pin)
       if (p) cudaFreeHost(p);
@@ -460,13 +463,40 @@ int ntt_default_threads(size_t n) {
   return int(std::min<size_t>(n >= 16384 ? 1024 : 512, std::max<size_t>(32, n / 8)));
 }
 
+// Largest degree whose plane one CTA transforms in shared memory.
+constexpr size_t kMaxPlaneN = 16384;
+
+// Batched transforms of `planes` planes on `stream` (prime mapping of
+// k_ntt8); N = 32768 runs as the cross stage plus two half-plane transforms.
+// d may be a ring's or a plain ring's constants.  Shared-memory sizes are
+// within the attributes set at ring creation.
+cudaError_t ntt_planes(size_t n, cudaStream_t stream, RingDev* d, u64* data, long long planes, int prime_base,
+                       int prime_mod, int prime_block, int inverse, int threads = 0, int radix_log = 3) {
+  if (planes <= 0) return cudaSuccess;
+  const size_t smem = plane_smem_words(int(std::min(n, kMaxPlaneN))) * sizeof(u64);
+  if (n > kMaxPlaneN) {
+    const unsigned cross = blocks_for(planes * (long long)(n / 2), 256);
+    const int th = ntt_default_threads(n / 2);
+    if (!inverse) {
+      k_ntt_cross<false><<<cross, 256, 0, stream>>>(data, planes, d, prime_base, prime_mod, prime_block);
+      k_ntt_half<false><<<unsigned(planes * 2), th, smem, stream>>>(data, d, prime_base, prime_mod, prime_block);
+    } else {
+      k_ntt_half<true><<<unsigned(planes * 2), th, smem, stream>>>(data, d, prime_base, prime_mod, prime_block);
+      k_ntt_cross<true><<<cross, 256, 0, stream>>>(data, planes, d, prime_base, prime_mod, prime_block);
+    }
+    return cudaGetLastError();
+  }
+  if (threads == 0) threads = ntt_default_threads(n);
+  if (radix_log <= 3)
+    k_ntt8<<<unsigned(planes), threads, smem, stream>>>(data, d, prime_base, prime_mod, prime_block, inverse, radix_log);
+  else
+    k_ntt<<<unsigned(planes), threads, smem, stream>>>(data, d, prime_base, prime_mod, prime_block, inverse, radix_log);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, u64* data, long long planes, int prime_base, int prime_mod,
                        int prime_block, int inverse) {
-  if (planes <= 0) return cudaSuccess;
-  const int threads = ntt_default_threads(r->plan.n);
-  // the shared-memory size is within the attribute set at ring creation
-  k_ntt8<<<unsigned(planes), threads, ntt_smem(r), ln.stream>>>(data, d, prime_base, prime_mod, prime_block, inverse, 3);
-  return cudaGetLastError();
+  return ntt_planes(r->plan.n, ln.stream, d, data, planes, prime_base, prime_mod, prime_block, inverse);
 }
 
 // Compose ops then key-switch ops (one launch each).
@@ -489,10 +519,40 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
       // accumulators in tensor memory, two CTAs per SM (shared-memory size
       // within the attribute set at ring creation)
       k_keyswitch_tm<3><<<grid, 512, smem, ln.stream>>>(d_sops, d);
-    } else {
+    } else if (P.n <= kMaxPlaneN) {
       BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32, 512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                "smem");
       k_keyswitch<32, 512, 4><<<grid, 512, smem, ln.stream>>>(d_sops, d);
+    } else {
+      // N = 32768: no plane fits one CTA, so the switch runs unfused over
+      // the lane's scratch (digit planes, NTTs, products, inverse NTTs,
+      // epilogue), a bounded number of ops at a time
+      const size_t n = P.n, L = r->residue ? P.residue_count : r->switch_prime_count, D = P.digits;
+      const size_t per_op = (L * D + 2 * L) * n * sizeof(u64);
+      const size_t fit = std::max<size_t>(1, (size_t(768) << 20) / per_op);
+      const size_t chunk = std::min({sops.size(), fit, size_t(65535) / (L * D)});
+      const size_t need = chunk * per_op;
+      if (ln.ks_scratch_bytes < need) {
+        if (ln.ks_scratch) {
+          BFV_CUDA(cudaStreamSynchronize(ln.stream), "scratch drain");
+          BFV_CUDA(cudaFree(ln.ks_scratch), "scratch free");
+          ln.ks_scratch = nullptr;
+          ln.ks_scratch_bytes = 0;
+        }
+        BFV_CUDA(cudaMalloc(&ln.ks_scratch, need), "key-switch scratch");
+        ln.ks_scratch_bytes = need;
+      }
+      const unsigned bx = blocks_for((long long)n, 256);
+      for (size_t c0 = 0; c0 < sops.size(); c0 += chunk) {
+        const size_t cnt = std::min(chunk, sops.size() - c0);
+        u64* digits = ln.ks_scratch;
+        u64* acc = ln.ks_scratch + cnt * L * D * n;
+        k_ks_digits<<<dim3(bx, unsigned(cnt * L * D)), 256, 0, ln.stream>>>(d_sops + c0, int(L), digits, d);
+        BFV_CUDA(ntt_planes(n, ln.stream, d, digits, (long long)(cnt * L * D), 0, int(L), int(D), 0), "digit ntt");
+        k_ks_mac<<<dim3(bx, unsigned(cnt * 2 * L)), 256, 0, ln.stream>>>(d_sops + c0, int(L), digits, acc, d);
+        BFV_CUDA(ntt_planes(n, ln.stream, d, acc, (long long)(cnt * 2 * L), 0, int(L), 1, 1), "switch intt");
+        k_ks_finish<<<dim3(bx, unsigned(cnt * 2 * L)), 256, 0, ln.stream>>>(d_sops + c0, int(L), acc, d);
+      }
     }
     BFV_CUDA(cudaGetLastError(), "keyswitch launch");
   }
@@ -963,7 +1023,7 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   try {
     const H::Big q = H::from_hex(q_hex);
     r->plan = H::build_ring(size_t(n), q, unsigned(digit_bits), residue != 0);
-    if (r->plan.n > 16384) throw std::invalid_argument("the B200 evaluator supports N <= 16384");
+
     if (r->plan.primes.size() > size_t(kMaxPrimes)) throw std::invalid_argument("too many auxiliary primes");
     if (!residue) {
       const H::Big qm1 = H::sub(q, H::Big(1));
@@ -1083,6 +1143,12 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_keyswitch_tm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(plane_smem_words(8192) * sizeof(u64)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ntt_half<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(plane_smem_words(16384) * sizeof(u64)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ntt_half<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(plane_smem_words(16384) * sizeof(u64)));
 
   if (e != cudaSuccess) {
     delete r;
@@ -1109,13 +1175,9 @@ int cuhe_bfv_ntt(cuhe_bfv_ring* r, uint64_t* planes_dev, uint64_t planes, int pr
   DeviceGuard guard(r->device);
   RingDev* d = nullptr;
   if (int rc = device_ring(r, 0, &d)) return rc;
-  if (radix_log <= 3)
-    k_ntt8<<<unsigned(planes), threads, ntt_smem(r), static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<u64*>(planes_dev), d, 0, primes, 1, inverse ? 1 : 0, radix_log);
-  else
-    k_ntt<<<unsigned(planes), threads, ntt_smem(r), static_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<u64*>(planes_dev), d, 0, primes, 1, inverse ? 1 : 0, radix_log);
-  BFV_CUDA(cudaGetLastError(), "ntt launch");
+  BFV_CUDA(ntt_planes(P.n, static_cast<cudaStream_t>(stream), d, reinterpret_cast<u64*>(planes_dev), (long long)planes,
+                      0, primes, 1, inverse ? 1 : 0, threads, radix_log),
+           "ntt launch");
   return CUHE_OK;
 }
 
@@ -2106,8 +2168,7 @@ int cuhe_bfv_batch_encode(cuhe_bfv_ring* r, uint64_t t, const uint32_t* slots, u
     k_scatter_slots<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_slots, pr.d_perm, (long long)cc,
                                                                                  int(n), uint32_t(t), m, d_status);
     BFV_CUDA(cudaGetLastError(), "scatter");
-    k_ntt8<<<unsigned(cc), ntt_default_threads(n), ntt_smem(r), ln.stream>>>(m, pr.d, 0, 1, 1, 1, 3);
-    BFV_CUDA(cudaGetLastError(), "batch encode");
+    BFV_CUDA(ntt_planes(n, ln.stream, pr.d, m, (long long)cc, 0, 1, 1, 1), "batch encode");
     int status = 0;
     BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
     BFV_CUDA(cudaMemcpyAsync(out + c0 * n, m, cc * n * 8, cudaMemcpyDeviceToHost, ln.stream), "download");
@@ -2182,8 +2243,7 @@ int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint
     k_scatter_slots<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_slots, pr.d_perm, (long long)cc,
                                                                                  int(n), uint32_t(t), m, d_status);
     BFV_CUDA(cudaGetLastError(), "scatter");
-    k_ntt8<<<unsigned(cc), ntt_default_threads(n), ntt_smem(r), ln.stream>>>(m, pr.d, 0, 1, 1, 1, 3);
-    BFV_CUDA(cudaGetLastError(), "batch encode");
+    BFV_CUDA(ntt_planes(n, ln.stream, pr.d, m, (long long)cc, 0, 1, 1, 1), "batch encode");
     // (b, a) * u + (e0 + delta m, e1)
     k_small_residues<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_u, (long long)cc, int(L), u_ntt, d);
     BFV_CUDA(cudaGetLastError(), "u residues");

@@ -123,7 +123,9 @@ int cuhe_bfv_last_profile(const cuhe_bfv_server* server, double* ms, int capacit
  * threads: CTA size (0: N/8, at most 1024; radix 16 has a smaller,
  * register-bound limit that a larger request exceeds with an error);
  * radix_log: register pass width, 1..4 stages (0: 3).  These two are the
- * knobs of the autotuner.  The transform the reference runs per prime
+ * knobs of the autotuner (at N = 32768 they are checked but the fixed split
+ * transform runs: the two halves of a plane in shared memory, the stage that
+ * pairs them on global memory).  The transform the reference runs per prime
  * (rns_ntt.h:178-255), batched. */
 int cuhe_bfv_ntt(cuhe_bfv_ring* ring, uint64_t* planes, uint64_t count, int primes, int inverse, int threads,
                  int radix_log, void* stream);
