@@ -74,7 +74,8 @@ def _ring_pair(n, q_bits, gadget, t=None):
 
 
 @pytest.mark.parametrize("n,q_bits,gadget", [(16, 60, 4), (16, 180, 30), (64, 480, 127), (1024, 180, 30),
-                                             (8192, 180, 30), (64, 120, 61), (32, 180, 1)])
+                                             (8192, 180, 30), (64, 120, 61), (32, 180, 1), (8, 120, 30),
+                                             (16384, 180, 30)])
 def test_primitives_match_reference_checker(n, q_bits, gadget):
     ref, m, q, rring, ring = _ring_pair(n, q_bits, gadget)
     assert m.ring_info(ring)["primes"] == ref.ring_info(rring)["primes"]

@@ -79,6 +79,8 @@ NATIVE_RINGS = [
     (16, ob.coefficient_modulus(300), 30),
     (16, ob.coefficient_modulus(480), 127),
     (32, (1 << 512) - 1, 61),
+    (8, ob.coefficient_modulus(100), 15),
+    (16384, ob.coefficient_modulus(180), 30),
 ]
 
 
