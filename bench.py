@@ -385,7 +385,8 @@ def run_gpu(args) -> dict | None:
     if not args.no_client and world == 1:
         result["client"] = run_client()
     if not args.no_textbook and world == 1:
-        result["textbook"] = [run_textbook(512), run_textbook(1024)]
+        result["textbook"] = [run_textbook(512), run_textbook(1024),
+                              run_textbook(2048, count=1024, plain_sample=8, cpu_sample=4)]
     if not args.no_mixed and world == 1:
         result["mixed"] = run_mixed()
     if not args.no_serving and world == 1:
@@ -750,8 +751,8 @@ def run_reference(args) -> dict | None:
 
 def run_textbook(key_len: int, count: int = 4096, plain_sample: int = 32, cpu_sample: int = 8) -> dict:
     """Plain Paillier at one key_len: keys from seed 0 (the reference's
-    key_gen with seeded primes), 4096 plaintexts uniform in [0, 2^32)
-    (seed 1), r uniform in Z_n* (seed 2); encrypt all, add 2048 pairs,
+    key_gen with seeded primes), `count` plaintexts uniform in [0, 2^32)
+    (seed 1), r uniform in Z_n* (seed 2); encrypt all, add count/2 pairs,
     decrypt all (c^phi, by CRT).  Batched = one launch per batch; plain = one
     launch per ciphertext (timed on a sample, host-synchronised); the CPU
     baseline (textbook_cpu_baseline) timed on a few operations beside it."""
@@ -1268,7 +1269,8 @@ def main() -> None:
                                                 native=True)}))
         return
     if args.textbook_only:
-        print(json.dumps({"textbook": [run_textbook(512), run_textbook(1024)]}))
+        print(json.dumps({"textbook": [run_textbook(512), run_textbook(1024),
+                                         run_textbook(2048, count=1024, plain_sample=8, cpu_sample=4)]}))
         return
     if args.mixed_only:
         print(json.dumps(run_mixed()))

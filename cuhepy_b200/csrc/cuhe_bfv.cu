@@ -121,10 +121,11 @@ struct PolySource {
 // host-to-device copy to d_dst on the lane's stream.  The caller
 // synchronises the stream before the lane stages again.
 // Copy polys [first, first + count) of src to dst, with up to max_workers
-// host threads (one per 16 MiB).
-void copy_polys(const PolySource& src, size_t first, size_t count, uint8_t* dst, size_t max_workers) {
+// host threads (one per 2^shift bytes).
+void copy_polys(const PolySource& src, size_t first, size_t count, uint8_t* dst, size_t max_workers,
+                unsigned shift = 24) {
   const size_t bytes = count * src.poly_bytes;
-  const size_t workers = std::min<size_t>(std::max<size_t>(1, bytes >> 24), max_workers);
+  const size_t workers = std::min<size_t>(std::max<size_t>(1, bytes >> shift), max_workers);
   auto copy = [&](size_t lo, size_t hi) {
     for (size_t k = lo; k < hi; ++k) std::memcpy(dst + k * src.poly_bytes, src.poly(first + k), src.poly_bytes);
   };
@@ -1823,7 +1824,8 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
           uint8_t* pin = ln.pin[k % 2];
           cudaError_t e = k >= 2 ? cudaEventSynchronize(up[k - 2]) : cudaSuccess;  // its half is free again
           if (e == cudaSuccess) {
-            copy_polys(*index, (first + t0) * 2, tc * 2, pin, 4);
+            // the first piece is on the critical path: more threads for it
+            copy_polys(*index, (first + t0) * 2, tc * 2, pin, k == 0 ? 8 : 4, k == 0 ? 21 : 22);
             e = cudaMemcpyAsync(d_ib + t0 * 2 * in_bytes, pin, tc * 2 * in_bytes, cudaMemcpyHostToDevice, ln.copy);
           }
           if (e == cudaSuccess) e = cudaEventRecord(up[k], ln.copy);
