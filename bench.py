@@ -377,11 +377,12 @@ def run_gpu(args) -> dict | None:
                 "path": "C ABI with pinned host buffers, every stage staged over PCIe"},
         "gpu_launches": 6 * args.steps,
     }
+    # the CPU baselines are taken on rank 0 of a one-GPU run only
+    cpu = not args.no_cpu_baseline and world == 1
     if not args.no_bfv:
-        result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)
+        result["bfv"] = run_bfv(max(3, args.steps), args.warmup, cpu=cpu)
         if world == 1:
-            result["bfv_native"] = run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline,
-                                           native=True)
+            result["bfv_native"] = run_bfv(max(3, args.steps), args.warmup, cpu=cpu, native=True)
     if not args.no_client and world == 1:
         result["client"] = run_client()
     if not args.no_textbook and world == 1:
@@ -393,7 +394,7 @@ def run_gpu(args) -> dict | None:
         del prod, dist_out, index_ct, flush  # the serving section needs the HBM
         torch.cuda.empty_cache()
         result["serving"] = run_serving()
-    if not args.no_cpu_baseline:
+    if cpu:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
     if dist:
         dist.destroy_process_group()
