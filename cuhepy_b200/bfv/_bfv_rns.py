@@ -449,11 +449,12 @@ def encrypt_packed(ring: Ring, public_key: Any, t: int, slots, u, e) -> list[tup
     if slots.shape != (count, ring.n) or u.shape != (count, ring.n) or e.shape != (count, 2, ring.n):
         raise ValueError("slots, u and e must be [count, N], [count, N] and [count, 2, N]")
     size = (ring.n * ring.q_bits + 7) // 8
-    out = ctypes.create_string_buffer(max(1, count * 2 * size))
+    out = np.empty(max(1, count * 2 * size), dtype=np.uint8)  # filled by the call: no zeroing
     _check(lib().cuhe_bfv_encrypt(ring.ptr, pk, int(t), slots.ctypes.data, u.ctypes.data, e.ctypes.data, count,
-                                  out))
-    raw = out.raw
-    return [(raw[2 * i * size:(2 * i + 1) * size], raw[(2 * i + 1) * size:(2 * i + 2) * size]) for i in range(count)]
+                                  out.ctypes.data))
+    view = memoryview(out)
+    return [(bytes(view[2 * i * size:(2 * i + 1) * size]), bytes(view[(2 * i + 1) * size:(2 * i + 2) * size]))
+            for i in range(count)]
 
 
 def set_lanes(ring: Ring, lanes: int) -> None:

@@ -19,6 +19,18 @@ import numpy as np
 from cuhepy_b200.bfv import _bfv_rns
 
 
+def _keystream(nbytes: int) -> bytes:
+    """`nbytes` of ChaCha20 keystream under a fresh key and nonce from the
+    operating system's CSPRNG (os.urandom itself when the `cryptography`
+    package is absent)."""
+    try:
+        from cryptography.hazmat.primitives.ciphers import Cipher, algorithms
+    except ImportError:  # pragma: no cover - the image ships cryptography
+        return secrets.token_bytes(nbytes)
+    enc = Cipher(algorithms.ChaCha20(secrets.token_bytes(32), secrets.token_bytes(16)), mode=None).encryptor()
+    return enc.update(bytes(nbytes))
+
+
 def draw_noise(count: int, n: int, eta: int = 21, rng: Any = None) -> tuple[np.ndarray, np.ndarray]:
     """(u [count, n] ternary, e [count, 2, n]) as int8.
 
@@ -26,8 +38,10 @@ def draw_noise(count: int, n: int, eta: int = 21, rng: Any = None) -> tuple[np.n
     ``secrets``) the draws are made one value at a time in the reference's
     order per ciphertext (u, then e0, then e1; scheme.py:236-246, 438-439),
     so a seeded ``rng`` reproduces the reference's ciphertexts.  Without it,
-    the same distributions are drawn in bulk from the operating system's
-    CSPRNG."""
+    the same distributions are drawn in bulk from a cryptographic keystream
+    (ChaCha20 keyed from the operating system's CSPRNG): u uniform on
+    {-1, 0, 1} by rejection on bytes (0..254 are uniform mod 3), each e the
+    difference of the popcounts of two independent eta-bit words."""
     if not 1 <= eta <= 63:
         raise ValueError("eta must be 1..63")
     if rng is not None:
@@ -38,20 +52,20 @@ def draw_noise(count: int, n: int, eta: int = 21, rng: Any = None) -> tuple[np.n
             for k in range(2):
                 e[c, k] = [rng.randbits(eta).bit_count() - rng.randbits(eta).bit_count() for _ in range(n)]
         return u, e
-    gen = np.random.Generator(np.random.PCG64DXSM(secrets.randbits(128)))
-    # ternary by rejection on bytes (0..254 are uniform mod 3)
+    halves = count * 2 * n * 2
+    wide = np.uint64 if eta > 31 else np.uint32
+    size = np.dtype(wide).itemsize
+    words = np.frombuffer(_keystream(size * halves), dtype=wide) & wide((1 << eta) - 1)
+    pops = np.bitwise_count(words).astype(np.int8).reshape(count, 2, n, 2)
+    e = pops[..., 0] - pops[..., 1]
     u = np.empty(count * n, dtype=np.int8)
     filled = 0
     while filled < u.size:
-        raw = np.frombuffer(secrets.token_bytes(2 * (u.size - filled) + 64), dtype=np.uint8)
-        raw = raw[raw < 255][: u.size - filled]
+        want = u.size - filled
+        raw = np.frombuffer(_keystream(want + want // 64 + 64), dtype=np.uint8)
+        raw = raw[raw < 255][:want]
         u[filled:filled + raw.size] = (raw % 3).astype(np.int8) - 1
         filled += raw.size
-    mask = (1 << eta) - 1
-    pos = gen.integers(0, 1 << 63, size=(count, 2, n), dtype=np.int64) & mask
-    neg = gen.integers(0, 1 << 63, size=(count, 2, n), dtype=np.int64) & mask
-    popcount = np.vectorize(int.bit_count, otypes=[np.int64]) if not hasattr(np, "bitwise_count") else np.bitwise_count
-    e = (popcount(pos).astype(np.int16) - popcount(neg).astype(np.int16)).astype(np.int8)
     return u.reshape(count, n), e
 
 

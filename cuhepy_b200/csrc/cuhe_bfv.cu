@@ -2235,7 +2235,7 @@ int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint
   k_words_to_residues<<<blocks_for((long long)(2 * n), 256), 256, 0, ln.stream>>>(pk_w, 2, int(L), pk_ntt, d);
   BFV_CUDA(cudaGetLastError(), "pk residues");
   BFV_CUDA(launch_ntt(r, ln, d, pk_ntt, (long long)(2 * L), 0, int(L), 1, 0), "pk ntt");
-  std::vector<u64> host(chunk * 2 * out_words);
+  std::unique_ptr<u64[]> host(out_words * 8 == in_bytes ? nullptr : new u64[chunk * 2 * out_words]);
   for (size_t c0 = 0; c0 < size_t(count); c0 += chunk) {
     const size_t cc = std::min(chunk, size_t(count) - c0);
     BFV_CUDA(cudaMemcpyAsync(d_slots, slots + c0 * n, cc * n * 4, cudaMemcpyHostToDevice, ln.stream), "slots");
@@ -2265,13 +2265,17 @@ int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint
     BFV_CUDA(cudaGetLastError(), "pack");
     int status = 0;
     BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
-    BFV_CUDA(cudaMemcpyAsync(host.data(), packed, cc * 2 * out_words * 8, cudaMemcpyDeviceToHost, ln.stream),
+    // packed polys that fill whole words go straight to the caller's buffer
+    const bool direct = out_words * 8 == in_bytes;
+    BFV_CUDA(cudaMemcpyAsync(direct ? static_cast<void*>(out + c0 * 2 * in_bytes) : static_cast<void*>(host.get()),
+                             packed, cc * 2 * out_words * 8, cudaMemcpyDeviceToHost, ln.stream),
              "download");
     BFV_CUDA(cudaStreamSynchronize(ln.stream), "encrypt");
     if (status) return fail(CUHE_INVALID_ARGUMENT, "slot value not below the plaintext modulus");
-    for (size_t k = 0; k < cc * 2; ++k)
-      std::memcpy(out + (c0 * 2 + k) * in_bytes, reinterpret_cast<const uint8_t*>(host.data() + k * out_words),
-                  in_bytes);
+    if (!direct)
+      for (size_t k = 0; k < cc * 2; ++k)
+        std::memcpy(out + (c0 * 2 + k) * in_bytes, reinterpret_cast<const uint8_t*>(host.get() + k * out_words),
+                    in_bytes);
   }
   return CUHE_OK;
 }
