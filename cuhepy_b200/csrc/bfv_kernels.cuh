@@ -615,51 +615,70 @@ struct ComposeOp {
 };
 
 // Garner: canonical integer in [0, Q) of each coefficient, written to the
-// position of X^g (negated when the exponent wraps past N).
+// position of X^g (negated when the exponent wraps past N).  kL: the ring's
+// residue count as a compile-time constant (its words then equal kL: 60-bit
+// primes), which keeps the digits and words in registers; 0 = any.
+template <int kL>
 __global__ void k_compose(const ComposeOp* __restrict__ ops, const RingDev* __restrict__ ring) {
+  constexpr int kD = kL ? kL : kMaxResidue, kWw = kL ? kL : kMaxWords;
   const RingDev& R = *ring;
   const ComposeOp op = ops[blockIdx.y];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= R.n) return;
-  const int L = R.residue, W = R.words;
-  u64 digit[kMaxResidue];
-  for (int j = 0; j < L; ++j) {
+  const int L = kL ? kL : R.residue, W = kL ? kL : R.words;
+  u64 digit[kD];
+#pragma unroll
+  for (int j = 0; j < kD; ++j) {
+    if (j >= L) break;
     const u64 p = R.prime[j].p;
     u64 value = op.x1[(long long)j * R.n + i];
-    for (int k = 0; k < j; ++k) {
+#pragma unroll
+    for (int k = 0; k < kD; ++k) {
+      if (k >= j) break;
       const u64 d = digit[k] >= p ? digit[k] - p : digit[k];
       value = shoup(value + p - d, R.garner[j][k], R.garner_q[j][k], p);
     }
     digit[j] = value;
   }
-  u64 w[kMaxWords];
-  for (int k = 0; k < kMaxWords; ++k) w[k] = 0;
+  // Horner over the mixed radix; every partial value is below the product
+  // of the primes used so far, so W words always hold it
+  u64 w[kWw];
+#pragma unroll
+  for (int k = 0; k < kWw; ++k) w[k] = 0;
   w[0] = digit[L - 1];
-  int used = 1;
-  for (int j = L - 1; j > 0; --j) {
-    u64 carry = digit[j - 1];
-    const u64 p = R.prime[j - 1].p;
-    for (int k = 0; k < used; ++k) {
+#pragma unroll
+  for (int jj = kD - 1; jj > 0; --jj) {
+    if (jj > L - 1) continue;
+    u64 carry = digit[jj - 1];
+    const u64 p = R.prime[jj - 1].p;
+#pragma unroll
+    for (int k = 0; k < kWw; ++k) {
+      if (k >= W) break;
       const u128 prod = u128(w[k]) * p + carry;
       w[k] = u64(prod);
       carry = u64(prod >> 64);
     }
-    if (carry) w[used++] = carry;
   }
   const unsigned at = unsigned((unsigned long long)i * op.g % (2u * unsigned(R.n)));
   const int dst = int(at % unsigned(R.n));
   bool nonzero = false;
-  for (int k = 0; k < W; ++k) nonzero |= w[k] != 0;
+#pragma unroll
+  for (int k = 0; k < kWw; ++k)
+    if (k < W) nonzero |= w[k] != 0;
   if (at >= unsigned(R.n) && nonzero) {
     u64 borrow = 0;
-    for (int k = 0; k < W; ++k) {
+#pragma unroll
+    for (int k = 0; k < kWw; ++k) {
+      if (k >= W) break;
       const u128 x = u128(R.q_words[k]) - w[k] - borrow;
       w[k] = u64(x);
       borrow = u64(x >> 64) ? 1 : 0;
     }
   }
   u64* o = op.words + (long long)dst * W;
-  for (int k = 0; k < W; ++k) o[k] = w[k];
+#pragma unroll
+  for (int k = 0; k < kWw; ++k)
+    if (k < W) o[k] = w[k];
 }
 
 // digit d of a composed integer, reduced mod p_j

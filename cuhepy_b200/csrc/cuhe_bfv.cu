@@ -508,7 +508,21 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
     BFV_CUDA(cudaMemcpyAsync(d_cops, cops.data(), cops.size() * sizeof(ComposeOp), cudaMemcpyHostToDevice, ln.stream),
              "compose ops");
     dim3 grid(blocks_for((long long)(P.n), 256), unsigned(cops.size()));
-    k_compose<<<grid, 256, 0, ln.stream>>>(d_cops, d);
+    const int L = int(P.residue_count);
+    if (r->residue && r->host_dev.words == L) {
+      switch (L) {
+        case 1: k_compose<1><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        case 2: k_compose<2><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        case 3: k_compose<3><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        case 4: k_compose<4><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        case 5: k_compose<5><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        case 6: k_compose<6><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        case 7: k_compose<7><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+        default: k_compose<8><<<grid, 256, 0, ln.stream>>>(d_cops, d); break;
+      }
+    } else {
+      k_compose<0><<<grid, 256, 0, ln.stream>>>(d_cops, d);
+    }
     BFV_CUDA(cudaGetLastError(), "compose launch");
   }
   if (!sops.empty()) {
