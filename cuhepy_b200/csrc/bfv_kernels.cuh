@@ -711,96 +711,6 @@ __device__ __forceinline__ u64 gadget_digit(const u64* w, int W, int d, const Ri
   return r;
 }
 
-// CTA per (op, prime j < L): D forward NTTs of the digits, multiply-accumulate
-// with the key in the NTT domain, two inverse NTTs, epilogue additions.
-// kSwitchThreads threads per CTA; MAXP stages per register pass (radix
-// 2^MAXP): 1024 threads with radix-8 passes keeps a thread within 64
-// registers, so a whole CTA of 32 warps is resident beside the accumulators.
-template <int kSwitchPer, int kSwitchThreads, int MAXP>  // kSwitchPer: coefficients per thread, 0 = shared accumulators
-__global__ void __launch_bounds__(kSwitchThreads, 1)
-k_keyswitch(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) {
-  extern __shared__ __align__(16) u64 s_plane[];
-  const RingDev& R = *ring;
-  const SwitchOp op = ops[blockIdx.x];
-  const int j = blockIdx.y;
-  const int n = R.n, L = R.residue, W = R.words;
-  const Prime& m = R.prime[j];
-  // Accumulators: kSwitchPer == 0 keeps them in shared memory after the
-  // padded plane (N <= 8192); otherwise in registers, kSwitchPer per thread.
-  constexpr bool kSmemAcc = kSwitchPer == 0;
-  constexpr int kRegs = kSmemAcc ? 1 : kSwitchPer;
-  u64* s_acc = s_plane + plane_smem_words(n);
-  const int per = (n - int(threadIdx.x) + kSwitchThreads - 1) / kSwitchThreads;
-  u64 acc0[kRegs], acc1[kRegs];
-#pragma unroll
-  for (int k = 0; k < kRegs; ++k) { acc0[k] = 0; acc1[k] = 0; }
-  if (kSmemAcc)
-    for (int i = threadIdx.x; i < 2 * n; i += kSwitchThreads) s_acc[i] = 0;
-  for (int d = 0; d < R.digits; ++d) {
-    for (int i = threadIdx.x; i < n; i += kSwitchThreads)
-      s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
-    __syncthreads();
-    ntt_forward_fast(s_plane, R, j, MAXP);
-    // key products by Shoup with the precomputed quotients; accumulators
-    // stay in [0, 2p) and are made canonical before the inverse transforms
-    const long long k0o = ((long long)(d * 2 + 0) * L + j) * n, k1o = ((long long)(d * 2 + 1) * L + j) * n;
-    const u64 two_p = 2 * m.p;
-    if (kSmemAcc) {
-      for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
-        const u64 v = s_plane[sp(i)];
-        u64 a0 = s_acc[i] + shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), m.p);
-        u64 a1 = s_acc[n + i] + shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), m.p);
-        s_acc[i] = a0 >= two_p ? a0 - two_p : a0;
-        s_acc[n + i] = a1 >= two_p ? a1 - two_p : a1;
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < kRegs; ++k) {
-        if (k < per) {
-          const int i = threadIdx.x + k * kSwitchThreads;
-          const u64 v = s_plane[sp(i)];
-          const u64 a0 = acc0[k] + shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), m.p);
-          const u64 a1 = acc1[k] + shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), m.p);
-          acc0[k] = a0 >= two_p ? a0 - two_p : a0;
-          acc1[k] = a1 >= two_p ? a1 - two_p : a1;
-        }
-      }
-    }
-    __syncthreads();
-  }
-  for (int comp = 0; comp < 2; ++comp) {
-    if (kSmemAcc) {
-      for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
-        const u64 a = s_acc[comp * n + i];
-        s_plane[sp(i)] = a >= m.p ? a - m.p : a;
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < kRegs; ++k)
-        if (k < per) {
-          const u64 a = comp ? acc1[k] : acc0[k];
-          s_plane[sp(threadIdx.x + k * kSwitchThreads)] = a >= m.p ? a - m.p : a;
-        }
-    }
-    __syncthreads();
-    ntt_inverse_fast(s_plane, R, j, MAXP);
-    u64* out = op.out + ((long long)comp * L + j) * n;
-    const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
-    for (int i = threadIdx.x; i < n; i += kSwitchThreads) {
-      u64 v = s_plane[sp(i)];
-      if (base) v = addmod(v, base[i], m.p);
-      if (comp == 0 && op.x0) {
-        const unsigned s = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));
-        u64 x = s < unsigned(n) ? op.x0[(long long)j * n + s] : op.x0[(long long)j * n + (s - n)];
-        if (s >= unsigned(n) && x) x = m.p - x;
-        v = addmod(v, x, m.p);
-      }
-      out[i] = v;
-    }
-    __syncthreads();
-  }
-}
-
 // ---- tensor memory (TMEM) as accumulator storage ------------------------------
 // Each SM has 512 TMEM columns x 128 lanes of 32 bits.  A CTA allocates
 // columns with tcgen05.alloc (one warp; the address lands in shared memory),
@@ -838,21 +748,27 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
-// The key switch of k_keyswitch with its accumulators in TMEM instead of
-// shared memory: shared memory holds only the plane (70 KB at N = 8192), so
-// two 512-thread CTAs (64 registers each) are resident per SM and one CTA's
-// global loads and barriers overlap the other's butterflies.  Thread t owns
-// coefficients i = t + 512 k (k < 16) and keeps (acc0, acc1) of each as four
-// 32-bit columns: 64 columns per thread, lanes by warp quarter, 4 warps per
-// quarter -> 256 columns per CTA, 512 for the two CTAs of an SM (the whole
-// TMEM; a third co-resident CTA would wait in tcgen05.alloc until one of
-// them deallocates).  Every tcgen05 instruction is executed by whole warps
-// (the coefficient guard i < n covers only the arithmetic), and no thread
-// leaves before the final dealloc.
-template <int MAXP>
-__global__ void __launch_bounds__(512, 2)
+// The fused key switch.  CTA per (op, prime j < L): the D forward NTTs of
+// the op's gadget digits mod p_j, their products with the key in the NTT
+// domain (Shoup, precomputed quotients) accumulated over the digits, two
+// inverse NTTs, and the epilogue additions (base, the permuted x0).  The
+// accumulators live in TMEM: shared memory holds only the plane (70 KB at
+// N = 8192), so two 512-thread CTAs (64 registers each) are resident per SM
+// and one CTA's global loads and barriers overlap the other's butterflies.  Thread t owns
+// coefficients i = t + 512 k (k < kCoef) and keeps (acc0, acc1) of each as
+// four 32-bit columns: 4 kCoef columns per thread, lanes by warp quarter, 4
+// warps per quarter -> 16 kCoef columns per CTA.  N <= 8192 (kCoef = 16):
+// 256 columns, 512 for the two CTAs of an SM (the whole TMEM); N = 16384
+// (kCoef = 32, a 139 KB plane, one CTA per SM): 512 columns.  A further
+// co-resident CTA would wait in tcgen05.alloc until another deallocates.
+// Every tcgen05 instruction is executed by whole warps (the coefficient
+// guard i < n covers only the arithmetic), and no thread leaves before the
+// final dealloc.
+template <int MAXP, int kCoef = 16>
+__global__ void __launch_bounds__(512, kCoef == 16 ? 2 : 1)
 k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ ring) {
-  constexpr int kThreads = 512, kChunks = 4, kCols = 256;  // 16 coefficients per thread, 4 per chunk
+  static_assert(kCoef == 16 || kCoef == 32, "16 or 32 coefficients per thread");
+  constexpr int kThreads = 512, kChunks = kCoef / 4, kCols = 16 * kCoef;  // 4 coefficients per chunk
   extern __shared__ __align__(16) u64 s_plane[];
   __shared__ uint32_t s_tmem;
   const RingDev& R = *ring;
@@ -868,7 +784,7 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
   tmem_fence_before_sync();
   __syncthreads();
   tmem_fence_after_sync();
-  const uint32_t tbase = s_tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t((warp >> 2) * 64);
+  const uint32_t tbase = s_tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t((warp >> 2) * 4 * kCoef);
   for (int d = 0; d < R.digits; ++d) {
     for (int i = threadIdx.x; i < n; i += kThreads)
       s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);

@@ -535,9 +535,8 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
       // within the attribute set at ring creation)
       k_keyswitch_tm<3><<<grid, 512, smem, ln.stream>>>(d_sops, d);
     } else if (P.n <= kMaxPlaneN) {
-      BFV_CUDA(cudaFuncSetAttribute(k_keyswitch<32, 512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-               "smem");
-      k_keyswitch<32, 512, 4><<<grid, 512, smem, ln.stream>>>(d_sops, d);
+      // N = 16384: 32 coefficients per thread, the whole TMEM, one CTA per SM
+      k_keyswitch_tm<3, 32><<<grid, 512, smem, ln.stream>>>(d_sops, d);
     } else {
       // N = 32768: no plane fits one CTA, so the switch runs unfused over
       // the lane's scratch (digit planes, NTTs, products, inverse NTTs,
@@ -1158,6 +1157,9 @@ int cuhe_bfv_create_ring(uint64_t n, const char* q_hex, uint64_t digit_bits, int
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_keyswitch_tm<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(plane_smem_words(8192) * sizeof(u64)));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_keyswitch_tm<3, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(plane_smem_words(16384) * sizeof(u64)));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_ntt_half<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(plane_smem_words(16384) * sizeof(u64)));
