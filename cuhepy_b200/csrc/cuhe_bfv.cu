@@ -56,7 +56,8 @@ struct DeviceGuard {
 struct Arena {
   char* base = nullptr;
   size_t cap = 0, used = 0;
-  ~Arena() { if (base) cudaFree(base); }
+  bool owned = true;  // false: a view of another arena's slice
+  ~Arena() { if (base && owned) cudaFree(base); }
   cudaError_t reserve(size_t bytes) {
     if (bytes <= cap) return cudaSuccess;
     if (base) cudaFree(base);
@@ -97,8 +98,13 @@ struct Lane {
   size_t pin_cap[2] = {0, 0};
   u64* ks_scratch = nullptr;  // N = 32768 key switches: digit and accumulator planes (grow-only)
   size_t ks_scratch_bytes = 0;
+  cudaStream_t side = nullptr;  // second compute stream of split tile batches
   ~Lane() {
     if (copy) cudaStreamSynchronize(copy);
+    if (side) {
+      cudaStreamSynchronize(side);
+      cudaStreamDestroy(side);
+    }
     if (ks_scratch) cudaFree(ks_scratch);
     if (host_stage) cudaFreeHost(host_stage);
     for (uint8_t* p : pin)
@@ -159,6 +165,8 @@ cudaError_t stage_polys(Lane& ln, const PolySource& src, size_t first, size_t co
 
 // Index tiles per upload sub-batch of a search over a host-memory index.
 constexpr size_t kPipeTiles = 256;
+// Tile batches of at least this many tiles run as two halves on two streams.
+constexpr size_t kSplitTiles = 128;
 
 constexpr int kMaxLanes = 8;
 
@@ -1782,10 +1790,116 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     NativeScratch sc{};
     if (!r->residue)
       if (int rc = native_scratch(ln.arena, r, ct, s->mask_primes, &sc)) return rc;
-    // tile circuits of chunk tiles [t0, t0 + tc) into their dist slots
-    auto run_tiles = [&](size_t t0, size_t tc) -> int {
-      const size_t mark = ln.arena.used;  // the circuit's workspace is free again when it returns
-      int rc;
+    // Merge trees (bfv_server.h:15-45) of the chunk's response groups
+    // [g_lo, g_hi), executed in waves of independent merges on `lane`;
+    // native rings use `nsc` (scratch for the groups' tiles), residue rings
+    // the lane's arena.  Writes each group's result slot.
+    std::vector<size_t> result_slot(gc, 0);
+    std::vector<char> merged(gc, 0);
+    auto merge_groups = [&](Lane& lane, size_t g_lo, size_t g_hi, const NativeScratch& nsc, double* pr) -> int {
+      if (g_lo >= g_hi) return CUHE_OK;
+      cudaEvent_t m0, m1;
+      cudaEventCreate(&m0);
+      cudaEventCreate(&m1);
+      cudaEventRecord(m0, lane.stream);
+      struct Merge { size_t left, right; size_t level; size_t wave; };
+      std::vector<Merge> merges;
+      for (size_t gi = g_lo; gi < g_hi; ++gi) {
+        struct Node { size_t slot, ready; };
+        std::vector<std::pair<Node, size_t>> stack;
+        const size_t gs = gi * s->padded, ge = std::min(gs + s->padded, ct);
+        for (size_t at = gs; at < ge; ++at) {
+          Node node{at, 0};
+          size_t size = 1, level = 0;
+          while (!stack.empty() && stack.back().second == size) {
+            const Node left = stack.back().first;
+            stack.pop_back();
+            const size_t wave = std::max(left.ready, node.ready);
+            merges.push_back({left.slot, node.slot, level, wave});
+            node = Node{left.slot, wave + 1};
+            size *= 2;
+            ++level;
+          }
+          stack.emplace_back(node, size);
+        }
+        Node result = stack.back().first;
+        stack.pop_back();
+        while (!stack.empty()) {
+          const size_t size = stack.back().second;
+          size_t level = 0;
+          while ((size_t(1) << level) < size) ++level;
+          const Node left = stack.back().first;
+          stack.pop_back();
+          const size_t wave = std::max(left.ready, result.ready);
+          merges.push_back({left.slot, result.slot, level, wave});
+          result = Node{left.slot, wave + 1};
+        }
+        result_slot[gi] = result.slot;
+      }
+      size_t waves = 0;
+      for (const auto& m : merges) waves = std::max(waves, m.wave + 1);
+      if (!r->residue) {
+        // native: rotate each right operand (grouped by level, one key each),
+        // then add it into its left operand
+        for (size_t w = 0; w < waves; ++w) {
+          std::vector<NativeOp> adds;
+          size_t used = 0;
+          for (size_t level = 0; level < s->right.size(); ++level) {
+            std::vector<NativeOp> rots;
+            for (const auto& m : merges) {
+              if (m.wave != w || m.level != level) continue;
+              const size_t k = used + rots.size();
+              rots.push_back(NativeOp{dist + m.right * 2 * n * W, nsc.perm + k * 2 * n * W, nsc.tmp + k * 2 * n * W,
+                                      nullptr});
+              adds.push_back(NativeOp{dist + m.left * 2 * n * W, nsc.tmp + k * 2 * n * W,
+                                      dist + m.left * 2 * n * W, nullptr});
+            }
+            if (rots.empty()) continue;
+            const u64 g = s->right.at(level);
+            if (int rc = native_rotate(r, lane, d, rots, unsigned(g), s->keys.at(g), nsc.d_nops, nsc.ksres,
+                                       nsc.ksw + used * 2 * n * W, nsc.d_sops))
+              return rc;
+            used += rots.size();
+          }
+          if (int rc = native_add_ops(r, lane, d, adds, nsc.d_nops)) return rc;
+        }
+      } else {
+        const size_t mark = lane.arena.used;
+        const size_t most = merges.size();
+        u64* mwords = lane.arena.take<u64>(std::max<size_t>(1, most) * n * W);
+        ComposeOp* d_cops = lane.arena.take<ComposeOp>(std::max<size_t>(1, most));
+        SwitchOp* d_sops = lane.arena.take<SwitchOp>(std::max<size_t>(1, most));
+        BFV_ARENA(lane.arena);
+        for (size_t w = 0; w < waves; ++w) {
+          std::vector<ComposeOp> cops;
+          std::vector<SwitchOp> sops;
+          for (const auto& m : merges) {
+            if (m.wave != w) continue;
+            const u64 g = s->right.at(m.level);
+            u64* words = mwords + cops.size() * n * W;
+            cops.push_back(ComposeOp{dist + (m.right * 2 + 1) * L * n, words, unsigned(g), 0u});
+            const cuhe_bfv_key* key = s->keys.at(g);
+            sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, key->d_key,
+                                    key->d_key_q, dist + m.left * 2 * L * n, inverse_mod_2n(g, n), 0u});
+          }
+          if (int rc = run_switch(r, lane, d, cops, sops, d_cops, d_sops)) return rc;
+        }
+        lane.arena.used = mark;
+      }
+      cudaEventRecord(m1, lane.stream);
+      BFV_CUDA(cudaEventSynchronize(m1), "merge");
+      float x = 0;
+      cudaEventElapsedTime(&x, m0, m1);
+      pr[4] += x;
+      cudaEventDestroy(m0);
+      cudaEventDestroy(m1);
+      for (size_t gi = g_lo; gi < g_hi; ++gi) merged[gi] = 1;
+      return CUHE_OK;
+    };
+    // tile circuits of chunk tiles [t0, t0 + tc) into their dist slots, on
+    // `lane` (its stream; residue rings take their workspace from its
+    // arena, native rings use `nsc`, scratch for tc tiles)
+    auto circuit = [&](Lane& lane, size_t t0, size_t tc, const NativeScratch& nsc, double* pr) -> int {
       if (r->residue) {
         TileArgs a;
         a.q_words = qw;
@@ -1798,16 +1912,101 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
         }
         a.masks.assign(tc, s->d_full_mask);
         if (partial && first + t0 + tc == size_t(tiles)) a.masks[tc - 1] = partial;
-        rc = tile_circuit(r, ln, d, a, dist + t0 * 2 * L * n, prof);
-      } else {
-        std::vector<u64> exps(s->left.begin(), s->left.end());
-        std::vector<const cuhe_bfv_key*> rkeys;
-        for (u64 g : s->left) rkeys.push_back(s->keys.at(g));
-        std::vector<const u64*> masks(tc, s->d_full_mask);
-        if (partial && first + t0 + tc == size_t(tiles)) masks[tc - 1] = partial;
-        rc = native_tile_circuit(r, ln, d, qw, tw + t0 * 2 * n * W, tc, s->t, s->relin, exps, rkeys, masks,
-                                 s->mask_primes, sc, dist + t0 * 2 * n * W, prof);
+        return tile_circuit(r, lane, d, a, dist + t0 * 2 * L * n, pr);
       }
+      std::vector<u64> exps(s->left.begin(), s->left.end());
+      std::vector<const cuhe_bfv_key*> rkeys;
+      for (u64 g : s->left) rkeys.push_back(s->keys.at(g));
+      std::vector<const u64*> masks(tc, s->d_full_mask);
+      if (partial && first + t0 + tc == size_t(tiles)) masks[tc - 1] = partial;
+      return native_tile_circuit(r, lane, d, qw, tw + t0 * 2 * n * W, tc, s->t, s->relin, exps, rkeys, masks,
+                                 s->mask_primes, nsc, dist + t0 * 2 * n * W, pr);
+    };
+    auto run_tiles = [&](size_t t0, size_t tc) -> int {
+      const size_t mark = ln.arena.used;  // the circuit's workspace is free again when it returns
+      if (P.n > kMaxPlaneN || tc < kSplitTiles) {
+        const int rc = circuit(ln, t0, tc, sc, prof);
+        ln.arena.used = mark;
+        return rc;
+      }
+      // Two halves on two streams, each driven by its own host thread: a
+      // launch's last partial wave of CTAs overlaps the other half's
+      // launches, and one half's host synchronisations leave the GPU to the
+      // other.  Each half takes its own slice of the workspace (residue
+      // rings) or of the chunk's scratch (native rings).  The split falls on
+      // a response-group boundary where one lies near the middle.
+      size_t ha = tc / 2;
+      {
+        const size_t mid = t0 + tc / 2, pad = s->padded;
+        const size_t lo = (mid / pad) * pad, hi = lo + pad;
+        const size_t pick = mid - lo <= hi - mid ? lo : hi;
+        if (pick >= t0 + tc / 4 && pick <= t0 + tc - tc / 4) ha = pick - t0;
+      }
+      const size_t hb = tc - ha;
+      const size_t bytes_a = r->residue ? tile_arena_bytes(r, ha) : 0;
+      const size_t bytes_b = r->residue ? tile_arena_bytes(r, hb) : 0;
+      if (mark + bytes_a + bytes_b > ln.arena.cap) return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted");
+      if (!ln.side) {
+        int prio = 0;
+        BFV_CUDA(cudaStreamGetPriority(ln.stream, &prio), "stream priority");
+        BFV_CUDA(cudaStreamCreateWithPriority(&ln.side, cudaStreamNonBlocking, prio), "side stream");
+      }
+      Lane half[2];
+      half[0].stream = ln.stream;
+      half[1].stream = ln.side;
+      half[0].arena.base = ln.arena.base + mark;
+      half[0].arena.cap = bytes_a;
+      half[1].arena.base = ln.arena.base + mark + bytes_a;
+      half[1].arena.cap = bytes_b;
+      for (Lane& h : half) h.arena.owned = false;
+      NativeScratch sc_b = sc;  // scratch of tiles [ha, tc): every array offset by ha tiles
+      if (!r->residue) {
+        const size_t T = P.tensor_count, S = r->switch_prime_count, M = s->mask_primes;
+        sc_b.diff += ha * 2 * n * W;
+        sc_b.dres += ha * 2 * T * n;
+        sc_b.tens += ha * 3 * T * n;
+        sc_b.words3 += ha * 3 * n * W;
+        sc_b.ksres += ha * 2 * S * n;
+        sc_b.ksw += ha * 2 * n * W;
+        sc_b.perm += ha * 2 * n * W;
+        sc_b.tmp += ha * 2 * n * W;
+        sc_b.mres += ha * 2 * M * n;
+        sc_b.d_sops += ha;
+        sc_b.d_nops += ha;
+      }
+      cudaEvent_t ready;
+      BFV_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+      cudaError_t e = cudaEventRecord(ready, ln.stream);  // unpacked tiles and query
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ln.side, ready, 0);
+      cudaEventDestroy(ready);
+      BFV_CUDA(e, "side stream order");
+      double prof_a[6] = {0, 0, 0, 0, 0, 0}, prof_b[6] = {0, 0, 0, 0, 0, 0};
+      int rc_b = CUHE_OK;
+      std::string err_b;
+      const int device = r->device;
+      // circuits of tiles [h0, h0 + hc), then, when this batch is the whole
+      // chunk, the merges of the groups they hold whole (the batches of a
+      // pipelined upload leave all merges to the end, where the waves of
+      // every group together fill the GPU)
+      auto run_half = [&](Lane& lane, size_t h0, size_t hc, const NativeScratch& nsc, double* pr) -> int {
+        if (int rc = circuit(lane, h0, hc, nsc, pr)) return rc;
+        if (tc != ct) return CUHE_OK;
+        lane.arena.used = 0;
+        const size_t pad = s->padded, h1 = h0 + hc;
+        const size_t g_lo = (h0 + pad - 1) / pad;
+        const size_t g_hi = h1 == ct ? gc : h1 / pad;
+        return merge_groups(lane, g_lo, std::max(g_lo, g_hi), nsc, pr);
+      };
+      std::thread side([&] {
+        cudaSetDevice(device);
+        rc_b = run_half(half[1], t0 + ha, hb, sc_b, prof_b);
+        if (rc_b) err_b = t_error;
+      });
+      int rc = run_half(half[0], t0, ha, sc, prof_a);
+      side.join();
+      cudaStreamSynchronize(ln.side);  // the side stream is idle whatever happened
+      if (!rc && rc_b) rc = fail(rc_b, err_b);
+      for (int k = 0; k < 6; ++k) prof[k] += 0.5 * (prof_a[k] + prof_b[k]);  // the halves overlap
       ln.arena.used = mark;
       return rc;
     };
@@ -1891,94 +2090,24 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
       BFV_CUDA(cudaStreamSynchronize(ln.stream), "unpack");
       if (status) return fail(CUHE_INVALID_ARGUMENT, "Noncanonical packed polynomial coefficient");
     }
-    // merge tree (bfv_server.h:15-45), executed in waves of independent merges
-    cudaEvent_t m0, m1;
-    cudaEventCreate(&m0);
+    // groups not merged with their tiles' half batches
+    for (size_t gi = 0; gi < gc;) {
+      if (merged[gi]) {
+        ++gi;
+        continue;
+      }
+      size_t ge = gi;
+      while (ge < gc && !merged[ge]) ++ge;
+      const size_t mark = ln.arena.used;
+      if (int rc = merge_groups(ln, gi, ge, sc, prof)) return rc;
+      ln.arena.used = mark;
+      gi = ge;
+    }
+    cudaEvent_t m1;
     cudaEventCreate(&m1);
-    cudaEventRecord(m0, ln.stream);
-    struct Merge { size_t left, right; size_t level; size_t wave; };
-    std::vector<Merge> merges;
-    std::vector<size_t> result_slot;
-    for (size_t gs = 0; gs < ct; gs += s->padded) {
-      struct Node { size_t slot, ready; };
-      std::vector<std::pair<Node, size_t>> stack;
-      const size_t ge = std::min(gs + s->padded, ct);
-      for (size_t at = gs; at < ge; ++at) {
-        Node node{at, 0};
-        size_t size = 1, level = 0;
-        while (!stack.empty() && stack.back().second == size) {
-          const Node left = stack.back().first;
-          stack.pop_back();
-          const size_t wave = std::max(left.ready, node.ready);
-          merges.push_back({left.slot, node.slot, level, wave});
-          node = Node{left.slot, wave + 1};
-          size *= 2;
-          ++level;
-        }
-        stack.emplace_back(node, size);
-      }
-      Node result = stack.back().first;
-      stack.pop_back();
-      while (!stack.empty()) {
-        const size_t size = stack.back().second;
-        size_t level = 0;
-        while ((size_t(1) << level) < size) ++level;
-        const Node left = stack.back().first;
-        stack.pop_back();
-        const size_t wave = std::max(left.ready, result.ready);
-        merges.push_back({left.slot, result.slot, level, wave});
-        result = Node{left.slot, wave + 1};
-      }
-      result_slot.push_back(result.slot);
-    }
-    size_t waves = 0;
-    for (const auto& m : merges) waves = std::max(waves, m.wave + 1);
-    if (!r->residue) {
-      // native: rotate each right operand (grouped by level, one key each),
-      // then add it into its left operand
-      for (size_t w = 0; w < waves; ++w) {
-        std::vector<NativeOp> adds;
-        size_t used = 0;
-        for (size_t level = 0; level < s->right.size(); ++level) {
-          std::vector<NativeOp> rots;
-          for (const auto& m : merges) {
-            if (m.wave != w || m.level != level) continue;
-            const size_t k = used + rots.size();
-            rots.push_back(NativeOp{dist + m.right * 2 * n * W, sc.perm + k * 2 * n * W, sc.tmp + k * 2 * n * W,
-                                    nullptr});
-            adds.push_back(NativeOp{dist + m.left * 2 * n * W, sc.tmp + k * 2 * n * W, dist + m.left * 2 * n * W,
-                                    nullptr});
-          }
-          if (rots.empty()) continue;
-          const u64 g = s->right.at(level);
-          if (int rc = native_rotate(r, ln, d, rots, unsigned(g), s->keys.at(g), sc.d_nops, sc.ksres,
-                                     sc.ksw + used * 2 * n * W, sc.d_sops))
-            return rc;
-          used += rots.size();
-        }
-        if (int rc = native_add_ops(r, ln, d, adds, sc.d_nops)) return rc;
-      }
-      waves = 0;  // the residue waves below are skipped
-    }
-    u64* mwords = ln.arena.take<u64>(std::max<size_t>(1, ct) * n * W);
-    ComposeOp* d_cops = ln.arena.take<ComposeOp>(std::max<size_t>(1, ct));
-    SwitchOp* d_sops = ln.arena.take<SwitchOp>(std::max<size_t>(1, ct));
-    BFV_ARENA(ln.arena);
-    for (size_t w = 0; w < waves; ++w) {
-      std::vector<ComposeOp> cops;
-      std::vector<SwitchOp> sops;
-      for (const auto& m : merges) {
-        if (m.wave != w) continue;
-        const u64 g = s->right.at(m.level);
-        u64* words = mwords + cops.size() * n * W;
-        cops.push_back(ComposeOp{dist + (m.right * 2 + 1) * L * n, words, unsigned(g), 0u});
-        const cuhe_bfv_key* key = s->keys.at(g);
-        sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, key->d_key, key->d_key_q,
-                                dist + m.left * 2 * L * n, inverse_mod_2n(g, n), 0u});
-      }
-      if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
-    }
     cudaEventRecord(m1, ln.stream);
+    ComposeOp* d_cops = ln.arena.take<ComposeOp>(std::max<size_t>(1, 2 * gc));
+    BFV_ARENA(ln.arena);
     // outputs: compose, optional compaction, packing
     if (r->residue) {
       std::vector<ComposeOp> cops;
@@ -2007,11 +2136,8 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
     cudaEventRecord(o1, ln.stream);
     BFV_CUDA(cudaStreamSynchronize(ln.stream), "search");
     float x = 0;
-    cudaEventElapsedTime(&x, m0, m1);
-    prof[4] += x;
     cudaEventElapsedTime(&x, m1, o1);
     prof[5] += x;
-    cudaEventDestroy(m0);
     cudaEventDestroy(m1);
     cudaEventDestroy(o1);
     for (size_t gi = 0; gi < gc * 2; ++gi)
