@@ -53,6 +53,11 @@ struct DeviceGuard {
 };
 
 // Growable device workspace carved into aligned slices for one call.
+// Tile batches of at least kSplitTiles tiles run as kSplitWays parts, each on
+// its own stream.
+constexpr int kSplitWays = 2;  // 3 and 4 parts measured the same
+constexpr size_t kSplitTiles = 128;
+
 struct Arena {
   char* base = nullptr;
   size_t cap = 0, used = 0;
@@ -98,13 +103,14 @@ struct Lane {
   size_t pin_cap[2] = {0, 0};
   u64* ks_scratch = nullptr;  // N = 32768 key switches: digit and accumulator planes (grow-only)
   size_t ks_scratch_bytes = 0;
-  cudaStream_t side = nullptr;  // second compute stream of split tile batches
+  cudaStream_t side[kSplitWays - 1] = {};  // further compute streams of split tile batches
   ~Lane() {
     if (copy) cudaStreamSynchronize(copy);
-    if (side) {
-      cudaStreamSynchronize(side);
-      cudaStreamDestroy(side);
-    }
+    for (cudaStream_t st : side)
+      if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
     if (ks_scratch) cudaFree(ks_scratch);
     if (host_stage) cudaFreeHost(host_stage);
     for (uint8_t* p : pin)
@@ -165,8 +171,6 @@ cudaError_t stage_polys(Lane& ln, const PolySource& src, size_t first, size_t co
 
 // Index tiles per upload sub-batch of a search over a host-memory index.
 constexpr size_t kPipeTiles = 256;
-// Tile batches of at least this many tiles run as two halves on two streams.
-constexpr size_t kSplitTiles = 128;
 
 constexpr int kMaxLanes = 8;
 
@@ -1929,84 +1933,100 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
         ln.arena.used = mark;
         return rc;
       }
-      // Two halves on two streams, each driven by its own host thread: a
-      // launch's last partial wave of CTAs overlaps the other half's
-      // launches, and one half's host synchronisations leave the GPU to the
-      // other.  Each half takes its own slice of the workspace (residue
-      // rings) or of the chunk's scratch (native rings).  The split falls on
-      // a response-group boundary where one lies near the middle.
-      size_t ha = tc / 2;
-      {
-        const size_t mid = t0 + tc / 2, pad = s->padded;
+      // kSplitWays parts on as many streams, each driven by its own host
+      // thread: a launch's last partial wave of CTAs overlaps the other
+      // parts' launches, and one part's host synchronisations leave the GPU
+      // to the others.  Each part takes its own slice of the workspace
+      // (residue rings) or of the chunk's scratch (native rings).  Part
+      // boundaries fall on response-group boundaries where one lies near.
+      constexpr int K = kSplitWays;
+      size_t bound[K + 1];
+      bound[0] = t0;
+      bound[K] = t0 + tc;
+      for (int k = 1; k < K; ++k) {
+        const size_t mid = t0 + tc * k / K, pad = s->padded, slack = tc / (4 * K);  // parts stay non-empty
         const size_t lo = (mid / pad) * pad, hi = lo + pad;
         const size_t pick = mid - lo <= hi - mid ? lo : hi;
-        if (pick >= t0 + tc / 4 && pick <= t0 + tc - tc / 4) ha = pick - t0;
+        bound[k] = pick + slack >= mid && pick <= mid + slack ? pick : mid;
       }
-      const size_t hb = tc - ha;
-      const size_t bytes_a = r->residue ? tile_arena_bytes(r, ha) : 0;
-      const size_t bytes_b = r->residue ? tile_arena_bytes(r, hb) : 0;
-      if (mark + bytes_a + bytes_b > ln.arena.cap) return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted");
-      if (!ln.side) {
-        int prio = 0;
-        BFV_CUDA(cudaStreamGetPriority(ln.stream, &prio), "stream priority");
-        BFV_CUDA(cudaStreamCreateWithPriority(&ln.side, cudaStreamNonBlocking, prio), "side stream");
+      Lane part[K];
+      size_t offset = mark;
+      for (int k = 0; k < K; ++k) {
+        part[k].arena.owned = false;
+        const size_t bytes = r->residue ? tile_arena_bytes(r, bound[k + 1] - bound[k]) : 0;
+        part[k].arena.base = ln.arena.base + offset;
+        part[k].arena.cap = bytes;
+        offset += bytes;
       }
-      Lane half[2];
-      half[0].stream = ln.stream;
-      half[1].stream = ln.side;
-      half[0].arena.base = ln.arena.base + mark;
-      half[0].arena.cap = bytes_a;
-      half[1].arena.base = ln.arena.base + mark + bytes_a;
-      half[1].arena.cap = bytes_b;
-      for (Lane& h : half) h.arena.owned = false;
-      NativeScratch sc_b = sc;  // scratch of tiles [ha, tc): every array offset by ha tiles
-      if (!r->residue) {
+      if (offset > ln.arena.cap) return fail(CUHE_OUT_OF_MEMORY, "internal workspace exhausted");
+      part[0].stream = ln.stream;
+      for (int k = 1; k < K; ++k) {
+        if (!ln.side[k - 1]) {
+          int prio = 0;
+          BFV_CUDA(cudaStreamGetPriority(ln.stream, &prio), "stream priority");
+          BFV_CUDA(cudaStreamCreateWithPriority(&ln.side[k - 1], cudaStreamNonBlocking, prio), "side stream");
+        }
+        part[k].stream = ln.side[k - 1];
+      }
+      NativeScratch nsc[K];  // scratch of each part's tiles: every array offset by the part's first tile
+      for (int k = 0; k < K; ++k) {
+        const size_t off = bound[k] - t0;
+        nsc[k] = sc;
+        if (r->residue) continue;
         const size_t T = P.tensor_count, S = r->switch_prime_count, M = s->mask_primes;
-        sc_b.diff += ha * 2 * n * W;
-        sc_b.dres += ha * 2 * T * n;
-        sc_b.tens += ha * 3 * T * n;
-        sc_b.words3 += ha * 3 * n * W;
-        sc_b.ksres += ha * 2 * S * n;
-        sc_b.ksw += ha * 2 * n * W;
-        sc_b.perm += ha * 2 * n * W;
-        sc_b.tmp += ha * 2 * n * W;
-        sc_b.mres += ha * 2 * M * n;
-        sc_b.d_sops += ha;
-        sc_b.d_nops += ha;
+        nsc[k].diff += off * 2 * n * W;
+        nsc[k].dres += off * 2 * T * n;
+        nsc[k].tens += off * 3 * T * n;
+        nsc[k].words3 += off * 3 * n * W;
+        nsc[k].ksres += off * 2 * S * n;
+        nsc[k].ksw += off * 2 * n * W;
+        nsc[k].perm += off * 2 * n * W;
+        nsc[k].tmp += off * 2 * n * W;
+        nsc[k].mres += off * 2 * M * n;
+        nsc[k].d_sops += off;
+        nsc[k].d_nops += off;
       }
       cudaEvent_t ready;
       BFV_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
       cudaError_t e = cudaEventRecord(ready, ln.stream);  // unpacked tiles and query
-      if (e == cudaSuccess) e = cudaStreamWaitEvent(ln.side, ready, 0);
+      for (int k = 1; k < K && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(part[k].stream, ready, 0);
       cudaEventDestroy(ready);
       BFV_CUDA(e, "side stream order");
-      double prof_a[6] = {0, 0, 0, 0, 0, 0}, prof_b[6] = {0, 0, 0, 0, 0, 0};
-      int rc_b = CUHE_OK;
-      std::string err_b;
+      double part_prof[K][6] = {};
+      int part_rc[K] = {};
+      std::string part_err[K];
       const int device = r->device;
-      // circuits of tiles [h0, h0 + hc), then, when this batch is the whole
+      // circuits of tiles [h0, h1), then, when this batch is the whole
       // chunk, the merges of the groups they hold whole (the batches of a
       // pipelined upload leave all merges to the end, where the waves of
       // every group together fill the GPU)
-      auto run_half = [&](Lane& lane, size_t h0, size_t hc, const NativeScratch& nsc, double* pr) -> int {
-        if (int rc = circuit(lane, h0, hc, nsc, pr)) return rc;
-        if (tc != ct) return CUHE_OK;
-        lane.arena.used = 0;
-        const size_t pad = s->padded, h1 = h0 + hc;
-        const size_t g_lo = (h0 + pad - 1) / pad;
-        const size_t g_hi = h1 == ct ? gc : h1 / pad;
-        return merge_groups(lane, g_lo, std::max(g_lo, g_hi), nsc, pr);
+      auto run_part = [&](int k) {
+        const size_t h0 = bound[k], h1 = bound[k + 1];
+        int rc = circuit(part[k], h0, h1 - h0, nsc[k], part_prof[k]);
+        if (!rc && tc == ct) {
+          part[k].arena.used = 0;
+          const size_t pad = s->padded;
+          const size_t g_lo = (h0 + pad - 1) / pad;
+          const size_t g_hi = h1 == ct ? gc : h1 / pad;
+          rc = merge_groups(part[k], g_lo, std::max(g_lo, g_hi), nsc[k], part_prof[k]);
+        }
+        part_rc[k] = rc;
+        if (rc) part_err[k] = t_error;
       };
-      std::thread side([&] {
-        cudaSetDevice(device);
-        rc_b = run_half(half[1], t0 + ha, hb, sc_b, prof_b);
-        if (rc_b) err_b = t_error;
-      });
-      int rc = run_half(half[0], t0, ha, sc, prof_a);
-      side.join();
-      cudaStreamSynchronize(ln.side);  // the side stream is idle whatever happened
-      if (!rc && rc_b) rc = fail(rc_b, err_b);
-      for (int k = 0; k < 6; ++k) prof[k] += 0.5 * (prof_a[k] + prof_b[k]);  // the halves overlap
+      std::vector<std::thread> helpers;
+      for (int k = 1; k < K; ++k)
+        helpers.emplace_back([&, k] {
+          cudaSetDevice(device);
+          run_part(k);
+        });
+      run_part(0);
+      for (auto& h : helpers) h.join();
+      for (int k = 1; k < K; ++k) cudaStreamSynchronize(part[k].stream);  // idle whatever happened
+      int rc = CUHE_OK;
+      for (int k = 0; k < K && !rc; ++k)
+        if (part_rc[k]) rc = fail(part_rc[k], part_err[k]);
+      for (int k = 0; k < K; ++k)
+        for (int j = 0; j < 6; ++j) prof[j] += part_prof[k][j] / K;  // the parts overlap
       ln.arena.used = mark;
       return rc;
     };
