@@ -513,8 +513,47 @@ cudaError_t launch_ntt(cuhe_bfv_ring* r, Lane& ln, RingDev* d, u64* data, long l
 }
 
 // Compose ops then key-switch ops (one launch each).
+// The unfused key switch over `scratch` (digit planes, NTTs, products,
+// inverse NTTs, epilogue), `chunk` ops at a time: N = 32768, where no plane
+// fits one CTA, and the small waves of a merge tree, where one CTA per
+// (op, prime) would leave most SMs idle.
+int switch_unfused(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const SwitchOp* d_sops, size_t ops, u64* scratch,
+                   size_t chunk) {
+  const auto& P = r->plan;
+  const size_t n = P.n, L = r->residue ? P.residue_count : r->switch_prime_count, D = P.digits;
+  const unsigned bx = blocks_for((long long)n, 256);
+  for (size_t c0 = 0; c0 < ops; c0 += chunk) {
+    const size_t cnt = std::min(chunk, ops - c0);
+    u64* digits = scratch;
+    u64* acc = scratch + cnt * L * D * n;
+    k_ks_digits<<<dim3(bx, unsigned(cnt * L * D)), 256, 0, ln.stream>>>(d_sops + c0, int(L), digits, d);
+    BFV_CUDA(ntt_planes(n, ln.stream, d, digits, (long long)(cnt * L * D), 0, int(L), int(D), 0), "digit ntt");
+    k_ks_mac<<<dim3(bx, unsigned(cnt * 2 * L)), 256, 0, ln.stream>>>(d_sops + c0, int(L), digits, acc, d);
+    BFV_CUDA(ntt_planes(n, ln.stream, d, acc, (long long)(cnt * 2 * L), 0, int(L), 1, 1), "switch intt");
+    k_ks_finish<<<dim3(bx, unsigned(cnt * 2 * L)), 256, 0, ln.stream>>>(d_sops + c0, int(L), acc, d);
+  }
+  return CUHE_OK;
+}
+
+// Device bytes of the unfused key switch's scratch per op.
+size_t unfused_bytes_per_op(const cuhe_bfv_ring* r) {
+  const auto& P = r->plan;
+  const size_t L = r->residue ? P.residue_count : r->switch_prime_count;
+  return (L * P.digits + 2 * L) * P.n * sizeof(u64);
+}
+
+// Waves of at most this many (op, prime) pairs take the unfused key switch
+// when the caller lends scratch.
+constexpr size_t kSmallSwitchPairs = 148;
+
+// Scratch bytes of the largest such wave.
+size_t small_switch_bytes(const cuhe_bfv_ring* r) {
+  const size_t L = r->residue ? r->plan.residue_count : r->switch_prime_count;
+  return slice(std::max<size_t>(1, kSmallSwitchPairs / L) * unfused_bytes_per_op(r));
+}
+
 int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<ComposeOp>& cops, const std::vector<SwitchOp>& sops,
-               ComposeOp* d_cops, SwitchOp* d_sops) {
+               ComposeOp* d_cops, SwitchOp* d_sops, Arena* small = nullptr) {
   const auto& P = r->plan;
   if (!cops.empty()) {
     BFV_CUDA(cudaMemcpyAsync(d_cops, cops.data(), cops.size() * sizeof(ComposeOp), cudaMemcpyHostToDevice, ln.stream),
@@ -542,7 +581,13 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
              "switch ops");
     const size_t smem = ntt_smem(r);
     dim3 grid(unsigned(sops.size()), unsigned(r->residue ? P.residue_count : r->switch_prime_count));
-    if (P.n <= 8192) {
+    const size_t pairs = size_t(grid.x) * grid.y;
+    const size_t small_need = slice(sops.size() * unfused_bytes_per_op(r));
+    if (small && P.n <= kMaxPlaneN && pairs <= kSmallSwitchPairs && small->used + small_need <= small->cap) {
+      // few ops: six times as many CTAs per op in the digit transforms
+      u64* scratch = reinterpret_cast<u64*>(small->base + small->used);
+      if (int rc = switch_unfused(r, ln, d, d_sops, sops.size(), scratch, sops.size())) return rc;
+    } else if (P.n <= 8192) {
       // accumulators in tensor memory, two CTAs per SM (shared-memory size
       // within the attribute set at ring creation)
       k_keyswitch_tm<3><<<grid, 512, smem, ln.stream>>>(d_sops, d);
@@ -551,12 +596,11 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
       k_keyswitch_tm<3, 32><<<grid, 512, smem, ln.stream>>>(d_sops, d);
     } else {
       // N = 32768: no plane fits one CTA, so the switch runs unfused over
-      // the lane's scratch (digit planes, NTTs, products, inverse NTTs,
-      // epilogue), a bounded number of ops at a time
-      const size_t n = P.n, L = r->residue ? P.residue_count : r->switch_prime_count, D = P.digits;
-      const size_t per_op = (L * D + 2 * L) * n * sizeof(u64);
+      // the lane's scratch, a bounded number of ops at a time
+      const size_t per_op = unfused_bytes_per_op(r);
+      const size_t L = r->residue ? P.residue_count : r->switch_prime_count;
       const size_t fit = std::max<size_t>(1, (size_t(768) << 20) / per_op);
-      const size_t chunk = std::min({sops.size(), fit, size_t(65535) / (L * D)});
+      const size_t chunk = std::min({sops.size(), fit, size_t(65535) / (L * P.digits)});
       const size_t need = chunk * per_op;
       if (ln.ks_scratch_bytes < need) {
         if (ln.ks_scratch) {
@@ -568,17 +612,7 @@ int run_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<Compose
         BFV_CUDA(cudaMalloc(&ln.ks_scratch, need), "key-switch scratch");
         ln.ks_scratch_bytes = need;
       }
-      const unsigned bx = blocks_for((long long)n, 256);
-      for (size_t c0 = 0; c0 < sops.size(); c0 += chunk) {
-        const size_t cnt = std::min(chunk, sops.size() - c0);
-        u64* digits = ln.ks_scratch;
-        u64* acc = ln.ks_scratch + cnt * L * D * n;
-        k_ks_digits<<<dim3(bx, unsigned(cnt * L * D)), 256, 0, ln.stream>>>(d_sops + c0, int(L), digits, d);
-        BFV_CUDA(ntt_planes(n, ln.stream, d, digits, (long long)(cnt * L * D), 0, int(L), int(D), 0), "digit ntt");
-        k_ks_mac<<<dim3(bx, unsigned(cnt * 2 * L)), 256, 0, ln.stream>>>(d_sops + c0, int(L), digits, acc, d);
-        BFV_CUDA(ntt_planes(n, ln.stream, d, acc, (long long)(cnt * 2 * L), 0, int(L), 1, 1), "switch intt");
-        k_ks_finish<<<dim3(bx, unsigned(cnt * 2 * L)), 256, 0, ln.stream>>>(d_sops + c0, int(L), acc, d);
-      }
+      if (int rc = switch_unfused(r, ln, d, d_sops, sops.size(), ln.ks_scratch, chunk)) return rc;
     }
     BFV_CUDA(cudaGetLastError(), "keyswitch launch");
   }
@@ -882,12 +916,13 @@ int native_mul_plain(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* words, s
 // key switches: out[k] = (key_k . digits(in[k])) mod q as two word polys
 // ([ops][2][N][W]); res: [ops][2][S][N] scratch
 int native_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<const u64*>& in,
-                  const std::vector<const cuhe_bfv_key*>& keys, u64* res, u64* out, SwitchOp* d_sops) {
+                  const std::vector<const cuhe_bfv_key*>& keys, u64* res, u64* out, SwitchOp* d_sops,
+                  Arena* small = nullptr) {
   const size_t n = r->plan.n, S = r->switch_prime_count;
   std::vector<SwitchOp> sops(in.size());
   for (size_t k = 0; k < in.size(); ++k)
     sops[k] = SwitchOp{nullptr, nullptr, in[k], keys[k]->d_key, keys[k]->d_key_q, res + k * 2 * S * n, 1u, 0u};
-  if (int rc = run_switch(r, ln, d, {}, sops, nullptr, d_sops)) return rc;
+  if (int rc = run_switch(r, ln, d, {}, sops, nullptr, d_sops, small)) return rc;
   return native_reduce(r, ln, d, res, in.size() * 2, S, out, 0, 0);
 }
 
@@ -896,7 +931,8 @@ int native_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<cons
 // per-ciphertext scratch (two word polys each); d_ops, res and ks_all sized
 // for ops.size()
 int native_rotate(cuhe_bfv_ring* r, Lane& ln, RingDev* d, std::vector<NativeOp> ops, unsigned g,
-                  const cuhe_bfv_key* key, NativeOp* d_ops, u64* res, u64* ks_all, SwitchOp* d_sops) {
+                  const cuhe_bfv_key* key, NativeOp* d_ops, u64* res, u64* ks_all, SwitchOp* d_sops,
+                  Arena* small = nullptr) {
   const size_t n = r->plan.n, W = size_t(r->host_dev.words);
   if (ops.empty()) return CUHE_OK;
   for (size_t k = 0; k < ops.size(); ++k) ops[k].ks = ks_all + k * 2 * n * W;
@@ -908,7 +944,7 @@ int native_rotate(cuhe_bfv_ring* r, Lane& ln, RingDev* d, std::vector<NativeOp> 
   std::vector<const u64*> c1(ops.size());
   std::vector<const cuhe_bfv_key*> keys(ops.size(), key);
   for (size_t k = 0; k < ops.size(); ++k) c1[k] = ops[k].perm + n * W;
-  if (int rc = native_switch(r, ln, d, c1, keys, res, ks_all, d_sops)) return rc;
+  if (int rc = native_switch(r, ln, d, c1, keys, res, ks_all, d_sops, small)) return rc;
   k_native_finish<<<grid, 256, 0, ln.stream>>>(d_ops, d);
   BFV_CUDA(cudaGetLastError(), "rotation finish");
   return CUHE_OK;
@@ -1681,15 +1717,16 @@ size_t search_chunk_bytes(const cuhe_bfv_server* s, size_t ct, unsigned out_bits
   const size_t in_bytes = (n * P.q_bits + 7) / 8;
   const size_t out_words = (n * out_bits + 63) / 64;
   const size_t gc = (ct + s->padded - 1) / s->padded;
+  const size_t small = (kSplitWays + 1) * small_switch_bytes(r);  // merge-wave scratch of every part
   if (!r->residue)
     return native_tile_bytes(r, ct, s->mask_primes) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) +
            slice(2 * n * W * 8) + slice(ct * 2 * n * W * 8) * 2 + slice(gc * 2 * n * W * 8) +
            slice(gc * 2 * out_words * 8) + slice(sizeof(int)) + slice(ct * n * W * 8) +
-           slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp)) + 65536;
+           slice(ct * sizeof(ComposeOp)) + slice(ct * sizeof(SwitchOp)) + small + 65536;
   return tile_arena_bytes(r, ct) + slice(2 * in_bytes) + slice(ct * 2 * in_bytes) + slice(2 * n * W * 8) +
          slice(ct * 2 * n * W * 8) + slice(ct * 2 * L * n * 8) + slice(gc * 2 * n * W * 8) +
          slice(gc * 2 * out_words * 8) + slice(sizeof(int)) + slice(ct * n * W * 8) + slice(ct * sizeof(ComposeOp)) +
-         slice(ct * sizeof(SwitchOp)) + 65536;
+         slice(ct * sizeof(SwitchOp)) + small + 65536;
 }
 
 // Tiles per search chunk: whole response groups, about 1024 tiles.
@@ -1861,7 +1898,7 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
             if (rots.empty()) continue;
             const u64 g = s->right.at(level);
             if (int rc = native_rotate(r, lane, d, rots, unsigned(g), s->keys.at(g), nsc.d_nops, nsc.ksres,
-                                       nsc.ksw + used * 2 * n * W, nsc.d_sops))
+                                       nsc.ksw + used * 2 * n * W, nsc.d_sops, &lane.arena))
               return rc;
             used += rots.size();
           }
@@ -1886,7 +1923,8 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
             sops.push_back(SwitchOp{dist + m.left * 2 * L * n, dist + m.right * 2 * L * n, words, key->d_key,
                                     key->d_key_q, dist + m.left * 2 * L * n, inverse_mod_2n(g, n), 0u});
           }
-          if (int rc = run_switch(r, lane, d, cops, sops, d_cops, d_sops)) return rc;
+          // the arena past the op tables lends scratch to the small waves
+          if (int rc = run_switch(r, lane, d, cops, sops, d_cops, d_sops, &lane.arena)) return rc;
         }
         lane.arena.used = mark;
       }
@@ -1953,7 +1991,7 @@ int search_impl(cuhe_bfv_server* s, const uint8_t* query, const PolySource* inde
       size_t offset = mark;
       for (int k = 0; k < K; ++k) {
         part[k].arena.owned = false;
-        const size_t bytes = r->residue ? tile_arena_bytes(r, bound[k + 1] - bound[k]) : 0;
+        const size_t bytes = r->residue ? tile_arena_bytes(r, bound[k + 1] - bound[k]) : small_switch_bytes(r);
         part[k].arena.base = ln.arena.base + offset;
         part[k].arena.cap = bytes;
         offset += bytes;
