@@ -103,6 +103,8 @@ struct cuhe_paillier {
   int noise_entries = 0;
   DeviceBuffer work;
   DeviceBuffer tmp_ops;
+  cudaStream_t copy = nullptr;  // host-buffer pipelines: transfers beside the compute
+  cudaStream_t side = nullptr;  // and a second compute stream (created on first use)
   std::string error;
   std::mutex mu;
 };
@@ -392,12 +394,45 @@ class Stager {
     return CUHE_OK;
   }
   bool staged() const { return staged_; }
+  // item i lives in the workspace (its caller buffer is host memory)
+  bool is_staged(size_t i) const { return items_[i].src && items_[i].dev != items_[i].src; }
 
  private:
   cuhe_paillier* ctx_;
   std::vector<Staged> items_;
   bool staged_ = false;
 };
+
+// Host buffers of at least this many bytes move piece by piece beside the
+// compute instead of before or after it.
+constexpr size_t kPipeBytes = size_t(64) << 20;
+
+// The context's copy and side streams, created on first use; both start
+// after the work already queued on the context's stream (which may still
+// use the workspace the pipeline is about to fill).
+int pipeline_streams(cuhe_paillier* ctx) {
+  for (cudaStream_t* st : {&ctx->copy, &ctx->side})
+    if (!*st) CUHE_CUDA(ctx, cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "pipeline stream");
+  cudaEvent_t ready;
+  CUHE_CUDA(ctx, cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event");
+  cudaError_t e = cudaEventRecord(ready, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy, ready, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ready, 0);
+  cudaEventDestroy(ready);
+  CUHE_CUDA(ctx, e, "pipeline order");
+  return CUHE_OK;
+}
+
+// `waiter` waits for the work queued so far on `from`.
+cudaError_t stream_after(cudaStream_t waiter, cudaStream_t from) {
+  cudaEvent_t ev;
+  cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) return e;
+  e = cudaEventRecord(ev, from);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(waiter, ev, 0);
+  cudaEventDestroy(ev);
+  return e;
+}
 
 int check_status(cuhe_paillier* ctx, bool synchronous) {
   // Range errors are reported by the kernels through d_status; reading it
@@ -549,8 +584,12 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_crt);
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_noise);
+  for (cudaStream_t st : {ctx->copy, ctx->side})
+    if (st) cudaStreamSynchronize(st);
   ctx->work.release();
   ctx->tmp_ops.release();
+  for (cudaStream_t st : {ctx->copy, ctx->side})
+    if (st) cudaStreamDestroy(st);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
 }
@@ -734,14 +773,46 @@ int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t 
   Dispatch d;
   find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
   const int64_t total = vectors * chunk_num;
+  const size_t cbytes = size_t(total) * ctx->K * 4;
+  // A large host input moves in two pieces on the copy stream: the first
+  // sixteenth, decoded on the context's stream as soon as it has arrived,
+  // and the rest, decoded on the side stream (so the first launch's last
+  // wave overlaps the second) while only the first piece's copy is exposed.
+  const bool pipe = cbytes >= kPipeBytes && vectors >= 32 && !is_device_pointer(c);
   Stager st(ctx);
-  st.add(c, size_t(total) * ctx->K * 4, true, false);
+  st.add(c, cbytes, !pipe, false);
   st.add_scratch(size_t(total) * 4);  // per-chunk popcounts
   st.add(distance, size_t(vectors) * 8, false, true);
   if (int rc = st.bind()) return rc;
   uint32_t* d_counts = static_cast<uint32_t*>(st.dev(1));
-  CUHE_CUDA(ctx, secret_modexp(ctx, d, (const uint32_t*)st.dev(0), d_counts, total, cuhe::EXP_DECODE, chunk_len / 32),
-            "decode launch");
+  const uint32_t* d_c = static_cast<const uint32_t*>(st.dev(0));
+  if (pipe && st.is_staged(0)) {
+    if (int rc = pipeline_streams(ctx)) return rc;
+    const int64_t first = std::max<int64_t>(1, vectors / 16) * chunk_num;
+    const size_t fbytes = size_t(first) * ctx->K * 4;
+    cudaEvent_t arrived[2];
+    for (auto& ev : arrived) CUHE_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+    cudaError_t e = cudaMemcpyAsync(const_cast<uint32_t*>(d_c), c, fbytes, cudaMemcpyHostToDevice, ctx->copy);
+    if (e == cudaSuccess) e = cudaEventRecord(arrived[0], ctx->copy);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(const_cast<uint32_t*>(d_c) + size_t(first) * ctx->K, c + size_t(first) * ctx->K,
+                          cbytes - fbytes, cudaMemcpyHostToDevice, ctx->copy);
+    if (e == cudaSuccess) e = cudaEventRecord(arrived[1], ctx->copy);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, arrived[0], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, arrived[1], 0);
+    for (auto& ev : arrived) cudaEventDestroy(ev);
+    CUHE_CUDA(ctx, e, "piecewise upload");
+    CUHE_CUDA(ctx, secret_modexp(ctx, d, d_c, d_counts, first, cuhe::EXP_DECODE, chunk_len / 32), "decode launch");
+    cudaStream_t own = ctx->stream;
+    ctx->stream = ctx->side;  // the launchers queue on ctx->stream
+    e = secret_modexp(ctx, d, d_c + size_t(first) * ctx->K, d_counts + first, total - first, cuhe::EXP_DECODE,
+                      chunk_len / 32);
+    ctx->stream = own;
+    CUHE_CUDA(ctx, e, "decode launch");
+    CUHE_CUDA(ctx, stream_after(ctx->stream, ctx->side), "decode join");
+  } else {
+    CUHE_CUDA(ctx, secret_modexp(ctx, d, d_c, d_counts, total, cuhe::EXP_DECODE, chunk_len / 32), "decode launch");
+  }
   cuhe::k_sum_chunks<<<unsigned((vectors + 255) / 256), 256, 0, ctx->stream>>>(
       d_counts, vectors, chunk_num, reinterpret_cast<long long*>(st.dev(2)));
   CUHE_CUDA(ctx, cudaGetLastError(), "decode reduction");
@@ -942,15 +1013,37 @@ int cuhe_paillier_mulmod_outer(cuhe_paillier* ctx, const uint32_t* query, int64_
   Dispatch d;
   find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
   const size_t kb = size_t(ctx->K) * 4;
+  const size_t obytes = size_t(nq) * size_t(nx) * kb;
+  // A large host output moves in query-row blocks on the copy stream, each
+  // block's download beside the next block's products.
+  const bool pipe = obytes >= kPipeBytes && nq >= 2 && !is_device_pointer(out);
   Stager st(ctx);
   st.add(query, size_t(nq) * kb, true, false);
   st.add(index, size_t(nx) * kb, true, false);
-  st.add(out, size_t(nq) * size_t(nx) * kb, false, true);
+  st.add(out, obytes, false, !pipe);
   st.add_scratch(size_t(nq) * kb);  // queries in Montgomery form
   if (int rc = st.bind()) return rc;
   uint32_t* qm = static_cast<uint32_t*>(st.dev(3));
+  uint32_t* d_out = static_cast<uint32_t*>(st.dev(2));
   CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(0), qm, nq, 1), "query conversion");
-  CUHE_CUDA(ctx, d.outer(ctx, qm, nq, (const uint32_t*)st.dev(1), nx, (uint32_t*)st.dev(2)), "mulmod_outer launch");
+  if (pipe && st.is_staged(2)) {
+    if (int rc = pipeline_streams(ctx)) return rc;
+    const int64_t rows = std::max<int64_t>(1, nq / 8);
+    const size_t row_words = size_t(nx) * ctx->K;
+    for (int64_t q0 = 0; q0 < nq; q0 += rows) {
+      const int64_t qn = std::min(rows, nq - q0);
+      CUHE_CUDA(ctx, d.outer(ctx, qm + size_t(q0) * ctx->K, qn, (const uint32_t*)st.dev(1), nx,
+                             d_out + size_t(q0) * row_words),
+                "mulmod_outer launch");
+      CUHE_CUDA(ctx, stream_after(ctx->copy, ctx->stream), "download order");
+      CUHE_CUDA(ctx, cudaMemcpyAsync(out + size_t(q0) * row_words, d_out + size_t(q0) * row_words,
+                                     size_t(qn) * row_words * 4, cudaMemcpyDeviceToHost, ctx->copy),
+                "piecewise download");
+    }
+    CUHE_CUDA(ctx, stream_after(ctx->stream, ctx->copy), "download join");
+  } else {
+    CUHE_CUDA(ctx, d.outer(ctx, qm, nq, (const uint32_t*)st.dev(1), nx, d_out), "mulmod_outer launch");
+  }
   if (int rc = st.finish()) return rc;
   // the scratch slice is reused by the next call: keep host order
   if (!st.staged()) CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "mulmod_outer synchronize");

@@ -235,3 +235,48 @@ def test_static_decode_with_factors_matches_allocating_decode():
     rows = [vals[chunk_num * i:chunk_num * i + chunk_num] for i in range(vectors)]
     want = np.array(direct.decode_hamming(rows, chunk_num, chunk_len))
     assert np.array_equal(a.cpu().numpy(), want)
+
+
+def test_host_buffer_pipelines_match_device_buffers():
+    """Host inputs of decode and host outputs of mulmod_outer above 64 MiB
+    move piece by piece beside the compute (copy and side streams); the
+    results equal the same calls on device buffers, from pageable and from
+    pinned host memory."""
+    import torch
+
+    data = load_golden("lookup_1024.json")
+    pk, keys = _keys(data)
+    _, crt, _, _ = _pair(pk["n"], (keys["sk"]["a"], keys["sk"]["g_a_inv"]), keys["sk"]["phi"])
+    rng = np.random.default_rng(64)
+
+    def below_n2(count):
+        # a zero top word keeps every value below n^2 (a 4096-bit modulus)
+        x = rng.integers(0, 2**32, size=(count, crt.words), dtype=np.uint64).astype(np.uint32)
+        x[:, -1] = 0
+        return x
+
+    vectors, chunk_num, chunk_len = 70_001, 2, 2 * data["key_len"]
+    c_host = below_n2(vectors * chunk_num)
+    assert c_host.nbytes >= 64 << 20
+    want = torch.zeros(vectors, dtype=torch.int64, device="cuda")
+    crt.decode_array(torch.from_numpy(c_host.view(np.int32)).cuda(), vectors, chunk_num, chunk_len, want)
+    torch.cuda.synchronize()
+    want = want.cpu().numpy()
+    got = np.zeros(vectors, dtype=np.int64)
+    crt.decode_array(c_host, vectors, chunk_num, chunk_len, got)
+    assert np.array_equal(got, want)
+    pinned = torch.from_numpy(c_host.view(np.int32)).pin_memory()
+    got_pinned = torch.zeros(vectors, dtype=torch.int64).pin_memory()
+    crt.decode_array(pinned.numpy(), vectors, chunk_num, chunk_len, got_pinned.numpy())
+    assert np.array_equal(got_pinned.numpy(), want)
+
+    nq, nx = 3, 44_000
+    q_host, x_host = below_n2(nq), below_n2(nx)
+    dev = torch.zeros((nq * nx, crt.words), dtype=torch.int32, device="cuda")
+    crt.mulmod_outer_array(torch.from_numpy(q_host.view(np.int32)).cuda(), nq,
+                           torch.from_numpy(x_host.view(np.int32)).cuda(), nx, dev)
+    torch.cuda.synchronize()
+    out = np.zeros((nq * nx, crt.words), dtype=np.uint32)
+    assert out.nbytes >= 64 << 20
+    crt.mulmod_outer_array(q_host, nq, x_host, nx, out)
+    assert np.array_equal(out.view(np.int32), dev.cpu().numpy())
