@@ -605,6 +605,10 @@ struct SwitchOp {
   u64* out;          // [2][L][N]
   unsigned g_inv;    // inverse of g mod 2N (gather for x0)
   unsigned pad;
+  // [L][N] NTT-domain plaintext or null: the output is multiplied by it
+  // (k_keyswitch_tm only).  out may alias base and x0: each CTA reads its
+  // prime's planes of them whole before it writes that prime's output.
+  const u64* mask = nullptr;
 };
 
 struct ComposeOp {
@@ -828,8 +832,26 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
     tmem_wait_st();
     __syncthreads();
   }
-  for (int comp = 0; comp < 2; ++comp) {
-    if (comp == 1) {
+  if (op.mask) {
+    // masked output: NTT(out) = acc + NTT(base + sigma(x0)) exactly, so each
+    // component transforms its addends forward, adds the accumulator, takes
+    // the product with the mask and transforms back once
+    const Prime& pr = R.prime[j];
+    const u64* m = op.mask + (long long)j * n;
+    for (int comp = 0; comp < 2; ++comp) {
+      const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
+      for (int i = threadIdx.x; i < n; i += kThreads) {
+        u64 v = base ? base[i] : 0;
+        if (comp == 0 && op.x0) {
+          const unsigned sidx = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));
+          u64 x = sidx < unsigned(n) ? op.x0[(long long)j * n + sidx] : op.x0[(long long)j * n + (sidx - n)];
+          if (sidx >= unsigned(n) && x) x = p - x;
+          v = addmod(v, x, p);
+        }
+        s_plane[sp(i)] = v;
+      }
+      __syncthreads();
+      ntt_forward_fast(s_plane, R, j, MAXP);
 #pragma unroll 1
       for (int c = 0; c < kChunks; ++c) {
         uint32_t acc[16];
@@ -837,26 +859,51 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
           const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
-          if (i < n) s_plane[sp(i)] = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+          if (i < n) {
+            const u64 a0 = u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
+            const u64 a1 = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+            const u64 a = comp == 0 ? a0 : a1;  // static register indices
+            s_plane[sp(i)] = reduce128(u128(addmod(s_plane[sp(i)], a, p)) * m[i], pr);
+          }
         }
       }
       __syncthreads();
+      ntt_inverse_fast(s_plane, R, j, MAXP);
+      u64* out = op.out + ((long long)comp * L + j) * n;
+      for (int i = threadIdx.x; i < n; i += kThreads) out[i] = s_plane[sp(i)];
+      __syncthreads();
     }
-    ntt_inverse_fast(s_plane, R, j, MAXP);
-    u64* out = op.out + ((long long)comp * L + j) * n;
-    const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
-    for (int i = threadIdx.x; i < n; i += kThreads) {
-      u64 v = s_plane[sp(i)];
-      if (base) v = addmod(v, base[i], p);
-      if (comp == 0 && op.x0) {
-        const unsigned sidx = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));
-        u64 x = sidx < unsigned(n) ? op.x0[(long long)j * n + sidx] : op.x0[(long long)j * n + (sidx - n)];
-        if (sidx >= unsigned(n) && x) x = p - x;
-        v = addmod(v, x, p);
+  } else {
+    for (int comp = 0; comp < 2; ++comp) {
+      if (comp == 1) {
+#pragma unroll 1
+        for (int c = 0; c < kChunks; ++c) {
+          uint32_t acc[16];
+          tmem_ld16(tbase + uint32_t(c * 16), acc);
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
+            if (i < n) s_plane[sp(i)] = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+          }
+        }
+        __syncthreads();
       }
-      out[i] = v;
+      ntt_inverse_fast(s_plane, R, j, MAXP);
+      u64* out = op.out + ((long long)comp * L + j) * n;
+      const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
+      for (int i = threadIdx.x; i < n; i += kThreads) {
+        u64 v = s_plane[sp(i)];
+        if (base) v = addmod(v, base[i], p);
+        if (comp == 0 && op.x0) {
+          const unsigned sidx = unsigned((unsigned long long)i * op.g_inv % (2u * unsigned(n)));
+          u64 x = sidx < unsigned(n) ? op.x0[(long long)j * n + sidx] : op.x0[(long long)j * n + (sidx - n)];
+          if (sidx >= unsigned(n) && x) x = p - x;
+          v = addmod(v, x, p);
+        }
+        out[i] = v;
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   tmem_fence_before_sync();
   __syncthreads();

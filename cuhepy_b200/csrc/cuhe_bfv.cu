@@ -745,9 +745,12 @@ int tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const TileArgs& a, u64*
   }
   if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
   cudaEventRecord(ev[2], ln.stream);
-  // rotations: dist += rotate(dist, g)
+  // rotations: dist += rotate(dist, g); the last one, when a key switch on
+  // planes that fit one CTA, also applies the masks (its output is then
+  // multiplied in the NTT domain before its single inverse transform)
   u64* cur = dist;
   u64* nxt = other;
+  const bool fused_mask = !a.exps.empty() && a.exps.back() != 1 && n <= size_t(kMaxPlaneN);
   for (size_t k = 0; k < a.exps.size(); ++k) {
     const u64 g = a.exps[k];
     if (g == 1) {
@@ -755,28 +758,34 @@ int tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const TileArgs& a, u64*
       BFV_CUDA(cudaGetLastError(), "double");
     } else {
       const unsigned ginv = inverse_mod_2n(g, n);
+      const bool masked = fused_mask && k + 1 == a.exps.size();
+      u64* target = masked ? cur : nxt;  // a masked switch may write in place
       for (size_t t = 0; t < ct; ++t) {
         cops[t] = ComposeOp{cur + (t * 2 + 1) * L * n, words + t * n * W, unsigned(g), 0u};
         sops[t] = SwitchOp{cur + t * 2 * L * n, cur + t * 2 * L * n, words + t * n * W, a.keys[k]->d_key,
-                           a.keys[k]->d_key_q, nxt + t * 2 * L * n, ginv, 0u};
+                           a.keys[k]->d_key_q, target + t * 2 * L * n, ginv, 0u};
+        if (masked) sops[t].mask = a.masks[t];
       }
       if (int rc = run_switch(r, ln, d, cops, sops, d_cops, d_sops)) return rc;
+      if (masked) break;
     }
     std::swap(cur, nxt);
   }
   cudaEventRecord(ev[3], ln.stream);
-  // masks in the NTT domain
-  BFV_CUDA(launch_ntt(r, ln, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 0), "mask ntt");
-  for (size_t t = 0; t < ct; ++t) {
-    const u64* m = a.masks[t];
-    size_t run = 1;
-    while (t + run < ct && a.masks[t + run] == m) ++run;
-    k_mul_plain<<<blocks_for((long long)(run * 2 * L * n), 256), 256, 0, ln.stream>>>(cur + t * 2 * L * n,
-                                                                                      (long long)(run * 2 * L), int(L), m, d);
-    BFV_CUDA(cudaGetLastError(), "mask");
-    t += run - 1;
+  // masks in the NTT domain (unless the last rotation applied them)
+  if (!fused_mask) {
+    BFV_CUDA(launch_ntt(r, ln, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 0), "mask ntt");
+    for (size_t t = 0; t < ct; ++t) {
+      const u64* m = a.masks[t];
+      size_t run = 1;
+      while (t + run < ct && a.masks[t + run] == m) ++run;
+      k_mul_plain<<<blocks_for((long long)(run * 2 * L * n), 256), 256, 0, ln.stream>>>(
+          cur + t * 2 * L * n, (long long)(run * 2 * L), int(L), m, d);
+      BFV_CUDA(cudaGetLastError(), "mask");
+      t += run - 1;
+    }
+    BFV_CUDA(launch_ntt(r, ln, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 1), "mask intt");
   }
-  BFV_CUDA(launch_ntt(r, ln, d, cur, (long long)(ct * 2 * L), 0, int(L), 1, 1), "mask intt");
   if (cur != dist)
     BFV_CUDA(cudaMemcpyAsync(dist, cur, ct * 2 * L * n * 8, cudaMemcpyDeviceToDevice, ln.stream), "dist copy");
   cudaEventRecord(ev[4], ln.stream);
