@@ -196,6 +196,24 @@ __device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j
   }
 }
 
+// The first `stages` stages of the forward transform (outputs below 4p);
+// the caller applies the rest.
+__device__ __forceinline__ void ntt_forward_stages(u64* a, const RingDev& R, int j, int max_p, int stages) {
+  const int logn = R.logn;
+  const u64 p = R.prime[j].p;
+  const ulonglong2* w2 = R.fwd2[j];
+  for (int s0 = 0; s0 < stages; s0 += max_p) {
+    const int P = stages - s0 < max_p ? stages - s0 : max_p;
+    switch (P) {
+      case 4: ntt_forward_pass<4, false>(a, s0, logn, w2, p, false, 0); break;
+      case 3: ntt_forward_pass<3, false>(a, s0, logn, w2, p, false, 0); break;
+      case 2: ntt_forward_pass<2, false>(a, s0, logn, w2, p, false, 0); break;
+      default: ntt_forward_pass<1, false>(a, s0, logn, w2, p, false, 0); break;
+    }
+    __syncthreads();
+  }
+}
+
 template <bool kHalf = false>
 __device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j, int max_p = 4, int half_id = 0) {
   const int logn = kHalf ? R.logn - 1 : R.logn;
@@ -789,11 +807,25 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
   __syncthreads();
   tmem_fence_after_sync();
   const uint32_t tbase = s_tmem + (uint32_t((warp & 3) * 32) << 16) + uint32_t((warp >> 2) * 4 * kCoef);
+  // When the forward transform's last pass would be a single stage (log2 N
+  // = 1 mod MAXP), that stage runs in the product loop instead: thread t
+  // takes coefficient pairs (2b, 2b + 1), b = t + kThreads k, applies the
+  // stage's butterfly in registers and reads the key pairs as 16-byte
+  // loads.  Column group kk of chunk c then holds coefficient
+  // 2 (t + kThreads (2c + kk / 2)) + kk % 2 (else t + kThreads (4c + kk)).
+  const bool pairs = R.logn % MAXP == 1 && R.logn > 1;
+  auto coef = [&](int c, int kk) {
+    return pairs ? 2 * (int(threadIdx.x) + (c * 2 + (kk >> 1)) * kThreads) + (kk & 1)
+                 : int(threadIdx.x) + (c * 4 + kk) * kThreads;
+  };
+  const ulonglong2* w2 = R.fwd2[j];
+  const int half_n = n >> 1;
   for (int d = 0; d < R.digits; ++d) {
     for (int i = threadIdx.x; i < n; i += kThreads)
       s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
     __syncthreads();
-    ntt_forward_fast(s_plane, R, j, MAXP);
+    if (pairs) ntt_forward_stages(s_plane, R, j, MAXP, R.logn - 1);
+    else ntt_forward_fast(s_plane, R, j, MAXP);
     const long long k0o = ((long long)(d * 2 + 0) * L + j) * n, k1o = ((long long)(d * 2 + 1) * L + j) * n;
     const bool last = d + 1 == R.digits;
 #pragma unroll 1
@@ -805,26 +837,67 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
 #pragma unroll
         for (int k = 0; k < 16; ++k) acc[k] = 0;
       }
+      if (pairs) {
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
-        if (i < n) {
-          const u64 v = s_plane[sp(i)];
-          u64 a0 = shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), p);
-          u64 a1 = shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), p);
-          a0 += u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
-          a1 += u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
-          a0 = a0 >= two_p ? a0 - two_p : a0;
-          a1 = a1 >= two_p ? a1 - two_p : a1;
-          if (last) {
-            a0 = a0 >= p ? a0 - p : a0;
-            a1 = a1 >= p ? a1 - p : a1;
-            s_plane[sp(i)] = a0;  // component 0 transforms first
+        for (int kp = 0; kp < 2; ++kp) {
+          const int b = int(threadIdx.x) + (c * 2 + kp) * kThreads;
+          if (b < half_n) {
+            // the last forward stage: gap 1, twiddle (N/2 + b)
+            u64 u = s_plane[sp(2 * b)];
+            const u64 x1 = s_plane[sp(2 * b + 1)];
+            const ulonglong2 tw = __ldg(w2 + half_n + b);
+            if (u >= two_p) u -= two_p;
+            const u64 v = shoup_lazy(x1, tw.x, tw.y, p);
+            u64 y[2] = {u + v, u + two_p - v};
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              y[e] = y[e] >= two_p ? y[e] - two_p : y[e];
+              y[e] = y[e] >= p ? y[e] - p : y[e];
+            }
+            // one key component at a time keeps fewer registers live
+#pragma unroll
+            for (int comp = 0; comp < 2; ++comp) {
+              const long long ko = comp ? k1o : k0o;
+              const ulonglong2 kv = __ldg(reinterpret_cast<const ulonglong2*>(op.key + ko) + b);
+              const ulonglong2 kq = __ldg(reinterpret_cast<const ulonglong2*>(op.key_q + ko) + b);
+#pragma unroll
+              for (int e = 0; e < 2; ++e) {
+                const int col = 4 * (2 * kp + e) + 2 * comp;
+                u64 a = shoup_lazy(y[e], e ? kv.y : kv.x, e ? kq.y : kq.x, p);
+                a += u64(acc[col]) | (u64(acc[col + 1]) << 32);
+                a = a >= two_p ? a - two_p : a;
+                if (last) {
+                  a = a >= p ? a - p : a;
+                  if (comp == 0) s_plane[sp(2 * b + e)] = a;  // component 0 transforms first
+                }
+                acc[col] = uint32_t(a);
+                acc[col + 1] = uint32_t(a >> 32);
+              }
+            }
           }
-          acc[4 * kk] = uint32_t(a0);
-          acc[4 * kk + 1] = uint32_t(a0 >> 32);
-          acc[4 * kk + 2] = uint32_t(a1);
-          acc[4 * kk + 3] = uint32_t(a1 >> 32);
+        }
+      } else {
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
+          if (i < n) {
+            const u64 v = s_plane[sp(i)];
+            u64 a0 = shoup_lazy(v, __ldg(op.key + k0o + i), __ldg(op.key_q + k0o + i), p);
+            u64 a1 = shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), p);
+            a0 += u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
+            a1 += u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+            a0 = a0 >= two_p ? a0 - two_p : a0;
+            a1 = a1 >= two_p ? a1 - two_p : a1;
+            if (last) {
+              a0 = a0 >= p ? a0 - p : a0;
+              a1 = a1 >= p ? a1 - p : a1;
+              s_plane[sp(i)] = a0;  // component 0 transforms first
+            }
+            acc[4 * kk] = uint32_t(a0);
+            acc[4 * kk + 1] = uint32_t(a0 >> 32);
+            acc[4 * kk + 2] = uint32_t(a1);
+            acc[4 * kk + 3] = uint32_t(a1 >> 32);
+          }
         }
       }
       tmem_st16(tbase + uint32_t(c * 16), acc);
@@ -858,7 +931,7 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
         tmem_ld16(tbase + uint32_t(c * 16), acc);
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
-          const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
+          const int i = coef(c, kk);
           if (i < n) {
             const u64 a0 = u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
             const u64 a1 = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
@@ -882,7 +955,7 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
           tmem_ld16(tbase + uint32_t(c * 16), acc);
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
-            const int i = int(threadIdx.x) + (c * 4 + kk) * kThreads;
+            const int i = coef(c, kk);
             if (i < n) s_plane[sp(i)] = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
           }
         }
