@@ -239,6 +239,43 @@ __device__ __forceinline__ void ntt_inverse_fast(u64* a, const RingDev& R, int j
   }
 }
 
+// The inverse transform from stage `first` on (the caller applied the
+// earlier ones; inputs below 2p), including the final 1/N and twist.
+__device__ __forceinline__ void ntt_inverse_from(u64* a, const RingDev& R, int j, int max_p, int first) {
+  const int logn = R.logn;
+  const u64 p = R.prime[j].p;
+  const ulonglong2* w2 = R.inv2[j];
+  for (int u0 = first; u0 < logn; u0 += max_p) {
+    const int P = logn - u0 < max_p ? logn - u0 : max_p;
+    const int key = P * 2 + (u0 + P == logn ? 1 : 0);
+#define CUHE_INV_PASS(PP, F) \
+  ntt_inverse_pass<PP, false, F>(a, u0, logn, w2, p, R.n_inv[j], R.n_inv_q[j], R.last[j], R.last_q[j], 0)
+    switch (key) {
+      case 9: CUHE_INV_PASS(4, true); break;
+      case 8: CUHE_INV_PASS(4, false); break;
+      case 7: CUHE_INV_PASS(3, true); break;
+      case 6: CUHE_INV_PASS(3, false); break;
+      case 5: CUHE_INV_PASS(2, true); break;
+      case 4: CUHE_INV_PASS(2, false); break;
+      case 3: CUHE_INV_PASS(1, true); break;
+      default: CUHE_INV_PASS(1, false); break;
+    }
+#undef CUHE_INV_PASS
+    __syncthreads();
+  }
+}
+
+// The inverse transform's first stage (gap 1) on the pair (x0, x1) =
+// coefficients (2b, 2b + 1), inputs below 2p, outputs below 2p.
+__device__ __forceinline__ void inverse_stage0(u64& x0, u64& x1, const ulonglong2* __restrict__ w2, int half_n,
+                                               int b, u64 p) {
+  const ulonglong2 tw = __ldg(w2 + half_n + b);
+  const u64 two_p = 2 * p, u = x0, v = x1;
+  const u64 s = u + v;
+  x0 = s >= two_p ? s - two_p : s;
+  x1 = shoup_lazy(u + two_p - v, tw.x, tw.y, p);
+}
+
 // Batched transform: plane b of `data` (stride n) uses prime prime_of(b).
 // prime = (b / prime_block) % prime_mod + prime_base.  MAXP bounds the
 // register pass width at compile time: radix-8 passes fit 64 registers, so
@@ -855,6 +892,7 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
               y[e] = y[e] >= p ? y[e] - p : y[e];
             }
             // one key component at a time keeps fewer registers live
+            u64 out0[2];
 #pragma unroll
             for (int comp = 0; comp < 2; ++comp) {
               const long long ko = comp ? k1o : k0o;
@@ -866,13 +904,17 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
                 u64 a = shoup_lazy(y[e], e ? kv.y : kv.x, e ? kq.y : kq.x, p);
                 a += u64(acc[col]) | (u64(acc[col + 1]) << 32);
                 a = a >= two_p ? a - two_p : a;
-                if (last) {
-                  a = a >= p ? a - p : a;
-                  if (comp == 0) s_plane[sp(2 * b + e)] = a;  // component 0 transforms first
-                }
+                if (last) a = a >= p ? a - p : a;
+                if (comp == 0) out0[e] = a;
                 acc[col] = uint32_t(a);
                 acc[col + 1] = uint32_t(a >> 32);
               }
+            }
+            if (last && !op.mask) {
+              // component 0 transforms first, its first inverse stage here
+              inverse_stage0(out0[0], out0[1], R.inv2[j], half_n, b, p);
+              s_plane[sp(2 * b)] = out0[0];
+              s_plane[sp(2 * b + 1)] = out0[1];
             }
           }
         }
@@ -929,19 +971,34 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
       for (int c = 0; c < kChunks; ++c) {
         uint32_t acc[16];
         tmem_ld16(tbase + uint32_t(c * 16), acc);
+        auto masked = [&](int kk, int i) {
+          const u64 a0 = u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
+          const u64 a1 = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+          const u64 a = comp == 0 ? a0 : a1;  // static register indices
+          return reduce128(u128(addmod(s_plane[sp(i)], a, p)) * m[i], pr);
+        };
+        if (pairs) {
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-          const int i = coef(c, kk);
-          if (i < n) {
-            const u64 a0 = u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
-            const u64 a1 = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
-            const u64 a = comp == 0 ? a0 : a1;  // static register indices
-            s_plane[sp(i)] = reduce128(u128(addmod(s_plane[sp(i)], a, p)) * m[i], pr);
+          for (int kp = 0; kp < 2; ++kp) {
+            const int b = int(threadIdx.x) + (c * 2 + kp) * kThreads;
+            if (b < half_n) {
+              u64 x0 = masked(2 * kp, 2 * b), x1 = masked(2 * kp + 1, 2 * b + 1);
+              inverse_stage0(x0, x1, R.inv2[j], half_n, b, p);
+              s_plane[sp(2 * b)] = x0;
+              s_plane[sp(2 * b + 1)] = x1;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const int i = coef(c, kk);
+            if (i < n) s_plane[sp(i)] = masked(kk, i);
           }
         }
       }
       __syncthreads();
-      ntt_inverse_fast(s_plane, R, j, MAXP);
+      if (pairs) ntt_inverse_from(s_plane, R, j, MAXP, 1);
+      else ntt_inverse_fast(s_plane, R, j, MAXP);
       u64* out = op.out + ((long long)comp * L + j) * n;
       for (int i = threadIdx.x; i < n; i += kThreads) out[i] = s_plane[sp(i)];
       __syncthreads();
@@ -953,15 +1010,30 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
         for (int c = 0; c < kChunks; ++c) {
           uint32_t acc[16];
           tmem_ld16(tbase + uint32_t(c * 16), acc);
+          if (pairs) {
 #pragma unroll
-          for (int kk = 0; kk < 4; ++kk) {
-            const int i = coef(c, kk);
-            if (i < n) s_plane[sp(i)] = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+            for (int kp = 0; kp < 2; ++kp) {
+              const int b = int(threadIdx.x) + (c * 2 + kp) * kThreads;
+              if (b < half_n) {
+                u64 x0 = u64(acc[8 * kp + 2]) | (u64(acc[8 * kp + 3]) << 32);
+                u64 x1 = u64(acc[8 * kp + 6]) | (u64(acc[8 * kp + 7]) << 32);
+                inverse_stage0(x0, x1, R.inv2[j], half_n, b, p);
+                s_plane[sp(2 * b)] = x0;
+                s_plane[sp(2 * b + 1)] = x1;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+              const int i = coef(c, kk);
+              if (i < n) s_plane[sp(i)] = u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
+            }
           }
         }
         __syncthreads();
       }
-      ntt_inverse_fast(s_plane, R, j, MAXP);
+      if (pairs) ntt_inverse_from(s_plane, R, j, MAXP, 1);
+      else ntt_inverse_fast(s_plane, R, j, MAXP);
       u64* out = op.out + ((long long)comp * L + j) * n;
       const u64* base = op.base ? op.base + ((long long)comp * L + j) * n : nullptr;
       for (int i = threadIdx.x; i < n; i += kThreads) {
