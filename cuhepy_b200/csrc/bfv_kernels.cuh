@@ -299,28 +299,55 @@ __device__ __forceinline__ void ntt_plane(u64* data, const RingDev* __restrict__
   }
   const int j = prime_base + int((b / prime_block) % prime_mod);
   u64* plane = data + b * n;
+  const u64 p = R.prime[j].p;
+  max_p = max_p < MAXP ? max_p : MAXP;
   // 16-byte global accesses when the plane allows them (pairs 2i, 2i + 1
-  // never straddle a padding gap of sp, which falls every 16 words)
+  // never straddle a padding gap of sp, which falls every 16 words).  When
+  // the stages leave a single one over (log2 N = 1 mod max_p), the gap-1
+  // stage runs on those pairs in registers: the forward transform's last
+  // before the store, the inverse transform's first after the load.
   const bool wide = (reinterpret_cast<uintptr_t>(plane) & 15) == 0;
+  const bool pairs = wide && R.logn % max_p == 1 && R.logn > 1;
+  const int half_n = n / 2;
   if (wide) {
     const ulonglong2* src = reinterpret_cast<const ulonglong2*>(plane);
-    for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+    for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
       const ulonglong2 v = src[i];
-      s_plane[sp(2 * i)] = v.x;
-      s_plane[sp(2 * i) + 1] = v.y;
+      u64 x0 = v.x, x1 = v.y;
+      if (pairs && inverse) inverse_stage0(x0, x1, R.inv2[j], half_n, i, p);
+      s_plane[sp(2 * i)] = x0;
+      s_plane[sp(2 * i) + 1] = x1;
     }
   } else {
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_plane[sp(i)] = plane[i];
   }
   __syncthreads();
-  max_p = max_p < MAXP ? max_p : MAXP;
-  if (inverse) ntt_inverse_fast(s_plane, R, j, max_p);
-  else ntt_forward_fast(s_plane, R, j, max_p);
+  if (inverse) {
+    if (pairs) ntt_inverse_from(s_plane, R, j, max_p, 1);
+    else ntt_inverse_fast(s_plane, R, j, max_p);
+  } else {
+    if (pairs) ntt_forward_stages(s_plane, R, j, max_p, R.logn - 1);
+    else ntt_forward_fast(s_plane, R, j, max_p);
+  }
   if (wide) {
     ulonglong2* dst = reinterpret_cast<ulonglong2*>(plane);
-    for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+    const ulonglong2* w2 = R.fwd2[j];
+    const u64 two_p = 2 * p;
+    for (int i = threadIdx.x; i < half_n; i += blockDim.x) {
       const int at = sp(2 * i);
-      dst[i] = make_ulonglong2(s_plane[at], s_plane[at + 1]);
+      u64 x0 = s_plane[at], x1 = s_plane[at + 1];
+      if (pairs && !inverse) {
+        // the last forward stage: gap 1, twiddle (N/2 + i), canonical outputs
+        const ulonglong2 tw = __ldg(w2 + half_n + i);
+        if (x0 >= two_p) x0 -= two_p;
+        const u64 v = shoup_lazy(x1, tw.x, tw.y, p);
+        u64 y0 = x0 + v, y1 = x0 + two_p - v;
+        y0 = y0 >= two_p ? y0 - two_p : y0;
+        y1 = y1 >= two_p ? y1 - two_p : y1;
+        x0 = y0 >= p ? y0 - p : y0;
+        x1 = y1 >= p ? y1 - p : y1;
+      }
+      dst[i] = make_ulonglong2(x0, x1);
     }
   } else {
     for (int i = threadIdx.x; i < n; i += blockDim.x) plane[i] = s_plane[sp(i)];
