@@ -1800,6 +1800,10 @@ __global__ void k_native_permute(const NativeOp* __restrict__ ops, unsigned g, c
   }
 }
 
+// out = (ks_0 + perm_0, ks_1); with kAccumulate, out = in + that (the
+// rotation added into its input: out may be in, each thread reading its
+// words before writing them)
+template <bool kAccumulate>
 __global__ void k_native_finish(const NativeOp* __restrict__ ops, const RingDev* __restrict__ ring) {
   const RingDev& R = *ring;
   const NativeOp op = ops[blockIdx.y];
@@ -1807,10 +1811,20 @@ __global__ void k_native_finish(const NativeOp* __restrict__ ops, const RingDev*
   if (idx >= 2 * R.n) return;
   const int W = R.words;
   const long long off = (long long)idx * W;
+  if (!kAccumulate) {
+    if (idx < R.n) {
+      words_add_modq(op.ks + off, op.perm + off, op.out + off, R);
+    } else {
+      for (int k = 0; k < W; ++k) op.out[off + k] = op.ks[off + k];
+    }
+    return;
+  }
+  u64 t[kMaxWords];
   if (idx < R.n) {
-    words_add_modq(op.ks + off, op.perm + off, op.out + off, R);
+    words_add_modq(op.ks + off, op.perm + off, t, R);
+    words_add_modq(t, op.in + off, op.out + off, R);
   } else {
-    for (int k = 0; k < W; ++k) op.out[off + k] = op.ks[off + k];
+    words_add_modq(op.ks + off, op.in + off, op.out + off, R);
   }
 }
 

@@ -941,7 +941,7 @@ int native_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<cons
 // for ops.size()
 int native_rotate(cuhe_bfv_ring* r, Lane& ln, RingDev* d, std::vector<NativeOp> ops, unsigned g,
                   const cuhe_bfv_key* key, NativeOp* d_ops, u64* res, u64* ks_all, SwitchOp* d_sops,
-                  Arena* small = nullptr) {
+                  Arena* small = nullptr, bool accumulate = false) {
   const size_t n = r->plan.n, W = size_t(r->host_dev.words);
   if (ops.empty()) return CUHE_OK;
   for (size_t k = 0; k < ops.size(); ++k) ops[k].ks = ks_all + k * 2 * n * W;
@@ -954,7 +954,8 @@ int native_rotate(cuhe_bfv_ring* r, Lane& ln, RingDev* d, std::vector<NativeOp> 
   std::vector<const cuhe_bfv_key*> keys(ops.size(), key);
   for (size_t k = 0; k < ops.size(); ++k) c1[k] = ops[k].perm + n * W;
   if (int rc = native_switch(r, ln, d, c1, keys, res, ks_all, d_sops, small)) return rc;
-  k_native_finish<<<grid, 256, 0, ln.stream>>>(d_ops, d);
+  if (accumulate) k_native_finish<true><<<grid, 256, 0, ln.stream>>>(d_ops, d);
+  else k_native_finish<false><<<grid, 256, 0, ln.stream>>>(d_ops, d);
   BFV_CUDA(cudaGetLastError(), "rotation finish");
   return CUHE_OK;
 }
@@ -1041,12 +1042,13 @@ int native_tile_circuit(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* qw, c
       if (int rc = words_addsub(r, ln, d, dist, n, dist, n, dist, n, ct * 2, 0)) return rc;
       continue;
     }
+    // the finish adds the rotation into dist in place
     std::vector<NativeOp> ops(ct);
     for (size_t k = 0; k < ct; ++k)
-      ops[k] = NativeOp{dist + k * 2 * n * W, s.perm + k * 2 * n * W, s.tmp + k * 2 * n * W, nullptr};
-    if (int rc = native_rotate(r, ln, d, ops, unsigned(exps[e]), keys[e], s.d_nops, s.ksres, s.ksw, s.d_sops))
+      ops[k] = NativeOp{dist + k * 2 * n * W, s.perm + k * 2 * n * W, dist + k * 2 * n * W, nullptr};
+    if (int rc = native_rotate(r, ln, d, ops, unsigned(exps[e]), keys[e], s.d_nops, s.ksres, s.ksw, s.d_sops,
+                               nullptr, true))
       return rc;
-    if (int rc = words_addsub(r, ln, d, dist, n, s.tmp, n, dist, n, ct * 2, 0)) return rc;
   }
   cudaEventRecord(ev[3], ln.stream);
   std::vector<const u64*> pm(ct * 2);
