@@ -523,7 +523,7 @@ def run_bfv(steps: int, warmup: int, cpu: bool, native: bool = False) -> dict:
     mac_bytes = switches * (6 * L * BFV_N * 8 + 2 * 6 * L * BFV_N * 8 + 2 * L * BFV_N * 8)
     out_roofline = {
         "bound": "imad",
-        "kernel": "whole search (k_keyswitch_tm<3>, the key switch, ~75% of device time)",
+        "kernel": "whole search (k_keyswitch_tm<3, 16>, the key switch, ~78% of the search kernel time in the ncu launch list)",
         "transforms_per_query": fwd + inv, "butterflies_per_query": butterflies,
         "achieved": butterflies * 10 / step_s / 1e12, "peak": imad / 1e12, "unit": "Twp/s",
         "frac": butterflies * 10 / step_s / imad,
