@@ -58,6 +58,8 @@ BFV_SIGNATURES: dict[str, tuple] = {
     "cuhe_bfv_batch_encode": (ctypes.c_int, [_vp, ctypes.c_uint64, _vp, ctypes.c_uint64, _vp]),
     "cuhe_bfv_encrypt": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint64, _vp, _vp, _vp, ctypes.c_uint64,
                                         _vp]),
+    "cuhe_bfv_encrypt_keyed": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_uint64, _vp, ctypes.c_char_p,
+                                              ctypes.c_char_p, ctypes.c_uint, ctypes.c_uint64, _vp]),
     "cuhe_bfv_packed_search_parts": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p),
                                                     ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _vp,
                                                     ctypes.c_uint64, _u64p]),
@@ -87,6 +89,14 @@ def _check(rc: int) -> None:
     if rc == -2:
         raise MemoryError(text)
     raise RuntimeError(text)
+
+
+CUHE_RANGE = -5
+
+
+class KeystreamRejected(ValueError):
+    """A keyed noise draw met eight bytes of 255 for one coefficient
+    (probability 2^-64): encrypt again under a new key."""
 
 
 class _Handle:
@@ -452,6 +462,37 @@ def encrypt_packed(ring: Ring, public_key: Any, t: int, slots, u, e) -> list[tup
     out = np.empty(max(1, count * 2 * size), dtype=np.uint8)  # filled by the call: no zeroing
     _check(lib().cuhe_bfv_encrypt(ring.ptr, pk, int(t), slots.ctypes.data, u.ctypes.data, e.ctypes.data, count,
                                   out.ctypes.data))
+    view = memoryview(out)
+    return [(bytes(view[2 * i * size:(2 * i + 1) * size]), bytes(view[(2 * i + 1) * size:(2 * i + 2) * size]))
+            for i in range(count)]
+
+
+def encrypt_packed_keyed(ring: Ring, public_key: Any, t: int, slots, key: bytes, nonce: bytes,
+                         eta: int = 21) -> list[tuple[bytes, bytes]]:
+    """encrypt_packed with the noise drawn on the device from the ChaCha20
+    keystream of (key, nonce) (layout: cuhe_bfv_encrypt_keyed).  Raises
+    KeystreamRejected in the 2^-64-per-coefficient case that needs a new
+    key."""
+    import numpy as np
+
+    ring = _get(ring, Ring)
+    if not isinstance(public_key, tuple) or len(public_key) != 2:
+        raise ValueError("public key must be (b, a)")
+    if len(key) != 32 or len(nonce) != 12:
+        raise ValueError("key must be 32 bytes and nonce 12 bytes")
+    pk = b"".join(_poly(p, ring) for p in public_key)
+    slots = np.ascontiguousarray(slots, dtype=np.uint32)
+    count = slots.shape[0] if slots.ndim == 2 else -1
+    if slots.shape != (count, ring.n):
+        raise ValueError("slots must be [count, N]")
+    size = (ring.n * ring.q_bits + 7) // 8
+    out = np.empty(max(1, count * 2 * size), dtype=np.uint8)
+    rc = lib().cuhe_bfv_encrypt_keyed(ring.ptr, pk, int(t), slots.ctypes.data, bytes(key), bytes(nonce), int(eta),
+                                      count, out.ctypes.data)
+    if rc == CUHE_RANGE:
+        message = lib().cuhe_bfv_last_error()
+        raise KeystreamRejected(message.decode() if message else "keystream draw rejected")
+    _check(rc)
     view = memoryview(out)
     return [(bytes(view[2 * i * size:(2 * i + 1) * size]), bytes(view[(2 * i + 1) * size:(2 * i + 2) * size]))
             for i in range(count)]

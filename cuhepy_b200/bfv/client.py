@@ -4,9 +4,12 @@ The reference's client encrypts one plaintext at a time in Python
 (``BFV.encrypt``, src/cuhepy/bfv/scheme.py:426-444, with the batch encoding
 of scheme.py:371-394): u ternary, e0 and e1 centred binomial with ``eta``
 bits per side, c0 = b u + e0 + floor(Q/t) m and c1 = a u + e1.  Here the
-noise is drawn on the host and every ring product, the batch encoding and
-the wire packing run on the GPU for the whole batch (``cuhe_bfv_encrypt``).
-Given the same draws, the ciphertexts are the reference's.
+noise is drawn on the GPU from a ChaCha20 keystream keyed from the operating
+system's CSPRNG (``cuhe_bfv_encrypt_keyed``), or, with a seeded ``rng``, on
+the host one draw at a time in the reference's order
+(``cuhe_bfv_encrypt``); every ring product, the batch encoding and the wire
+packing run on the GPU for the whole batch.  Given the same draws, the
+ciphertexts are the reference's.
 """
 
 from __future__ import annotations
@@ -76,5 +79,23 @@ def encrypt_batch(ring, public_key: tuple, t: int, slots, eta: int = 21, rng: An
     slots = np.ascontiguousarray(slots, dtype=np.uint32)
     if slots.ndim != 2:
         raise ValueError("slots must be [count, N]")
-    u, e = draw_noise(slots.shape[0], slots.shape[1], eta, rng)
-    return _bfv_rns.encrypt_packed(ring, public_key, t, slots, u, e)
+    if rng is not None:
+        u, e = draw_noise(slots.shape[0], slots.shape[1], eta, rng)
+        return _bfv_rns.encrypt_packed(ring, public_key, t, slots, u, e)
+    if not 1 <= eta <= 63:
+        raise ValueError("eta must be 1..63")
+    n = slots.shape[1]
+    blocks = (n // 4 if eta <= 31 else n // 2) + n // 8  # keystream blocks per ciphertext
+    per_key = max(1, (1 << 32) // max(1, blocks))
+    out: list[tuple[bytes, bytes]] = []
+    for first in range(0, slots.shape[0], per_key):
+        part = slots[first:first + per_key]
+        for attempt in range(4):
+            try:
+                out += _bfv_rns.encrypt_packed_keyed(ring, public_key, t, part, secrets.token_bytes(32),
+                                                     secrets.token_bytes(12), eta)
+                break
+            except _bfv_rns.KeystreamRejected:
+                if attempt == 3:
+                    raise
+    return out

@@ -1855,6 +1855,98 @@ __global__ void k_scatter_slots(const uint32_t* __restrict__ slots, const int32_
   planes[c * n + perm[j]] = v;
 }
 
+// ---- client noise from a ChaCha20 keystream (RFC 8439 block function) ----------
+// State: the constant "expand 32-byte k", the key (8 little-endian words), a
+// 32-bit block counter and the nonce (3 words); 20 rounds (10 column +
+// diagonal double rounds) of the quarter round, then the input added back.
+__device__ __forceinline__ uint32_t rotl32(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
+__device__ __forceinline__ void chacha_quarter(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d) {
+  a += b; d ^= a; d = rotl32(d, 16);
+  c += d; b ^= c; b = rotl32(b, 12);
+  a += b; d ^= a; d = rotl32(d, 8);
+  c += d; b ^= c; b = rotl32(b, 7);
+}
+__device__ __forceinline__ void chacha20_block(const uint32_t (&key)[8], uint32_t counter, const uint32_t (&nonce)[3],
+                                               uint32_t (&out)[16]) {
+  uint32_t x[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u, key[0], key[1], key[2], key[3],
+                    key[4],      key[5],      key[6],      key[7],      counter, nonce[0], nonce[1], nonce[2]};
+  uint32_t s[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s[k] = x[k];
+#pragma unroll 1
+  for (int r = 0; r < 10; ++r) {
+    chacha_quarter(x[0], x[4], x[8], x[12]);
+    chacha_quarter(x[1], x[5], x[9], x[13]);
+    chacha_quarter(x[2], x[6], x[10], x[14]);
+    chacha_quarter(x[3], x[7], x[11], x[15]);
+    chacha_quarter(x[0], x[5], x[10], x[15]);
+    chacha_quarter(x[1], x[6], x[11], x[12]);
+    chacha_quarter(x[2], x[7], x[8], x[13]);
+    chacha_quarter(x[3], x[4], x[9], x[14]);
+  }
+#pragma unroll
+  for (int k = 0; k < 16; ++k) out[k] = x[k] + s[k];
+}
+
+struct NoiseKey {
+  uint32_t key[8];
+  uint32_t nonce[3];
+  uint32_t eta;              // e = popcount of an eta-bit word minus another's
+  uint64_t first_ct;         // ciphertext index of the batch's first row
+  uint32_t blocks_per_ct;    // e blocks, then u blocks
+  uint32_t e_blocks;
+};
+
+// One thread per 64-byte keystream block of ciphertext (first_ct + row):
+// counter = (first_ct + row) * blocks_per_ct + b.  Blocks [0, e_blocks)
+// give e: words of 4 bytes (eta <= 31) or 8 bytes, in pairs, pair v giving
+// e[row][v / N][v % N] = popcount(w0 & mask) - popcount(w1 & mask).  The
+// remaining N / 8 blocks give u: 8 bytes per coefficient, u = (first byte
+// below 255) % 3 - 1; eight bytes of 255 (probability 2^-64) set *status.
+__global__ void k_keyed_noise(NoiseKey nk, long long rows, int n, int8_t* __restrict__ u, int8_t* __restrict__ e,
+                              int* __restrict__ status) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= rows * nk.blocks_per_ct) return;
+  const long long row = idx / nk.blocks_per_ct;
+  const uint32_t b = uint32_t(idx % nk.blocks_per_ct);
+  uint32_t w[16];
+  chacha20_block(nk.key, uint32_t((nk.first_ct + row) * nk.blocks_per_ct + b), nk.nonce, w);
+  if (b < nk.e_blocks) {
+    int8_t* er = e + row * 2 * n;
+    if (nk.eta <= 31) {
+      const uint32_t mask = (1u << nk.eta) - 1u;
+#pragma unroll
+      for (int v = 0; v < 8; ++v)
+        er[b * 8 + v] = int8_t(__popc(w[2 * v] & mask) - __popc(w[2 * v + 1] & mask));
+    } else {
+      const uint64_t mask = (uint64_t(1) << nk.eta) - 1u;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const uint64_t w0 = uint64_t(w[4 * v]) | (uint64_t(w[4 * v + 1]) << 32);
+        const uint64_t w1 = uint64_t(w[4 * v + 2]) | (uint64_t(w[4 * v + 3]) << 32);
+        er[b * 4 + v] = int8_t(__popcll(w0 & mask) - __popcll(w1 & mask));
+      }
+    }
+    return;
+  }
+  int8_t* ur = u + row * n;
+  const uint32_t ub = b - nk.e_blocks;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    int chosen = -1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t byte = (w[2 * v + (k >> 2)] >> (8 * (k & 3))) & 0xffu;
+      if (chosen < 0 && byte < 255u) chosen = int(byte);
+    }
+    if (chosen < 0) {
+      atomicOr(status, 2);
+      chosen = 1;
+    }
+    ur[ub * 8 + v] = int8_t(chosen % 3 - 1);
+  }
+}
+
 // out[poly][j][i] = v mod p_j for signed small v (u, e): residues mod the
 // first L primes.
 __global__ void k_small_residues(const int8_t* __restrict__ v, long long polys, int L, u64* __restrict__ out,

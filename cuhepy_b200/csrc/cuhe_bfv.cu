@@ -2391,16 +2391,24 @@ int cuhe_bfv_batch_encode(cuhe_bfv_ring* r, uint64_t t, const uint32_t* slots, u
   return CUHE_OK;
 }
 
-int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
-                     const int8_t* e, uint64_t count, uint8_t* out) {
-  if (!r || !pk || (count && (!slots || !u || !e || !out))) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+}  // extern "C"
+
+namespace {
+
+// Public-key encryption with the noise either from the caller (u, e) or,
+// with `keyed`, drawn on the device from a ChaCha20 keystream.
+int encrypt_impl(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
+                 const int8_t* e, const NoiseKey* keyed, uint64_t count, uint8_t* out) {
+  if (!r || !pk || (count && (!slots || (!keyed && (!u || !e)) || !out)))
+    return fail(CUHE_INVALID_ARGUMENT, "null argument");
   if (!r->residue) return fail(CUHE_INVALID_ARGUMENT, "client encryption needs a residue ring");
   if (count == 0) return CUHE_OK;
   const auto& P = r->plan;
   const size_t n = P.n, L = P.residue_count, W = size_t(r->host_dev.words);
   const size_t in_bytes = (n * P.q_bits + 7) / 8;
-  for (uint64_t k = 0; k < count * n; ++k)
-    if (u[k] < -1 || u[k] > 1) return fail(CUHE_INVALID_ARGUMENT, "u must be ternary");
+  if (!keyed)
+    for (uint64_t k = 0; k < count * n; ++k)
+      if (u[k] < -1 || u[k] > 1) return fail(CUHE_INVALID_ARGUMENT, "u must be ternary");
   std::vector<u64> pk_words;
   if (int rc = parse_polys(r, pk, 2, pk_words)) return rc;
   Lane& ln = *r->lanes[0];
@@ -2450,8 +2458,16 @@ int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint
   for (size_t c0 = 0; c0 < size_t(count); c0 += chunk) {
     const size_t cc = std::min(chunk, size_t(count) - c0);
     BFV_CUDA(cudaMemcpyAsync(d_slots, slots + c0 * n, cc * n * 4, cudaMemcpyHostToDevice, ln.stream), "slots");
-    BFV_CUDA(cudaMemcpyAsync(d_u, u + c0 * n, cc * n, cudaMemcpyHostToDevice, ln.stream), "u");
-    BFV_CUDA(cudaMemcpyAsync(d_e, e + c0 * 2 * n, cc * 2 * n, cudaMemcpyHostToDevice, ln.stream), "e");
+    if (keyed) {
+      NoiseKey nk = *keyed;
+      nk.first_ct += c0;
+      k_keyed_noise<<<blocks_for((long long)(cc * nk.blocks_per_ct), 256), 256, 0, ln.stream>>>(
+          nk, (long long)cc, int(n), d_u, d_e, d_status);
+      BFV_CUDA(cudaGetLastError(), "keyed noise");
+    } else {
+      BFV_CUDA(cudaMemcpyAsync(d_u, u + c0 * n, cc * n, cudaMemcpyHostToDevice, ln.stream), "u");
+      BFV_CUDA(cudaMemcpyAsync(d_e, e + c0 * 2 * n, cc * 2 * n, cudaMemcpyHostToDevice, ln.stream), "e");
+    }
     // batch encoding: m = INTT_t(scattered slots)
     k_scatter_slots<<<blocks_for((long long)(cc * n), 256), 256, 0, ln.stream>>>(d_slots, pr.d_perm, (long long)cc,
                                                                                  int(n), uint32_t(t), m, d_status);
@@ -2482,13 +2498,45 @@ int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint
                              packed, cc * 2 * out_words * 8, cudaMemcpyDeviceToHost, ln.stream),
              "download");
     BFV_CUDA(cudaStreamSynchronize(ln.stream), "encrypt");
-    if (status) return fail(CUHE_INVALID_ARGUMENT, "slot value not below the plaintext modulus");
+    if (status & 1) return fail(CUHE_INVALID_ARGUMENT, "slot value not below the plaintext modulus");
+    if (status & 2) return fail(CUHE_RANGE, "keystream draw rejected (eight bytes of 255): encrypt again with a new key");
     if (!direct)
       for (size_t k = 0; k < cc * 2; ++k)
         std::memcpy(out + (c0 * 2 + k) * in_bytes, reinterpret_cast<const uint8_t*>(host.get() + k * out_words),
                     in_bytes);
   }
   return CUHE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cuhe_bfv_encrypt(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
+                     const int8_t* e, uint64_t count, uint8_t* out) {
+  return encrypt_impl(r, pk, t, slots, u, e, nullptr, count, out);
+}
+
+int cuhe_bfv_encrypt_keyed(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t* slots,
+                           const uint8_t* key, const uint8_t* nonce, unsigned eta, uint64_t count, uint8_t* out) {
+  if (!r || !key || !nonce) return fail(CUHE_INVALID_ARGUMENT, "null argument");
+  if (eta < 1 || eta > 63) return fail(CUHE_INVALID_ARGUMENT, "eta must be 1..63");
+  const uint64_t n = r->plan.n;
+  if (n % 8) return fail(CUHE_INVALID_ARGUMENT, "ring degree must be a multiple of 8");
+  NoiseKey nk{};
+  for (int k = 0; k < 8; ++k)
+    nk.key[k] = uint32_t(key[4 * k]) | uint32_t(key[4 * k + 1]) << 8 | uint32_t(key[4 * k + 2]) << 16 |
+                uint32_t(key[4 * k + 3]) << 24;
+  for (int k = 0; k < 3; ++k)
+    nk.nonce[k] = uint32_t(nonce[4 * k]) | uint32_t(nonce[4 * k + 1]) << 8 | uint32_t(nonce[4 * k + 2]) << 16 |
+                  uint32_t(nonce[4 * k + 3]) << 24;
+  nk.eta = eta;
+  nk.first_ct = 0;
+  nk.e_blocks = uint32_t(eta <= 31 ? n / 4 : n / 2);
+  nk.blocks_per_ct = nk.e_blocks + uint32_t(n / 8);
+  if (count > (uint64_t(1) << 32) / nk.blocks_per_ct)
+    return fail(CUHE_INVALID_ARGUMENT, "too many ciphertexts for one key: the 32-bit block counter would wrap");
+  return encrypt_impl(r, pk, t, slots, nullptr, nullptr, &nk, count, out);
 }
 
 }  // extern "C"

@@ -147,6 +147,25 @@ int cuhe_bfv_batch_encode(cuhe_bfv_ring* ring, uint64_t t, const uint32_t* slots
 int cuhe_bfv_encrypt(cuhe_bfv_ring* ring, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
                      const int8_t* e, uint64_t count, uint8_t* out);
 
+/* The same encryption with the noise drawn on the device from a ChaCha20
+ * keystream (RFC 8439 block function) under `key` (32 bytes) and `nonce`
+ * (12 bytes), which the caller takes from a cryptographic generator and never
+ * reuses.  The distributions are the reference's (bfv/scheme.py:236-246):
+ * u uniform on {-1, 0, 1}, each e the difference of the popcounts of two
+ * independent eta-bit words (eta 1..63).  Ciphertext c of the call uses the
+ * keystream blocks with counters c * B .. c * B + B - 1, B = E + N/8:
+ *   blocks [0, E), E = N/4 (eta <= 31) or N/2: the e words, little-endian,
+ *     4 bytes each (eta <= 31) or 8, in pairs; pair v gives
+ *     e[c][v / N][v % N] = popcount(w0 & mask) - popcount(w1 & mask);
+ *   blocks [E, B): 8 bytes per coefficient i, u[c][i] = (first byte below
+ *     255) % 3 - 1.
+ * Eight bytes of 255 (probability 2^-64 per coefficient) return CUHE_RANGE:
+ * encrypt again with a new key.  count * B must not exceed 2^32.  Replaces
+ * the host-side draws of bfv/scheme.py:236-246 feeding BFV.encrypt
+ * (scheme.py:426-444). */
+int cuhe_bfv_encrypt_keyed(cuhe_bfv_ring* ring, const uint8_t* pk, uint64_t t, const uint32_t* slots,
+                           const uint8_t* key, const uint8_t* nonce, unsigned eta, uint64_t count, uint8_t* out);
+
 /* Execution lanes of a ring (1..8; 1 after create_ring).  Each lane is a
  * CUDA stream with its own device workspace.  packed_search / search_index
  * calls issued concurrently from several host threads take free lanes and

@@ -94,3 +94,48 @@ def test_gpu_batch_encode_matches_the_oracle(n):
         assert [int(c) for c in coeffs] == ob.batch_encode(row, n, t)
     with pytest.raises(ValueError):
         m.batch_encode(ring, 65539, np.array(rows[:1], dtype=np.uint32))  # 65539 != 1 mod 2N
+
+
+def _keystream_noise(key, nonce, count, n, eta):
+    """The keyed draws of cuhe_bfv_encrypt_keyed rebuilt on the host from the
+    `cryptography` package's ChaCha20 (16-byte nonce = 32-bit little-endian
+    block counter, then the 12-byte nonce)."""
+    from cryptography.hazmat.primitives.ciphers import Cipher, algorithms
+
+    e_blocks = n // 4 if eta <= 31 else n // 2
+    blocks = e_blocks + n // 8
+    wide = np.uint32 if eta <= 31 else np.uint64
+    mask = wide((1 << eta) - 1)
+    u = np.empty((count, n), dtype=np.int8)
+    e = np.empty((count, 2, n), dtype=np.int8)
+    for c in range(count):
+        counter = (c * blocks).to_bytes(4, "little")
+        stream = Cipher(algorithms.ChaCha20(key, counter + nonce), mode=None).encryptor().update(bytes(64 * blocks))
+        words = np.frombuffer(stream[:64 * e_blocks], dtype=wide) & mask
+        pops = np.bitwise_count(words).astype(np.int16).reshape(2 * n, 2)
+        e[c] = (pops[:, 0] - pops[:, 1]).astype(np.int8).reshape(2, n)
+        raw = np.frombuffer(stream[64 * e_blocks:], dtype=np.uint8).reshape(n, 8)
+        first = np.argmax(raw < 255, axis=1)
+        assert (raw < 255).any(axis=1).all()
+        u[c] = (raw[np.arange(n), first] % 3).astype(np.int8) - 1
+    return u, e
+
+
+@pytest.mark.parametrize("n,eta", [(256, 21), (256, 40), (8192, 21)])
+def test_keyed_device_noise_is_the_documented_chacha20_draw(n, eta):
+    """cuhe_bfv_encrypt_keyed equals cuhe_bfv_encrypt given the noise rebuilt
+    on the host from the same key and nonce: the device keystream and the
+    noise derivation are exact."""
+    from cuhepy_b200.bfv import _bfv_rns as m
+
+    params = ob.Params(n, 65537, 180, 30, eta)
+    q, t = params.q, params.t
+    ring = m.create_ring(n, format(q, "x"), params.gadget_bits, True, True, 2)
+    r = random.Random(n + eta)
+    pk = tuple(fixed([r.randrange(q) for _ in range(n)], q) for _ in range(2))  # any (b, a) below q
+    count = 3
+    slots = np.array([[r.randrange(t) for _ in range(n)] for _ in range(count)], dtype=np.uint32)
+    key, nonce = bytes(range(32)), bytes(range(100, 112))
+    u, e = _keystream_noise(key, nonce, count, n, eta)
+    assert set(np.unique(u)) <= {-1, 0, 1} and np.abs(e).max() <= eta
+    assert m.encrypt_packed_keyed(ring, pk, t, slots, key, nonce, eta) == m.encrypt_packed(ring, pk, t, slots, u, e)
