@@ -2493,17 +2493,34 @@ int encrypt_impl(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t
     int status = 0;
     BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
     // packed polys that fill whole words go straight to the caller's buffer
+    // packed polys that fill whole words move through the lane's pinned
+    // staging (full-speed DMA) and then to the caller's buffer on several
+    // host threads
     const bool direct = out_words * 8 == in_bytes;
-    BFV_CUDA(cudaMemcpyAsync(direct ? static_cast<void*>(out + c0 * 2 * in_bytes) : static_cast<void*>(host.get()),
-                             packed, cc * 2 * out_words * 8, cudaMemcpyDeviceToHost, ln.stream),
+    const size_t down = cc * 2 * out_words * 8;
+    if (direct && ln.host_cap < down) {
+      if (ln.host_stage) cudaFreeHost(ln.host_stage);
+      ln.host_stage = nullptr;
+      ln.host_cap = 0;
+      BFV_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ln.host_stage), down, cudaHostAllocDefault), "pinned");
+      ln.host_cap = down;
+    }
+    BFV_CUDA(cudaMemcpyAsync(direct ? static_cast<void*>(ln.host_stage) : static_cast<void*>(host.get()), packed,
+                             down, cudaMemcpyDeviceToHost, ln.stream),
              "download");
     BFV_CUDA(cudaStreamSynchronize(ln.stream), "encrypt");
     if (status & 1) return fail(CUHE_INVALID_ARGUMENT, "slot value not below the plaintext modulus");
     if (status & 2) return fail(CUHE_RANGE, "keystream draw rejected (eight bytes of 255): encrypt again with a new key");
-    if (!direct)
+    if (direct) {
+      PolySource staged;
+      staged.contiguous = ln.host_stage;
+      staged.poly_bytes = in_bytes;
+      copy_polys(staged, 0, cc * 2, out + c0 * 2 * in_bytes, 8, 21);
+    } else {
       for (size_t k = 0; k < cc * 2; ++k)
         std::memcpy(out + (c0 * 2 + k) * in_bytes, reinterpret_cast<const uint8_t*>(host.get() + k * out_words),
                     in_bytes);
+    }
   }
   return CUHE_OK;
 }
