@@ -91,6 +91,18 @@ def modexp_count(index: int, queries: int) -> int:
     return index + queries + queries * index
 
 
+def knn_config() -> dict:
+    """The workload both arms report (the device arm and --impl reference)."""
+    return {
+        "workload": WORKLOAD,
+        "key_len": KEY_LEN, "n_squared_bits": 4 * KEY_LEN, "alpha_len": ALPHA_LEN,
+        "embed_len": EMBED_LEN, "index_vectors_per_gpu": INDEX_VECTORS, "queries_per_step": QUERY_BATCH,
+        "modexps_per_step_per_gpu": modexp_count(INDEX_VECTORS, QUERY_BATCH),
+        "server_products_per_step_per_gpu": QUERY_BATCH * INDEX_VECTORS,
+        "l2": "flushed (256 MB write) before every timed step",
+    }
+
+
 # ---------------------------------------------------------------------------
 # clocks sampling (nvidia-smi in the background during the timed region)
 # ---------------------------------------------------------------------------
@@ -343,15 +355,8 @@ def run_gpu(args) -> dict | None:
         "vs_baseline": None,
         "dtype": "u32",
         "data": "synthetic: Bernoulli(0.5) 512-bit embeddings (seed 1337+rank), keys from a seeded generator",
-        "config": {
-            "workload": WORKLOAD,
-            "key_len": KEY_LEN, "n_squared_bits": 4 * KEY_LEN, "alpha_len": ALPHA_LEN,
-            "embed_len": EMBED_LEN, "index_vectors_per_gpu": INDEX_VECTORS, "queries_per_step": QUERY_BATCH,
-            "modexps_per_step_per_gpu": modexp_count(INDEX_VECTORS, QUERY_BATCH),
-            "server_products_per_step_per_gpu": QUERY_BATCH * INDEX_VECTORS,
-            "l2": "flushed (256 MB write) before every timed step",
-            "tuning": {"threads_per_instance": ctx.tuning()[0], "window": ctx.tuning()[1]},
-        },
+        "config": knn_config(),
+        "tuning": {"threads_per_instance": ctx.tuning()[0], "window": ctx.tuning()[1]},
         "stage_ms": {name: statistics.mean(v) for name, v in kernel_ms.items()},
         "decode_direct_ms": statistics.mean(direct_ms),
         "decode_direct": "the same decode batch on k_modexp (c^a mod n^2, no CRT), outside the timed steps",
@@ -396,9 +401,43 @@ def run_gpu(args) -> dict | None:
         result["serving"] = run_serving()
     if cpu:
         result["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        attach_bfv_cpu_baselines(result)
+    for name in ("bfv", "bfv_native"):
+        if name in result:
+            result[name].pop("_setup", None)
+    if "bfv" in result:
+        result["bfv_summary"] = bfv_summary(result)
     if dist:
         dist.destroy_process_group()
     return result
+
+
+def attach_bfv_cpu_baselines(result: dict) -> None:
+    setups = {name: result[name].pop("_setup") for name in ("bfv", "bfv_native")
+              if name in result and "_setup" in result[name]}
+    if setups:
+        for name, base in bfv_cpu_baseline(setups).items():
+            result[name]["cpu_baseline"] = base
+
+
+def bfv_summary(result: dict) -> dict:
+    """The BFV half of the metric, compact, for the end of the JSON line."""
+    out = {"metric": "BFV kNN queries/s, 16,384 x 512-bit index at N=8192 (1,024 tiles, 2 compacted responses)"}
+    for name in ("bfv", "bfv_native"):
+        sec = result.get(name)
+        if not sec:
+            continue
+        roof = sec["roofline"]
+        base = sec.get("cpu_baseline") or {}
+        out[name] = {
+            "ring": "Q = 3 x 60-bit primes" if name == "bfv" else "q = largest prime below 2^180",
+            "value": sec["value"], "unit": "queries/s", "p50_ms": sec["p50_ms"], "p99_ms": sec["p99_ms"],
+            "e2e": sec["e2e"]["value"], "plain_value": sec["plain_value"],
+            "roofline": {k: roof[k] for k in ("bound", "achieved", "peak", "unit", "frac", "peak_nominal",
+                                               "frac_of_nominal") if k in roof},
+            "cpu_baseline": {k: base[k] for k in ("value", "cores", "kind", "query_s") if k in base},
+        }
+    return out
 
 
 BFV_N, BFV_Q_BITS, BFV_GADGET, BFV_T, BFV_EMBED = 8192, 180, 30, 65537, 512
@@ -465,10 +504,12 @@ def run_bfv(steps: int, warmup: int, cpu: bool, native: bool = False) -> dict:
     for _ in range(warmup):
         m.search_index(server, resident, query, BFV_VECTORS, True)
     times = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        resp = m.search_index(server, resident, query, BFV_VECTORS, True)
-        times.append(time.perf_counter() - t0)
+    with ClockSampler(0) as clocks:
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            resp = m.search_index(server, resident, query, BFV_VECTORS, True)
+            times.append(time.perf_counter() - t0)
+    clock = clocks.summary()
     _, prof = m.profile_packed_search(server, query, index, BFV_VECTORS, True)
     e2e_t = []
     for _ in range(max(1, min(steps, 2))):
@@ -521,12 +562,18 @@ def run_bfv(steps: int, warmup: int, cpu: bool, native: bool = False) -> dict:
     switches = tiles * 10 + merges
     ntt_bytes = (fwd + inv) * 16 * BFV_N                               # u64 read + write per transform
     mac_bytes = switches * (6 * L * BFV_N * 8 + 2 * 6 * L * BFV_N * 8 + 2 * L * BFV_N * 8)
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    nominal = sms * 64 * (clock.get("sm_mhz") or 1965.0) * 1e6 / 2
     out_roofline = {
         "bound": "imad",
         "kernel": "whole search (k_keyswitch_tm<3, 16>, the key switch, ~78% of the search kernel time in the ncu launch list)",
         "transforms_per_query": fwd + inv, "butterflies_per_query": butterflies,
         "achieved": butterflies * 10 / step_s / 1e12, "peak": imad / 1e12, "unit": "Twp/s",
         "frac": butterflies * 10 / step_s / imad,
+        "peak_nominal": nominal / 1e12, "frac_of_nominal": butterflies * 10 / step_s / nominal,
+        "peak_nominal_source": "SMs x 64 IMAD/clk x median SM clock during the timed searches / 2 IMAD per word product",
         "work_per_unit": "10 word products per 60-bit Shoup butterfly, (N/2) log2 N butterflies per transform",
         "hbm_effective_gbs": (ntt_bytes + mac_bytes) / step_s / 1e9,
         "hbm_frac": (ntt_bytes + mac_bytes) / step_s / 1e9 / hbm_peak,
@@ -548,13 +595,14 @@ def run_bfv(steps: int, warmup: int, cpu: bool, native: bool = False) -> dict:
         "plain_value": 1.0 / (per_tile * tiles),
         "plain": "one hamming_tile call per tile (merge tree not included)",
         "tiles": tiles,
+        "clocks": clock,
         "data": "seeded uniform keys and ciphertexts (evaluation work is value-independent)",
     }
     if native:
         out["roofline"]["kernel"] = "whole search (key switches, transforms and Garner reductions)"
         out["primes"] = {"tensor": len(info["primes"]), "switch": info["switch_prime_count"]}
     if cpu:
-        out["cpu_baseline"] = bfv_cpu_baseline(q, layout, exps, keys, query, index, target, native=native)
+        out["_setup"] = (q, layout, exps, keys, query, index, target, native)
     return out
 
 
@@ -569,11 +617,17 @@ def native_mask_primes(primes, q: int, n: int, t: int) -> int:
     raise ValueError("not enough auxiliary primes")
 
 
-def bfv_cpu_baseline(q, layout, exps, keys, query, index, target, sample_tiles: int = 2,
-                     native: bool = False) -> dict:
-    """The reference's own compiled _bfv_rns (oracle/_ref) on the host cores:
-    one search of `sample_tiles` tiles per thread (the module releases the GIL),
-    extrapolated linearly to the 1,024-tile query."""
+def bfv_cpu_baseline(setups: dict, native_tiles: int = 256) -> dict:
+    """The reference's own compiled _bfv_rns (oracle/_ref, GMP 6.3.0) on the
+    host cores, each thread running one query (the module releases the GIL),
+    the rings given an equal share of the cores and run side by side.  The
+    residue ring runs whole 1,024-tile queries (tile circuits, merge tree,
+    compaction, wire export: ResidueServer::search, bfv_residue.h:225-241).
+    The native ring's reference search is about three times slower (GMP
+    products per tile), so each of its threads runs the first `native_tiles`
+    tiles (a partial response group with its merge tree) and the query time
+    is scaled by tiles.  `setups` maps a section name to
+    (q, layout, exps, keys, query, index, target, native)."""
     from concurrent.futures import ThreadPoolExecutor
 
     sys.path.insert(0, str(REPO / "tests"))
@@ -581,30 +635,41 @@ def bfv_cpu_baseline(q, layout, exps, keys, query, index, target, sample_tiles: 
 
     ref = reference_native()
     if ref is None:
-        return {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
-                "sample": "oracle/_ref not built on this machine"}
-    ring = ref.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, not native, 0 if native else 2)
-    relin = ref.compile_key(ring, keys[0])
-    galois = tuple((g, ref.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
-    server = ref.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
-    sample = index[:sample_tiles]
-    count = sample_tiles * layout.capacity
-    ref.packed_search(server, query, sample, count, True)
+        return {name: {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference",
+                       "sample": "oracle/_ref not built on this machine"} for name in setups}
     cores = len(os.sched_getaffinity(0))
-    t0 = time.perf_counter()
-    ref.packed_search(server, query, sample, count, True)
-    single = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(cores) as pool:
-        list(pool.map(lambda _: ref.packed_search(server, query, sample, count, True), range(cores)))
-    multi = time.perf_counter() - t0
-    tiles = len(index)
-    per_query_1 = single / sample_tiles * tiles
-    per_query_all = multi / (cores * sample_tiles) * tiles
-    return {"value": 1.0 / per_query_all, "unit": "queries/s", "cores": cores, "kind": "reference",
-            "single_thread_value": 1.0 / per_query_1,
-            "sample": f"reference _bfv_rns.packed_search (oracle/_ref, GMP 6.3.0) over {sample_tiles} tiles "
-                      f"per thread on {cores} threads, extrapolated to {tiles} tiles"}
+    per_ring = max(1, min(8, cores // len(setups)))
+    servers = {}
+    for name, (q, layout, exps, keys, query, index, target, native) in setups.items():
+        ring = ref.create_ring(BFV_N, format(q, "x"), BFV_GADGET, True, not native, 0 if native else 2)
+        relin = ref.compile_key(ring, keys[0])
+        galois = tuple((g, ref.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
+        tiles = native_tiles if native else len(index)
+        servers[name] = (ref.create_server(relin, galois, layout.padded, BFV_T, format(target, "x")), query,
+                         index[:tiles], len(index))
+
+    def one(name):
+        server, query, index, _ = servers[name]
+        t0 = time.perf_counter()
+        ref.packed_search(server, query, index, len(index) * BFV_VECTORS // servers[name][3], True)
+        return name, time.perf_counter() - t0
+
+    jobs = [name for _ in range(per_ring) for name in setups]
+    with ThreadPoolExecutor(len(jobs)) as pool:
+        results = list(pool.map(one, jobs))
+    out = {}
+    for name in setups:
+        times = [t for n, t in results if n == name]
+        ran, tiles = len(servers[name][2]), servers[name][3]
+        scale = tiles / ran
+        what = (f"whole {tiles}-tile queries" if ran == tiles else
+                f"{ran}-tile searches (of the {tiles}-tile query, scaled by tiles)")
+        out[name] = {"value": len(times) / (max(times) * scale), "unit": "queries/s", "cores": len(times),
+                     "kind": "reference", "query_s": statistics.mean(times) * scale,
+                     "sample": f"{len(times)} {what}, merge tree and compaction included, one per thread, "
+                               f"reference _bfv_rns.packed_search (oracle/_ref) on {len(times)} of {cores} host "
+                               f"cores beside the other ring's {len(jobs) - len(times)}"}
+    return out
 
 
 def ctypes_imad_peak(native, device: int) -> float:
@@ -635,6 +700,10 @@ def ncu_traffic(items: int) -> float:
 # CPU baseline / reference arm: the oracle port on the host cores
 # ---------------------------------------------------------------------------
 def _cpu_worker(payload):
+    """One host process of the CPU arms: the kNN step's own mix, one index
+    encryption per QUERY_BATCH decode pipelines (server product, c^a
+    decryption, odd-bit count), as in the device step (65,552 encryptions
+    and 1,048,576 decodes), repeated until the time budget is spent."""
     sys.path.insert(0, str(REPO))
     from oracle import paillier as oracle
 
@@ -642,27 +711,23 @@ def _cpu_worker(payload):
     pk = keys["pk"]
     chunks = len(table)
     rng = random.Random(len(vectors))
-    done = 0
-    t0 = time.perf_counter()
-    cts = []
-    for bits in vectors:
-        (m,) = oracle.encode_bits(bits, KEY_LEN)
-        idx = [rng.randrange(256) for _ in range(14)]
-        cts.append(oracle.lookup_encrypt(m, pk, table, noise, idx, chunks))
-        done += 1
-        if time.perf_counter() - t0 > seconds / 2:
-            break
     (qm,) = oracle.encode_bits(qvec, KEY_LEN)
     q = oracle.lookup_encrypt(qm, pk, table, noise, [1] * 14, chunks)
-    done += 1
+    encrypted = decoded = 0
+    t0 = time.perf_counter()
     i = 0
-    while time.perf_counter() - t0 < seconds:
-        prod = oracle.add(q, cts[i % len(cts)], pk["n_squared"])
-        d = oracle.lookup_decrypt(prod, keys)
-        oracle.decode_distance([d], KEY_LEN)
-        done += 1
+    while True:
+        (m,) = oracle.encode_bits(vectors[i % len(vectors)], KEY_LEN)
+        ct = oracle.lookup_encrypt(m, pk, table, noise, [rng.randrange(256) for _ in range(14)], chunks)
+        encrypted += 1
+        for _ in range(QUERY_BATCH):
+            prod = oracle.add(q, ct, pk["n_squared"])
+            oracle.decode_distance([oracle.lookup_decrypt(prod, keys)], KEY_LEN)
+            decoded += 1
         i += 1
-    return done, time.perf_counter() - t0
+        if time.perf_counter() - t0 >= seconds:
+            break
+    return encrypted + decoded, time.perf_counter() - t0
 
 
 def seeded_lookup_keys_cpu(seed: int = 0) -> dict:
@@ -721,9 +786,10 @@ def cpu_baseline(seconds: float = 20.0) -> dict:
     done = sum(r[0] for r in results)
     wall = max(r[1] for r in results)
     _ = oracle
-    return {"value": done / wall, "unit": "modexp/s", "cores": cores, "kind": "port",
-            "sample": f"{done} modexps (lookup encryptions + server product/decrypt/decode per distance) "
-                      f"over {wall:.1f} s on {cores} processes; oracle/paillier.py over GMP 6.3.0 powm"}
+    return {"value": done / wall, "unit": "modexp/s", "cores": cores, "kind": "port", "wall_s": wall,
+            "sample": f"{done} modexps in the device step's mix (1 index encryption per {QUERY_BATCH} "
+                      f"product+decrypt+decode) over {wall:.1f} s on {cores} processes; oracle/paillier.py, "
+                      f"GMP 6.3.0 powm"}
 
 
 def run_reference(args) -> dict | None:
@@ -735,17 +801,23 @@ def run_reference(args) -> dict | None:
         base = cpu_baseline(max(2.0, args.cpu_seconds / max(1, args.steps)))
         per_step.append(base)
     timed = per_step[args.warmup:]
-    value = statistics.mean(b["value"] for b in timed)
+    done = sum(b["value"] * b["wall_s"] for b in timed)
+    wall = sum(b["wall_s"] for b in timed)
+    value = done / wall
     last = timed[-1]
     return {
         "impl": "reference",
         "metric": "modexp/s mod n^2 (Paillier-Lookup kNN, key_len=1024: n^2 4096-bit)",
         "value": value, "unit": "modexp/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "key_len": KEY_LEN, "alpha_len": ALPHA_LEN, "embed_len": EMBED_LEN},
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * modexp_count(INDEX_VECTORS, QUERY_BATCH) / value,
+        "ms_per_step_note": "time one full step's modexps would take at the sampled rate",
+        "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: Bernoulli(0.5) 512-bit embeddings (seed 1337+rank), keys from a seeded generator",
+        "config": knn_config(),
         "cpu_baseline": {"value": value, "unit": "modexp/s", "cores": last["cores"], "kind": "port",
-                         "sample": last["sample"]},
+                         "sample": last["sample"] + f"; {len(timed)} timed steps of {last['wall_s']:.1f} s"},
         "e2e": {"value": value, "unit": "modexp/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -1231,10 +1303,17 @@ def profile_case(which: str) -> None:
         relin = m.compile_key(ring, keys[0])
         galois = tuple((g, m.compile_key(ring, keys[1 + i])) for i, g in enumerate(exps))
         server = m.create_server(relin, galois, layout.padded, BFV_T, format(target, "x"))
-        small = index[:64]
-        resident = m.upload_index(server, small)
-        for _ in range(2):
-            m.search_index(server, resident, query, 64 * layout.capacity, True)
+        if which == "bfv_full":
+            # the timed configuration itself: one search of the resident
+            # 1,024-tile index (two halves of 512 tiles, 1,536-CTA key-switch
+            # launches, about 2 GB on the device)
+            resident = m.upload_index(server, index)
+            m.search_index(server, resident, query, BFV_VECTORS, True)
+        else:
+            small = index[:64]
+            resident = m.upload_index(server, small)
+            for _ in range(2):
+                m.search_index(server, resident, query, 64 * layout.capacity, True)
         print("bfv profile case done")
 
 
@@ -1258,7 +1337,7 @@ def main() -> None:
     parser.add_argument("--no-client", action="store_true", help="skip the BFV client encryption section")
     parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
-    parser.add_argument("--profile-case", choices=["paillier", "bfv", "bfv_native"],
+    parser.add_argument("--profile-case", choices=["paillier", "bfv", "bfv_full", "bfv_native"],
                         help="run one small step of a hot kernel (for ncu captures) and exit")
     args = parser.parse_args()
     if args.profile_case:
@@ -1270,12 +1349,13 @@ def main() -> None:
     if args.client_only:
         print(json.dumps({"client": run_client()}))
         return
-    if args.bfv_only:
-        print(json.dumps({"bfv": run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline)}))
-        return
-    if args.bfv_native_only:
-        print(json.dumps({"bfv_native": run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline,
-                                                native=True)}))
+    if args.bfv_only or args.bfv_native_only:
+        name = "bfv" if args.bfv_only else "bfv_native"
+        out = {name: run_bfv(max(3, args.steps), args.warmup, cpu=not args.no_cpu_baseline,
+                             native=args.bfv_native_only)}
+        if not args.no_cpu_baseline:
+            attach_bfv_cpu_baselines(out)
+        print(json.dumps(out))
         return
     if args.textbook_only:
         print(json.dumps({"textbook": [run_textbook(512), run_textbook(1024),

@@ -2448,6 +2448,17 @@ int encrypt_impl(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t
   u64* packed = ln.arena.take<u64>(chunk * 2 * out_words);
   ComposeOp* d_cops = ln.arena.take<ComposeOp>(chunk * 2);
   BFV_ARENA(ln.arena);
+  // The client's secrets (message slots, u, e, the encoded message, NTT(u))
+  // do not outlive the call in the lane's arena: cleared on every return.
+  struct Wipe {
+    cudaStream_t stream;
+    std::pair<void*, size_t> spans[5];
+    ~Wipe() {
+      for (const auto& s : spans) cudaMemsetAsync(s.first, 0, s.second, stream);
+      cudaStreamSynchronize(stream);
+    }
+  } wipe{ln.stream, {{d_slots, chunk * n * 4}, {d_u, chunk * n}, {d_e, chunk * 2 * n}, {m, chunk * n * 8},
+                     {u_ntt, chunk * L * n * 8}}};
   BFV_CUDA(cudaMemcpyAsync(pk_w, pk_words.data(), pk_words.size() * 8, cudaMemcpyHostToDevice, ln.stream), "pk");
   BFV_CUDA(cudaMemcpyAsync(d_delta, delta.data(), L * 8, cudaMemcpyHostToDevice, ln.stream), "delta");
   BFV_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), ln.stream), "status");
@@ -2492,7 +2503,6 @@ int encrypt_impl(cuhe_bfv_ring* r, const uint8_t* pk, uint64_t t, const uint32_t
     BFV_CUDA(cudaGetLastError(), "pack");
     int status = 0;
     BFV_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, ln.stream), "status");
-    // packed polys that fill whole words go straight to the caller's buffer
     // packed polys that fill whole words move through the lane's pinned
     // staging (full-speed DMA) and then to the caller's buffer on several
     // host threads

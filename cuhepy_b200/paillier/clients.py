@@ -54,6 +54,51 @@ def _as_int(value) -> int:
     return int(value)
 
 
+def _ciphertexts(values, n_squared: int) -> list[int]:
+    """Ciphertext operands as the reference's bigint_to_mem takes them
+    (paillier_GPU_lookup_client.cu:525-533): any value of the context's
+    width, reduced mod n^2 here (every kernel result depends on c mod n^2
+    only); wider values are rejected with the reference's message."""
+    limit = 1 << (32 * max(1, (n_squared.bit_length() + 31) // 32))
+    out = []
+    for v in values:
+        c = _as_int(v)
+        if not 0 <= c < limit:
+            raise RuntimeError("bigint_to_mem: value does not fit in mem_t")
+        out.append(c % n_squared)
+    return out
+
+
+def _g_table_from_py(obj, message_chunks: int) -> dict[int, list[int]]:
+    """g_table_from_py (paillier_GPU_lookup_client.cu:1377-1426): a dict keyed
+    by row number (int or str) or a sequence of exactly message_chunks rows,
+    each of 256 entries; rows past message_chunks in a dict are ignored."""
+    if obj is None:
+        return {}
+
+    def row(values) -> list[int]:
+        values = list(values)
+        if len(values) != 256:
+            raise RuntimeError("g_table row length mismatch")
+        return [_as_int(v) for v in values]
+
+    if isinstance(obj, dict):
+        out = {}
+        for i in range(message_chunks):
+            if i in obj:
+                out[i] = row(obj[i])
+            elif str(i) in obj:
+                out[i] = row(obj[str(i)])
+            else:
+                raise RuntimeError("g_table missing row")
+        return out
+    if isinstance(obj, Sequence) and not isinstance(obj, (str, bytes)):
+        if len(obj) != message_chunks:
+            raise RuntimeError("g_table outer length mismatch")
+        return {i: row(obj[i]) for i in range(message_chunks)}
+    raise RuntimeError("g_table must be dict or sequence")
+
+
 class PaillierGPULookupClient:
     """Paillier-Lookup client whose arithmetic runs on the B200."""
 
@@ -93,12 +138,25 @@ class PaillierGPULookupClient:
         return device_for(int(keys["pk"]["n"]), (int(keys["sk"]["a"]), int(keys["sk"]["g_a_inv"])),
                           phi=keys["sk"].get("phi"))
 
+    def _table_fingerprint(self) -> tuple:
+        keys = self._need_keys("tables")
+        rows, noise = keys.get("g_table") or {}, keys.get("noise_table") or []
+        if not rows or not noise:
+            return ()
+        last = rows[self.message_chunks - 1]
+        return (self.message_chunks, len(noise), int(rows[0][1]), int(last[1]), int(last[255]),
+                int(noise[0]), int(noise[-1]))
+
     def _install_tables(self) -> None:
+        """Put this client's tables on its device context.  Contexts are
+        shared by key, so the installed tables carry a fingerprint and a
+        client whose tables differ reinstalls its own before encrypting."""
         keys = self._need_keys("tables")
         ctx = self._ctx()
         rows = [keys["g_table"][i] for i in range(self.message_chunks)]
         if rows and keys["noise_table"]:
             ctx.set_tables(rows, keys["noise_table"])
+            ctx._client_tables = self._table_fingerprint()
 
     def _ensure_tables(self) -> None:
         keys = self._need_keys("tables")
@@ -109,7 +167,7 @@ class PaillierGPULookupClient:
             keys["noise_table"] = PaillierLookup.precompute_noise_table(keys["pk"]["g"], keys["pk"]["n"])
             keys["message_chunks"] = chunks
         ctx = self._ctx()
-        if ctx.tables != (self.message_chunks, len(keys["noise_table"])):
+        if getattr(ctx, "_client_tables", None) != self._table_fingerprint():
             self._install_tables()
 
     # -- encryption -------------------------------------------------------
@@ -129,16 +187,19 @@ class PaillierGPULookupClient:
         return self._ctx().lookup_encrypt_bits(bits, self._chunk_len, self._chunk_num, noise_index)
 
     def encrypt_cts(self, plaintexts: Sequence[int], noise_index: np.ndarray | None = None) -> list[int]:
-        self._need_keys("encrypt_cts")
+        keys = self._need_keys("encrypt_cts")
         self._ensure_tables()
         values = [_as_int(v) for v in plaintexts]
+        n = int(keys["pk"]["n"])
+        if any(not 0 <= v < n for v in values):
+            raise RuntimeError("encrypt_cts: plaintext out of range [0, n)")
         if noise_index is None:
             noise_index = self._noise_indices(len(values))
         return self._ctx().lookup_encrypt_ints(values, noise_index)
 
     def decrypt_cts(self, ciphers: Sequence[int]) -> list[int]:
-        self._need_keys("decrypt_cts")
-        return self._ctx().decrypt([_as_int(c) for c in ciphers])
+        keys = self._need_keys("decrypt_cts")
+        return self._ctx().decrypt(_ciphertexts(ciphers, int(keys["pk"]["n_squared"])))
 
     def decrypt_then_reencrypt(self, ciphers: Sequence[int], key_a: dict, key_b: dict) -> list[int]:
         """paillier_GPU_lookup_client.cu:2134-2286: decrypt under key_a, re-encrypt under key_b."""
@@ -172,12 +233,13 @@ class PaillierGPULookupClient:
         return device_for(n).mulmod([_as_int(c) for c in ct1], [_as_int(c) for c in ct2])
 
     def decode_hamming_client(self, ciphers_batch: Sequence[Sequence[int]]) -> list[int]:
-        self._need_keys("decode_hamming_client")
+        keys = self._need_keys("decode_hamming_client")
+        n2 = int(keys["pk"]["n_squared"])
         rows = []
         for row in ciphers_batch:
             if len(row) != self._chunk_num:
                 raise RuntimeError("decode_hamming_client: each inner list must have length == chunk_num")
-            rows.append([_as_int(c) for c in row])
+            rows.append(_ciphertexts(row, n2))
         return self._ctx().decode_hamming(rows, self._chunk_num, self._chunk_len)
 
     # -- keys and configuration -------------------------------------------
@@ -224,7 +286,9 @@ class PaillierGPULookupClient:
         self.message_chunks = 0
 
     def load_config(self, config: dict, tables: dict | None = None) -> None:
-        keys = self._need_keys("load_config")
+        if self.keys is None:
+            raise RuntimeError("load_config: keys must be loaded first")
+        keys = self.keys
         key_len = int(config["key_len"])
         if key_len > KEY_BITS:
             raise RuntimeError(f"load_config: key_len={key_len} exceeds KEY_BITS={KEY_BITS}")
@@ -238,9 +302,8 @@ class PaillierGPULookupClient:
         if tables is not None:
             if not isinstance(tables, dict):
                 raise RuntimeError("load_config: tables must be a dict")
-            g_table, noise = PaillierLookup.load_tables(tables)
-            if g_table and len(g_table) * 256 != self.message_chunks * 256:
-                raise RuntimeError("load_config: g_table size mismatch")
+            g_table = _g_table_from_py(tables.get("g_table"), self.message_chunks)
+            noise = [_as_int(v) for v in (tables.get("noise_table") or [])]
             if noise and len(noise) != 256:
                 raise RuntimeError("load_config: noise_table size mismatch")
             keys["g_table"], keys["noise_table"] = g_table, noise
@@ -308,7 +371,7 @@ class PaillierGPUClient:
     @staticmethod
     def encode_hamming_server(ct1: Sequence[str], ct2: Sequence[str], pk: dict) -> list[str]:
         if len(ct1) != len(ct2):
-            raise RuntimeError("encode_hamming_server: ct1 and ct2 must have the same length")
+            raise RuntimeError("encode_hamming_*: ct1 and ct2 must have the same length")
         n2 = int(str(pk["n_squared"]), 16)
         n = math.isqrt(n2)
         if n * n != n2:

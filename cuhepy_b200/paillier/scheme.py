@@ -5,8 +5,10 @@ the same key dictionaries, the same ``ValueError`` range checks and the same
 randomness rule for r (``secrets.randbelow(n-1)+1`` until gcd(r, n) = 1,
 scheme.py:47-60).  ``encrypt``/``decrypt``/``add`` each run one kernel launch
 (the per-operation form); the ``*_batch`` methods run a whole batch in one
-launch.  Encryption uses g^m = 1 + m*n mod n^2, which equals the reference's
-powmod(g, m, n^2) for g = n + 1, the only generator ``key_gen`` produces.
+launch.  For g = n + 1, the generator ``key_gen`` produces, encryption uses
+g^m = 1 + m*n mod n^2 inside the r^n kernel; keys with any other g (loaded
+from elsewhere) take g^m by a per-item exponentiation and one product, so
+every g the reference accepts gives the reference's powmod(g, m, n^2) * r^n.
 """
 
 from __future__ import annotations
@@ -17,11 +19,6 @@ from collections.abc import Sequence
 
 from cuhepy_b200 import _numbers
 from cuhepy_b200.paillier.gpu import device_for
-
-
-def _check_generator(pk: dict) -> None:
-    if int(pk["g"]) != int(pk["n"]) + 1:
-        raise ValueError("this implementation requires the Paillier generator g = n + 1")
 
 
 class Paillier:
@@ -56,7 +53,6 @@ class Paillier:
     @staticmethod
     def encrypt_batch(plaintexts: Sequence[int], pk: dict, rs: Sequence[int] | None = None) -> list[int]:
         """Batched encryption; r values are drawn like the reference unless given."""
-        _check_generator(pk)
         n = int(pk["n"])
         for m in plaintexts:
             if not 0 <= int(m) < n:
@@ -66,7 +62,14 @@ class Paillier:
         for r in rs:
             if math.gcd(int(r), n) != 1:
                 raise ValueError("random r is not coprime with n")
-        return device_for(n).encrypt([int(m) for m in plaintexts], [int(r) for r in rs])
+        ctx = device_for(n)
+        ms, rs = [int(m) for m in plaintexts], [int(r) for r in rs]
+        g = int(pk["g"]) % (n * n)
+        if g == n + 1:
+            return ctx.encrypt(ms, rs)
+        # scheme.py:81-83 for a general g: powmod(g, m, n^2) * powmod(r, n, n^2)
+        r_n = ctx.encrypt([0] * len(ms), rs)
+        return ctx.mulmod(ctx.modexp_each([g] * len(ms), ms), r_n)
 
     @staticmethod
     def decrypt(ciphertext: int, keys: dict) -> int:

@@ -143,7 +143,9 @@ int cuhe_bfv_batch_encode(cuhe_bfv_ring* ring, uint64_t t, const uint32_t* slots
  * reference's slot order), u [count][N] ternary and e [count][2][N] signed
  * small noise drawn by the caller.  out receives count * 2 packed polys
  * (bits(Q) bits per coefficient, the packed_search wire), c0 then c1.
- * Residue rings only; t prime with t = 1 mod 2N. */
+ * Residue rings only; t prime with t = 1 mod 2N.  The device copies of the
+ * slots, u, e, the encoded message and NTT(u) are zeroed before the call
+ * returns (on success and on error). */
 int cuhe_bfv_encrypt(cuhe_bfv_ring* ring, const uint8_t* pk, uint64_t t, const uint32_t* slots, const int8_t* u,
                      const int8_t* e, uint64_t count, uint8_t* out);
 

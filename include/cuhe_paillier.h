@@ -101,10 +101,10 @@ int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t 
                                  int chunk_len, int64_t* distance);
 
 /* Allocation-free variant of cuhe_paillier_decode_hamming.  It has no
- * counterpart in the reference.  It is for callers that cannot allocate GPU
- * memory while they run: code inside a CUDA graph capture, and serving
- * processes whose device memory is owned by a caching allocator or a fixed
- * reservation.  cuhe_paillier_decode_hamming takes its per-chunk scratch from
+ * counterpart in the reference.  It is for callers that must not allocate GPU
+ * memory while they run: serving processes whose device memory is owned by a
+ * caching allocator or a fixed reservation, and runtimes that give the
+ * library only buffers they already own.  cuhe_paillier_decode_hamming takes its per-chunk scratch from
  * the context workspace, which cudaMalloc's on growth; this entry point instead
  * keeps that scratch in a file-scope device array of
  * CUHE_STATIC_DECODE_MAX_CHUNKS uint32 counts (256 KiB), which every GPU that
@@ -115,8 +115,9 @@ int cuhe_paillier_decode_hamming(cuhe_paillier* ctx, const uint32_t* c, int64_t 
  *  - vectors*chunk_num above CUHE_STATIC_DECODE_MAX_CHUNKS is rejected with
  *    CUHE_INVALID_ARGUMENT before anything is launched.
  *  - The first call on a device, with that device current, looks up the
- *    array's device address once (cudaGetSymbolAddress); make that first call
- *    before any stream capture.
+ *    array's device address once (cudaGetSymbolAddress) and keeps it for the
+ *    life of the process; make that first call before any stream capture.  A
+ *    device reset (cudaDeviceReset) after that first call is not supported.
  *  - Work is queued on the context stream and the call returns without waiting;
  *    range errors surface at the next cuhe_synchronize.
  *  - All calls in the process share the one array per device, so two calls

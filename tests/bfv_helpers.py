@@ -7,6 +7,8 @@ import random
 import sys
 from pathlib import Path
 
+import numpy as np
+
 from oracle import bfv as ob
 
 REPO = Path(__file__).resolve().parents[1]
@@ -63,6 +65,48 @@ def random_keys(n, q, digits, count, seed):
 
 def key_bytes(key, q):
     return tuple((fixed(b, q), fixed(a, q)) for b, a in key)
+
+
+def _below_q_bits(rng, rows, q):
+    """rows x bits(q) little-endian bit matrix of uniform draws, those at or
+    above q mapped below 2^(bits-1) by clearing their top bit."""
+    bits = q.bit_length()
+    x = rng.integers(0, 2, size=(rows, bits), dtype=np.uint8)
+    qb = np.array([(q >> i) & 1 for i in range(bits)], dtype=np.uint8)
+    rev = (x != qb)[:, ::-1]
+    first = rev.argmax(axis=1)
+    ge = ~rev.any(axis=1) | (x[:, ::-1][np.arange(rows), first] == 1)
+    x[ge, bits - 1] = 0
+    return x
+
+
+def random_fixed_poly(rng, n, q):
+    """One canonical polynomial (coefficients < q) as fixed-width bytes."""
+    bits = q.bit_length()
+    width = (bits + 7) // 8
+    x = _below_q_bits(rng, n, q)
+    padded = np.zeros((n, 8 * width), dtype=np.uint8)
+    padded[:, :bits] = x
+    return np.packbits(padded, axis=1, bitorder="little").tobytes()
+
+
+def random_packed_poly(rng, n, q):
+    """One canonical polynomial as the bit-packed wire (bits(q) per coefficient)."""
+    x = _below_q_bits(rng, n, q).reshape(-1)
+    return np.packbits(x, bitorder="little").tobytes()
+
+
+def with_head(poly, q, values):
+    """A packed polynomial with its first len(values) coefficients replaced."""
+    bits = q.bit_length()
+    count = len(values)
+    span = (count * bits + 7) // 8
+    head = int.from_bytes(poly[:span], "little")
+    keep = head >> (count * bits)
+    new = 0
+    for i, v in enumerate(values):
+        new |= int(v) << (i * bits)
+    return (new | (keep << (count * bits))).to_bytes(span, "little") + poly[span:]
 
 
 def regenerate_fixture(data):

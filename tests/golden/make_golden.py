@@ -2,7 +2,7 @@
 
 Run in a container where the reference project is present (read-only):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <reference tree>]   (default: $CUHEPY_REFERENCE)
 
 The reference's own Python package is imported unmodified.  Its missing
 third-party wheels are replaced by the test-only shims in tests/golden/shims
@@ -20,6 +20,7 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import os
 import random
 import sys
 from pathlib import Path
@@ -231,7 +232,7 @@ def bfv_fixture(bfv_scheme, n: int, t: int, bits: int, gadget: int, embed_len: i
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference", type=Path)
+    parser.add_argument("--reference", default=os.environ.get("CUHEPY_REFERENCE") or "/root/reference", type=Path)
     parser.add_argument("--only", default="")
     args = parser.parse_args()
     scheme, lookup, bfv_scheme, number = setup(args.reference)

@@ -90,6 +90,27 @@ def test_textbook_static_api_uses_reference_randomness(monkeypatch):
         scheme.Paillier.decrypt(pk["n_squared"], keys)
 
 
+def test_textbook_general_generator_vs_oracle():
+    """Keys with g != n + 1 (loaded from elsewhere): the reference encrypts as
+    powmod(g, m, n^2) * powmod(r, n, n^2) for any g (scheme.py:79-83), and so
+    does Paillier.encrypt_batch; decryption depends on phi and inv only."""
+    from cuhepy_b200.paillier import scheme
+
+    data = load_golden("paillier_512.json")
+    pk, keys = _keys(data)
+    n, n2 = pk["n"], pk["n_squared"]
+    rng = random.Random(31)
+    ms = [rng.randrange(n) for _ in range(40)] + [0, 1, n - 1]
+    rs = [rng.randrange(1, n) for _ in ms]
+    for g in (pow(n + 1, 3, n2), rng.randrange(2, n2), n + 1 + n2):
+        gpk = dict(pk, g=g)
+        assert scheme.Paillier.encrypt_batch(ms, gpk, rs) == [oracle.encrypt(m, r, dict(pk, g=g % n2))
+                                                              for m, r in zip(ms, rs)]
+    # g = (n+1)^3 is a valid generator: decrypt(encrypt(m)) = 3 m mod n with the g = n + 1 secret
+    cs = scheme.Paillier.encrypt_batch(ms, dict(pk, g=pow(n + 1, 3, n2)), rs)
+    assert scheme.Paillier.decrypt_batch(cs, keys) == [3 * m % n for m in ms]
+
+
 def test_textbook_random_batch_and_edges_vs_oracle():
     data = load_golden("paillier_1024.json")
     pk, keys = _keys(data)
