@@ -1069,22 +1069,27 @@ def run_mixed(steps: int = 5, seed: int = 5) -> dict:
         ntts += 64 * limbs
     tune = mb.autotune(reps=1)
     mb.capture()
-    stream = torch.cuda.current_stream()
     for _ in range(2):
         mb.replay()
     torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
+    mb.run_plain()
+    torch.cuda.synchronize()
+    # both forms on the same clock: host wall time per repetition, the device
+    # drained before and after each (graph: one replay; plain: one launch
+    # per operation, each waited for)
+    graph_s, plain_s = [], []
     for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         mb.replay()
-    b.record(stream)
-    b.synchronize()
-    graph_ms = a.elapsed_time(b) / steps
-    mb.check()
-    t0 = time.perf_counter()
-    for _ in range(steps):
+        torch.cuda.synchronize()
+        graph_s.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
         mb.run_plain()
-    plain_ms = (time.perf_counter() - t0) * 1e3 / steps
+        torch.cuda.synchronize()
+        plain_s.append(time.perf_counter() - t0)
+    mb.check()
+    graph_ms, plain_ms = 1e3 * statistics.median(graph_s), 1e3 * statistics.median(plain_s)
     widths = mb.widths()
     mb.close()
     return {
@@ -1098,8 +1103,8 @@ def run_mixed(steps: int = 5, seed: int = 5) -> dict:
         "autotune": {"paillier": {str(k): v["best"] for k, v in tune["paillier"].items()},
                      "ntt": {str(k): {"threads": v["best"][0], "radix": 1 << v["best"][1]}
                              for k, v in tune["ntt"].items()}},
-        "note": "graph time: CUDA events around replays; plain: host wall clock around per-op launches, "
-                "each waited for",
+        "note": "both forms timed by the host clock per repetition (median of the alternating runs), the "
+                "device drained before and after each; widths of the graph run on forked streams",
     }
 
 
@@ -1267,14 +1272,15 @@ def profile_case(which: str) -> None:
     larger than L2 where the kernel streams memory, a few GB at most)."""
     import torch
 
-    if which == "paillier":
+    if which in ("paillier", "paillier_int"):
         from cuhepy_b200.paillier.gpu import PaillierDevice
 
-        keys = seeded_lookup_keys(0)  # k_modexp_crt serves only the decodes
+        keys = seeded_lookup_keys(0)  # k_modexp_crt52 (k_modexp_crt: paillier_int) serves only the decodes
         pk, sk = keys["pk"], keys["sk"]
         ctx = PaillierDevice(pk["n"])
         ctx.set_secret(sk["a"], sk["g_a_inv"])
         ctx.set_factors(*factors_from_phi(pk["n"], sk["phi"]))
+        ctx.set_fp64(which == "paillier")
         ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
         stream = torch.cuda.Stream()
         ctx.set_stream(stream.cuda_stream)
@@ -1337,7 +1343,7 @@ def main() -> None:
     parser.add_argument("--no-client", action="store_true", help="skip the BFV client encryption section")
     parser.add_argument("--no-textbook", action="store_true", help="skip the plain Paillier section")
     parser.add_argument("--no-mixed", action="store_true", help="skip the mixed-batch section")
-    parser.add_argument("--profile-case", choices=["paillier", "bfv", "bfv_full", "bfv_native"],
+    parser.add_argument("--profile-case", choices=["paillier", "paillier_int", "bfv", "bfv_full", "bfv_native"],
                         help="run one small step of a hot kernel (for ncu captures) and exit")
     args = parser.parse_args()
     if args.profile_case:

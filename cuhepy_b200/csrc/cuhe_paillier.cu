@@ -95,8 +95,10 @@ struct cuhe_paillier {
   int32_t* d_ops_sec = nullptr;
   int nops_sec = 0;
   uint32_t* d_crt = nullptr;  // CRT constant block, present once the factors are installed
+  double* d_crt52 = nullptr;  // per side: M and R52 mod M as 52-bit limbs (FP64-pipe CRT kernel)
   cuhe::CrtScalars cs{};
   bool have_factors = false;
+  bool fp64 = true;           // decrypt / decode exponentiations on the FP64 pipe where compiled
   uint32_t* d_gtab = nullptr;
   int message_chunks = 0;
   uint32_t* d_noise = nullptr;
@@ -168,6 +170,29 @@ cudaError_t launch_modexp_crt(cuhe_paillier* ctx, const uint32_t* base, uint32_t
   cuhe::k_modexp_crt<KH, TPI, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
       base, out, count, ctx->d_consts, ctx->ks, ctx->d_crt, ctx->cs, ctx->d_ops_sec, ctx->nops_sec, mode,
       pop_words, ctx->d_status);
+  return cudaGetLastError();
+}
+
+// The same with both exponentiations on the FP64 pipe (TPI = KH / 8 lanes per side).
+template <int KH, int W>
+size_t modexp_crt52_smem() {
+  constexpr int TPI = KH / 8, K52 = 5 * TPI;
+  constexpr int IPB = cuhe::kBlockThreads / (2 * TPI);
+  return size_t(7 * 2 * KH) * 4 + size_t(K52 + IPB * 2 * (((1 << (W - 1)) + 1) * K52 + 2)) * 8;
+}
+
+template <int KH, int W>
+cudaError_t launch_modexp_crt52(cuhe_paillier* ctx, const uint32_t* base, uint32_t* out, long long count,
+                                int mode, int pop_words) {
+  constexpr int IPB = cuhe::kBlockThreads / (2 * (KH / 8));
+  const size_t smem = modexp_crt52_smem<KH, W>();
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp_crt52<KH, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_modexp_crt52<KH, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      base, out, count, ctx->d_consts, ctx->ks, ctx->d_crt, ctx->cs, ctx->d_crt52, ctx->d_ops_sec,
+      ctx->nops_sec, mode, pop_words, ctx->d_status);
   return cudaGetLastError();
 }
 
@@ -283,6 +308,7 @@ struct Dispatch {
                         int, int, int) = nullptr;
   cudaError_t (*modexp_var)(cuhe_paillier*, const uint32_t*, const uint32_t*, int, int, uint32_t*, long long) = nullptr;
   cudaError_t (*modexp_crt)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int, int) = nullptr;
+  cudaError_t (*modexp_crt52)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int, int) = nullptr;
   cudaError_t (*mulmod)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long) = nullptr;
   cudaError_t (*convert)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int) = nullptr;
   cudaError_t (*outer)(cuhe_paillier*, const uint32_t*, long long, const uint32_t*, long long, uint32_t*) = nullptr;
@@ -300,6 +326,7 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
     d->modexp = &launch_modexp<k, t, w>;                           \
     d->modexp_var = &launch_modexp_var<k, t>;                      \
     d->modexp_crt = &launch_modexp_crt<k / 2, t / 2, w>;           \
+    d->modexp_crt52 = t == k / 8 ? &launch_modexp_crt52<k / 2, w> : nullptr; \
     d->mulmod = &launch_mulmod<k, t>;                              \
     d->convert = &launch_convert<k, t>;                            \
     d->outer = &launch_outer<k, t>;                                \
@@ -318,6 +345,7 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
 // when the factorisation is installed, else the direct kernel mod n^2.
 cudaError_t secret_modexp(cuhe_paillier* ctx, const Dispatch& d, const uint32_t* base, uint32_t* out,
                           long long count, int mode, int pop_words) {
+  if (ctx->have_factors && ctx->fp64 && d.modexp_crt52) return d.modexp_crt52(ctx, base, out, count, mode, pop_words);
   if (ctx->have_factors) return d.modexp_crt(ctx, base, out, count, mode, pop_words);
   return d.modexp(ctx, base, nullptr, out, count, ctx->d_ops_sec, ctx->nops_sec, mode, pop_words);
 }
@@ -582,6 +610,7 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_ops_n);
   cudaFree(ctx->d_ops_sec);
   cudaFree(ctx->d_crt);
+  cudaFree(ctx->d_crt52);
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_noise);
   for (cudaStream_t st : {ctx->copy, ctx->side})
@@ -699,12 +728,33 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p_in, int p_wo
   auto put_half = [&](int row, int s, const Limbs& v) {
     std::memcpy(block.data() + size_t(row) * k + size_t(s) * kh, v.data(), 4 * kh);
   };
+  // FP64-pipe kernel: K52 = 5 (KH / 8) limbs of 52 bits per side, R52 = 2^(52 K52)
+  const size_t k52 = 5 * (kh / 8);
+  std::vector<double> block52(2 * 2 * k52, 0.0);
+  auto put52 = [&](int s, int row, const Limbs& v) {
+    for (size_t i = 0; i < k52; ++i) {
+      uint64_t limb = 0;
+      for (int b = 0; b < 52; ++b) {
+        const size_t bit = 52 * i + size_t(b);
+        if (bit / 32 < v.size() && ((v[bit / 32] >> (bit % 32)) & 1u)) limb |= 1ull << b;
+      }
+      block52[(size_t(s) * 2 + size_t(row)) * k52 + i] = double(limb);
+    }
+  };
   for (int s = 0; s < 2; ++s) {
     Limbs rm = cuhe::host::shift_mod(one, 32 * kh, side[s]);
     put_half(cuhe::CR_M, s, side[s]);
     put_half(cuhe::CR_RM, s, rm);
     put_half(cuhe::CR_R3, s, cuhe::host::shift_mod(rm, 64 * kh, side[s]));
+    put_half(cuhe::CR_R52, s, cuhe::host::shift_mod(one, 52 * k52 + 64 * kh, side[s]));
     ctx->cs.ninv[s] = 0u - cuhe::host::inv32(side[s][0]);
+    // -(M^-1) mod 2^52 by Newton's iteration on the low 64 bits of M
+    const uint64_t m0 = (uint64_t(side[s][1]) << 32) | side[s][0];
+    uint64_t inv = m0;
+    for (int it = 0; it < 6; ++it) inv *= 2 - m0 * inv;
+    ctx->cs.ninv52[s] = double((0 - inv) & ((1ull << 52) - 1));
+    put52(s, 0, side[s]);
+    put52(s, 1, cuhe::host::shift_mod(one, 52 * k52, side[s]));
   }
   put_half(cuhe::CR_H, 0, cuhe::host::shift_mod(qinv, 32 * kh, side[0]));
   Limbs cq = cuhe::host::shift_mod(cuhe::host::resized(side[1].data(), kh, k), 32 * k, ctx->n2);
@@ -713,11 +763,23 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p_in, int p_wo
   CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "synchronize before CRT constants upload");
   if (!ctx->d_crt) CUHE_CUDA(ctx, cudaMalloc(&ctx->d_crt, block.size() * 4), "CRT constants allocation");
   CUHE_CUDA(ctx, cudaMemcpy(ctx->d_crt, block.data(), block.size() * 4, cudaMemcpyHostToDevice), "CRT constants upload");
+  if (!ctx->d_crt52) CUHE_CUDA(ctx, cudaMalloc(&ctx->d_crt52, block52.size() * 8), "CRT constants allocation");
+  CUHE_CUDA(ctx, cudaMemcpy(ctx->d_crt52, block52.data(), block52.size() * 8, cudaMemcpyHostToDevice),
+            "CRT constants upload");
   ctx->have_factors = true;
   return CUHE_OK;
 }
 
 int cuhe_paillier_has_factors(const cuhe_paillier* ctx) { return ctx && ctx->have_factors ? 1 : 0; }
+
+int cuhe_paillier_set_fp64(cuhe_paillier* ctx, int enable) {
+  if (!ctx) return CUHE_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->fp64 = enable != 0;
+  return CUHE_OK;
+}
+
+int cuhe_paillier_get_fp64(const cuhe_paillier* ctx) { return ctx && ctx->fp64 ? 1 : 0; }
 
 int cuhe_paillier_encrypt(cuhe_paillier* ctx, const uint32_t* m, const uint32_t* r, uint32_t* c, int64_t count) {
   if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
@@ -1239,6 +1301,12 @@ struct cuhe_mix {
   int* d_status = nullptr;
   bool planned = false;
   std::string error;
+  // widths after the first run on their own streams, forked from and joined
+  // back to the launch stream, so that one width's last wave overlaps the
+  // next width's kernel (created by the plan: a launch allocates nothing)
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> done;
+  cudaEvent_t fork = nullptr;
 
   void release_plan() {
     for (auto& w : widths) {
@@ -1248,6 +1316,12 @@ struct cuhe_mix {
     widths.clear();
     cudaFree(d_counters);
     d_counters = nullptr;
+    for (cudaStream_t st : side) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : done) cudaEventDestroy(ev);
+    side.clear();
+    done.clear();
+    if (fork) cudaEventDestroy(fork);
+    fork = nullptr;
     planned = false;
   }
 };
@@ -1381,6 +1455,20 @@ int cuhe_mix_plan(cuhe_mix* mix) {
     cudaGetLastError();
     return mix_fail(mix, CUHE_OUT_OF_MEMORY, "counter allocation");
   }
+  if (mix->widths.size() > 1) {
+    if (cudaEventCreateWithFlags(&mix->fork, cudaEventDisableTiming) != cudaSuccess)
+      return mix_fail(mix, CUHE_CUDA_ERROR, "mixed launch events");
+    for (size_t i = 1; i < mix->widths.size(); ++i) {
+      cudaStream_t st = nullptr;
+      cudaEvent_t ev = nullptr;
+      if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        return mix_fail(mix, CUHE_CUDA_ERROR, "mixed launch streams");
+      mix->side.push_back(st);
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return mix_fail(mix, CUHE_CUDA_ERROR, "mixed launch events");
+      mix->done.push_back(ev);
+    }
+  }
   mix->planned = true;
   return CUHE_OK;
 }
@@ -1392,9 +1480,15 @@ int cuhe_mix_launch(cuhe_mix* mix, void* stream) {
   DeviceGuard guard(mix->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaMemsetAsync(mix->d_counters, 0, mix->widths.size() * sizeof(unsigned long long), s);
+  if (e == cudaSuccess && mix->fork) e = cudaEventRecord(mix->fork, s);
   for (size_t i = 0; i < mix->widths.size() && e == cudaSuccess; ++i) {
     const auto& w = mix->widths[i];
-    e = w.d.launch_tasks(w.d_tasks, w.ntasks, w.units, mix->d_counters + i, mix->d_status, w.grid, s);
+    cudaStream_t ws = i == 0 ? s : mix->side[i - 1];
+    if (i > 0) e = cudaStreamWaitEvent(ws, mix->fork, 0);
+    if (e == cudaSuccess)
+      e = w.d.launch_tasks(w.d_tasks, w.ntasks, w.units, mix->d_counters + i, mix->d_status, w.grid, ws);
+    if (e == cudaSuccess && i > 0) e = cudaEventRecord(mix->done[i - 1], ws);
+    if (e == cudaSuccess && i > 0) e = cudaStreamWaitEvent(s, mix->done[i - 1], 0);
   }
   if (e != cudaSuccess) return mix_fail(mix, CUHE_CUDA_ERROR, std::string("mixed launch: ") + cudaGetErrorString(e));
   return CUHE_OK;

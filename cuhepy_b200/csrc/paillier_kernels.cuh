@@ -6,6 +6,7 @@
 // routines with n zero-padded to K limbs.
 #pragma once
 #include <cstdint>
+#include "bigint52.cuh"
 #include "bigint_group.cuh"
 
 namespace cuhe {
@@ -32,11 +33,13 @@ enum CrtRow : int {
   CR_R3 = 2,   // R_h^3 mod p^2 | R_h^3 mod q^2
   CR_H = 3,    // (q^2)^-1 R_h mod p^2 | 0
   CR_CQ = 4,   // q^2 R mod n^2 (full row)
-  CR_ROWS = 5
+  CR_R52 = 5,  // R52 R_h^2 mod p^2 | R52 R_h^2 mod q^2, R52 = 2^(52 K52) (FP64-pipe kernel)
+  CR_ROWS = 6
 };
 
 struct CrtScalars {
-  uint32_t ninv[2];  // -(p^2)^-1, -(q^2)^-1 mod 2^32
+  uint32_t ninv[2];   // -(p^2)^-1, -(q^2)^-1 mod 2^32
+  double ninv52[2];   // -(p^2)^-1, -(q^2)^-1 mod 2^52 (exact doubles)
 };
 
 struct KeyScalars {
@@ -486,6 +489,194 @@ k_modexp_crt(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, long
   __syncwarp(g.mask);
   uint32_t* s_xp = s_item;
   uint32_t* s_xq = s_item + SIDE;
+  if (side == 0) {
+    // h = x_p (q^2)^-1 - x_q (q^2)^-1 mod p^2   (x_q may exceed p^2; x_q < R_h)
+    uint32_t xq[L], v[L], u[L];
+    h.load(xq, s_xq);
+    h.mont_mul(v, xs, s_h, m, ninv);
+    h.mont_mul(u, xq, s_h, m, ninv);
+    sub_mod<KH, TPI>(h, v, u, m);
+    __syncwarp(h.mask);
+    h.store(s_xp, v);
+  }
+  __syncwarp(g.mask);
+  // x = x_q + q^2 h over the whole group: side 0 lanes hold the low words
+  uint32_t hv[L], xq[L], x[L];
+  if (side == 0) {
+    h.load(hv, s_xp);
+    h.load(xq, s_xq);
+  } else {
+#pragma unroll
+    for (int j = 0; j < L; ++j) hv[j] = xq[j] = 0u;
+  }
+  uint32_t n2[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.mont_mul(x, hv, s_cq, n2, ks.ninv2);  // h q^2 mod n^2 = h q^2
+  (void)add_group<K, 2 * TPI>(g, x, xq);
+  decrypt_epilogue<K, 2 * TPI>(g, x, out, inst, consts, ks, s_one, s_r2n, s_multr, mode, pop_words);
+}
+
+// ---------------------------------------------------------------------------
+// The same CRT decrypt / decode with both exponentiations on the FP64 pipe.
+//
+// Per side the value mod M (p^2 or q^2, KH 32-bit words) is carried as
+// K52 = 5 TPI limbs of 52 bits, TPI = KH / 8 lanes (five limbs per lane),
+// in the Montgomery domain of R52 = 2^(52 K52) (cuhe52::Group52).  Entry and
+// exit stay in 32-bit words: c R_h^-1 by the 32-bit reduction as in
+// k_modexp_crt, then * (R52 R_h^2 mod M) gives c R52 mod M, which is
+// re-cut into 52-bit limbs through shared memory; the odd-power table and
+// the window schedule run as 52-bit Montgomery products; the result mod M
+// is re-cut into 32-bit words and the Garner recombination and epilogue of
+// k_modexp_crt follow unchanged, so the output equals k_modexp_crt's (and
+// the direct kernel's) for every c < n^2.
+// ---------------------------------------------------------------------------
+
+// limb i (52 bits at 52 i) of a little-endian array of nwords 32-bit words
+__device__ __forceinline__ uint64_t limb52_from_words(const uint32_t* w, int nwords, int i) {
+  const int bit = 52 * i, j = bit >> 5, off = bit & 31;
+  const uint64_t w0 = j < nwords ? w[j] : 0u;
+  const uint64_t w1 = j + 1 < nwords ? w[j + 1] : 0u;
+  const uint64_t w2 = j + 2 < nwords ? w[j + 2] : 0u;
+  uint64_t v = (w0 | (w1 << 32)) >> off;
+  if (off) v |= w2 << (64 - off);
+  return v & cuhe52::kMask;
+}
+
+// word i (32 bits at 32 i) of an array of nlimbs 52-bit limbs
+__device__ __forceinline__ uint32_t word_from_limbs52(const uint64_t* l, int nlimbs, int i) {
+  const int bit = 32 * i, j = bit / 52, off = bit - 52 * j;
+  const uint64_t l0 = j < nlimbs ? l[j] : 0u;
+  const uint64_t l1 = j + 1 < nlimbs ? l[j + 1] : 0u;
+  uint64_t v = l0 >> off;
+  if (off > 20) v |= l1 << (52 - off);
+  return uint32_t(v);
+}
+
+template <int KH, int W>
+__global__ void __launch_bounds__(kBlockThreads)
+k_modexp_crt52(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, long long count,
+               const uint32_t* __restrict__ consts, KeyScalars ks, const uint32_t* __restrict__ crt, CrtScalars cs,
+               const double* __restrict__ crt52, const int32_t* __restrict__ ops, int nops, int mode,
+               int pop_words, int* status) {
+  constexpr int K = 2 * KH;
+  constexpr int TPI = KH / 8;   // lanes per side
+  constexpr int L = 8;          // 32-bit words per lane and side
+  constexpr int K52 = 5 * TPI;  // 52-bit limbs per side
+  constexpr int L52 = 5;
+  static_assert(52 * K52 > 32 * KH + 1, "R52 must exceed 2 M");
+  constexpr int T = 1 << (W - 1);
+  constexpr int IPB = kBlockThreads / (2 * TPI);
+  constexpr int SIDE = (T + 1) * K52 + 2;  // doubles per side: x, then T odd powers; +2 moves the banks
+  extern __shared__ __align__(16) uint32_t smem[];
+  // block rows: ONE, R2N, MULTR (K words each), RM, R52, H (two halves), CQ; then 1 as K52 doubles
+  uint32_t* s_one = smem;
+  uint32_t* s_r2n = smem + K;
+  uint32_t* s_multr = smem + 2 * K;
+  uint32_t* s_rm = smem + 3 * K;
+  uint32_t* s_r52 = smem + 4 * K;
+  uint32_t* s_h = smem + 5 * K;
+  uint32_t* s_cq = smem + 6 * K;
+  double* s_one52 = reinterpret_cast<double*>(smem + 7 * K);
+  double* s_items = s_one52 + K52;
+  {
+    const int rows[3] = {C_ONE, C_R2N, C_MULTR};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 3);
+    const int crows[4] = {CR_RM, CR_R52, CR_H, CR_CQ};
+    copy_rows_to_smem<K, TPI>(smem + 3 * K, crt, crows, 4);
+    for (int i = threadIdx.x; i < K52; i += blockDim.x) s_one52[i] = i == 0 ? 1.0 : 0.0;
+  }
+  __syncthreads();
+
+  Group<K, 2 * TPI> g;            // the whole ciphertext, 32-bit words
+  Group<KH, TPI> h;               // this side's half, 32-bit words
+  cuhe52::Group52<K52, TPI> f;    // this side's half, 52-bit limbs
+  const int side = (threadIdx.x / TPI) & 1;
+  const int slot = threadIdx.x / (2 * TPI);
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;  // both halves leave together
+  double* s_x = s_items + (slot * 2 + side) * SIDE;
+  double* s_tab = s_x + K52;
+
+  {
+    uint32_t c[L], n2[L];
+    g.load_ro(n2, consts + C_N2 * K);
+    g.load(c, base + inst * K);
+    if (!g.less_than(c, n2)) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
+    }
+  }
+  const uint32_t ninv = cs.ninv[side];
+  uint32_t m[L], lo[L], hi[L], acc[L];
+  h.load_ro(m, crt + CR_M * K + side * KH);
+  h.load(lo, base + inst * K);
+  h.load(hi, base + inst * K + KH);
+  // c = lo + hi R_h:  (lo + hi * (R_h mod M)) R_h^-1 = c R_h^-1, then * R52 R_h^2 R_h^-1 = c R52
+  h.mont_mul_acc(acc, lo, hi, s_rm + side * KH, m, ninv);
+  h.mont_mul(acc, acc, s_r52 + side * KH, m, ninv);
+  uint32_t* s_w = reinterpret_cast<uint32_t*>(s_x);  // KH words fit in the K52 doubles of x
+  h.publish(s_w, acc);
+  double x52[L52], m52[L52], acc52[L52];
+  const double* cm = crt52 + side * 2 * K52;  // M, then R52 mod M
+#pragma unroll
+  for (int k = 0; k < L52; ++k) {
+    x52[k] = cuhe52::to_f64(limb52_from_words(s_w, KH, f.gl * L52 + k));
+    m52[k] = __ldg(cm + f.gl * L52 + k);
+  }
+  const double ninv52 = cs.ninv52[side];
+  f.publish(s_tab, x52);
+#pragma unroll
+  for (int k = 0; k < L52; ++k) acc52[k] = x52[k];
+  if (T > 1) {
+    double sq[L52];
+    f.mont_mul(sq, x52, s_tab, m52, ninv52);  // x^2 R52
+    f.publish(s_x, sq);
+#pragma unroll 1
+    for (int t = 1; t < T; ++t) {
+      f.mont_mul(acc52, acc52, s_x, m52, ninv52);
+      f.publish(s_tab + t * K52, acc52);
+    }
+  }
+  if (nops == 0) {
+#pragma unroll
+    for (int k = 0; k < L52; ++k) acc52[k] = __ldg(cm + K52 + f.gl * L52 + k);  // e = 0: R52 mod M
+  } else {
+    const int first = __ldg(ops) & 0xffff;
+    __syncwarp(f.mask);
+#pragma unroll
+    for (int k = 0; k < L52; ++k) acc52[k] = s_tab[(first - 1) * K52 + f.gl * L52 + k];
+  }
+  f.publish(s_x, acc52);
+#pragma unroll 1
+  for (int o = 1; o < nops; ++o) {
+    const int op = __ldg(ops + o);
+    const int sq = op >> 16;
+    const int idx = op & 0xffff;
+#pragma unroll 1
+    for (int s = 0; s < sq; ++s) {
+      f.mont_mul(acc52, acc52, s_x, m52, ninv52);
+      f.publish(s_x, acc52);
+    }
+    if (idx) {
+      f.mont_mul(acc52, acc52, s_tab + (idx - 1) * K52, m52, ninv52);
+      f.publish(s_x, acc52);
+    }
+  }
+  double xs52[L52];
+  f.mont_mul(xs52, acc52, s_one52, m52, ninv52);  // x_side, canonical
+  uint64_t* s_l = reinterpret_cast<uint64_t*>(s_x);
+  __syncwarp(f.mask);
+#pragma unroll
+  for (int k = 0; k < L52; ++k) s_l[f.gl * L52 + k] = cuhe52::to_u64(xs52[k]);
+  __syncwarp(f.mask);
+  uint32_t xs[L];
+#pragma unroll
+  for (int j = 0; j < L; ++j) xs[j] = word_from_limbs52(s_l, K52, h.gl * L + j);
+  __syncwarp(g.mask);
+  uint32_t* s_xp = reinterpret_cast<uint32_t*>(s_items + (slot * 2) * SIDE);
+  uint32_t* s_xq = reinterpret_cast<uint32_t*>(s_items + (slot * 2 + 1) * SIDE);
+  h.store(side == 0 ? s_xp : s_xq, xs);
+  __syncwarp(g.mask);
   if (side == 0) {
     // h = x_p (q^2)^-1 - x_q (q^2)^-1 mod p^2   (x_q may exceed p^2; x_q < R_h)
     uint32_t xq[L], v[L], u[L];

@@ -80,6 +80,18 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p, int p_words
 /* 1 when factors are installed (decrypt / decode use the CRT kernel). */
 int cuhe_paillier_has_factors(const cuhe_paillier* ctx);
 
+/* Pipe of the CRT exponentiations (on by default).  With enable != 0 and the
+ * factors installed, decrypt / decode run both half-width exponentiations as
+ * Montgomery products of 52-bit limbs on the FP64 pipe (three exact FP64
+ * instructions per 52x52-bit product, sums in 64-bit integers; the tunings
+ * with eight 32-bit words per lane and side), entering and leaving through
+ * the same 32-bit reduction, Garner recombination and epilogue, so results
+ * are identical to the integer-pipe kernel; enable = 0 keeps every product
+ * on the integer pipe.  No reference counterpart (the reference's CGBN
+ * kernels multiply 32-bit words on the integer pipe). */
+int cuhe_paillier_set_fp64(cuhe_paillier* ctx, int enable);
+int cuhe_paillier_get_fp64(const cuhe_paillier* ctx);
+
 /* c[i] = (1 + m[i]*n) * r[i]^n mod n^2, i.e. g^m r^n with g = n + 1.
  * Replaces Paillier.encrypt (src/cuhepy/paillier/scheme.py:63-83) with the
  * randomness r supplied by the caller, and the device half of
@@ -210,8 +222,11 @@ int cuhe_paillier_get_tuning(const cuhe_paillier* ctx, int* threads_per_instance
  * global counter until every batch is done, so small batches do not leave
  * the GPU idle between launches.  cuhe_mix_launch only enqueues work on the
  * given stream (no allocation, no synchronisation), so it can be captured
- * in a CUDA graph; cuhe_mix_plan (after the last add or tuning change)
- * builds the schedules and task tables and must run outside capture.
+ * in a CUDA graph; the kernels of the second and later widths run on the
+ * mix's own streams, forked from and joined back to the given stream, so a
+ * width's last wave overlaps the next width's kernel.  cuhe_mix_plan (after
+ * the last add or tuning change) builds the schedules, task tables and
+ * those streams and must run outside capture.
  * cuhe_mix_check waits for the device and reports range errors (a base not
  * below n^2).  Contexts and buffers must outlive the mix.  No counterpart in
  * the reference, which launches one kernel per call

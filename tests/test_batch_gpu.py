@@ -198,3 +198,42 @@ def test_autotune_keeps_results_and_range_errors_are_reported():
     bad.replay()
     with pytest.raises(ValueError):
         bad.check()
+
+
+def test_graph_replays_repeat_identically():
+    """Three widths on forked streams inside one graph: every replay gives
+    the same exponentiations, and the in-place NTT batches, restored between
+    replays, the same transforms."""
+    import torch
+
+    from cuhepy_b200.batch import MixedBatch
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    rng = random.Random(17)
+    ctxs = _keys()
+    n8192 = (1 << 4095) + 2 * rng.getrandbits(4000) + 1  # odd modulus of the 8192-bit n^2 width
+    ctxs.append(PaillierDevice(n8192))
+    mb = MixedBatch()
+    outs = []
+    for ctx, count, bits in ((ctxs[0], 900, 1024), (ctxs[2], 300, 2048), (ctxs[3], 40, 4096), (ctxs[1], 77, 280)):
+        _, bases = _bases(ctx, count, rng)
+        outs.append(mb.add_modexp(ctx, bases, rng.getrandbits(bits)))
+    ring, primes = _ring(8192, 3)
+    planes = _planes(8192, primes, 6, 23)
+    mb.add_ntt(ring, planes, 3)
+    assert [w["words"] for w in mb.widths()] == [64, 128, 256]
+    mb.capture()
+    first = None
+    for _ in range(4):
+        for out in outs:
+            out.zero_()
+        mb.restore_ntt_inputs()
+        mb.replay()
+        mb.check()
+        got = [out.clone() for out in outs] + [planes.clone()]
+        if first is None:
+            first = got
+        else:
+            assert all(torch.equal(a, b) for a, b in zip(got, first))
+    assert all(int(out.abs().sum()) > 0 for out in outs)
+    mb.close()

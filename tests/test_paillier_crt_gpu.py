@@ -118,6 +118,43 @@ def test_crt_matches_direct_on_a_large_device_batch():
     assert decoded == [oracle.lookup_decrypt(vals[i], keys) for i in sample]
 
 
+@pytest.mark.parametrize("name", ["paillier_512.json", "lookup_1024.json", "paillier_1024.json"])
+def test_fp64_pipe_equals_integer_pipe(name):
+    """The CRT exponentiations as 52-bit-limb products on the FP64 pipe give
+    the integer-pipe kernel's results, decrypt and decode, on ciphertexts
+    and on awkward values (several waves of a device batch)."""
+    import torch
+
+    data = load_golden(name)
+    pk, keys = _keys(data)
+    n = pk["n"]
+    sk = keys["sk"]
+    secret = (sk["a"], sk["g_a_inv"]) if "a" in sk else (sk["phi"], sk["inv"])
+    _, crt, p, q = _pair(n, secret, sk["phi"])
+    assert crt.fp64
+    rng = random.Random(52)
+    vals = _awkward(n, p, q, rng, count=3000)
+    limbs = torch.from_numpy(crt.limbs(vals).view(np.int32)).cuda()
+    outs, dists = [], []
+    for fp64 in (True, False):
+        crt.set_fp64(fp64)
+        assert crt.fp64 == fp64
+        out = torch.zeros((len(vals), crt.words), dtype=torch.int32, device="cuda")
+        dist = torch.full((len(vals) // 2,), -1, dtype=torch.int64, device="cuda")
+        crt.decrypt_array(limbs, out, len(vals))
+        crt.decode_array(limbs, len(vals) // 2, 2, 64, dist)
+        crt.synchronize()
+        outs.append(out)
+        dists.append(dist)
+    crt.set_fp64(True)
+    assert torch.equal(outs[0], outs[1]) and torch.equal(dists[0], dists[1])
+    from cuhepy_b200._limbs import from_limbs
+
+    sample = rng.sample(range(len(vals)), 40)
+    decrypt = oracle.lookup_decrypt if "a" in sk else oracle.decrypt
+    assert from_limbs(outs[0].cpu().numpy().view(np.uint32)[sample]) == [decrypt(vals[i], keys) for i in sample]
+
+
 def test_crt_8192_bit_modulus_vs_oracle():
     rng = random.Random(4096)
     from oracle.gmp import powmod
