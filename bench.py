@@ -1120,8 +1120,9 @@ def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
     (batch of 1-64 encrypted queries, answer = encode_hamming_server against
     the whole index, kept on the device) and half BFV (one packed query,
     embed_len drawn from the three).  The same arrival trace runs through
-    the served evaluator (continuous batching: one Paillier lane fed back to
-    back, three high-priority BFV lanes; admission by free HBM) and through
+    the served evaluator (continuous batching: two Paillier lanes, shortest
+    request first with aging, three high-priority BFV lanes; admission by
+    free HBM) and through
     the plain path (one request at a time, one launch per
     query).  Rates are set for about 80% offered load from single-query
     timings taken first."""
@@ -1151,7 +1152,7 @@ def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
     torch.cuda.synchronize()
     qpool = qpool.cpu()  # queries arrive from the host
 
-    ev = KnnEvaluator(paillier_lanes=1, bfv_lanes=3, max_batch=64)
+    ev = KnnEvaluator(paillier_lanes=2, bfv_lanes=3, max_batch=64)
     ev.add_paillier_index("paillier", pk["n"], index.view(SERVE_VECTORS, 1, K))
     bfv_queries = {}
     for e in SERVE_EMBEDS:
@@ -1226,8 +1227,8 @@ def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
         for f in futs:
             f.result(600)
         out = summarize(lat, max(done_at) - t_start,
-                        "served: continuous batching; 1 Paillier lane fed back to back, 3 high-priority BFV lanes; "
-                        "admission by free HBM")
+                        "served: continuous batching; 2 Paillier lanes sharing the GPU, shortest request first "
+                        "(aged after 0.3 s), 3 high-priority BFV lanes; admission by free HBM")
         sched = ev.scheduler
         out.update({"launches": sched.launches, "max_concurrent": sched.max_concurrent,
                     "peak_answer_bytes": sched.peak_in_use, "budget_bytes": sched.budget})

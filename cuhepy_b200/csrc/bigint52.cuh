@@ -17,7 +17,8 @@
 // removed where a value is needed.  This is the double-precision technique
 // of Emmart, Zheng and Weems ("Faster modular exponentiation using double
 // precision floating point arithmetic on the GPU", ARITH 2018), written here
-// as a warp-cooperative CIOS for this library's lane groups.
+// as a warp-cooperative CIOS for this library's lane groups.  The word
+// products of m = acc_0 (-M^-1) mod 2^52 stay on the integer pipe.
 //
 // A value below M < 2^(52K) is K limbs of 52 bits spread over a group of TPI
 // lanes, lane g owning limbs [gL, gL+L), L = K/TPI, as doubles.  One CIOS
@@ -98,36 +99,63 @@ struct Group52 {
   // acc (raw) += a * b over K steps; b: K doubles in shared memory.
   // On return acc holds positions gL..gL+L-1 of the result (columns K.. of
   // the full sum) with the bias of each position still included.
+  //
+  // The critical path of a step is acc_0 -> m -> m*M.  m is formed on the
+  // integer pipe (a 64-bit multiply, low 52 bits; the FP64 pipe is the busy
+  // one here) and broadcast as an integer, and the products a * b_(i+1) of
+  // the next step, which do not depend on m, are issued while it is formed.
+  // Steps run in unrolled blocks of U (a multiple of 2 and of L): the shift
+  // of the accumulator is a rotation of register names (logical position k
+  // is register (k + s) mod L in step s of a block) and the two product
+  // buffers alternate by step parity, so neither costs a move.
+  static constexpr int U = (L % 2 == 0) ? L : 2 * L;
+  static_assert(K % U == 0, "K must be a multiple of the unrolled block");
+
   __device__ __forceinline__ void cios(uint64_t (&acc)[L], const double (&a)[L], const double* __restrict__ b,
-                                       const double (&n)[L], double ninv) const {
+                                       const double (&n)[L], uint64_t ninv) const {
     uint64_t off = kLoBias;  // bias of column i at position 0 when m_i is taken
+    uint64_t hab[2][L], lab[2][L];
+    {
+      const double b0 = b[0];
+#pragma unroll
+      for (int k = 0; k < L; ++k) mul52(a[k], b0, hab[0][k], lab[0][k]);
+    }
 #pragma unroll 1
-    for (int i = 0; i < K; ++i) {
-      const double bi = b[i];
-      uint64_t hab[L], lab[L];
+    for (int i0 = 0; i0 < K; i0 += U) {
 #pragma unroll
-      for (int k = 0; k < L; ++k) mul52(a[k], bi, hab[k], lab[k]);
-      acc[0] += lab[0];
-      // m = (acc_0 mod 2^52) * (-M^-1) mod 2^52, on every lane, lane 0's kept
-      uint64_t mh, ml;
-      mul52(to_f64((acc[0] - off) & kMask), ninv, mh, ml);
-      const double m = shfl_f64(mask, __dsub_rn(__longlong_as_double(static_cast<long long>(ml)), kTwo52), 0, TPI);
-      uint64_t hnm[L], lnm[L];
+      for (int s = 0; s < U; ++s) {
+        const int i = i0 + s;
+        const int cur = s & 1, nxt = cur ^ 1;
+        uint64_t& a0 = acc[s % L];  // logical position 0
+        a0 += lab[cur][0];
+        // m = (acc_0 mod 2^52) * (-M^-1) mod 2^52 by lane 0, broadcast
+        const uint64_t mi = ((a0 - off) * ninv) & kMask;
+        const uint32_t mlo = __shfl_sync(mask, static_cast<uint32_t>(mi), 0, TPI);
+        const uint32_t mhi = __shfl_sync(mask, static_cast<uint32_t>(mi >> 32), 0, TPI);
+        // the next step's a * b_(i+1) (independent of m)
+        const double bn = b[i + 1 < K ? i + 1 : i];
 #pragma unroll
-      for (int k = 0; k < L; ++k) mul52(n[k], m, hnm[k], lnm[k]);
-      acc[0] += lnm[0];
+        for (int k = 0; k < L; ++k) mul52(a[k], bn, hab[nxt][k], lab[nxt][k]);
+        const double m = to_f64((static_cast<uint64_t>(mhi) << 32) | mlo);
+        uint64_t hnm[L], lnm[L];
 #pragma unroll
-      for (int k = 1; k < L; ++k) acc[k] += (lab[k] + hab[k - 1]) + (lnm[k] + hnm[k - 1]);
-      const uint64_t pend = hab[L - 1] + hnm[L - 1];
-      // column i leaves: its exact value is a multiple of 2^52
-      const uint64_t carry = (acc[0] - off - kLoBias) >> kBits;
-      uint64_t next = shfl_down64(mask, acc[0], 1, TPI);
-      if (gl == TPI - 1) next = 0;
+        for (int k = 0; k < L; ++k) mul52(n[k], m, hnm[k], lnm[k]);
+        a0 += lnm[0];
 #pragma unroll
-      for (int k = 0; k < L - 1; ++k) acc[k] = acc[k + 1];
-      acc[L - 1] = next + pend;
-      if (gl == 0) acc[0] += carry;
-      off += kStep;
+        for (int k = 1; k < L; ++k) {
+          uint64_t& ak = acc[(k + s) % L];
+          ak = ak + lab[cur][k] + hab[cur][k - 1];
+          ak = ak + lnm[k] + hnm[k - 1];
+        }
+        const uint64_t pend = hab[cur][L - 1] + hnm[L - 1];
+        // column i leaves: its exact value is a multiple of 2^52
+        const uint64_t carry = (a0 - off - kLoBias) >> kBits;
+        uint64_t next = shfl_down64(mask, a0, 1, TPI);
+        if (gl == TPI - 1) next = 0;
+        a0 = next + pend;                           // becomes logical position L - 1
+        if (gl == 0) acc[(s + 1) % L] += carry;      // the new logical position 0
+        off += kStep;
+      }
     }
   }
 
@@ -200,7 +228,7 @@ struct Group52 {
 
   // r = a * b * 2^(-52K) mod M.  a: registers (< M), b: shared memory (< M).
   __device__ __forceinline__ void mont_mul(double (&r)[L], const double (&a)[L], const double* __restrict__ b,
-                                           const double (&n)[L], double ninv) const {
+                                           const double (&n)[L], uint64_t ninv) const {
     uint64_t acc[L];
 #pragma unroll
     for (int k = 0; k < L; ++k) acc[k] = 0;
@@ -211,7 +239,7 @@ struct Group52 {
   // r = (init + a * b) * 2^(-52K) mod M, init < 2^(52K) in canonical limbs.
   __device__ __forceinline__ void mont_mul_acc(double (&r)[L], const double (&init)[L], const double (&a)[L],
                                                const double* __restrict__ b, const double (&n)[L],
-                                               double ninv) const {
+                                               uint64_t ninv) const {
     uint64_t acc[L];
 #pragma unroll
     for (int k = 0; k < L; ++k) acc[k] = to_u64(init[k]);

@@ -94,6 +94,8 @@ struct cuhe_paillier {
   int nops_n = 0;
   int32_t* d_ops_sec = nullptr;
   int nops_sec = 0;
+  int32_t* d_ops_sec52 = nullptr;  // the secret exponent's schedule for the FP64-pipe kernel's window
+  int nops_sec52 = 0;
   uint32_t* d_crt = nullptr;  // CRT constant block, present once the factors are installed
   double* d_crt52 = nullptr;  // per side: M and R52 mod M as 52-bit limbs (FP64-pipe CRT kernel)
   cuhe::CrtScalars cs{};
@@ -173,10 +175,14 @@ cudaError_t launch_modexp_crt(cuhe_paillier* ctx, const uint32_t* base, uint32_t
   return cudaGetLastError();
 }
 
-// The same with both exponentiations on the FP64 pipe (TPI = KH / 8 lanes per side).
+// The same with both exponentiations on the FP64 pipe (KH / 16 lanes per
+// side, ten 52-bit limbs per lane; a 3-bit window, with the secret
+// exponent's own schedule).  Independent of the integer kernels' (threads
+// per instance, window) tuning.
+constexpr int kCrt52Window = 3;
 template <int KH, int W>
 size_t modexp_crt52_smem() {
-  constexpr int TPI = KH / 8, K52 = 5 * TPI;
+  constexpr int TPI = KH / 16, K52 = 5 * KH / 8;
   constexpr int IPB = cuhe::kBlockThreads / (2 * TPI);
   return size_t(7 * 2 * KH) * 4 + size_t(K52 + IPB * 2 * (((1 << (W - 1)) + 1) * K52 + 2)) * 8;
 }
@@ -184,15 +190,15 @@ size_t modexp_crt52_smem() {
 template <int KH, int W>
 cudaError_t launch_modexp_crt52(cuhe_paillier* ctx, const uint32_t* base, uint32_t* out, long long count,
                                 int mode, int pop_words) {
-  constexpr int IPB = cuhe::kBlockThreads / (2 * (KH / 8));
+  constexpr int IPB = cuhe::kBlockThreads / (2 * (KH / 16));
   const size_t smem = modexp_crt52_smem<KH, W>();
   cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp_crt52<KH, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;
   const long long blocks = (count + IPB - 1) / IPB;
   cuhe::k_modexp_crt52<KH, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
-      base, out, count, ctx->d_consts, ctx->ks, ctx->d_crt, ctx->cs, ctx->d_crt52, ctx->d_ops_sec,
-      ctx->nops_sec, mode, pop_words, ctx->d_status);
+      base, out, count, ctx->d_consts, ctx->ks, ctx->d_crt, ctx->cs, ctx->d_crt52, ctx->d_ops_sec52,
+      ctx->nops_sec52, mode, pop_words, ctx->d_status);
   return cudaGetLastError();
 }
 
@@ -308,7 +314,6 @@ struct Dispatch {
                         int, int, int) = nullptr;
   cudaError_t (*modexp_var)(cuhe_paillier*, const uint32_t*, const uint32_t*, int, int, uint32_t*, long long) = nullptr;
   cudaError_t (*modexp_crt)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int, int) = nullptr;
-  cudaError_t (*modexp_crt52)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int, int) = nullptr;
   cudaError_t (*mulmod)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long) = nullptr;
   cudaError_t (*convert)(cuhe_paillier*, const uint32_t*, uint32_t*, long long, int) = nullptr;
   cudaError_t (*outer)(cuhe_paillier*, const uint32_t*, long long, const uint32_t*, long long, uint32_t*) = nullptr;
@@ -326,7 +331,6 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
     d->modexp = &launch_modexp<k, t, w>;                           \
     d->modexp_var = &launch_modexp_var<k, t>;                      \
     d->modexp_crt = &launch_modexp_crt<k / 2, t / 2, w>;           \
-    d->modexp_crt52 = t == k / 8 ? &launch_modexp_crt52<k / 2, w> : nullptr; \
     d->mulmod = &launch_mulmod<k, t>;                              \
     d->convert = &launch_convert<k, t>;                            \
     d->outer = &launch_outer<k, t>;                                \
@@ -345,7 +349,11 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
 // when the factorisation is installed, else the direct kernel mod n^2.
 cudaError_t secret_modexp(cuhe_paillier* ctx, const Dispatch& d, const uint32_t* base, uint32_t* out,
                           long long count, int mode, int pop_words) {
-  if (ctx->have_factors && ctx->fp64 && d.modexp_crt52) return d.modexp_crt52(ctx, base, out, count, mode, pop_words);
+  if (ctx->have_factors && ctx->fp64) {
+    if (ctx->K == 64) return launch_modexp_crt52<32, kCrt52Window>(ctx, base, out, count, mode, pop_words);
+    if (ctx->K == 128) return launch_modexp_crt52<64, kCrt52Window>(ctx, base, out, count, mode, pop_words);
+    if (ctx->K == 256) return launch_modexp_crt52<128, kCrt52Window>(ctx, base, out, count, mode, pop_words);
+  }
   if (ctx->have_factors) return d.modexp_crt(ctx, base, out, count, mode, pop_words);
   return d.modexp(ctx, base, nullptr, out, count, ctx->d_ops_sec, ctx->nops_sec, mode, pop_words);
 }
@@ -477,8 +485,8 @@ int check_status(cuhe_paillier* ctx, bool synchronous) {
   return CUHE_OK;
 }
 
-int upload_schedule(cuhe_paillier* ctx, const Limbs& e, int32_t** dptr, int* nops) {
-  std::vector<int32_t> ops = cuhe::host::window_schedule(e, ctx->window);
+int upload_schedule(cuhe_paillier* ctx, const Limbs& e, int32_t** dptr, int* nops, int window = 0) {
+  std::vector<int32_t> ops = cuhe::host::window_schedule(e, window ? window : ctx->window);
   if (*dptr) cudaFree(*dptr);
   *dptr = nullptr;
   *nops = int(ops.size());
@@ -609,6 +617,7 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_status);
   cudaFree(ctx->d_ops_n);
   cudaFree(ctx->d_ops_sec);
+  cudaFree(ctx->d_ops_sec52);
   cudaFree(ctx->d_crt);
   cudaFree(ctx->d_crt52);
   cudaFree(ctx->d_gtab);
@@ -695,6 +704,7 @@ int cuhe_paillier_set_secret(cuhe_paillier* ctx, const uint32_t* exponent, int e
   ctx->ks.mult_is_zero = cuhe::host::is_zero(mult) ? 1u : 0u;
   ctx->secret_exp = e;
   ctx->have_secret = true;
+  if (int rc = upload_schedule(ctx, e, &ctx->d_ops_sec52, &ctx->nops_sec52, kCrt52Window)) return rc;
   return upload_schedule(ctx, e, &ctx->d_ops_sec, &ctx->nops_sec);
 }
 
@@ -728,8 +738,8 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p_in, int p_wo
   auto put_half = [&](int row, int s, const Limbs& v) {
     std::memcpy(block.data() + size_t(row) * k + size_t(s) * kh, v.data(), 4 * kh);
   };
-  // FP64-pipe kernel: K52 = 5 (KH / 8) limbs of 52 bits per side, R52 = 2^(52 K52)
-  const size_t k52 = 5 * (kh / 8);
+  // FP64-pipe kernel: K52 = 5 KH / 8 limbs of 52 bits per side, R52 = 2^(52 K52)
+  const size_t k52 = 5 * kh / 8;
   std::vector<double> block52(2 * 2 * k52, 0.0);
   auto put52 = [&](int s, int row, const Limbs& v) {
     for (size_t i = 0; i < k52; ++i) {
@@ -752,7 +762,7 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p_in, int p_wo
     const uint64_t m0 = (uint64_t(side[s][1]) << 32) | side[s][0];
     uint64_t inv = m0;
     for (int it = 0; it < 6; ++it) inv *= 2 - m0 * inv;
-    ctx->cs.ninv52[s] = double((0 - inv) & ((1ull << 52) - 1));
+    ctx->cs.ninv52[s] = (0 - inv) & ((1ull << 52) - 1);
     put52(s, 0, side[s]);
     put52(s, 1, cuhe::host::shift_mod(one, 52 * k52, side[s]));
   }

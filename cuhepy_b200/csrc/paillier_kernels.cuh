@@ -39,7 +39,7 @@ enum CrtRow : int {
 
 struct CrtScalars {
   uint32_t ninv[2];   // -(p^2)^-1, -(q^2)^-1 mod 2^32
-  double ninv52[2];   // -(p^2)^-1, -(q^2)^-1 mod 2^52 (exact doubles)
+  unsigned long long ninv52[2];  // -(p^2)^-1, -(q^2)^-1 mod 2^52
 };
 
 struct KeyScalars {
@@ -520,8 +520,11 @@ k_modexp_crt(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, long
 // The same CRT decrypt / decode with both exponentiations on the FP64 pipe.
 //
 // Per side the value mod M (p^2 or q^2, KH 32-bit words) is carried as
-// K52 = 5 TPI limbs of 52 bits, TPI = KH / 8 lanes (five limbs per lane),
-// in the Montgomery domain of R52 = 2^(52 K52) (cuhe52::Group52).  Entry and
+// K52 = 5 KH / 8 limbs of 52 bits on TPI = KH / 16 lanes (ten limbs per
+// lane, sixteen 32-bit words), in the Montgomery domain of R52 = 2^(52 K52)
+// (cuhe52::Group52).  Ten limbs per lane give each lane twenty independent
+// products per step to cover the latency of the step's m; a 3-bit window
+// keeps the table small enough for four CTAs per SM.  Entry and
 // exit stay in 32-bit words: c R_h^-1 by the 32-bit reduction as in
 // k_modexp_crt, then * (R52 R_h^2 mod M) gives c R52 mod M, which is
 // re-cut into 52-bit limbs through shared memory; the odd-power table and
@@ -553,16 +556,17 @@ __device__ __forceinline__ uint32_t word_from_limbs52(const uint64_t* l, int nli
 }
 
 template <int KH, int W>
-__global__ void __launch_bounds__(kBlockThreads)
+__global__ void __launch_bounds__(kBlockThreads, 3)
 k_modexp_crt52(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, long long count,
                const uint32_t* __restrict__ consts, KeyScalars ks, const uint32_t* __restrict__ crt, CrtScalars cs,
                const double* __restrict__ crt52, const int32_t* __restrict__ ops, int nops, int mode,
                int pop_words, int* status) {
   constexpr int K = 2 * KH;
-  constexpr int TPI = KH / 8;   // lanes per side
-  constexpr int L = 8;          // 32-bit words per lane and side
-  constexpr int K52 = 5 * TPI;  // 52-bit limbs per side
-  constexpr int L52 = 5;
+  constexpr int TPI = KH / 16;     // lanes per side
+  constexpr int L = 16;            // 32-bit words per lane and side
+  constexpr int K52 = 5 * KH / 8;  // 52-bit limbs per side
+  constexpr int L52 = K52 / TPI;   // ten
+  static_assert(L52 == 10, "ten limbs per lane");
   static_assert(52 * K52 > 32 * KH + 1, "R52 must exceed 2 M");
   constexpr int T = 1 << (W - 1);
   constexpr int IPB = kBlockThreads / (2 * TPI);
@@ -607,15 +611,17 @@ k_modexp_crt52(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, lo
     }
   }
   const uint32_t ninv = cs.ninv[side];
-  uint32_t m[L], lo[L], hi[L], acc[L];
-  h.load_ro(m, crt + CR_M * K + side * KH);
-  h.load(lo, base + inst * K);
-  h.load(hi, base + inst * K + KH);
-  // c = lo + hi R_h:  (lo + hi * (R_h mod M)) R_h^-1 = c R_h^-1, then * R52 R_h^2 R_h^-1 = c R52
-  h.mont_mul_acc(acc, lo, hi, s_rm + side * KH, m, ninv);
-  h.mont_mul(acc, acc, s_r52 + side * KH, m, ninv);
   uint32_t* s_w = reinterpret_cast<uint32_t*>(s_x);  // KH words fit in the K52 doubles of x
-  h.publish(s_w, acc);
+  {
+    // c = lo + hi R_h:  (lo + hi * (R_h mod M)) R_h^-1 = c R_h^-1, then * R52 R_h^2 R_h^-1 = c R52
+    uint32_t m[L], lo[L], hi[L], acc[L];
+    h.load_ro(m, crt + CR_M * K + side * KH);
+    h.load(lo, base + inst * K);
+    h.load(hi, base + inst * K + KH);
+    h.mont_mul_acc(acc, lo, hi, s_rm + side * KH, m, ninv);
+    h.mont_mul(acc, acc, s_r52 + side * KH, m, ninv);
+    h.publish(s_w, acc);
+  }
   double x52[L52], m52[L52], acc52[L52];
   const double* cm = crt52 + side * 2 * K52;  // M, then R52 mod M
 #pragma unroll
@@ -623,47 +629,74 @@ k_modexp_crt52(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, lo
     x52[k] = cuhe52::to_f64(limb52_from_words(s_w, KH, f.gl * L52 + k));
     m52[k] = __ldg(cm + f.gl * L52 + k);
   }
-  const double ninv52 = cs.ninv52[side];
+  const uint64_t ninv52 = cs.ninv52[side];
   f.publish(s_tab, x52);
 #pragma unroll
   for (int k = 0; k < L52; ++k) acc52[k] = x52[k];
-  if (T > 1) {
-    double sq[L52];
-    f.mont_mul(sq, x52, s_tab, m52, ninv52);  // x^2 R52
-    f.publish(s_x, sq);
-#pragma unroll 1
-    for (int t = 1; t < T; ++t) {
-      f.mont_mul(acc52, acc52, s_x, m52, ninv52);
-      f.publish(s_tab + t * K52, acc52);
-    }
-  }
-  if (nops == 0) {
-#pragma unroll
-    for (int k = 0; k < L52; ++k) acc52[k] = __ldg(cm + K52 + f.gl * L52 + k);  // e = 0: R52 mod M
-  } else {
-    const int first = __ldg(ops) & 0xffff;
-    __syncwarp(f.mask);
-#pragma unroll
-    for (int k = 0; k < L52; ++k) acc52[k] = s_tab[(first - 1) * K52 + f.gl * L52 + k];
-  }
-  f.publish(s_x, acc52);
-#pragma unroll 1
-  for (int o = 1; o < nops; ++o) {
-    const int op = __ldg(ops + o);
-    const int sq = op >> 16;
-    const int idx = op & 0xffff;
-#pragma unroll 1
-    for (int s = 0; s < sq; ++s) {
-      f.mont_mul(acc52, acc52, s_x, m52, ninv52);
-      f.publish(s_x, acc52);
-    }
-    if (idx) {
-      f.mont_mul(acc52, acc52, s_tab + (idx - 1) * K52, m52, ninv52);
-      f.publish(s_x, acc52);
-    }
-  }
+  // Every Montgomery product of the exponentiation goes through the one
+  // call site below: the unrolled product is large, and a single copy of it
+  // stays in the instruction cache.  Phases: the odd-power table (x^2 to
+  // s_x, then x^3 .. x^(2T-1)), the window schedule (squarings of s_x and
+  // products with table entries), the final product with 1.
+  enum { kTable = 0, kSchedule = 1, kFinal = 2, kDone = 3 };
+  int phase = T > 1 ? kTable : kSchedule, pc = 0, o = 1, sq_left = 0, idx = 0;
+  if (phase == kSchedule) pc = T;  // no table products: go straight to the schedule set-up
   double xs52[L52];
-  f.mont_mul(xs52, acc52, s_one52, m52, ninv52);  // x_side, canonical
+  while (phase != kDone) {
+    if (phase == kTable || pc == T) {
+      // (after the table) the schedule starts from its first table entry
+      if (phase == kSchedule && pc == T) {
+        pc = 0;
+        if (nops == 0) {
+#pragma unroll
+          for (int k = 0; k < L52; ++k) acc52[k] = __ldg(cm + K52 + f.gl * L52 + k);  // e = 0: R52 mod M
+        } else {
+          const int first = __ldg(ops) & 0xffff;
+          __syncwarp(f.mask);
+#pragma unroll
+          for (int k = 0; k < L52; ++k) acc52[k] = s_tab[(first - 1) * K52 + f.gl * L52 + k];
+        }
+        f.publish(s_x, acc52);
+        while (sq_left == 0 && idx == 0) {
+          if (o >= nops) {
+            phase = kFinal;
+            break;
+          }
+          const int op = __ldg(ops + o++);
+          sq_left = op >> 16;
+          idx = op & 0xffff;
+        }
+      }
+    }
+    const double* bsrc = phase == kTable   ? (pc == 0 ? s_tab : s_x)
+                         : phase == kFinal ? s_one52
+                         : sq_left > 0     ? s_x
+                                           : s_tab + (idx - 1) * K52;
+    f.mont_mul(xs52, acc52, bsrc, m52, ninv52);
+    if (phase == kFinal) break;  // xs52 = x_side, canonical
+    if (phase == kTable && pc == 0) {
+      f.publish(s_x, xs52);  // x^2 R52; acc52 stays x
+    } else {
+#pragma unroll
+      for (int k = 0; k < L52; ++k) acc52[k] = xs52[k];
+      f.publish(phase == kTable ? s_tab + pc * K52 : s_x, acc52);
+    }
+    if (phase == kTable) {
+      if (++pc == T) phase = kSchedule;  // pc == T: set-up at the top of the next pass
+      continue;
+    }
+    if (sq_left > 0) --sq_left;
+    else idx = 0;
+    while (sq_left == 0 && idx == 0) {
+      if (o >= nops) {
+        phase = kFinal;
+        break;
+      }
+      const int op = __ldg(ops + o++);
+      sq_left = op >> 16;
+      idx = op & 0xffff;
+    }
+  }
   uint64_t* s_l = reinterpret_cast<uint64_t*>(s_x);
   __syncwarp(f.mask);
 #pragma unroll
@@ -679,7 +712,8 @@ k_modexp_crt52(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, lo
   __syncwarp(g.mask);
   if (side == 0) {
     // h = x_p (q^2)^-1 - x_q (q^2)^-1 mod p^2   (x_q may exceed p^2; x_q < R_h)
-    uint32_t xq[L], v[L], u[L];
+    uint32_t m[L], xq[L], v[L], u[L];
+    h.load_ro(m, crt + CR_M * K);
     h.load(xq, s_xq);
     h.mont_mul(v, xs, s_h, m, ninv);
     h.mont_mul(u, xq, s_h, m, ninv);

@@ -12,22 +12,25 @@ in HBM and answers two kinds of request:
   index; the answer is the list of packed response ciphertexts of
   ``packed_search`` (``bfv/_cpu_ext/bindings.cpp:329-367``).
 
-Continuous batching.  Requests wait in one FIFO queue per kind.  A scheduler
-thread admits the oldest request of a kind as soon as one of that kind's
-execution lanes is free and the device memory the request needs fits in the
-budget (free HBM at start minus a reserve and the BFV lanes' workspaces).
-Admitted work runs on the lane's own CUDA stream, so requests that arrive
-while others are on the GPU overlap with them.  Paillier work saturates the
-GPU by itself (one query against a million vectors is a million products), so
-it gets one lane fed back to back; BFV searches are chains of short kernels
-and run concurrently on several lanes whose streams have the highest
-priority, so their blocks are scheduled ahead of queued Paillier blocks.
-Paillier requests for the same index that are waiting when the lane frees up
-are taken together (up to ``max_batch`` queries): one merged launch for small
-indexes, back-to-back launches with each answer delivered as soon as its own
-launch ends for large ones.  The memory of a Paillier answer stays reserved
-until the caller releases the result; a request larger than the whole budget
-is refused at submission.
+Continuous batching.  Requests wait in one queue per kind.  A scheduler
+thread admits a request of a kind as soon as one of that kind's execution
+lanes is free and the device memory the request needs fits in the budget
+(free HBM at start minus a reserve and the BFV lanes' workspaces).  Admitted
+work runs on the lane's own CUDA stream, so requests that arrive while
+others are on the GPU overlap with them.  BFV searches are chains of short
+kernels and run concurrently on several lanes whose streams have the
+highest priority, so their blocks are scheduled ahead of queued Paillier
+blocks; they are admitted in arrival order.  Paillier work saturates the GPU
+by itself (one query against a million vectors is a million products): it
+gets two lanes, so a request that arrives while a long one runs starts at
+once and the two share the GPU block by block, and the waiting request with
+the fewest queries goes next (shortest job first), unless the oldest has
+waited longer than ``age_limit_s``.  Paillier requests on a small index
+(a launch over one query would not fill the GPU) that are waiting when a
+lane frees up are merged into one launch (up to ``max_batch`` queries).
+The memory of a Paillier answer stays reserved until the caller releases
+the result; a request larger than the whole budget is refused at
+submission.
 
 ``run_plain`` is the comparison point: one request at a time, one launch per
 query, every launch waited for.
@@ -82,7 +85,9 @@ class Scheduler:
     def __init__(self, execute: Callable[..., list[Any]], lanes: dict[str, int] | int,
                  budget_bytes: int, max_batch: int = 64,
                  holds_memory: Callable[[str], bool] = lambda kind: True,
-                 merge: Callable[[str], bool] = lambda kind: kind == "paillier") -> None:
+                 merge: Callable[[str], bool] = lambda kind: kind == "paillier",
+                 mergeable: Callable[[Request], bool] = lambda req: True,
+                 pick: Callable[[str, Any, float], int] | None = None) -> None:
         if isinstance(lanes, int):
             lanes = {"paillier": lanes, "bfv": lanes}
         if not lanes or min(lanes.values()) < 1:
@@ -90,6 +95,8 @@ class Scheduler:
         self._execute = execute
         self._holds = holds_memory
         self._merge = merge
+        self._mergeable = mergeable
+        self._pick = pick or (lambda kind, queue, now: 0)
         self.lanes = dict(lanes)
         self.budget = int(budget_bytes)
         self.max_batch = int(max_batch)
@@ -173,23 +180,27 @@ class Scheduler:
 
     # -- scheduling ---------------------------------------------------------
     def _admit(self) -> tuple[list[Request], int] | None:
-        """The oldest request of a kind with a free lane, if its memory fits;
-        later requests of the same index join it while the group stays within
+        """The head request of a kind with a free lane (the oldest, unless
+        the ``pick`` policy names another), if its memory fits; later
+        requests of the same index join it while the group stays within
         max_batch queries and the budget."""
+        now = time.perf_counter()
         for kind, queue in self._queues.items():
             if not queue or not self._free[kind]:
                 continue
-            head = queue[0]
+            at = self._pick(kind, queue, now)
+            head = queue[at]
             if self.in_use + head.nbytes > self.budget:
                 continue
-            group = [queue.popleft()]
+            del queue[at]
+            group = [head]
             need = head.nbytes
-            if self._merge(kind):
+            if self._merge(kind) and self._mergeable(head):
                 total = head.queries
                 keep: collections.deque[Request] = collections.deque()
                 while queue:
                     r = queue.popleft()
-                    if (r.index == head.index and total + r.queries <= self.max_batch
+                    if (r.index == head.index and self._mergeable(r) and total + r.queries <= self.max_batch
                             and self.in_use + need + r.nbytes <= self.budget):
                         group.append(r)
                         total += r.queries
@@ -270,6 +281,19 @@ class Scheduler:
                 self._cv.notify_all()
 
 
+def shortest_first(age_limit_s: float) -> Callable[[str, Any, float], int]:
+    """A ``pick`` policy for :class:`Scheduler`: the waiting request with the
+    fewest queries (the earliest among equals), unless the oldest request has
+    waited longer than ``age_limit_s``, which then goes first."""
+
+    def pick(kind: str, queue, now: float) -> int:
+        if len(queue) < 2 or now - queue[0].arrival > age_limit_s:
+            return 0
+        return min(range(len(queue)), key=lambda i: (queue[i].queries, i))
+
+    return pick
+
+
 class PaillierAnswer:
     """encode_hamming_server products of one request, on the device:
     ``tensor[c, b, v]`` = query b chunk c times index vector v chunk c mod n^2
@@ -303,14 +327,16 @@ class KnnEvaluator:
     #: soon as its own launch ends
     MERGE_BELOW_VECTORS = 1 << 18
 
-    def __init__(self, device: int = 0, paillier_lanes: int = 1, bfv_lanes: int = 3, max_batch: int = 64,
-                 reserve_bytes: int = 2 << 30, budget_bytes: int | None = None) -> None:
+    def __init__(self, device: int = 0, paillier_lanes: int = 2, bfv_lanes: int = 3, max_batch: int = 64,
+                 reserve_bytes: int = 2 << 30, budget_bytes: int | None = None,
+                 age_limit_s: float = 0.3) -> None:
         import torch
 
         self._torch = torch
         self.device = int(device)
         self.lane_counts = {"paillier": int(paillier_lanes), "bfv": int(bfv_lanes)}
         self.max_batch = int(max_batch)
+        self.age_limit_s = float(age_limit_s)
         self.reserve_bytes = int(reserve_bytes)
         self._budget_override = budget_bytes
         # bulk work on default-priority streams; BFV lanes are the ring's own
@@ -380,7 +406,8 @@ class KnnEvaluator:
         if budget <= 0:
             raise MemoryError("no device memory left for answers after the resident state")
         self._sched = Scheduler(self._execute, self.lane_counts, budget, self.max_batch,
-                                holds_memory=lambda kind: kind == "paillier")
+                                holds_memory=lambda kind: kind == "paillier",
+                                mergeable=self._mergeable, pick=self._pick)
         self._sched.start()
 
     def stop(self) -> None:
@@ -425,6 +452,18 @@ class KnnEvaluator:
         if name not in self._bfv:
             raise KeyError(name)
         return self.scheduler.submit(Request("bfv", name, 1, 0, query))
+
+    # -- policy -------------------------------------------------------------
+    def _mergeable(self, req: Request) -> bool:
+        """Requests on small Paillier indexes share one launch; on large ones
+        (a launch per query already fills the GPU) each is admitted alone,
+        so the next pick happens as soon as a lane frees."""
+        return req.kind != "paillier" or self._paillier[req.index]["vectors"] < self.MERGE_BELOW_VECTORS
+
+    def _pick(self, kind: str, queue, now: float) -> int:
+        """Paillier: shortest job first with aging; BFV searches (all of one
+        size) in arrival order."""
+        return shortest_first(self.age_limit_s)(kind, queue, now) if kind == "paillier" else 0
 
     # -- execution ----------------------------------------------------------
     def _execute(self, kind: str, name: str, group: list[Request], lane: int, deliver) -> list[Any]:

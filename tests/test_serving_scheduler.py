@@ -239,3 +239,43 @@ def test_kinds_do_not_wait_for_each_other_and_answers_can_come_early():
         for e in gate.events:
             e.set()
         s.stop()
+
+
+def test_shortest_first_with_aging():
+    """The serving policy for Paillier requests: the fewest queries go first,
+    but a request that has waited past the age limit is not overtaken."""
+    from cuhepy_b200.serving import shortest_first
+
+    gate = Gate()
+    s = Scheduler(gate, lanes=1, budget_bytes=1000, merge=lambda kind: False, pick=shortest_first(0.5))
+    s.start()
+    try:
+        s.submit(_req(queries=1, payload="running"))
+        gate.wait_groups(1)
+        reqs = {name: _req(queries=q, payload=name) for name, q in (("big", 40), ("mid", 9), ("small", 2))}
+        futs = {name: s.submit(r) for name, r in reqs.items()}
+        time.sleep(0.05)
+        for k in range(4):
+            gate.open(k)
+            if k < 3:
+                gate.wait_groups(k + 2)
+        assert [futs[name].result(5)[1] for name in ("small", "mid", "big")] == ["small", "mid", "big"]
+        assert reqs["small"].admitted < reqs["mid"].admitted < reqs["big"].admitted
+        # aged: the oldest waiting request goes first once past the limit
+        s.submit(_req(queries=1, payload="running2"))
+        gate.wait_groups(5)
+        old_req, young_req = _req(queries=50, payload="old"), _req(queries=1, payload="young")
+        old = s.submit(old_req)
+        time.sleep(0.6)
+        young = s.submit(young_req)
+        gate.open(4)
+        gate.wait_groups(6)
+        gate.open(5)
+        gate.wait_groups(7)
+        gate.open(6)
+        assert old.result(5)[1] == "old" and young.result(5)[1] == "young"
+        assert old_req.admitted < young_req.admitted
+    finally:
+        for e in gate.events:
+            e.set()
+        s.stop()
