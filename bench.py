@@ -311,32 +311,47 @@ def run_gpu(args) -> dict | None:
         stream.synchronize()
     plain_value = plain_n / (time.perf_counter() - t0)
 
-    # ---- the same decode batch on the direct kernel mod n^2 (no CRT) ------
+    # ---- the same decode batch on the integer-pipe CRT kernel and on the
+    # direct kernel mod n^2 (no CRT), outside the timed steps --------------
+    def time_decode() -> list[float]:
+        out = []
+        for _ in range(2):
+            flush.fill_(1)
+            a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                a_ev.record(stream)
+                ctx.decode_array(prod, QUERY_BATCH * INDEX_VECTORS, 1, chunk_len, dist_out)
+                b_ev.record(stream)
+            b_ev.synchronize()
+            out.append(a_ev.elapsed_time(b_ev))
+        return out
+
+    ctx.set_fp64(0)
+    int_ms = time_decode()
+    ctx.set_fp64(1)
     ctx.set_factors(None, None)
-    direct_ms = []
-    for _ in range(2):
-        flush.fill_(1)
-        a_ev, b_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            a_ev.record(stream)
-            ctx.decode_array(prod, QUERY_BATCH * INDEX_VECTORS, 1, chunk_len, dist_out)
-            b_ev.record(stream)
-        b_ev.synchronize()
-        direct_ms.append(a_ev.elapsed_time(b_ev))
+    direct_ms = time_decode()
     ctx.set_factors(*factors)
 
-    # ---- roofline of the dominant kernel (decode: c^a by CRT) --------------
-    peak = ctypes_imad_peak(_native, local)
+    # ---- roofline of the dominant kernel (decode: c^a by CRT, FP64 pipe) ----
+    fp64_peak = ctypes_fp64_peak(_native, local)
+    imad_peak = ctypes_imad_peak(_native, local)
     k = words
     kh = k // 2
+    k52 = 5 * kh // 8
     a_bits = int(sk["a"]).bit_length()
     mm = a_bits + math.ceil(a_bits / 6) + 16
-    wp_per_decode = 2 * mm * (2 * kh * kh + kh)
+    fp64_per_decode = 2 * mm * (2 * k52 * k52 + k52) * 3   # three FP64 instructions per 52x52-bit limb product
+    wp_per_decode = 2 * mm * (2 * kh * kh + kh)            # the same products as 32x32-bit word products
     decode_ms = statistics.mean(kernel_ms["decode"])
+    decodes = QUERY_BATCH * INDEX_VECTORS
     sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
-    nominal = torch.cuda.get_device_properties(local).multi_processor_count * 64 * sm_mhz * 1e6 / 2
-    achieved = QUERY_BATCH * INDEX_VECTORS * wp_per_decode / (decode_ms / 1e3)
-    traffic = ncu_traffic(QUERY_BATCH * INDEX_VECTORS)
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    nominal_fp64 = sms * 64 * sm_mhz * 1e6
+    nominal_imad = sms * 64 * sm_mhz * 1e6 / 2
+    achieved = decodes * fp64_per_decode / (decode_ms / 1e3)
+    achieved_wp = decodes * wp_per_decode / (decode_ms / 1e3)
+    traffic = ncu_traffic(decodes)
     clock_summary = clocks.summary()
     if rank != 0:
         if dist:
@@ -356,25 +371,36 @@ def run_gpu(args) -> dict | None:
         "dtype": "u32",
         "data": "synthetic: Bernoulli(0.5) 512-bit embeddings (seed 1337+rank), keys from a seeded generator",
         "config": knn_config(),
-        "tuning": {"threads_per_instance": ctx.tuning()[0], "window": ctx.tuning()[1]},
+        "tuning": {"threads_per_instance": ctx.tuning()[0], "window": ctx.tuning()[1], "decode_pipe": "fp64"},
         "stage_ms": {name: statistics.mean(v) for name, v in kernel_ms.items()},
+        "decode_int_ms": statistics.mean(int_ms),
         "decode_direct_ms": statistics.mean(direct_ms),
-        "decode_direct": "the same decode batch on k_modexp (c^a mod n^2, no CRT), outside the timed steps",
+        "decode_compare": ("the same decode batch outside the timed steps: decode_int_ms on the integer-pipe CRT "
+                           "kernel k_modexp_crt<64,8,4>, decode_direct_ms on k_modexp (c^a mod n^2, no CRT)"),
         "p50_ms": statistics.median(step_ms),
         "p99_ms": float(np.percentile(step_ms, 99)),
         "plain_value": plain_value,
         "plain": "decode one ciphertext per launch (batch 1), host-synchronised",
         "roofline": {
-            "bound": "imad",
-            "kernel": "k_modexp_crt<64,8,4> decode (c^a mod p^2 and mod q^2, |a|=%d bits)" % a_bits,
-            "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "Twp/s",
-            "frac": achieved / peak, "traffic": traffic,
-            "peak_nominal": nominal / 1e12, "frac_of_nominal": achieved / nominal,
-            "peak_nominal_source": "SMs x 64 IMAD/clk x median SM clock / 2 IMAD per word product",
+            "bound": "fp64",
+            "kernel": ("k_modexp_crt52<64,3> decode (c^a mod p^2 and mod q^2 as 40 52-bit limbs, |a|=%d bits, "
+                       "on the FP64 pipe)" % a_bits),
+            "achieved": achieved / 1e12, "peak": fp64_peak / 1e12, "unit": "T fp64 instr/s",
+            "frac": achieved / fp64_peak, "traffic": traffic,
+            "peak_nominal": nominal_fp64 / 1e12, "frac_of_nominal": achieved / nominal_fp64,
+            "peak_source": "measured by cuhe_fp64_peak in this run (independent fma.rz.f64 chains)",
+            "peak_nominal_source": "SMs x 64 FP64 FMA/clk x median SM clock",
             "traffic_source": "ncu dram bytes of an 8,192-decode launch, scaled by decodes per launch",
-            "peak_source": "measured by cuhe_imad_peak in this run (best of mad.lo+mad.hi, mad.wide, carry-chain probes)",
-            "work_per_unit": (f"2 sides x MM(e)=e+ceil(e/6)+16={mm} modmuls x (2kh^2+kh)={2 * kh * kh + kh} wp, "
-                              f"kh={kh} (recombination and epilogue, under 2%, not counted)"),
+            "work_per_unit": (f"2 sides x MM(e)=e+ceil(e/6)+16={mm} modmuls x (2K52^2+K52)={2 * k52 * k52 + k52} "
+                              f"limb products x 3 FP64 instructions, K52={k52} (recombination and epilogue on the "
+                              f"integer pipe, under 2%, not counted)"),
+            "as_word_products": {
+                "achieved": achieved_wp / 1e12, "unit": "Twp/s",
+                "imad_peak_measured": imad_peak / 1e12, "frac_of_measured_imad": achieved_wp / imad_peak,
+                "imad_peak_nominal": nominal_imad / 1e12, "frac_of_nominal_imad": achieved_wp / nominal_imad,
+                "note": (f"the same decode counted as 2 x {mm} x (2kh^2+kh)={2 * kh * kh + kh} 32-bit word products, "
+                         f"kh={kh}, against the integer multiply pipe's measured and nominal rates"),
+            },
         },
         "clocks": clock_summary,
         "e2e": {"value": e2e_value, "unit": "modexp/s", "h2d_bytes_per_step": int(h2d),
@@ -672,6 +698,17 @@ def bfv_cpu_baseline(setups: dict, native_tiles: int = 256) -> dict:
     return out
 
 
+def ctypes_fp64_peak(native, device: int) -> float:
+    import ctypes
+
+    lib = native.paillier_lib()
+    out = ctypes.c_double()
+    rc = lib.cuhe_fp64_peak(device, ctypes.byref(out))
+    if rc != 0:
+        raise RuntimeError(lib.cuhe_last_error(None).decode())
+    return out.value
+
+
 def ctypes_imad_peak(native, device: int) -> float:
     import ctypes
 
@@ -683,11 +720,11 @@ def ctypes_imad_peak(native, device: int) -> float:
     return out.value
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one k_modexp_crt<64,8,4>
-# decode launch of 8,192 ciphertexts (ncu --set full, key_len 1024):
-# 4,350,976 + 0 bytes.  Each ciphertext is read once, so the traffic of a
-# larger launch scales with the number of decodes.
-DECODE_TRAFFIC_BYTES, DECODE_TRAFFIC_ITEMS = 4_350_976, 8192
+# dram__bytes_read.sum + dram__bytes_write.sum of one k_modexp_crt52<64,3>
+# decode launch of 8,192 ciphertexts (ncu, key_len 1024): 4,491,776 + 0
+# bytes.  Each ciphertext is read once, so the traffic of a larger launch
+# scales with the number of decodes.
+DECODE_TRAFFIC_BYTES, DECODE_TRAFFIC_ITEMS = 4_491_776, 8192
 
 
 def ncu_traffic(items: int) -> float:
@@ -1120,9 +1157,8 @@ def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
     (batch of 1-64 encrypted queries, answer = encode_hamming_server against
     the whole index, kept on the device) and half BFV (one packed query,
     embed_len drawn from the three).  The same arrival trace runs through
-    the served evaluator (continuous batching: two Paillier lanes, shortest
-    request first with aging, three high-priority BFV lanes; admission by
-    free HBM) and through
+    the served evaluator (continuous batching: one Paillier lane in arrival
+    order, three high-priority BFV lanes; admission by free HBM) and through
     the plain path (one request at a time, one launch per
     query).  Rates are set for about 80% offered load from single-query
     timings taken first."""
@@ -1152,7 +1188,7 @@ def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
     torch.cuda.synchronize()
     qpool = qpool.cpu()  # queries arrive from the host
 
-    ev = KnnEvaluator(paillier_lanes=2, bfv_lanes=3, max_batch=64)
+    ev = KnnEvaluator(paillier_lanes=1, bfv_lanes=3, max_batch=64)
     ev.add_paillier_index("paillier", pk["n"], index.view(SERVE_VECTORS, 1, K))
     bfv_queries = {}
     for e in SERVE_EMBEDS:
@@ -1227,8 +1263,8 @@ def run_serving(requests: int = SERVE_REQUESTS, seed: int = 7) -> dict:
         for f in futs:
             f.result(600)
         out = summarize(lat, max(done_at) - t_start,
-                        "served: continuous batching; 2 Paillier lanes sharing the GPU, shortest request first "
-                        "(aged after 0.3 s), 3 high-priority BFV lanes; admission by free HBM")
+                        "served: continuous batching; 1 Paillier lane in arrival order, 3 high-priority BFV lanes; "
+                        "admission by free HBM")
         sched = ev.scheduler
         out.update({"launches": sched.launches, "max_concurrent": sched.max_concurrent,
                     "peak_answer_bytes": sched.peak_in_use, "budget_bytes": sched.budget})
@@ -1281,7 +1317,7 @@ def profile_case(which: str) -> None:
         ctx = PaillierDevice(pk["n"])
         ctx.set_secret(sk["a"], sk["g_a_inv"])
         ctx.set_factors(*factors_from_phi(pk["n"], sk["phi"]))
-        ctx.set_fp64(which == "paillier")
+        ctx.set_fp64(1 if which == "paillier" else 0)
         ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
         stream = torch.cuda.Stream()
         ctx.set_stream(stream.cuda_stream)

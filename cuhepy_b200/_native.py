@@ -70,6 +70,7 @@ PAILLIER_SIGNATURES: dict[str, tuple] = {
     "cuhe_lookup_encrypt_ints": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                                 ctypes.c_void_p]),
     "cuhe_imad_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "cuhe_fp64_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "cuhe_window_schedule": (ctypes.c_int, [c_u32_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.c_int]),
     "cuhe_paillier_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),

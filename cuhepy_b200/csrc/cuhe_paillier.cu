@@ -100,7 +100,8 @@ struct cuhe_paillier {
   double* d_crt52 = nullptr;  // per side: M and R52 mod M as 52-bit limbs (FP64-pipe CRT kernel)
   cuhe::CrtScalars cs{};
   bool have_factors = false;
-  bool fp64 = true;           // decrypt / decode exponentiations on the FP64 pipe where compiled
+  bool fp64 = true;           // decrypt / decode exponentiations on the FP64 pipe (n^2 of 4096 bits or more)
+  bool fp64_small = false;    // ... and for n^2 of 2048 bits (set_fp64(ctx, 2))
   uint32_t* d_gtab = nullptr;
   int message_chunks = 0;
   uint32_t* d_noise = nullptr;
@@ -350,7 +351,8 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
 cudaError_t secret_modexp(cuhe_paillier* ctx, const Dispatch& d, const uint32_t* base, uint32_t* out,
                           long long count, int mode, int pop_words) {
   if (ctx->have_factors && ctx->fp64) {
-    if (ctx->K == 64) return launch_modexp_crt52<32, kCrt52Window>(ctx, base, out, count, mode, pop_words);
+    // n^2 of 2048 bits (1024-bit sides) stays on the integer pipe: measured faster there
+    if (ctx->K == 64 && ctx->fp64_small) return launch_modexp_crt52<32, kCrt52Window>(ctx, base, out, count, mode, pop_words);
     if (ctx->K == 128) return launch_modexp_crt52<64, kCrt52Window>(ctx, base, out, count, mode, pop_words);
     if (ctx->K == 256) return launch_modexp_crt52<128, kCrt52Window>(ctx, base, out, count, mode, pop_words);
   }
@@ -786,10 +788,11 @@ int cuhe_paillier_set_fp64(cuhe_paillier* ctx, int enable) {
   if (!ctx) return CUHE_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(ctx->mu);
   ctx->fp64 = enable != 0;
+  ctx->fp64_small = enable == 2;
   return CUHE_OK;
 }
 
-int cuhe_paillier_get_fp64(const cuhe_paillier* ctx) { return ctx && ctx->fp64 ? 1 : 0; }
+int cuhe_paillier_get_fp64(const cuhe_paillier* ctx) { return !ctx || !ctx->fp64 ? 0 : ctx->fp64_small ? 2 : 1; }
 
 int cuhe_paillier_encrypt(cuhe_paillier* ctx, const uint32_t* m, const uint32_t* r, uint32_t* c, int64_t count) {
   if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
@@ -943,6 +946,37 @@ int cuhe_paillier_decode_hamming_static(cuhe_paillier* ctx, const uint32_t* c, i
   cuhe::k_sum_chunks<<<unsigned((vectors + 255) / 256), 256, 0, ctx->stream>>>(
       counts, vectors, chunk_num, reinterpret_cast<long long*>(distance));
   CUHE_CUDA(ctx, cudaGetLastError(), "static decode reduction");
+  return CUHE_OK;
+}
+
+int cuhe_fp64_peak(int device, double* fp64_per_second) {
+  if (!fp64_per_second) return fail(nullptr, CUHE_INVALID_ARGUMENT, "null output");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    return fail(nullptr, CUHE_CUDA_ERROR, "no such CUDA device");
+  DeviceGuard guard(device);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  double* sink = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaMalloc(&sink, 8);
+  if (e == cudaSuccess) e = cudaEventCreate(&a);
+  if (e == cudaSuccess) e = cudaEventCreate(&b);
+  const int iters = 8192, blocks = sms * 8, threads = 256;
+  float ms = 0.f;
+  if (e == cudaSuccess) {
+    cuhe::k_fp64_probe<<<blocks, threads>>>(sink, iters, 1.0);  // warm-up
+    cudaEventRecord(a);
+    for (int r = 0; r < 5; ++r) cuhe::k_fp64_probe<<<blocks, threads>>>(sink, iters, 2.0 + r);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "fp64 probe");
+  *fp64_per_second = 5.0 * blocks * threads * double(iters) * 8.0 / (double(ms) * 1e-3);
   return CUHE_OK;
 }
 

@@ -823,6 +823,24 @@ __global__ void k_sum_chunks(const uint32_t* __restrict__ counts, long long vect
 // iteration by one mad.lo.cc/madc.hi.cc row (8 word products, the shape of
 // Group::mac_row) with no shuffles or memory traffic, so the probe is bound
 // only by the integer multiply pipe.  Each row is 8 word products.
+// FP64-pipe probe: eight independent fused multiply-add chains per thread
+// (round toward zero, the form of the limb products), FP64 instructions only.
+__global__ void __launch_bounds__(256) k_fp64_probe(double* sink, int iters, double seed) {
+  double x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = seed + 1e-3 * double(threadIdx.x) + double(j);
+  const double y = 1.0000000001, z = 1e-9;
+#pragma unroll 1
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = __fma_rz(x[j], y, z);
+  }
+  double folded = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) folded += x[j];
+  if (folded == 1.2345678) sink[0] = folded;
+}
+
 __global__ void __launch_bounds__(256) k_imad_chain_probe(uint32_t* sink, int iters, uint32_t seed) {
   uint32_t acc[4][8], c0[4], c1[4], a[8];
   const uint32_t b = seed * 2654435761u + blockIdx.x;

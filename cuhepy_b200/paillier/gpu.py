@@ -103,15 +103,15 @@ class PaillierDevice:
     def has_factors(self) -> bool:
         return bool(self._lib.cuhe_paillier_has_factors(self._ctx))
 
-    def set_fp64(self, enable: bool) -> None:
-        """CRT exponentiations as 52-bit-limb products on the FP64 pipe (the
-        default) or as 32-bit word products on the integer pipe; identical
-        results."""
-        self._check(self._lib.cuhe_paillier_set_fp64(self._ctx, int(bool(enable))))
+    def set_fp64(self, enable: int) -> None:
+        """CRT exponentiations as 52-bit-limb products on the FP64 pipe for n^2
+        of 4096 bits or more (1, the default; 2: also for 2048 bits) or as
+        32-bit word products on the integer pipe (0); identical results."""
+        self._check(self._lib.cuhe_paillier_set_fp64(self._ctx, int(enable)))
 
     @property
-    def fp64(self) -> bool:
-        return bool(self._lib.cuhe_paillier_get_fp64(self._ctx))
+    def fp64(self) -> int:
+        return int(self._lib.cuhe_paillier_get_fp64(self._ctx))
 
     def set_stream(self, stream: int | None) -> None:
         self._check(self._lib.cuhe_paillier_set_stream(self._ctx, ctypes.c_void_p(stream or 0)))

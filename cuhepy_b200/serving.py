@@ -22,10 +22,13 @@ kernels and run concurrently on several lanes whose streams have the
 highest priority, so their blocks are scheduled ahead of queued Paillier
 blocks; they are admitted in arrival order.  Paillier work saturates the GPU
 by itself (one query against a million vectors is a million products): it
-gets two lanes, so a request that arrives while a long one runs starts at
-once and the two share the GPU block by block, and the waiting request with
-the fewest queries goes next (shortest job first), unless the oldest has
-waited longer than ``age_limit_s``.  Paillier requests on a small index
+gets one lane fed in arrival order by default.  With ``age_limit_s`` > 0 the
+waiting request with the fewest queries goes next (shortest job first)
+unless the oldest has waited longer than that, and only while the oldest
+still fits in memory; with ``paillier_lanes`` > 1 requests share the GPU
+block by block.  (On the bench's 80%-load trace both lowered the median
+Paillier latency less than they raised its tail, so neither is the
+default.)  Paillier requests on a small index
 (a launch over one query would not fill the GPU) that are waiting when a
 lane frees up are merged into one launch (up to ``max_batch`` queries).
 The memory of a Paillier answer stays reserved until the caller releases
@@ -87,7 +90,7 @@ class Scheduler:
                  holds_memory: Callable[[str], bool] = lambda kind: True,
                  merge: Callable[[str], bool] = lambda kind: kind == "paillier",
                  mergeable: Callable[[Request], bool] = lambda req: True,
-                 pick: Callable[[str, Any, float], int] | None = None) -> None:
+                 pick: Callable[[str, Any, float, int], int] | None = None) -> None:
         if isinstance(lanes, int):
             lanes = {"paillier": lanes, "bfv": lanes}
         if not lanes or min(lanes.values()) < 1:
@@ -96,7 +99,7 @@ class Scheduler:
         self._holds = holds_memory
         self._merge = merge
         self._mergeable = mergeable
-        self._pick = pick or (lambda kind, queue, now: 0)
+        self._pick = pick or (lambda kind, queue, now, free: 0)
         self.lanes = dict(lanes)
         self.budget = int(budget_bytes)
         self.max_batch = int(max_batch)
@@ -188,7 +191,7 @@ class Scheduler:
         for kind, queue in self._queues.items():
             if not queue or not self._free[kind]:
                 continue
-            at = self._pick(kind, queue, now)
+            at = self._pick(kind, queue, now, self.budget - self.in_use)
             head = queue[at]
             if self.in_use + head.nbytes > self.budget:
                 continue
@@ -281,15 +284,22 @@ class Scheduler:
                 self._cv.notify_all()
 
 
-def shortest_first(age_limit_s: float) -> Callable[[str, Any, float], int]:
+def shortest_first(age_limit_s: float) -> Callable[[str, Any, float, int], int]:
     """A ``pick`` policy for :class:`Scheduler`: the waiting request with the
     fewest queries (the earliest among equals), unless the oldest request has
-    waited longer than ``age_limit_s``, which then goes first."""
+    waited longer than ``age_limit_s``, which then goes first.  A request may
+    overtake the oldest only if the oldest still fits in the free memory
+    after it, so an overtaking answer (whose memory stays reserved until its
+    caller releases it) never keeps the oldest request from being admitted:
+    a caller that reads its answers in submission order always progresses."""
 
-    def pick(kind: str, queue, now: float) -> int:
-        if len(queue) < 2 or now - queue[0].arrival > age_limit_s:
+    def pick(kind: str, queue, now: float, free: int) -> int:
+        head = queue[0]
+        if len(queue) < 2 or now - head.arrival > age_limit_s or head.nbytes > free:
             return 0
-        return min(range(len(queue)), key=lambda i: (queue[i].queries, i))
+        room = free - head.nbytes
+        return min((i for i in range(len(queue)) if i == 0 or queue[i].nbytes <= room),
+                   key=lambda i: (queue[i].queries, i))
 
     return pick
 
@@ -327,9 +337,9 @@ class KnnEvaluator:
     #: soon as its own launch ends
     MERGE_BELOW_VECTORS = 1 << 18
 
-    def __init__(self, device: int = 0, paillier_lanes: int = 2, bfv_lanes: int = 3, max_batch: int = 64,
+    def __init__(self, device: int = 0, paillier_lanes: int = 1, bfv_lanes: int = 3, max_batch: int = 64,
                  reserve_bytes: int = 2 << 30, budget_bytes: int | None = None,
-                 age_limit_s: float = 0.3) -> None:
+                 age_limit_s: float = 0.0) -> None:
         import torch
 
         self._torch = torch
@@ -460,10 +470,10 @@ class KnnEvaluator:
         so the next pick happens as soon as a lane frees."""
         return req.kind != "paillier" or self._paillier[req.index]["vectors"] < self.MERGE_BELOW_VECTORS
 
-    def _pick(self, kind: str, queue, now: float) -> int:
+    def _pick(self, kind: str, queue, now: float, free: int) -> int:
         """Paillier: shortest job first with aging; BFV searches (all of one
         size) in arrival order."""
-        return shortest_first(self.age_limit_s)(kind, queue, now) if kind == "paillier" else 0
+        return shortest_first(self.age_limit_s)(kind, queue, now, free) if kind == "paillier" else 0
 
     # -- execution ----------------------------------------------------------
     def _execute(self, kind: str, name: str, group: list[Request], lane: int, deliver) -> list[Any]:

@@ -80,15 +80,17 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p, int p_words
 /* 1 when factors are installed (decrypt / decode use the CRT kernel). */
 int cuhe_paillier_has_factors(const cuhe_paillier* ctx);
 
-/* Pipe of the CRT exponentiations (on by default).  With enable != 0 and the
- * factors installed, decrypt / decode run both half-width exponentiations as
- * Montgomery products of 52-bit limbs on the FP64 pipe (three exact FP64
- * instructions per 52x52-bit product, sums in 64-bit integers; the tunings
- * with eight 32-bit words per lane and side), entering and leaving through
- * the same 32-bit reduction, Garner recombination and epilogue, so results
- * are identical to the integer-pipe kernel; enable = 0 keeps every product
- * on the integer pipe.  No reference counterpart (the reference's CGBN
- * kernels multiply 32-bit words on the integer pipe). */
+/* Pipe of the CRT exponentiations.  With enable = 1 (the default) and the
+ * factors installed, decrypt / decode of keys with n^2 of 4096 or 8192 bits
+ * run both half-width exponentiations as Montgomery products of 52-bit limbs
+ * on the FP64 pipe (three exact FP64 instructions per 52x52-bit product,
+ * sums in 64-bit integers, ten limbs per lane, a 3-bit window), entering and
+ * leaving through the same 32-bit reduction, Garner recombination and
+ * epilogue, so results are identical to the integer-pipe kernel; n^2 of 2048
+ * bits stays on the integer pipe (measured faster there) unless enable = 2.
+ * enable = 0 keeps every product on the integer pipe.  get returns the
+ * setting.  No reference counterpart (the reference's CGBN kernels multiply
+ * 32-bit words on the integer pipe). */
 int cuhe_paillier_set_fp64(cuhe_paillier* ctx, int enable);
 int cuhe_paillier_get_fp64(const cuhe_paillier* ctx);
 
@@ -202,6 +204,10 @@ int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t coun
  * counterpart in the reference; it provides the denominator of the modexp
  * roofline. */
 int cuhe_imad_peak(int device, double* word_products_per_second);
+/* Measured FP64-pipe rate of `device` (fused multiply-adds per second, eight
+ * independent chains per thread, the rounding of the limb products), the
+ * ceiling of the FP64-pipe decode.  No reference counterpart. */
+int cuhe_fp64_peak(int device, double* fp64_per_second);
 
 /* Host-only helper (no device needed): the left-to-right sliding-window
  * schedule used for a fixed exponent.  Writes at most capacity ops, each

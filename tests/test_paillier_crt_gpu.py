@@ -131,12 +131,12 @@ def test_fp64_pipe_equals_integer_pipe(name):
     sk = keys["sk"]
     secret = (sk["a"], sk["g_a_inv"]) if "a" in sk else (sk["phi"], sk["inv"])
     _, crt, p, q = _pair(n, secret, sk["phi"])
-    assert crt.fp64
+    assert crt.fp64 == 1
     rng = random.Random(52)
     vals = _awkward(n, p, q, rng, count=3000)
     limbs = torch.from_numpy(crt.limbs(vals).view(np.int32)).cuda()
     outs, dists = [], []
-    for fp64 in (True, False):
+    for fp64 in (2, 0):
         crt.set_fp64(fp64)
         assert crt.fp64 == fp64
         out = torch.zeros((len(vals), crt.words), dtype=torch.int32, device="cuda")
@@ -146,7 +146,7 @@ def test_fp64_pipe_equals_integer_pipe(name):
         crt.synchronize()
         outs.append(out)
         dists.append(dist)
-    crt.set_fp64(True)
+    crt.set_fp64(1)
     assert torch.equal(outs[0], outs[1]) and torch.equal(dists[0], dists[1])
     from cuhepy_b200._limbs import from_limbs
 

@@ -279,3 +279,33 @@ def test_shortest_first_with_aging():
         for e in gate.events:
             e.set()
         s.stop()
+
+
+def test_overtaking_never_starves_the_oldest_of_memory():
+    """Shortest-first admission with answers that hold their memory: a small
+    request may overtake the oldest only while the oldest still fits, so a
+    caller reading answers in submission order is never blocked."""
+    from cuhepy_b200.serving import shortest_first
+
+    gate = Gate()
+    s = Scheduler(gate, lanes=2, budget_bytes=100, merge=lambda kind: False, pick=shortest_first(10.0))
+    s.start()
+    try:
+        s.submit(_req(queries=1, nbytes=30, payload="first"))
+        gate.wait_groups(1)
+        old_req = _req(queries=8, nbytes=60, payload="old")      # fits (30 + 60 <= 100) only alone
+        small_req = _req(queries=1, nbytes=20, payload="small")  # would leave 50 < 60: must not overtake
+        old, small = s.submit(old_req), s.submit(small_req)
+        gate.wait_groups(2)
+        assert old_req.admitted and not small_req.admitted
+        gate.open(0)
+        gate.open(1)
+        assert old.result(5)[1] == "old"
+        s.release(30)
+        s.release(60)
+        gate.open(2)
+        assert small.result(5)[1] == "small"
+    finally:
+        for e in gate.events:
+            e.set()
+        s.stop()
