@@ -44,6 +44,9 @@ PAILLIER_SIGNATURES: dict[str, tuple] = {
     "cuhe_paillier_set_factors": (ctypes.c_int, [ctypes.c_void_p, c_u32_p, ctypes.c_int, c_u32_p, ctypes.c_int]),
     "cuhe_paillier_has_factors": (ctypes.c_int, [ctypes.c_void_p]),
     "cuhe_paillier_set_fp64": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cuhe_paillier_from_hex": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64,
+                                              ctypes.c_int, ctypes.c_void_p]),
+    "cuhe_paillier_to_hex": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "cuhe_paillier_get_fp64": (ctypes.c_int, [ctypes.c_void_p]),
     "cuhe_paillier_encrypt": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_int64]),

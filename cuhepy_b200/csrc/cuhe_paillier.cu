@@ -1109,6 +1109,66 @@ int cuhe_paillier_mulmod(cuhe_paillier* ctx, const uint32_t* a, const uint32_t* 
   return check_status(ctx, st.staged());
 }
 
+int cuhe_paillier_from_hex(cuhe_paillier* ctx, const char* text, const int64_t* offsets, int64_t count, int reduce,
+                           uint32_t* out) {
+  if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (count == 0) return CUHE_OK;
+  if (!text || !offsets || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  if (offsets[0] != 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "offsets must start at 0");
+  for (int64_t i = 0; i < count; ++i)
+    if (offsets[i + 1] < offsets[i]) return fail(ctx, CUHE_INVALID_ARGUMENT, "offsets must not decrease");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  Dispatch d;
+  find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  const size_t text_bytes = size_t(offsets[count]);
+  const size_t bytes = size_t(count) * ctx->K * 4;
+  Stager st(ctx);
+  st.add(text, text_bytes ? text_bytes : 1, true, false);
+  st.add(offsets, size_t(count + 1) * 8, true, false);
+  st.add(out, bytes, false, true);
+  if (int rc = st.bind()) return rc;
+  const long long threads = count * ctx->K;
+  cuhe::k_hex_to_limbs<<<unsigned((threads + 255) / 256), 256, 0, ctx->stream>>>(
+      (const char*)st.dev(0), (const long long*)st.dev(1), count, ctx->K, (uint32_t*)st.dev(2), ctx->d_status);
+  CUHE_CUDA(ctx, cudaGetLastError(), "hex parse launch");
+  if (reduce) {
+    // x mod n^2 for any x < 2^(32K): (x R mod n^2) R^-1
+    CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(2), (uint32_t*)st.dev(2), count, 2), "reduce launch");
+    CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(2), (uint32_t*)st.dev(2), count, 0), "reduce launch");
+  }
+  if (int rc = st.finish()) return rc;
+  int status = 0;
+  CUHE_CUDA(ctx, cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status");
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "hex parse");
+  if (status) {
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+    if (status & cuhe::ST_HEX) return fail(ctx, CUHE_INVALID_ARGUMENT, "Invalid hex digit");
+    return fail(ctx, CUHE_RANGE, "input outside its valid range");
+  }
+  return CUHE_OK;
+}
+
+int cuhe_paillier_to_hex(cuhe_paillier* ctx, const uint32_t* limbs, int64_t count, char* out) {
+  if (!ctx || count < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");
+  if (count == 0) return CUHE_OK;
+  if (!limbs || !out) return fail(ctx, CUHE_INVALID_ARGUMENT, "null buffer");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  const size_t words = size_t(ctx->K);
+  Stager st(ctx);
+  st.add(limbs, size_t(count) * words * 4, true, false);
+  st.add(out, size_t(count) * words * 8, false, true);
+  if (int rc = st.bind()) return rc;
+  const long long threads = count * ctx->K;
+  cuhe::k_limbs_to_hex<<<unsigned((threads + 255) / 256), 256, 0, ctx->stream>>>(
+      (const uint32_t*)st.dev(0), count, ctx->K, (char*)st.dev(1));
+  CUHE_CUDA(ctx, cudaGetLastError(), "hex format launch");
+  if (int rc = st.finish()) return rc;
+  CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "hex format");
+  return CUHE_OK;
+}
+
 int cuhe_paillier_mulmod_outer(cuhe_paillier* ctx, const uint32_t* query, int64_t nq, const uint32_t* index,
                                int64_t nx, uint32_t* out) {
   if (!ctx || nq < 0 || nx < 0) return fail(ctx, CUHE_INVALID_ARGUMENT, "invalid argument");

@@ -995,12 +995,69 @@ k_convert(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long long
   uint32_t n2[L], x[L];
   g.load_ro(n2, consts + C_N2 * K);
   g.load(x, in + inst * K);
-  if (!g.less_than(x, n2)) {
+  // to_mont == 2: any x < 2^(32K) (x R mod n^2: the CIOS bound holds for any
+  // first operand below R), the first half of a reduction mod n^2
+  if (to_mont != 2 && !g.less_than(x, n2)) {
     if (g.gl == 0) atomicOr(status, ST_RANGE);
     return;
   }
   g.mont_mul(x, x, smem, n2, ks.ninv2);
   g.store(out + inst * K, x);
+}
+
+// Hexadecimal text <-> little-endian 32-bit limbs, one thread per limb.
+// Value i is text[offsets[i], offsets[i+1]) with an optional 0x / 0X
+// prefix; limb w holds the digits 8w .. 8w+7 counted from the right, digits
+// beyond the K-th limb are dropped (the reference's hex_to_le_words keeps
+// the low limbs), and any character that is not a hex digit sets ST_HEX.
+enum : int { ST_HEX = 2 };
+
+__device__ __forceinline__ int hex_value(char c) {
+  if (c >= '0' && c <= '9') return c - '0';
+  if (c >= 'a' && c <= 'f') return c - 'a' + 10;
+  if (c >= 'A' && c <= 'F') return c - 'A' + 10;
+  return -1;
+}
+
+__global__ void k_hex_to_limbs(const char* __restrict__ text, const long long* __restrict__ offsets, long long count,
+                               int words, uint32_t* __restrict__ out, int* status) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count * words) return;
+  const long long i = t / words;
+  const int w = int(t - i * words);
+  long long s = offsets[i];
+  const long long e = offsets[i + 1];
+  if (e - s >= 2 && text[s] == '0' && (text[s + 1] == 'x' || text[s + 1] == 'X')) s += 2;
+  uint32_t v = 0;
+  bool bad = false;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const long long pos = e - 1 - 8ll * w - j;
+    if (pos >= s) {
+      const int d = hex_value(text[pos]);
+      bad |= d < 0;
+      v |= uint32_t(d < 0 ? 0 : d) << (4 * j);
+    }
+  }
+  if (w == words - 1)
+    for (long long pos = s; pos < e - 8ll * words; ++pos) bad |= hex_value(text[pos]) < 0;
+  out[t] = v;
+  if (bad) atomicOr(status, ST_HEX);
+}
+
+// out[i * 8 words ...]: value i as 8 * words lowercase digits, most significant first
+__global__ void k_limbs_to_hex(const uint32_t* __restrict__ limbs, long long count, int words, char* __restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count * words) return;
+  const long long i = t / words;
+  const int w = int(t - i * words);
+  const uint32_t v = limbs[t];
+  char* o = out + i * 8ll * words + 8ll * (words - 1 - w);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const uint32_t d = (v >> (4 * (7 - j))) & 15u;
+    o[j] = char(d < 10 ? '0' + d : 'a' + d - 10);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -45,6 +45,26 @@ def _bits_array(embeddings: Sequence[Sequence[int]], embed_len: int) -> np.ndarr
     return np.ascontiguousarray(arr, dtype=np.uint8)
 
 
+def _chunk_plaintexts(bits: np.ndarray, chunk_len: int, chunk_num: int, words: int) -> np.ndarray:
+    """Hamming plaintexts [vectors * chunk_num, words] (little-endian u32) of
+    a [vectors, embed_len] bit matrix: bit j at padded position 2j + 1 of the
+    string "0 b_0 0 b_1 ...", cut into chunk_len-bit chunks, each read most
+    significant bit first (hamming/paillier.py:76-88), vectorised."""
+    vectors, embed = bits.shape
+    padded = np.zeros((vectors, 2 * embed), dtype=np.uint8)
+    padded[:, 1::2] = bits
+    # chunk c is the substring [c chunk_len, (c + 1) chunk_len) of the padded
+    # string (the last one possibly shorter), right-aligned in chunk_len bits
+    chunks = np.zeros((vectors, chunk_num, chunk_len), dtype=np.uint8)
+    for c in range(chunk_num):
+        piece = padded[:, c * chunk_len:(c + 1) * chunk_len]
+        chunks[:, c, chunk_len - piece.shape[1]:] = piece
+    big = np.packbits(chunks.reshape(vectors * chunk_num, chunk_len), axis=1, bitorder="big")  # MSB first
+    out = np.zeros((vectors * chunk_num, 4 * words), dtype=np.uint8)
+    out[:, :big.shape[1]] = big[:, ::-1]
+    return out.view(np.uint32)
+
+
 def _as_int(value) -> int:
     if isinstance(value, bytes):
         return int.from_bytes(value, "little")
@@ -350,18 +370,19 @@ class PaillierGPUClient:
         return self.keys
 
     def encrypt(self, embeddings: Sequence[Sequence[int]]) -> list[list[str]]:
+        """paillier_GPU_client.cu:873-974: each embedding's bits padded to "0b"
+        pairs, cut into chunk_len-bit chunks read most significant first (the
+        reference CPU client's int(bits, 2)), encrypted with r drawn as in
+        Paillier.encrypt; ciphertexts as hex strings formatted on the device."""
         keys = self._need_keys("encrypt")
         if len(embeddings) == 0:
             return []
         bits = _bits_array(embeddings, self._embed_len)
-        plaintexts = []
-        for row in bits:
-            padded = "".join("0" + str(int(b)) for b in row)
-            for c in range(self._chunk_num):
-                piece = padded[c * self._chunk_len:(c + 1) * self._chunk_len]
-                plaintexts.append(int(piece, 2) if piece else 0)
+        ctx = device_for(int(keys["pk"]["n"]))
+        m = _chunk_plaintexts(bits, self._chunk_len, self._chunk_num, ctx.words)
+        plaintexts = [int.from_bytes(row.tobytes(), "little") for row in m]
         cts = Paillier.encrypt_batch(plaintexts, keys["pk"])
-        hexes = [format(c, "x") for c in cts]
+        hexes = ctx.to_hex(ctx.limbs(cts))
         return [hexes[i * self._chunk_num:(i + 1) * self._chunk_num] for i in range(len(bits))]
 
     def encode_hamming_client(self, ct1: Sequence[str], ct2: Sequence[str]) -> list[str]:
@@ -370,25 +391,47 @@ class PaillierGPUClient:
 
     @staticmethod
     def encode_hamming_server(ct1: Sequence[str], ct2: Sequence[str], pk: dict) -> list[str]:
+        """ct1[i] * ct2[i] mod n^2 on hex strings (paillier_GPU_client.cu:672-732):
+        parsing, the products and formatting all on the device."""
         if len(ct1) != len(ct2):
             raise RuntimeError("encode_hamming_*: ct1 and ct2 must have the same length")
         n2 = int(str(pk["n_squared"]), 16)
         n = math.isqrt(n2)
         if n * n != n2:
             raise RuntimeError("encode_hamming_server: n_squared is not a perfect square")
-        out = device_for(n).mulmod([int(str(c), 16) for c in ct1], [int(str(c), 16) for c in ct2])
-        return [format(c, "x") for c in out]
+        if not ct1:
+            return []
+        ctx = device_for(n)
+        try:
+            a = ctx.from_hex([str(c) for c in ct1])
+            b = ctx.from_hex([str(c) for c in ct2])
+        except ValueError as exc:
+            raise RuntimeError(str(exc)) from exc
+        out = ctx.empty(len(ct1))
+        ctx.mulmod_array(a, b, out, len(ct1))
+        return ctx.to_hex(out)
 
     def decode_hamming_client(self, ciphers_hex_batch: Sequence[Sequence[str]]) -> list[int]:
+        """paillier_GPU_client.cu:995-1038 on the device: hex parsing, c^phi,
+        L(), * phi^-1 and the odd-bit count."""
         keys = self._need_keys("decode_hamming_client")
-        rows = []
+        flat = []
         for row in ciphers_hex_batch:
             if len(row) != self._chunk_num:
                 raise RuntimeError("decode_hamming_client: each inner list must have length == chunk_num")
-            rows.append([int(str(c), 16) for c in row])
+            flat.extend(str(c) for c in row)
+        if not flat:
+            return []
         ctx = device_for(int(keys["pk"]["n"]), (int(keys["sk"]["phi"]), int(keys["sk"]["inv"])),
                          phi=keys["sk"]["phi"])
-        return ctx.decode_hamming(rows, self._chunk_num, self._chunk_len)
+        try:
+            c = ctx.from_hex(flat)
+        except ValueError as exc:
+            raise RuntimeError(str(exc)) from exc
+        vectors = len(flat) // self._chunk_num
+        out = np.zeros(vectors, dtype=np.int64)
+        ctx.decode_array(c, vectors, self._chunk_num, self._chunk_len, out)
+        return [int(v) for v in out]
 
     def get_pk_hex(self) -> tuple[str, str]:
         pk = self._need_keys("get_pk_hex")["pk"]

@@ -214,6 +214,37 @@ class PaillierDevice:
     def lookup_encrypt_ints_array(self, m, count: int, noise_index, out) -> None:
         self._check(self._lib.cuhe_lookup_encrypt_ints(self._ctx, _ptr(m), int(count), _ptr(noise_index), _ptr(out)))
 
+    # -- hexadecimal wire format (parsed and formatted on the device) --------
+    def from_hex(self, strings: Sequence[str], reduce: bool = True) -> np.ndarray:
+        """Limb array [count, K] of hexadecimal strings (optional 0x prefix),
+        reduced mod n^2 unless reduce is False; digits beyond K words are
+        dropped.  ValueError("Invalid hex digit") on any other character."""
+        count = len(strings)
+        if count == 0:
+            return np.zeros((0, self.words), dtype=np.uint32)
+        try:
+            text = "".join(strings).encode("ascii")
+        except (UnicodeEncodeError, TypeError) as exc:
+            raise ValueError("Invalid hex digit") from exc
+        offsets = np.zeros(count + 1, dtype=np.int64)
+        np.cumsum(np.fromiter((len(x) for x in strings), dtype=np.int64, count=count), out=offsets[1:])
+        out = self.empty(count)
+        self._check(self._lib.cuhe_paillier_from_hex(self._ctx, text, offsets.ctypes.data, count, int(reduce),
+                                                     out.ctypes.data))
+        return out
+
+    def to_hex(self, limbs) -> list[str]:
+        """Lowercase hexadecimal strings (no prefix, no leading zeros, "0" for
+        zero) of a limb array [count, K], formatted on the device."""
+        count = int(limbs.shape[0])
+        if count == 0:
+            return []
+        width = 8 * self.words
+        buf = ctypes.create_string_buffer(count * width)
+        self._check(self._lib.cuhe_paillier_to_hex(self._ctx, _ptr(limbs), count, buf))
+        text = buf.raw.decode("ascii")
+        return [text[i * width:(i + 1) * width].lstrip("0") or "0" for i in range(count)]
+
     # -- Python-integer conveniences ----------------------------------------
     def encrypt(self, plaintexts: Sequence[int], rs: Sequence[int]) -> list[int]:
         if len(plaintexts) != len(rs):

@@ -157,6 +157,23 @@ int cuhe_paillier_modexp_each(cuhe_paillier* ctx, const uint32_t* base, const ui
 /* out[i] = a[i] * b[i] mod n^2.  Replaces Paillier.add / PaillierLookup.add
  * (scheme.py:107-119; lookup.py:282-294) and modmul_pointwise_kernel behind
  * encode_hamming_server (paillier_GPU_lookup_client.cu:811-835, 2312-2335). */
+/* Hexadecimal wire format on the device.  from_hex parses `count` strings
+ * given as one host text buffer and count + 1 host offsets (string i is
+ * text[offsets[i], offsets[i+1]), offsets[0] = 0): an optional 0x / 0X
+ * prefix, upper- or lower-case digits, leading zeros allowed; out (host or
+ * device, count x K words) receives the little-endian limbs, the digits
+ * beyond K words dropped as the reference's hex_to_le_words does
+ * (src/cuhepy/paillier/_gpu_ext/paillier_GPU_client.cu:218-262); any other
+ * character returns CUHE_INVALID_ARGUMENT with "Invalid hex digit" (its
+ * hex_nibble).  reduce != 0 then reduces every value mod n^2 on the device
+ * (the reference's CGBN products reduce inputs of any width).  to_hex writes
+ * count x 8K lowercase digits, most significant first, leading zeros kept
+ * (the reference's le_words_to_hex strips them; the caller does).  Replace
+ * the per-string host conversions of paillier_GPU_client.cu:235-279. */
+int cuhe_paillier_from_hex(cuhe_paillier* ctx, const char* text, const int64_t* offsets, int64_t count, int reduce,
+                           uint32_t* out);
+int cuhe_paillier_to_hex(cuhe_paillier* ctx, const uint32_t* limbs, int64_t count, char* out);
+
 int cuhe_paillier_mulmod(cuhe_paillier* ctx, const uint32_t* a, const uint32_t* b, uint32_t* out,
                          int64_t count);
 

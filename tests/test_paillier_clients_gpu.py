@@ -309,3 +309,46 @@ def test_reference_gpu_client_flow_small_embedding():
         again = clone.encode_hamming_server(clone.encrypt_vec_one(vectors[0]), clone.encrypt_vec_one(vectors[1]))
         assert clone.decode_hamming_client_one(again) == _hamming(vectors[0], vectors[1])
         assert json.loads(clone.stringify_config()) == config
+
+
+def test_hex_wire_format_on_the_device():
+    """Hex strings <-> limbs parsed and formatted on the device, with the
+    reference's hex_to_le_words / le_words_to_hex semantics
+    (paillier_GPU_client.cu:218-262): optional 0x / 0X prefix, either case,
+    leading zeros, digits beyond the width dropped, "Invalid hex digit"
+    otherwise; values at or above n^2 reduced when asked."""
+    from cuhepy_b200.paillier.clients import PaillierGPUClient
+    from cuhepy_b200.paillier.gpu import device_for
+
+    data = load_golden("paillier_1024.json")
+    n2 = hx(data["pk"]["n_squared"])
+    n = hx(data["pk"]["n"])
+    ctx = device_for(n)
+    width = 32 * ctx.words
+    rng = random.Random(16)
+    vals = [0, 1, n2 - 1, n2, n2 + 5, (1 << width) - 1] + [rng.randrange(1 << width) for _ in range(300)]
+    texts = [format(v, "x") for v in vals]
+    texts[2] = "0x" + texts[2].upper()
+    texts[3] = "000" + texts[3]
+    texts.append("")                                  # the reference reads an empty string as 0
+    texts.append("f" * 8 + format(12345, "x").zfill(8 * ctx.words))  # digits beyond the width are dropped
+    vals += [0, 12345]
+    from cuhepy_b200._limbs import from_limbs
+
+    raw = from_limbs(ctx.from_hex(texts, reduce=False))
+    assert raw == vals
+    reduced = from_limbs(ctx.from_hex(texts))
+    assert reduced == [v % n2 for v in vals]
+    assert ctx.to_hex(ctx.limbs(reduced)) == [format(v, "x") for v in reduced]
+    with pytest.raises(ValueError, match="Invalid hex digit"):
+        ctx.from_hex(["12g4"])
+    with pytest.raises(ValueError, match="Invalid hex digit"):
+        ctx.from_hex(["ab cd"])
+    with pytest.raises(ValueError, match="Invalid hex digit"):
+        ctx.from_hex(["é"])
+    # the client's products reduce inputs of any width, as the reference's CGBN kernel does
+    a, b = vals[10], vals[11]
+    out = PaillierGPUClient.encode_hamming_server([format(a, "x")], [format(b, "x")], {"n_squared": format(n2, "x")})
+    assert out == [format(a * b % n2, "x")]
+    with pytest.raises(RuntimeError, match="Invalid hex digit"):
+        PaillierGPUClient.encode_hamming_server(["zz"], ["1"], {"n_squared": format(n2, "x")})
