@@ -83,12 +83,26 @@ __host__ __device__ constexpr size_t plane_smem_words(int n) { return size_t(n) 
 // length whose first stage has already run; its stage s is the full
 // transform's stage s + 1, whose twiddles for this half start at m (2 + half)
 // instead of m.
+// Lazy bounds (every ring prime is below 2^60, so 16p < 2^64): a pass takes
+// values below 16p, its first stage brings u below 8p with one conditional
+// subtraction, and each stage adds less than 2p (the Shoup product is below
+// 2p for any 64-bit input), so after at most four stages the values are
+// below 16p again.  Only the first stage of a pass corrects u; `last` then
+// reduces the outputs to [0, p).
+__device__ __forceinline__ u64 reduce_below_16p(u64 v, u64 p) {
+  v = v >= 8 * p ? v - 8 * p : v;
+  v = v >= 4 * p ? v - 4 * p : v;
+  v = v >= 2 * p ? v - 2 * p : v;
+  return v >= p ? v - p : v;
+}
+
 template <int P, bool kHalf = false>
 __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const ulonglong2* __restrict__ w2,
                                                  u64 p, bool last, int half_id = 0) {
+  static_assert(P >= 1 && P <= 4, "at most four stages per pass keep values below 16p");
   constexpr int E = 1 << P;
   const int n = 1 << logn;
-  const u64 two_p = 2 * p;
+  const u64 two_p = 2 * p, eight_p = 8 * p;
   const int g = n >> (s0 + 1);
   const int stride = g >> (P - 1);
   const int log_stride = (logn - s0 - 1) - (P - 1);
@@ -110,21 +124,14 @@ __device__ __forceinline__ void ntt_forward_pass(u64* a, int s0, int logn, const
         const ulonglong2 tw = __ldg(w2 + idx);
         const u64 root = tw.x, rq = tw.y;
         u64 u = x[k];
-        if (u >= two_p) u -= two_p;
+        if (t == 0 && u >= eight_p) u -= eight_p;
         const u64 v = shoup_lazy(x[k + half], root, rq, p);
         x[k] = u + v;
         x[k + half] = u + two_p - v;
       }
     }
 #pragma unroll
-    for (int k = 0; k < E; ++k) {
-      u64 v = x[k];
-      if (last) {
-        if (v >= two_p) v -= two_p;
-        if (v >= p) v -= p;
-      }
-      a[sp(base + k * stride)] = v;
-    }
+    for (int k = 0; k < E; ++k) a[sp(base + k * stride)] = last ? reduce_below_16p(x[k], p) : x[k];
   }
 }
 
@@ -178,14 +185,17 @@ __device__ __forceinline__ void ntt_inverse_pass(u64* a, int u0, int logn, const
 // kHalf: the plane is half `half_id` of a transform of length 2^(logn + 1)
 // (logn = R.logn - 1): forward after that transform's first stage, inverse
 // before its last (whose 1/N and twist the caller applies).
+// canonical = false leaves the outputs below 16p (for callers that only
+// multiply them by Shoup products).
 template <bool kHalf = false>
-__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4, int half_id = 0) {
+__device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j, int max_p = 4, int half_id = 0,
+                                                 bool canonical = true) {
   const int logn = kHalf ? R.logn - 1 : R.logn;
   const u64 p = R.prime[j].p;
   const ulonglong2* w2 = R.fwd2[j];
   for (int s0 = 0; s0 < logn; s0 += max_p) {
     const int P = logn - s0 < max_p ? logn - s0 : max_p;
-    const bool last = s0 + P == logn;
+    const bool last = canonical && s0 + P == logn;
     switch (P) {
       case 4: ntt_forward_pass<4, kHalf>(a, s0, logn, w2, p, last, half_id); break;
       case 3: ntt_forward_pass<3, kHalf>(a, s0, logn, w2, p, last, half_id); break;
@@ -196,7 +206,7 @@ __device__ __forceinline__ void ntt_forward_fast(u64* a, const RingDev& R, int j
   }
 }
 
-// The first `stages` stages of the forward transform (outputs below 4p);
+// The first `stages` stages of the forward transform (outputs below 16p);
 // the caller applies the rest.
 __device__ __forceinline__ void ntt_forward_stages(u64* a, const RingDev& R, int j, int max_p, int stages) {
   const int logn = R.logn;
@@ -338,14 +348,12 @@ __device__ __forceinline__ void ntt_plane(u64* data, const RingDev* __restrict__
       u64 x0 = s_plane[at], x1 = s_plane[at + 1];
       if (pairs && !inverse) {
         // the last forward stage: gap 1, twiddle (N/2 + i), canonical outputs
+        // (inputs below 16p: u is brought below 8p, the outputs are below 10p)
         const ulonglong2 tw = __ldg(w2 + half_n + i);
-        if (x0 >= two_p) x0 -= two_p;
+        if (x0 >= 8 * p) x0 -= 8 * p;
         const u64 v = shoup_lazy(x1, tw.x, tw.y, p);
-        u64 y0 = x0 + v, y1 = x0 + two_p - v;
-        y0 = y0 >= two_p ? y0 - two_p : y0;
-        y1 = y1 >= two_p ? y1 - two_p : y1;
-        x0 = y0 >= p ? y0 - p : y0;
-        x1 = y1 >= p ? y1 - p : y1;
+        x1 = reduce_below_16p(x0 + two_p - v, p);
+        x0 = reduce_below_16p(x0 + v, p);
       }
       dst[i] = make_ulonglong2(x0, x1);
     }
@@ -375,7 +383,7 @@ __device__ __forceinline__ int plane_prime(long long b, int prime_base, int prim
   return prime_base + int((b / prime_block) % prime_mod);
 }
 
-// forward stage 0 (inputs canonical; outputs below 4p, as the passes take)
+// forward stage 0 (inputs canonical; outputs below 4p, within the passes' 16p)
 // or, with kInverse, the final inverse stage (inputs below 2p, outputs
 // canonical); one thread per pair (i, i + N/2)
 template <bool kInverse>
@@ -884,12 +892,16 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
   };
   const ulonglong2* w2 = R.fwd2[j];
   const int half_n = n >> 1;
+  // each digit adds a key product below 2p: with at most eight digits the
+  // sums stay below 16p and are reduced once, at the last digit
+  const bool lazy_sum = R.digits <= 8;
   for (int d = 0; d < R.digits; ++d) {
     for (int i = threadIdx.x; i < n; i += kThreads)
       s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
     __syncthreads();
+    // the digit transforms feed only the Shoup key products: no canonical pass
     if (pairs) ntt_forward_stages(s_plane, R, j, MAXP, R.logn - 1);
-    else ntt_forward_fast(s_plane, R, j, MAXP);
+    else ntt_forward_fast(s_plane, R, j, MAXP, 0, false);
     const long long k0o = ((long long)(d * 2 + 0) * L + j) * n, k1o = ((long long)(d * 2 + 1) * L + j) * n;
     const bool last = d + 1 == R.digits;
 #pragma unroll 1
@@ -906,18 +918,14 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
         for (int kp = 0; kp < 2; ++kp) {
           const int b = int(threadIdx.x) + (c * 2 + kp) * kThreads;
           if (b < half_n) {
-            // the last forward stage: gap 1, twiddle (N/2 + b)
+            // the last forward stage: gap 1, twiddle (N/2 + b); the outputs
+            // (below 10p) only enter Shoup products, so they stay unreduced
             u64 u = s_plane[sp(2 * b)];
             const u64 x1 = s_plane[sp(2 * b + 1)];
             const ulonglong2 tw = __ldg(w2 + half_n + b);
-            if (u >= two_p) u -= two_p;
+            if (u >= 8 * p) u -= 8 * p;
             const u64 v = shoup_lazy(x1, tw.x, tw.y, p);
-            u64 y[2] = {u + v, u + two_p - v};
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              y[e] = y[e] >= two_p ? y[e] - two_p : y[e];
-              y[e] = y[e] >= p ? y[e] - p : y[e];
-            }
+            const u64 y[2] = {u + v, u + two_p - v};
             // one key component at a time keeps fewer registers live
             u64 out0[2];
 #pragma unroll
@@ -930,8 +938,8 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
                 const int col = 4 * (2 * kp + e) + 2 * comp;
                 u64 a = shoup_lazy(y[e], e ? kv.y : kv.x, e ? kq.y : kq.x, p);
                 a += u64(acc[col]) | (u64(acc[col + 1]) << 32);
-                a = a >= two_p ? a - two_p : a;
-                if (last) a = a >= p ? a - p : a;
+                if (!lazy_sum) a = a >= two_p ? a - two_p : a;
+                if (last) a = lazy_sum ? reduce_below_16p(a, p) : a >= p ? a - p : a;
                 if (comp == 0) out0[e] = a;
                 acc[col] = uint32_t(a);
                 acc[col + 1] = uint32_t(a >> 32);
@@ -955,11 +963,13 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
             u64 a1 = shoup_lazy(v, __ldg(op.key + k1o + i), __ldg(op.key_q + k1o + i), p);
             a0 += u64(acc[4 * kk]) | (u64(acc[4 * kk + 1]) << 32);
             a1 += u64(acc[4 * kk + 2]) | (u64(acc[4 * kk + 3]) << 32);
-            a0 = a0 >= two_p ? a0 - two_p : a0;
-            a1 = a1 >= two_p ? a1 - two_p : a1;
+            if (!lazy_sum) {
+              a0 = a0 >= two_p ? a0 - two_p : a0;
+              a1 = a1 >= two_p ? a1 - two_p : a1;
+            }
             if (last) {
-              a0 = a0 >= p ? a0 - p : a0;
-              a1 = a1 >= p ? a1 - p : a1;
+              a0 = lazy_sum ? reduce_below_16p(a0, p) : a0 >= p ? a0 - p : a0;
+              a1 = lazy_sum ? reduce_below_16p(a1, p) : a1 >= p ? a1 - p : a1;
               s_plane[sp(i)] = a0;  // component 0 transforms first
             }
             acc[4 * kk] = uint32_t(a0);
