@@ -896,8 +896,33 @@ k_keyswitch_tm(const SwitchOp* __restrict__ ops, const RingDev* __restrict__ rin
   // sums stay below 16p and are reduced once, at the last digit
   const bool lazy_sum = R.digits <= 8;
   for (int d = 0; d < R.digits; ++d) {
-    for (int i = threadIdx.x; i < n; i += kThreads)
-      s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
+    const int start = d * R.digit_bits, limb = start / 64, off = start % 64;
+    if (R.digit_bits <= 63) {
+      // digits below 2^63 < 16p enter the lazy transform unreduced; the
+      // words of four coefficients are loaded before any is used
+      const u64 dmask = (u64(1) << R.digit_bits) - 1;
+      const bool two = off && off + R.digit_bits > 64 && limb + 1 < W;
+      for (int i0 = int(threadIdx.x); i0 < n; i0 += 4 * kThreads) {
+        u64 w0[4], w1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int i = i0 + u * kThreads;
+          const u64* w = op.words + (long long)i * W;
+          w0[u] = i < n && limb < W ? w[limb] : 0;
+          w1[u] = i < n && two ? w[limb + 1] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int i = i0 + u * kThreads;
+          u64 v = w0[u] >> off;
+          if (two) v |= w1[u] << (64 - off);
+          if (i < n) s_plane[sp(i)] = v & dmask;
+        }
+      }
+    } else {
+      for (int i = threadIdx.x; i < n; i += kThreads)
+        s_plane[sp(i)] = gadget_digit(op.words + (long long)i * W, W, d, R, j);
+    }
     __syncthreads();
     // the digit transforms feed only the Shoup key products: no canonical pass
     if (pairs) ntt_forward_stages(s_plane, R, j, MAXP, R.logn - 1);
