@@ -237,3 +237,60 @@ def test_graph_replays_repeat_identically():
             assert all(torch.equal(a, b) for a, b in zip(got, first))
     assert all(int(out.abs().sum()) > 0 for out in outs)
     mb.close()
+
+
+def test_ntt_extreme_values_round_trip_and_ring_map():
+    """Planes of p - 1 everywhere (and alternating p - 1 / 0) drive the lazy
+    forward butterflies to their bound: every degree's forward transform,
+    at every radix that compiles, must invert exactly and, at N = 256, still
+    be the ring map (NTT(a * b) = NTT(a) NTT(b) with a schoolbook product)."""
+    import numpy as np
+    import torch
+
+    from cuhepy_b200.bfv import _bfv_rns as m
+
+    for n in (8, 16, 64, 1024, 4096, 8192, 16384, 32768):
+        ring, primes = _ring(n, 2)
+        rows = []
+        for b in range(4):
+            p = primes[b % 2]
+            if b < 2:
+                rows.append([p - 1] * n)
+            elif b == 2:
+                rows.append([p - 1 if i % 2 == 0 else 0 for i in range(n)])
+            else:
+                rows.append([p - 1] * (n - 1) + [0])
+        base = torch.from_numpy(np.array(rows, dtype=np.uint64).view(np.int64)).cuda()
+        want = None
+        for radix in ((1, 2, 3, 4) if n in (4096, 8192) else (0,)):
+            x = base.clone()
+            m.ntt(ring, x, 2, radix_log=radix)
+            fwd = x.clone()
+            m.ntt(ring, x, 2, inverse=True, radix_log=radix)
+            torch.cuda.synchronize()
+            assert torch.equal(x, base), (n, radix)
+            vals = fwd.cpu().numpy().view(np.uint64)
+            for b in range(4):
+                assert int(vals[b].max()) < primes[b % 2], (n, radix, b)  # canonical outputs
+            if want is None:
+                want = fwd
+            assert torch.equal(fwd, want), (n, radix)
+    small, sp = _ring(256, 2)
+    for j, p in enumerate(sp):
+        a = [p - 1] * 256
+        b = [p - 1 if i % 3 else 0 for i in range(256)]
+        c = [0] * 256
+        for i, ai in enumerate(a):
+            for k, bk in enumerate(b):
+                if i + k < 256:
+                    c[i + k] += ai * bk
+                else:
+                    c[i + k - 256] -= ai * bk
+        c = [v % p for v in c]
+        full = torch.zeros((3 * len(sp), 256), dtype=torch.int64, device="cuda")
+        for k, row in enumerate((a, b, c)):
+            full[k * len(sp) + j] = torch.from_numpy(np.array(row, dtype=np.uint64).view(np.int64))
+        m.ntt(small, full, len(sp))
+        torch.cuda.synchronize()
+        fa, fb, fc = ([int(v) for v in full[k * len(sp) + j].cpu().numpy().view(np.uint64)] for k in range(3))
+        assert [x * y % p for x, y in zip(fa, fb)] == fc
