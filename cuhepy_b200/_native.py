@@ -68,6 +68,8 @@ PAILLIER_SIGNATURES: dict[str, tuple] = {
     "cuhe_lookup_build_tables": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                 ctypes.c_int]),
     "cuhe_lookup_get_g_table": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cuhe_lookup_set_wide_table": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "cuhe_lookup_wide_table_ready": (ctypes.c_int, [ctypes.c_void_p]),
     "cuhe_lookup_encrypt_bits": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
                                                 ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "cuhe_lookup_encrypt_ints": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,

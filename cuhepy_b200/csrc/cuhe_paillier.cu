@@ -104,6 +104,8 @@ struct cuhe_paillier {
   bool fp64_small = false;    // ... and for n^2 of 2048 bits (set_fp64(ctx, 2))
   uint32_t* d_gtab = nullptr;
   int message_chunks = 0;
+  uint32_t* d_wide = nullptr;  // 16-bit-digit table W[j][D], built on demand (see cuhe_lookup_set_wide_table)
+  int wide_mode = 1;           // 0 never, 1 for large batches when it fits, 2 always
   uint32_t* d_noise = nullptr;
   int noise_entries = 0;
   DeviceBuffer work;
@@ -261,15 +263,27 @@ template <int K, int TPI>
 cudaError_t launch_lookup(cuhe_paillier* ctx, const uint8_t* bits, int embed_len, int chunk_len, int chunk_num,
                           const uint32_t* plain, long long count, const uint8_t* idx, uint32_t* out) {
   constexpr int IPB = cuhe::kBlockThreads / TPI;
-  const size_t rows_bytes = size_t(IPB) * ctx->message_chunks * 2;
+  const size_t rows_bytes = size_t(IPB) * cuhe::lookup_rows_stride(ctx->message_chunks) * 2;
   const size_t smem = size_t(K + IPB * cuhe::inst_stride_words<K>(1)) * 4 + ((rows_bytes + 15) & ~size_t(15));
-  cudaError_t e = cudaFuncSetAttribute(cuhe::k_lookup_encrypt<K, TPI>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  const bool wide = ctx->d_wide != nullptr;
+  auto kernel = wide ? cuhe::k_lookup_encrypt<K, TPI, true> : cuhe::k_lookup_encrypt<K, TPI, false>;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   const long long blocks = (count + IPB - 1) / IPB;
-  cuhe::k_lookup_encrypt<K, TPI><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
-      bits, embed_len, chunk_len, chunk_num, plain, K, count, ctx->message_chunks, ctx->d_gtab, ctx->d_noise,
-      ctx->noise_entries, idx, out, ctx->d_consts, ctx->ks, ctx->d_status);
+  kernel<<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      bits, embed_len, chunk_len, chunk_num, plain, K, count, ctx->message_chunks, wide ? ctx->d_wide : ctx->d_gtab,
+      ctx->d_noise, ctx->noise_entries, idx, out, ctx->d_consts, ctx->ks, ctx->d_status);
+  return cudaGetLastError();
+}
+
+// W[j][D] = G[2j][D mod 256] * G[2j+1][D / 256] for every 16-bit D.
+template <int K, int TPI>
+cudaError_t launch_wide_table(cuhe_paillier* ctx, uint32_t* wide) {
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  const size_t smem = size_t(IPB * cuhe::inst_stride_words<K>(1)) * 4;
+  const long long entries = (long long)((ctx->message_chunks + 1) / 2) * 65536;
+  cuhe::k_wide_table<K, TPI><<<dim3(unsigned((entries + IPB - 1) / IPB)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      ctx->d_gtab, ctx->message_chunks, wide, ctx->d_consts, ctx->ks);
   return cudaGetLastError();
 }
 
@@ -321,6 +335,7 @@ struct Dispatch {
   cudaError_t (*lookup)(cuhe_paillier*, const uint8_t*, int, int, int, const uint32_t*, long long, const uint8_t*,
                         uint32_t*) = nullptr;
   cudaError_t (*table_rows)(cuhe_paillier*, const uint32_t*, int, uint32_t*) = nullptr;
+  cudaError_t (*wide_table)(cuhe_paillier*, uint32_t*) = nullptr;
   cudaError_t (*prepare_tasks)(int, int*) = nullptr;
   cudaError_t (*launch_tasks)(const cuhe::ModexpTask*, int, long long, unsigned long long*, int*, int,
                               cudaStream_t) = nullptr;
@@ -337,6 +352,7 @@ bool find_dispatch(int K, int TPI, int W, Dispatch* d) {
     d->outer = &launch_outer<k, t>;                                \
     d->lookup = &launch_lookup<k, t>;                              \
     d->table_rows = &launch_table_rows<k, t>;                      \
+    d->wide_table = &launch_wide_table<k, t>;                      \
     d->prepare_tasks = &prepare_tasks<k, t, w>;                    \
     d->launch_tasks = &launch_tasks<k, t, w>;                      \
     return true;                                                   \
@@ -471,6 +487,19 @@ cudaError_t stream_after(cudaStream_t waiter, cudaStream_t from) {
   cudaEventDestroy(ev);
   return e;
 }
+
+// The 16-bit-digit encryption table (W[j][D] = G[2j][D mod 256] *
+// G[2j+1][D / 256], 65,536 rows per pair of 8-bit digits): half the table
+// products per ciphertext, for (message_chunks + 1) / 2 * 65,536 * 4K bytes
+// (4 GiB at key_len 1024) and one product per entry to build, which about
+// 150,000 encryptions repay.  Mode 1 builds it for a call of at least
+// kWideMinItems ciphertexts when it takes at most kWideMaxBytes and a quarter
+// of the free device memory (else the 8-bit table serves); mode 2 builds it
+// for any call and fails without memory; mode 0 never.
+constexpr long long kWideMinItems = 1 << 16;
+constexpr size_t kWideMaxBytes = size_t(8) << 30;
+
+int ensure_wide_table(cuhe_paillier* ctx, const Dispatch& d, long long items);
 
 int check_status(cuhe_paillier* ctx, bool synchronous) {
   // Range errors are reported by the kernels through d_status; reading it
@@ -623,6 +652,7 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_crt);
   cudaFree(ctx->d_crt52);
   cudaFree(ctx->d_gtab);
+  cudaFree(ctx->d_wide);
   cudaFree(ctx->d_noise);
   for (cudaStream_t st : {ctx->copy, ctx->side})
     if (st) cudaStreamSynchronize(st);
@@ -1229,8 +1259,10 @@ int cuhe_lookup_set_tables(cuhe_paillier* ctx, const uint32_t* g_table, int mess
   const size_t gbytes = size_t(message_chunks) * 256 * kb;
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_noise);
+  cudaFree(ctx->d_wide);
   ctx->d_gtab = nullptr;
   ctx->d_noise = nullptr;
+  ctx->d_wide = nullptr;
   ctx->message_chunks = 0;
   ctx->noise_entries = 0;
   CUHE_CUDA(ctx, cudaMalloc(&ctx->d_gtab, gbytes), "table allocation");
@@ -1286,7 +1318,9 @@ int cuhe_lookup_build_tables(cuhe_paillier* ctx, const uint32_t* g, int message_
   CUHE_CUDA(ctx, bm.reserve(size_t(message_chunks) * kb), "table scratch");
   CUHE_CUDA(ctx, d.convert(ctx, b, (uint32_t*)bm.ptr, message_chunks, 1), "row conversion");
   cudaFree(ctx->d_gtab);
+  cudaFree(ctx->d_wide);
   ctx->d_gtab = nullptr;
+  ctx->d_wide = nullptr;
   ctx->message_chunks = 0;
   CUHE_CUDA(ctx, cudaMalloc(&ctx->d_gtab, size_t(message_chunks) * 256 * kb), "table allocation");
   CUHE_CUDA(ctx, d.table_rows(ctx, (const uint32_t*)bm.ptr, message_chunks, ctx->d_gtab), "table rows");
@@ -1328,6 +1362,54 @@ int cuhe_lookup_get_g_table(cuhe_paillier* ctx, uint32_t* out) {
   return check_status(ctx, true);
 }
 
+}  // extern "C"
+
+namespace {
+
+int ensure_wide_table(cuhe_paillier* ctx, const Dispatch& d, long long items) {
+  if (ctx->d_wide || ctx->wide_mode == 0 || !ctx->d_gtab) return CUHE_OK;
+  if (ctx->wide_mode == 1 && items < kWideMinItems) return CUHE_OK;
+  const size_t bytes = size_t((ctx->message_chunks + 1) / 2) * 65536 * size_t(ctx->K) * 4;
+  if (ctx->wide_mode == 1) {
+    size_t free_bytes = 0, total_bytes = 0;
+    CUHE_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes), "free memory");
+    if (bytes > kWideMaxBytes || bytes > free_bytes / 4) return CUHE_OK;
+  }
+  uint32_t* wide = nullptr;
+  cudaError_t e = cudaMalloc(&wide, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (ctx->wide_mode == 2) return fail(ctx, CUHE_OUT_OF_MEMORY, "wide table allocation");
+    return CUHE_OK;
+  }
+  e = d.wide_table(ctx, wide);
+  if (e != cudaSuccess) {
+    cudaFree(wide);
+    return cuda_fail(ctx, e, "wide table build");
+  }
+  ctx->d_wide = wide;
+  return CUHE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cuhe_lookup_set_wide_table(cuhe_paillier* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 2) return fail(ctx, CUHE_INVALID_ARGUMENT, "wide table mode must be 0, 1 or 2");
+  DeviceGuard guard(ctx->device);
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->wide_mode = mode;
+  if (mode == 0 && ctx->d_wide) {
+    CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "wide table release");
+    cudaFree(ctx->d_wide);
+    ctx->d_wide = nullptr;
+  }
+  return CUHE_OK;
+}
+
+int cuhe_lookup_wide_table_ready(const cuhe_paillier* ctx) { return ctx && ctx->d_wide ? 1 : 0; }
+
 int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t vectors, int embed_len, int chunk_len,
                              int chunk_num, const uint8_t* noise_index, uint32_t* out) {
   if (!ctx || vectors < 0 || embed_len <= 0 || chunk_len <= 0 || chunk_num <= 0)
@@ -1342,6 +1424,7 @@ int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t ve
   Dispatch d;
   find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
   const int64_t total = vectors * chunk_num;
+  if (int rc = ensure_wide_table(ctx, d, total)) return rc;
   Stager st(ctx);
   st.add(bits, size_t(vectors) * embed_len, true, false);
   st.add(noise_index, size_t(total) * cuhe::kNoiseMultiples, true, false);
@@ -1364,6 +1447,7 @@ int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t coun
   std::lock_guard<std::mutex> lock(ctx->mu);
   Dispatch d;
   find_dispatch(ctx->K, ctx->tpi, ctx->window, &d);
+  if (int rc = ensure_wide_table(ctx, d, count)) return rc;
   Stager st(ctx);
   st.add(m, size_t(count) * ctx->K * 4, true, false);
   st.add(noise_index, size_t(count) * cuhe::kNoiseMultiples, true, false);

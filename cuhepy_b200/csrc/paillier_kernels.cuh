@@ -1066,10 +1066,17 @@ __global__ void k_limbs_to_hex(const uint32_t* __restrict__ limbs, long long cou
 // G and NOISE are device-resident in Montgomery form.  The plaintext digits
 // come either from binary embeddings (Hamming padding "0b" per bit, read as
 // MSB-first chunks of chunk_len bits) or from little-endian plaintext words.
+// kWide: G is the 16-bit-digit table W[j][D] = G[2j][D mod 256] *
+// G[2j+1][D / 256] (k_wide_table), one product per pair of 8-bit digits; the
+// product of the same powers of g, so the ciphertext is the same.  The next
+// table row is loaded while the current product runs.
 // ---------------------------------------------------------------------------
 constexpr int kNoiseMultiples = 14;
 
-template <int K, int TPI>
+// 16-bit entries of row list per instance: message_chunks rounded up to even
+__host__ __device__ constexpr int lookup_rows_stride(int message_chunks) { return (message_chunks + 1) & ~1; }
+
+template <int K, int TPI, bool kWide = false>
 __global__ void __launch_bounds__(kBlockThreads)
 k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len, int chunk_num,
                  const uint32_t* __restrict__ plain, int plain_words, long long count, int message_chunks,
@@ -1091,12 +1098,30 @@ k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len,
   const long long inst = (long long)blockIdx.x * IPB + slot;
   if (inst >= count) return;
   uint32_t* s_acc = smem + K + slot * ACC_STRIDE;
-  uint16_t* s_rows = reinterpret_cast<uint16_t*>(smem + K + IPB * ACC_STRIDE) + slot * message_chunks;
+  // table rows of the nonzero digits: 8-bit digits as i * 256 + d (16 bits),
+  // 16-bit digits as j * 65536 + D (32 bits); lookup_rows_stride(message_chunks)
+  // 16-bit entries (a multiple of four bytes) a slot either way
+  uint16_t* s_rows16 =
+      reinterpret_cast<uint16_t*>(smem + K + IPB * ACC_STRIDE) + slot * lookup_rows_stride(message_chunks);
+  uint32_t* s_rows32 = reinterpret_cast<uint32_t*>(s_rows16);
   __shared__ int s_count[IPB];
 
   // nonzero digits -> list of table rows (lane 0 of the group)
   if (g.gl == 0) {
     int cnt = 0;
+    int pending = 0;  // kWide: the low byte of the current 16-bit digit
+    auto push = [&](int i, int d) {
+      if (kWide) {
+        if ((i & 1) == 0) {
+          pending = d;
+          if (i + 1 == message_chunks && d) s_rows32[cnt++] = uint32_t(i / 2) * 65536u + uint32_t(d);
+        } else if (pending | d) {
+          s_rows32[cnt++] = uint32_t(i / 2) * 65536u + uint32_t(pending + 256 * d);
+        }
+      } else if (d) {
+        s_rows16[cnt++] = uint16_t(i * 256 + d);
+      }
+    };
     if (bits) {
       const long long vec = inst / chunk_num;
       const int chunk = int(inst % chunk_num);
@@ -1116,31 +1141,31 @@ k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len,
             if (p & 1) d |= (vb[p >> 1] & 1) << b;
           }
         }
-        if (d) s_rows[cnt++] = uint16_t(i * 256 + d);
+        push(i, d);
       }
     } else {
       const uint8_t* mb = reinterpret_cast<const uint8_t*>(plain + inst * plain_words);
       const int bytes = plain_words * 4 < message_chunks ? plain_words * 4 : message_chunks;
-      for (int i = 0; i < bytes; ++i) {
-        const int d = mb[i];
-        if (d) s_rows[cnt++] = uint16_t(i * 256 + d);
-      }
+      for (int i = 0; i < message_chunks; ++i) push(i, i < bytes ? int(mb[i]) : 0);
     }
     s_count[slot] = cnt;
   }
   __syncwarp(g.mask);
   const int cnt = s_count[slot];
+  auto row_of = [&](int j) -> long long { return kWide ? (long long)s_rows32[j] : (long long)s_rows16[j]; };
 
-  uint32_t n2[L], acc[L], a[L];
+  uint32_t n2[L], acc[L], a[L], nx[L];
   g.load_ro(n2, consts + C_N2 * K);
   g.load_ro(acc, consts + C_RM * K);  // Montgomery one
   g.publish(s_acc, acc);
+  if (cnt > 0) g.load_ro(a, gtab + row_of(0) * K);
 #pragma unroll 1
   for (int j = 0; j < cnt; ++j) {
-    const int row = s_rows[j];
-    g.load_ro(a, gtab + (long long)row * K);
+    if (j + 1 < cnt) g.load_ro(nx, gtab + row_of(j + 1) * K);
     g.mont_mul(acc, a, s_acc, n2, ks.ninv2);
     g.publish(s_acc, acc);
+#pragma unroll
+    for (int k = 0; k < L; ++k) a[k] = nx[k];
   }
   const uint8_t* idx = noise_idx + inst * kNoiseMultiples;
 #pragma unroll 1
@@ -1156,6 +1181,34 @@ k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len,
   }
   g.mont_mul(a, acc, s_one, n2, ks.ninv2);
   g.store(out + inst * K, a);
+}
+
+// The 16-bit-digit table: W[j][D] = G[2j][D mod 256] * G[2j+1][D / 256]
+// (Montgomery form in and out; for an odd message_chunks the last row's high
+// factor is 1).  One group per entry.
+template <int K, int TPI>
+__global__ void __launch_bounds__(kBlockThreads)
+k_wide_table(const uint32_t* __restrict__ gtab, int message_chunks, uint32_t* __restrict__ wide,
+             const uint32_t* __restrict__ consts, KeyScalars ks) {
+  constexpr int L = K / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int STRIDE = inst_stride_words<K>(1);
+  extern __shared__ __align__(16) uint32_t smem[];
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;  // j * 65536 + D
+  const int wide_chunks = (message_chunks + 1) / 2;
+  if (inst >= (long long)wide_chunks * 65536) return;
+  const int j = int(inst >> 16), D = int(inst & 65535);
+  uint32_t* s_b = smem + slot * STRIDE;
+  uint32_t n2[L], lo[L], hi[L], r[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load_ro(lo, gtab + ((long long)(2 * j) * 256 + (D & 255)) * K);
+  if (2 * j + 1 < message_chunks) g.load_ro(hi, gtab + ((long long)(2 * j + 1) * 256 + (D >> 8)) * K);
+  else g.load_ro(hi, consts + C_RM * K);
+  g.publish(s_b, hi);
+  g.mont_mul(r, lo, s_b, n2, ks.ninv2);
+  g.store(wide + inst * K, r);
 }
 
 // ---------------------------------------------------------------------------

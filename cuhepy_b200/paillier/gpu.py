@@ -205,6 +205,15 @@ class PaillierDevice:
         self._check(self._lib.cuhe_paillier_modexp_each(
             self._ctx, _ptr(base), _ptr(exponents), int(exponent_words), _ptr(out), int(count)))
 
+    def set_wide_table(self, mode: int) -> None:
+        """16-bit-digit encryption table (half the table products, same
+        ciphertexts): 1 (default) built for calls of at least 65,536
+        ciphertexts when it fits, 2 always, 0 never."""
+        self._check(self._lib.cuhe_lookup_set_wide_table(self._ctx, int(mode)))
+
+    def wide_table_ready(self) -> bool:
+        return bool(self._lib.cuhe_lookup_wide_table_ready(self._ctx))
+
     def lookup_encrypt_bits_array(self, bits, vectors: int, embed_len: int, chunk_len: int, chunk_num: int,
                                   noise_index, out) -> None:
         self._check(self._lib.cuhe_lookup_encrypt_bits(

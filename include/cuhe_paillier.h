@@ -206,6 +206,22 @@ int cuhe_lookup_get_g_table(cuhe_paillier* ctx, uint32_t* out);
 int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t vectors, int embed_len,
                              int chunk_len, int chunk_num, const uint8_t* noise_index, uint32_t* out);
 
+/* The 16-bit-digit encryption table.  Pairs of the table's 8-bit digits are
+ * looked up as one entry W[j][D] = G[2j][D mod 256] * G[2j+1][D / 256] (mod
+ * n^2, Montgomery form), so each ciphertext takes half the table products and
+ * the ciphertexts are the same.  The table holds (message_chunks + 1) / 2 *
+ * 65,536 entries of K words (4 GiB at key_len 1024) and costs one product per
+ * entry to build, which about 150,000 encryptions repay.  mode 1 (the
+ * default) builds it during an encryption call of at least 65,536
+ * ciphertexts, when it takes at most 8 GiB and a quarter of the free device
+ * memory; mode 2 builds it at the next encryption call of any size
+ * (CUHE_OUT_OF_MEMORY without the memory); mode 0 frees it and keeps the
+ * 8-bit table.  Installing new tables drops it.  ready returns 1 once it is
+ * built.  No reference counterpart (the reference multiplies one entry per
+ * 8-bit digit, lookup.py:213-252). */
+int cuhe_lookup_set_wide_table(cuhe_paillier* ctx, int mode);
+int cuhe_lookup_wide_table_ready(const cuhe_paillier* ctx);
+
 /* Encrypt plaintexts m[i] < n (K-word stride) by table product.  Replaces
  * PaillierLookup.encrypt (lookup.py:213-252) and encrypt_cts
  * (paillier_GPU_lookup_client.cu:2006-2131, 951-1011). */
