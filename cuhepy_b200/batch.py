@@ -14,10 +14,14 @@ stream, the NTT batches forked onto a second stream so that the two kinds
 overlap, joined back before the graph ends.  ``replay()`` is then a single
 launch from the host.
 
-The autotuner picks, per Paillier width, the (threads per instance, window)
-variant whose persistent kernel finishes that width's own batches fastest, and
-per ring the (threads per CTA, radix) of its NTT batches, by timing the
-candidates on the batch's own data with CUDA events.
+A width whose contexts select the FP64 pipe (n^2 of 4096 or 8192 bits by
+default, ``PaillierDevice.set_fp64``) runs the persistent kernel of 52-bit-limb
+products on that pipe, as those contexts' own calls do.  The autotuner picks,
+per Paillier width, the (threads per instance, window) variant of the integer
+kernel or, for those widths, the FP64 kernel, whichever finishes that width's
+own batches fastest (and sets the contexts' pipe accordingly), and per ring
+the (threads per CTA, radix) of its NTT batches, by timing the candidates on
+the batch's own data with CUDA events.
 
 ``run_plain()`` is the comparison point: the same work as one launch per
 operation with a wait after each (``PaillierDevice.modexp_array`` per batch,
@@ -64,6 +68,7 @@ class MixedBatch:
         self._modexp: list[_Modexp] = []
         self._ntt: list[_Ntt] = []
         self.paillier_tuning: dict[int, tuple[int, int]] = {}
+        self.paillier_fp64: dict[int, bool] = {}  # width -> FP64-pipe kernel chosen by the autotuner
         self.ntt_tuning: dict[int, tuple[int, int]] = {}  # id(ring) -> (threads, radix_log)
         self._mix = None
         self._graph = None
@@ -110,7 +115,13 @@ class MixedBatch:
         text = msg.decode() if msg else str(rc)
         raise ValueError(text) if rc in (-1, -5) else RuntimeError(text)
 
+    def _select_pipe(self, entries: list[_Modexp]) -> None:
+        for e in entries:
+            if e.ctx.words in self.paillier_fp64:
+                e.ctx.set_fp64(1 if self.paillier_fp64[e.ctx.words] else 0)
+
     def _build_mix(self, entries: list[_Modexp], tuning: dict[int, tuple[int, int]]):
+        self._select_pipe(entries)
         handle = ctypes.c_void_p()
         self._check(self._lib.cuhe_mix_create(self.device, ctypes.byref(handle)))
         mix = handle
@@ -200,6 +211,7 @@ class MixedBatch:
         """One launch per operation, each waited for, same tuned variants."""
         torch = self._torch
         stream = torch.cuda.current_stream(self.device)
+        self._select_pipe(self._modexp)
         for e in self._modexp:
             tpi, w = self.paillier_tuning.get(e.ctx.words, (0, 0))
             e.ctx.set_tuning(tpi, w)
@@ -236,17 +248,39 @@ class MixedBatch:
             by_width.setdefault(e.ctx.words, []).append(e)
         for words, entries in sorted(by_width.items()):
             timings = {}
-            for tpi, w in PaillierDevice.VARIANTS[words]:
-                mix = self._build_mix(entries, {words: (tpi, w)})
+            self.paillier_fp64.pop(words, None)
+            saved = [e.ctx.fp64 for e in entries]
+
+            def timed(tuning):
+                mix = self._build_mix(entries, tuning)
                 try:
-                    timings[(tpi, w)] = self._time(
+                    return self._time(
                         lambda: self._check(self._lib.cuhe_mix_launch(mix, ctypes.c_void_p(stream.cuda_stream)),
                                             mix), reps)
                 finally:
                     self._lib.cuhe_mix_destroy(mix)
+
+            try:
+                for e in entries:
+                    e.ctx.set_fp64(0)
+                for tpi, w in PaillierDevice.VARIANTS[words]:
+                    timings[(tpi, w)] = timed({words: (tpi, w)})
+                if words >= 128:  # the FP64-pipe kernel's widths
+                    for e in entries:
+                        e.ctx.set_fp64(1)
+                    timings["fp64"] = timed({})
+            finally:
+                for e, f in zip(entries, saved):
+                    e.ctx.set_fp64(f)
             best = min(timings, key=timings.get)
-            self.paillier_tuning[words] = best
-            report["paillier"][words] = {"best": best, "ms": {f"{k[0]}x{k[1]}": v for k, v in timings.items()}}
+            if words >= 128:
+                self.paillier_fp64[words] = best == "fp64"
+            if best == "fp64":
+                self.paillier_tuning.pop(words, None)
+            else:
+                self.paillier_tuning[words] = best
+            report["paillier"][words] = {"best": best, "ms": {(k if isinstance(k, str) else f"{k[0]}x{k[1]}"): v
+                                                              for k, v in timings.items()}}
         rings: dict[int, list[_Ntt]] = {}
         for item in self._ntt:
             rings.setdefault(id(item.ring), []).append(item)

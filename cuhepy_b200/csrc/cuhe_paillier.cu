@@ -98,6 +98,10 @@ struct cuhe_paillier {
   int nops_sec52 = 0;
   uint32_t* d_crt = nullptr;  // CRT constant block, present once the factors are installed
   double* d_crt52 = nullptr;  // per side: M and R52 mod M as 52-bit limbs (FP64-pipe CRT kernel)
+  double* d_n52 = nullptr;    // n^2 and R52 mod n^2 as 52-bit limbs, then R52 R mod n^2 in words (k_modexp52)
+  unsigned long long ninv52 = 0;  // -(n^2)^-1 mod 2^52
+  int32_t* d_ops_n52 = nullptr;   // the schedule of n for k_modexp52's window
+  int nops_n52 = 0;
   cuhe::CrtScalars cs{};
   bool have_factors = false;
   bool fp64 = true;           // decrypt / decode exponentiations on the FP64 pipe (n^2 of 4096 bits or more)
@@ -202,6 +206,65 @@ cudaError_t launch_modexp_crt52(cuhe_paillier* ctx, const uint32_t* base, uint32
   cuhe::k_modexp_crt52<KH, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
       base, out, count, ctx->d_consts, ctx->ks, ctx->d_crt, ctx->cs, ctx->d_crt52, ctx->d_ops_sec52,
       ctx->nops_sec52, mode, pop_words, ctx->d_status);
+  return cudaGetLastError();
+}
+
+// The exponentiation mod n^2 on the FP64 pipe (no factors needed).
+template <int K, int W>
+size_t modexp52_smem() {
+  constexpr int TPI = K / 16, K52 = 5 * K / 8;
+  constexpr int IPB = cuhe::kBlockThreads / TPI;
+  return size_t(6 * K) * 4 + size_t(K52 + IPB * (((1 << (W - 1)) + 1) * K52 + 2)) * 8;
+}
+
+template <int K, int W>
+cudaError_t launch_modexp52(cuhe_paillier* ctx, const uint32_t* base, const uint32_t* aux, uint32_t* out,
+                            long long count, const int32_t* ops, int nops, int mode, int pop_words) {
+  constexpr int IPB = cuhe::kBlockThreads / (K / 16);
+  const size_t smem = modexp52_smem<K, W>();
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp52<K, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const long long blocks = (count + IPB - 1) / IPB;
+  cuhe::k_modexp52<K, W><<<dim3(unsigned(blocks)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      base, aux, K, out, count, ctx->d_consts, ctx->ks, ctx->d_n52, ctx->ninv52, ops, nops, mode, pop_words,
+      ctx->d_status);
+  return cudaGetLastError();
+}
+
+// k_modexp52 for this context's width when the FP64 pipe is selected for it
+// (n^2 of 4096 or 8192 bits; 2048 bits only with set_fp64(ctx, 2)), else null.
+using Modexp52 = cudaError_t (*)(cuhe_paillier*, const uint32_t*, const uint32_t*, uint32_t*, long long,
+                                 const int32_t*, int, int, int);
+Modexp52 direct52(const cuhe_paillier* ctx) {
+  if (!ctx->fp64 || !ctx->d_n52) return nullptr;
+  if (ctx->K == 64 && ctx->fp64_small) return &launch_modexp52<64, kCrt52Window>;
+  if (ctx->K == 128) return &launch_modexp52<128, kCrt52Window>;
+  if (ctx->K == 256) return &launch_modexp52<256, kCrt52Window>;
+  return nullptr;
+}
+
+template <int K>
+cudaError_t prepare_tasks52(int device, int* grid) {
+  const size_t smem = modexp52_smem<K, kCrt52Window>();
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_modexp52_tasks<K, kCrt52Window>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  int per_sm = 0, sms = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cuhe::k_modexp52_tasks<K, kCrt52Window>,
+                                                    cuhe::kBlockThreads, smem);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) return e;
+  *grid = std::max(1, per_sm) * sms;
+  return cudaSuccess;
+}
+
+template <int K>
+cudaError_t launch_tasks52(const cuhe::ModexpTask* tasks, int ntasks, long long units, unsigned long long* counter,
+                           int* status, int grid, cudaStream_t stream) {
+  cuhe::k_modexp52_tasks<K, kCrt52Window><<<grid, cuhe::kBlockThreads, modexp52_smem<K, kCrt52Window>(), stream>>>(
+      tasks, ntasks, units, counter, status);
   return cudaGetLastError();
 }
 
@@ -373,6 +436,8 @@ cudaError_t secret_modexp(cuhe_paillier* ctx, const Dispatch& d, const uint32_t*
     if (ctx->K == 256) return launch_modexp_crt52<128, kCrt52Window>(ctx, base, out, count, mode, pop_words);
   }
   if (ctx->have_factors) return d.modexp_crt(ctx, base, out, count, mode, pop_words);
+  if (Modexp52 f = direct52(ctx)) return f(ctx, base, nullptr, out, count, ctx->d_ops_sec52, ctx->nops_sec52, mode,
+                                           pop_words);
   return d.modexp(ctx, base, nullptr, out, count, ctx->d_ops_sec, ctx->nops_sec, mode, pop_words);
 }
 
@@ -528,6 +593,36 @@ int upload_schedule(cuhe_paillier* ctx, const Limbs& e, int32_t** dptr, int* nop
   return CUHE_OK;
 }
 
+// k_modexp52's constants: n^2 and R52 mod n^2 as K52 = 5K/8 limbs of 52 bits
+// (doubles), then R52 R mod n^2 as K words; R52 = 2^(52 K52), R = 2^(32K).
+int setup_direct52(cuhe_paillier* ctx) {
+  const size_t k = size_t(ctx->K), k52 = 5 * k / 8;
+  Limbs one(k, 0u);
+  one[0] = 1u;
+  std::vector<double> block(2 * k52 + k / 2, 0.0);
+  auto put52 = [&](size_t row, const Limbs& v) {
+    for (size_t i = 0; i < k52; ++i) {
+      uint64_t limb = 0;
+      for (int b = 0; b < 52; ++b) {
+        const size_t bit = 52 * i + size_t(b);
+        if (bit / 32 < v.size() && ((v[bit / 32] >> (bit % 32)) & 1u)) limb |= 1ull << b;
+      }
+      block[row * k52 + i] = double(limb);
+    }
+  };
+  put52(0, ctx->n2);
+  put52(1, cuhe::host::shift_mod(one, 52 * k52, ctx->n2));
+  const Limbs r52r = cuhe::host::shift_mod(one, 52 * k52 + 32 * k, ctx->n2);
+  std::memcpy(block.data() + 2 * k52, r52r.data(), 4 * k);
+  const uint64_t m0 = (uint64_t(ctx->n2[1]) << 32) | ctx->n2[0];
+  uint64_t inv = m0;
+  for (int it = 0; it < 6; ++it) inv *= 2 - m0 * inv;
+  ctx->ninv52 = (0 - inv) & ((1ull << 52) - 1);
+  CUHE_CUDA(ctx, cudaMalloc(&ctx->d_n52, block.size() * 8), "constants allocation");
+  CUHE_CUDA(ctx, cudaMemcpy(ctx->d_n52, block.data(), block.size() * 8, cudaMemcpyHostToDevice), "constants upload");
+  return CUHE_OK;
+}
+
 struct DeviceGuard {
   int prev = -1;
   explicit DeviceGuard(int dev) {
@@ -630,7 +725,9 @@ int cuhe_paillier_create(const uint32_t* n_in, int n_words, int device, cuhe_pai
     return rc;
   }
   ctx->stream = ctx->own_stream;
-  if (upload_schedule(ctx, nk, &ctx->d_ops_n, &ctx->nops_n) != CUHE_OK) {
+  if (upload_schedule(ctx, nk, &ctx->d_ops_n, &ctx->nops_n) != CUHE_OK ||
+      upload_schedule(ctx, nk, &ctx->d_ops_n52, &ctx->nops_n52, kCrt52Window) != CUHE_OK ||
+      setup_direct52(ctx) != CUHE_OK) {
     g_create_error = ctx->error;
     cuhe_paillier_destroy(ctx);
     return CUHE_CUDA_ERROR;
@@ -651,6 +748,8 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_ops_sec52);
   cudaFree(ctx->d_crt);
   cudaFree(ctx->d_crt52);
+  cudaFree(ctx->d_n52);
+  cudaFree(ctx->d_ops_n52);
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_wide);
   cudaFree(ctx->d_noise);
@@ -838,9 +937,15 @@ int cuhe_paillier_encrypt(cuhe_paillier* ctx, const uint32_t* m, const uint32_t*
   st.add(r, bytes, true, false);
   st.add(c, bytes, false, true);
   if (int rc = st.bind()) return rc;
-  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(1), (const uint32_t*)st.dev(0), (uint32_t*)st.dev(2), count,
-                          ctx->d_ops_n, ctx->nops_n, cuhe::EXP_ENCRYPT, 0),
-            "encrypt launch");
+  if (Modexp52 f = direct52(ctx)) {
+    CUHE_CUDA(ctx, f(ctx, (const uint32_t*)st.dev(1), (const uint32_t*)st.dev(0), (uint32_t*)st.dev(2), count,
+                     ctx->d_ops_n52, ctx->nops_n52, cuhe::EXP_ENCRYPT, 0),
+              "encrypt launch");
+  } else {
+    CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(1), (const uint32_t*)st.dev(0), (uint32_t*)st.dev(2), count,
+                            ctx->d_ops_n, ctx->nops_n, cuhe::EXP_ENCRYPT, 0),
+              "encrypt launch");
+  }
   if (int rc = st.finish()) return rc;
   return check_status(ctx, st.staged());
 }
@@ -1076,7 +1181,8 @@ int cuhe_paillier_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32_
   // exponent of any width: build its schedule
   Limbs e(exponent, exponent + exponent_words);
   while (e.size() > 1 && e.back() == 0) e.pop_back();
-  std::vector<int32_t> ops = cuhe::host::window_schedule(e, ctx->window);
+  const Modexp52 f52 = direct52(ctx);
+  std::vector<int32_t> ops = cuhe::host::window_schedule(e, f52 ? kCrt52Window : ctx->window);
   if (!ops.empty()) {
     if (cudaError_t ce = ctx->tmp_ops.reserve(ops.size() * 4)) return cuda_fail(ctx, ce, "schedule allocation");
     CUHE_CUDA(ctx, cudaMemcpyAsync(ctx->tmp_ops.ptr, ops.data(), ops.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
@@ -1087,9 +1193,15 @@ int cuhe_paillier_modexp(cuhe_paillier* ctx, const uint32_t* base, const uint32_
   st.add(base, bytes, true, false);
   st.add(out, bytes, false, true);
   if (int rc = st.bind()) return rc;
-  CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, (uint32_t*)st.dev(1), count,
-                          (const int32_t*)ctx->tmp_ops.ptr, int(ops.size()), cuhe::EXP_POW, 0),
-            "modexp launch");
+  if (f52) {
+    CUHE_CUDA(ctx, f52(ctx, (const uint32_t*)st.dev(0), nullptr, (uint32_t*)st.dev(1), count,
+                       (const int32_t*)ctx->tmp_ops.ptr, int(ops.size()), cuhe::EXP_POW, 0),
+              "modexp launch");
+  } else {
+    CUHE_CUDA(ctx, d.modexp(ctx, (const uint32_t*)st.dev(0), nullptr, (uint32_t*)st.dev(1), count,
+                            (const int32_t*)ctx->tmp_ops.ptr, int(ops.size()), cuhe::EXP_POW, 0),
+              "modexp launch");
+  }
   if (int rc = st.finish()) return rc;
   // the schedule buffer is reused by the next call: keep host order
   if (!st.staged()) CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "modexp synchronize");
@@ -1480,6 +1592,10 @@ struct cuhe_mix {
     cuhe::ModexpTask* d_tasks = nullptr;
     std::vector<int32_t*> d_ops;
     Dispatch d;
+    bool fp52 = false;  // k_modexp52_tasks: every context of the width selects the FP64 pipe
+    cudaError_t (*prepare)(int, int*) = nullptr;
+    cudaError_t (*launch)(const cuhe::ModexpTask*, int, long long, unsigned long long*, int*, int,
+                          cudaStream_t) = nullptr;
   };
   int device = 0;
   std::vector<Entry> entries;
@@ -1599,6 +1715,18 @@ int cuhe_mix_plan(cuhe_mix* mix) {
       default_tuning(w.K, &w.tpi, &w.window);
     }
     if (!find_dispatch(w.K, w.tpi, w.window, &w.d)) return mix_fail(mix, CUHE_INVALID_ARGUMENT, "no compiled variant");
+    // the pipe follows the contexts, as their one-launch-per-batch calls do
+    w.fp52 = true;
+    for (size_t i : kv.second) w.fp52 = w.fp52 && direct52(mix->entries[i].ctx) != nullptr;
+    w.prepare = w.d.prepare_tasks;
+    w.launch = w.d.launch_tasks;
+    if (w.fp52) {
+      w.window = kCrt52Window;
+      w.tpi = w.K / 16;
+      if (w.K == 64) { w.prepare = &prepare_tasks52<64>; w.launch = &launch_tasks52<64>; }
+      if (w.K == 128) { w.prepare = &prepare_tasks52<128>; w.launch = &launch_tasks52<128>; }
+      if (w.K == 256) { w.prepare = &prepare_tasks52<256>; w.launch = &launch_tasks52<256>; }
+    }
     const long long ipb = cuhe::kBlockThreads / w.tpi;
     std::vector<cuhe::ModexpTask> tasks;
     for (size_t i : kv.second) {
@@ -1624,6 +1752,8 @@ int cuhe_mix_plan(cuhe_mix* mix) {
       t.ks = e.ctx->ks;
       t.nops = int(ops.size());
       t.mode = cuhe::EXP_POW;
+      t.n52 = e.ctx->d_n52;
+      t.ninv52 = e.ctx->ninv52;
       tasks.push_back(t);
       w.units += (e.count + ipb - 1) / ipb;
     }
@@ -1634,7 +1764,7 @@ int cuhe_mix_plan(cuhe_mix* mix) {
       cudaGetLastError();
       return mix_fail(mix, CUHE_OUT_OF_MEMORY, "task table upload");
     }
-    cudaError_t e = w.d.prepare_tasks(mix->device, &w.grid);
+    cudaError_t e = w.prepare(mix->device, &w.grid);
     if (e != cudaSuccess) return mix_fail(mix, CUHE_CUDA_ERROR, std::string("mixed launch setup: ") + cudaGetErrorString(e));
     mix->widths.push_back(std::move(w));
   }
@@ -1674,7 +1804,7 @@ int cuhe_mix_launch(cuhe_mix* mix, void* stream) {
     cudaStream_t ws = i == 0 ? s : mix->side[i - 1];
     if (i > 0) e = cudaStreamWaitEvent(ws, mix->fork, 0);
     if (e == cudaSuccess)
-      e = w.d.launch_tasks(w.d_tasks, w.ntasks, w.units, mix->d_counters + i, mix->d_status, w.grid, ws);
+      e = w.launch(w.d_tasks, w.ntasks, w.units, mix->d_counters + i, mix->d_status, w.grid, ws);
     if (e == cudaSuccess && i > 0) e = cudaEventRecord(mix->done[i - 1], ws);
     if (e == cudaSuccess && i > 0) e = cudaStreamWaitEvent(s, mix->done[i - 1], 0);
   }

@@ -353,6 +353,8 @@ struct ModexpTask {
   KeyScalars ks;
   int nops;
   int mode;
+  const double* n52;            // k_modexp52_tasks: the key's 52-bit constants
+  unsigned long long ninv52;
 };
 
 // Persistent mixed launch: CTAs take units (IPB instances of one task) from
@@ -736,6 +738,205 @@ k_modexp_crt52(const uint32_t* __restrict__ base, uint32_t* __restrict__ out, lo
   g.mont_mul(x, hv, s_cq, n2, ks.ninv2);  // h q^2 mod n^2 = h q^2
   (void)add_group<K, 2 * TPI>(g, x, xq);
   decrypt_epilogue<K, 2 * TPI>(g, x, out, inst, consts, ks, s_one, s_r2n, s_multr, mode, pop_words);
+}
+
+// ---------------------------------------------------------------------------
+// The exponentiation mod n^2 itself on the FP64 pipe, for the exponents that
+// need no factors (encryption's r^n, any fixed public exponent) and for
+// decryption when the factors are not installed.  The value is carried as
+// K52 = 5K/8 limbs of 52 bits on K/16 lanes (ten limbs per lane) in the
+// Montgomery domain of R52 = 2^(52 K52), with k_modexp_crt52's product and
+// schedule; entry: x R52 mod n^2 by one 32-bit Montgomery product with
+// R52 R mod n^2, exit: the product with 1, re-cut into 32-bit words; then
+// k_modexp's modes on 32-bit words (the factor 1 + m n of an encryption,
+// the L() / popcount epilogue), so every output equals k_modexp's.
+// n52: n^2 and R52 mod n^2 as K52 doubles each, then R52 R mod n^2 as K words.
+// ---------------------------------------------------------------------------
+template <int K, int W>
+__device__ __forceinline__ void modexp52_unit(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux,
+                                              int aux_words, uint32_t* __restrict__ out, long long count,
+                                              const uint32_t* __restrict__ consts, const KeyScalars& ks,
+                                              const double* __restrict__ n52, unsigned long long ninv52,
+                                              const int32_t* __restrict__ ops, int nops, int mode, int pop_words,
+                                              int* status, long long block) {
+  constexpr int TPI = K / 16;      // lanes per value
+  constexpr int L = 16;            // 32-bit words per lane
+  constexpr int K52 = 5 * K / 8;   // 52-bit limbs
+  constexpr int L52 = K52 / TPI;   // ten
+  static_assert(L52 == 10, "ten limbs per lane");
+  static_assert(52 * K52 > 32 * K + 1, "R52 must exceed 2 n^2");
+  constexpr int T = 1 << (W - 1);
+  constexpr int IPB = kBlockThreads / TPI;
+  constexpr int SLOT = (T + 1) * K52 + 2;  // doubles per value: x, then T odd powers; +2 moves the banks
+  extern __shared__ __align__(16) uint32_t smem[];
+  // block rows: ONE, R2, NR, R2N, MULTR, R52 R (K words each); then 1 as K52 doubles
+  uint32_t* s_one = smem;
+  uint32_t* s_r2 = smem + K;
+  uint32_t* s_nr = smem + 2 * K;
+  uint32_t* s_r2n = smem + 3 * K;
+  uint32_t* s_multr = smem + 4 * K;
+  uint32_t* s_r52r = smem + 5 * K;
+  double* s_one52 = reinterpret_cast<double*>(smem + 6 * K);
+  double* s_items = s_one52 + K52;
+  {
+    const int rows[5] = {C_ONE, C_R2, C_NR, C_R2N, C_MULTR};
+    copy_rows_to_smem<K, TPI>(smem, consts, rows, 5);
+    const uint32_t* r52r = reinterpret_cast<const uint32_t*>(n52 + 2 * K52);
+    for (int i = threadIdx.x; i < K; i += blockDim.x) s_r52r[i] = r52r[i];
+    for (int i = threadIdx.x; i < K52; i += blockDim.x) s_one52[i] = i == 0 ? 1.0 : 0.0;
+  }
+  __syncthreads();
+
+  Group<K, TPI> g;                // the value, 32-bit words
+  cuhe52::Group52<K52, TPI> f;    // the value, 52-bit limbs (same lanes)
+  const int slot = threadIdx.x / TPI;
+  const long long inst = block * IPB + slot;
+  if (inst >= count) return;  // whole groups leave together
+  double* s_x = s_items + slot * SLOT;
+  double* s_tab = s_x + K52;
+  uint32_t* s_w = reinterpret_cast<uint32_t*>(s_x);  // K words fit in the K52 doubles of x
+  uint32_t n2[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  {
+    uint32_t x[L], xr[L];
+    g.load(x, base + inst * K);
+    if (!g.less_than(x, n2)) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
+    }
+    g.mont_mul(xr, x, s_r52r, n2, ks.ninv2);  // x R52 mod n^2
+    g.publish(s_w, xr);
+  }
+  double x52[L52], m52[L52], acc52[L52];
+#pragma unroll
+  for (int k = 0; k < L52; ++k) {
+    x52[k] = cuhe52::to_f64(limb52_from_words(s_w, K, f.gl * L52 + k));
+    m52[k] = __ldg(n52 + f.gl * L52 + k);
+  }
+  f.publish(s_tab, x52);
+#pragma unroll
+  for (int k = 0; k < L52; ++k) acc52[k] = x52[k];
+  // One call site for every product (k_modexp_crt52): the odd-power table,
+  // the window schedule, the final product with 1.
+  enum { kTable = 0, kSchedule = 1, kFinal = 2 };
+  int phase = T > 1 ? kTable : kSchedule, pc = 0, o = 1, sq_left = 0, idx = 0;
+  if (phase == kSchedule) pc = T;
+  double xs52[L52];
+  while (true) {
+    if (phase == kSchedule && pc == T) {
+      pc = 0;
+      if (nops == 0) {
+#pragma unroll
+        for (int k = 0; k < L52; ++k) acc52[k] = __ldg(n52 + K52 + f.gl * L52 + k);  // e = 0: R52 mod n^2
+      } else {
+        const int first = __ldg(ops) & 0xffff;
+        __syncwarp(f.mask);
+#pragma unroll
+        for (int k = 0; k < L52; ++k) acc52[k] = s_tab[(first - 1) * K52 + f.gl * L52 + k];
+      }
+      f.publish(s_x, acc52);
+      while (sq_left == 0 && idx == 0) {
+        if (o >= nops) {
+          phase = kFinal;
+          break;
+        }
+        const int op = __ldg(ops + o++);
+        sq_left = op >> 16;
+        idx = op & 0xffff;
+      }
+    }
+    const double* bsrc = phase == kTable   ? (pc == 0 ? s_tab : s_x)
+                         : phase == kFinal ? s_one52
+                         : sq_left > 0     ? s_x
+                                           : s_tab + (idx - 1) * K52;
+    f.mont_mul(xs52, acc52, bsrc, m52, ninv52);
+    if (phase == kFinal) break;  // xs52 = x^e, canonical
+    if (phase == kTable && pc == 0) {
+      f.publish(s_x, xs52);  // x^2 R52; acc52 stays x
+    } else {
+#pragma unroll
+      for (int k = 0; k < L52; ++k) acc52[k] = xs52[k];
+      f.publish(phase == kTable ? s_tab + pc * K52 : s_x, acc52);
+    }
+    if (phase == kTable) {
+      if (++pc == T) phase = kSchedule;  // pc == T: set-up at the top of the next pass
+      continue;
+    }
+    if (sq_left > 0) --sq_left;
+    else idx = 0;
+    while (sq_left == 0 && idx == 0) {
+      if (o >= nops) {
+        phase = kFinal;
+        break;
+      }
+      const int op = __ldg(ops + o++);
+      sq_left = op >> 16;
+      idx = op & 0xffff;
+    }
+  }
+  uint64_t* s_l = reinterpret_cast<uint64_t*>(s_x);
+  __syncwarp(f.mask);
+#pragma unroll
+  for (int k = 0; k < L52; ++k) s_l[f.gl * L52 + k] = cuhe52::to_u64(xs52[k]);
+  __syncwarp(f.mask);
+  uint32_t x[L];
+#pragma unroll
+  for (int j = 0; j < L; ++j) x[j] = word_from_limbs52(s_l, K52, g.gl * L + j);
+  if (mode == EXP_POW) {
+    g.store(out + inst * K, x);
+    return;
+  }
+  if (mode == EXP_ENCRYPT) {
+    uint32_t m[L], nn[L], gm[L], xr[L];
+    g.load(m, aux + inst * aux_words);  // aux_words == K (zero-padded m < n)
+    g.load_ro(nn, consts + C_N * K);
+    if (!g.less_than(m, nn)) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
+    }
+    g.mont_mul(gm, m, s_nr, n2, ks.ninv2);  // m*n (exact, < n^2)
+    add_small<K, TPI>(g, gm, 1u);           // 1 + m*n = g^m mod n^2
+    g.publish(s_w, gm);
+    g.mont_mul(xr, x, s_r2, n2, ks.ninv2);  // r^n R
+    g.mont_mul(x, xr, s_w, n2, ks.ninv2);   // r^n * g^m
+    g.store(out + inst * K, x);
+    return;
+  }
+  decrypt_epilogue<K, TPI>(g, x, out, inst, consts, ks, s_one, s_r2n, s_multr, mode, pop_words);
+}
+
+template <int K, int W>
+__global__ void __launch_bounds__(kBlockThreads, 3)
+k_modexp52(const uint32_t* __restrict__ base, const uint32_t* __restrict__ aux, int aux_words,
+           uint32_t* __restrict__ out, long long count, const uint32_t* __restrict__ consts, KeyScalars ks,
+           const double* __restrict__ n52, unsigned long long ninv52, const int32_t* __restrict__ ops, int nops,
+           int mode, int pop_words, int* status) {
+  modexp52_unit<K, W>(base, aux, aux_words, out, count, consts, ks, n52, ninv52, ops, nops, mode, pop_words, status,
+                      blockIdx.x);
+}
+
+// The persistent mixed launch (k_modexp_tasks) on the FP64 pipe: units of
+// IPB = 128 / (K/16) instances of one task.
+template <int K, int W>
+__global__ void __launch_bounds__(kBlockThreads, 3)
+k_modexp52_tasks(const ModexpTask* __restrict__ tasks, int ntasks, long long total_units,
+                 unsigned long long* __restrict__ counter, int* status) {
+  __shared__ long long s_unit;
+  while (true) {
+    if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
+    __syncthreads();
+    const long long unit = s_unit;
+    if (unit >= total_units) break;
+    int lo = 0, hi = ntasks - 1;  // last task with first_unit <= unit
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tasks[mid].first_unit <= unit) lo = mid; else hi = mid - 1;
+    }
+    const ModexpTask& t = tasks[lo];
+    modexp52_unit<K, W>(t.base, nullptr, K, t.out, t.count, t.consts, t.ks, t.n52, t.ninv52, t.ops, t.nops, t.mode,
+                        0, status, unit - t.first_unit);
+    __syncthreads();  // shared rows and tables are restaged by the next unit
+  }
 }
 
 // ---------------------------------------------------------------------------

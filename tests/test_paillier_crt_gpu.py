@@ -120,9 +120,11 @@ def test_crt_matches_direct_on_a_large_device_batch():
 
 @pytest.mark.parametrize("name", ["paillier_512.json", "lookup_1024.json", "paillier_1024.json"])
 def test_fp64_pipe_equals_integer_pipe(name):
-    """The CRT exponentiations as 52-bit-limb products on the FP64 pipe give
-    the integer-pipe kernel's results, decrypt and decode, on ciphertexts
-    and on awkward values (several waves of a device batch)."""
+    """The exponentiations as 52-bit-limb products on the FP64 pipe give the
+    integer-pipe kernels' results: by the CRT (decrypt and decode) and mod
+    n^2 itself (decrypt and decode without the factors, encryption, public
+    powers), on ciphertexts and on awkward values (several waves of a device
+    batch)."""
     import torch
 
     data = load_golden(name)
@@ -153,6 +155,32 @@ def test_fp64_pipe_equals_integer_pipe(name):
     sample = rng.sample(range(len(vals)), 40)
     decrypt = oracle.lookup_decrypt if "a" in sk else oracle.decrypt
     assert from_limbs(outs[0].cpu().numpy().view(np.uint32)[sample]) == [decrypt(vals[i], keys) for i in sample]
+
+    # the exponentiation mod n^2 itself (k_modexp52): decryption and decoding
+    # without the factors, encryption r^n (1 + m n), public powers
+    direct = _pair(n, secret, sk["phi"])[0]
+    n2 = n * n
+    ms = [rng.randrange(n) for _ in range(700)] + [0, 1, n - 1]
+    rs = [rng.randrange(1, n) for _ in range(len(ms))]
+    exps = [0, 1, 2, 3, n, rng.getrandbits(300), rng.getrandbits(2 * n.bit_length())]
+    bases = [rng.randrange(n2) for _ in range(300)] + [0, 1, n2 - 1]
+    got = []
+    for fp64 in (2, 0):
+        direct.set_fp64(fp64)
+        out = torch.zeros((len(vals), direct.words), dtype=torch.int32, device="cuda")
+        dist = torch.full((len(vals) // 2,), -1, dtype=torch.int64, device="cuda")
+        direct.decrypt_array(limbs, out, len(vals))
+        direct.decode_array(limbs, len(vals) // 2, 2, 64, dist)
+        direct.synchronize()
+        got.append((out, dist, direct.encrypt(ms, rs), [direct.modexp(bases, e) for e in exps]))
+    direct.set_fp64(1)
+    (o2, d2, c2, p2), (o0, d0, c0, p0) = got
+    assert torch.equal(o2, o0) and torch.equal(d2, d0) and torch.equal(o2, outs[0])
+    assert c2 == c0 and p2 == p0
+    for k in (0, 5, len(ms) - 1):
+        assert c2[k] == (1 + ms[k] * n) * pow(rs[k], n, n2) % n2
+    for e, row in zip(exps, p2):
+        assert [row[k] for k in (0, 7, len(bases) - 1)] == [pow(bases[k], e, n2) for k in (0, 7, len(bases) - 1)]
 
 
 def test_crt_8192_bit_modulus_vs_oracle():
