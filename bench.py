@@ -376,7 +376,8 @@ def run_gpu(args) -> dict | None:
         "decode_int_ms": statistics.mean(int_ms),
         "decode_direct_ms": statistics.mean(direct_ms),
         "decode_compare": ("the same decode batch outside the timed steps: decode_int_ms on the integer-pipe CRT "
-                           "kernel k_modexp_crt<64,8,4>, decode_direct_ms on k_modexp (c^a mod n^2, no CRT)"),
+                           "kernel k_modexp_crt<64,8,4>, decode_direct_ms without the factors (c^a mod n^2 itself, "
+                           "k_modexp52 on the FP64 pipe)"),
         "p50_ms": statistics.median(step_ms),
         "p99_ms": float(np.percentile(step_ms, 99)),
         "plain_value": plain_value,

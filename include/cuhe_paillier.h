@@ -80,17 +80,19 @@ int cuhe_paillier_set_factors(cuhe_paillier* ctx, const uint32_t* p, int p_words
 /* 1 when factors are installed (decrypt / decode use the CRT kernel). */
 int cuhe_paillier_has_factors(const cuhe_paillier* ctx);
 
-/* Pipe of the CRT exponentiations.  With enable = 1 (the default) and the
- * factors installed, decrypt / decode of keys with n^2 of 4096 or 8192 bits
- * run both half-width exponentiations as Montgomery products of 52-bit limbs
- * on the FP64 pipe (three exact FP64 instructions per 52x52-bit product,
- * sums in 64-bit integers, ten limbs per lane, a 3-bit window), entering and
- * leaving through the same 32-bit reduction, Garner recombination and
- * epilogue, so results are identical to the integer-pipe kernel; n^2 of 2048
- * bits stays on the integer pipe (measured faster there) unless enable = 2.
- * enable = 0 keeps every product on the integer pipe.  get returns the
- * setting.  No reference counterpart (the reference's CGBN kernels multiply
- * 32-bit words on the integer pipe). */
+/* Pipe of the exponentiations.  With enable = 1 (the default), keys with n^2
+ * of 4096 or 8192 bits run them as Montgomery products of 52-bit limbs on the
+ * FP64 pipe (three exact FP64 instructions per 52x52-bit product, sums in
+ * 64-bit integers, ten limbs per lane, a 3-bit window): decrypt / decode by
+ * the CRT when the factors are installed (both half-width exponentiations),
+ * and otherwise mod n^2 itself, as do encryption (r^n), cuhe_paillier_modexp
+ * and mixed batches (cuhe_mix_plan, per width whose contexts all select it).
+ * Entry and exit go through 32-bit Montgomery products and the same
+ * recombination and epilogues, so results are identical to the integer-pipe
+ * kernels.  n^2 of 2048 bits stays on the integer pipe (measured faster
+ * there) unless enable = 2; enable = 0 keeps every product on the integer
+ * pipe.  get returns the setting.  No reference counterpart (the reference's
+ * CGBN kernels multiply 32-bit words on the integer pipe). */
 int cuhe_paillier_set_fp64(cuhe_paillier* ctx, int enable);
 int cuhe_paillier_get_fp64(const cuhe_paillier* ctx);
 
