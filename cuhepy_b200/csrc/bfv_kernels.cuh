@@ -1410,6 +1410,43 @@ __global__ void k_native_reduce(const u64* __restrict__ res, long long polys, in
   native_reduce_one<MAXW>(res + poly * count * R.n + i, R.n, count, out + (poly * R.n + i) * R.words, mode, t, R);
 }
 
+// A rotation of word ciphertexts (k_native_permute / k_native_finish and the
+// finishing form of k_native_mod_q): in = (c0, c1), perm = (sigma(c0),
+// sigma(c1)), out = (sigma(c0) + KS_0, KS_1) [+ in, accumulating], ks = the
+// switched words; all [2][N][W].
+struct NativeOp {
+  const u64* in;
+  u64* perm;
+  u64* out;
+  const u64* ks;
+};
+
+__device__ __forceinline__ void words_add_modq(const u64* x, const u64* y, u64* o, const RingDev& R);
+
+// The rotation's last step for coefficient i of component c = poly % 2 of
+// ops[poly / 2], given the switched value v (k_native_finish for one
+// coefficient).
+template <int kW, bool kAccumulate>
+__device__ __forceinline__ void native_finish_one(const NativeOp* __restrict__ ops, long long poly, int i,
+                                                  const u64 (&v)[kW], const RingDev& R) {
+  const NativeOp op = ops[poly >> 1];
+  const int c = int(poly & 1);
+  const long long off = ((long long)c * R.n + i) * kW;
+  u64 t[kW];
+  if (c == 0) {
+    words_add_modq(v, op.perm + off, t, R);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kW; ++k) t[k] = v[k];
+  }
+  if (kAccumulate) {
+    words_add_modq(t, op.in + off, op.out + off, R);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kW; ++k) op.out[off + k] = t[k];
+  }
+}
+
 // Mode-0 reduction straight from the residues, after the reference's
 // certified CRT (rns_ntt.h:422-469): with y_j = r_j (P / p_j)^-1 mod p_j and
 // theta = sum y_j / p_j, the centred integer is x = sum y_j (P / p_j) - v P
@@ -1421,16 +1458,21 @@ __global__ void k_native_reduce(const u64* __restrict__ res, long long polys, in
 // - v pq' (c', pq' carry an extra factor 2^128) lies in [0, 2^65 q), and two
 // Montgomery word steps give A 2^-128 mod q = x mod q in [0, 2q).  kW = the
 // ring's words, a compile-time constant so that A stays in registers.
-template <int kW, int MAXW>
+// kFinish (1, 2 accumulating): poly 2k + c of res is component c of the key
+// switch of ops[k], and the reduced value is finished as k_native_finish
+// does (+ sigma(c0) for c = 0, + in when accumulating) into ops[k].out
+// instead of being written to out.
+template <int kW, int MAXW, int kFinish = 0>
 __global__ void k_native_mod_q(const u64* __restrict__ res, long long polys, int count, u64* __restrict__ out,
-                               const RingDev* __restrict__ ring) {
+                               const RingDev* __restrict__ ring, const NativeOp* __restrict__ ops = nullptr) {
   const RingDev& R = *ring;
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= polys * R.n) return;
   const long long poly = idx / R.n;
   const int i = int(idx % R.n);
   const u64* z = res + poly * count * R.n + i;
-  u64* o = out + (poly * R.n + i) * kW;
+  u64 fin[kW];  // kFinish: the reduced value, finished below
+  u64* o = kFinish ? fin : out + (poly * R.n + i) * kW;
   const NativeCrt& C = R.crt[count - 1];
   u64 a[kW + 2];
 #pragma unroll
@@ -1455,6 +1497,7 @@ __global__ void k_native_mod_q(const u64* __restrict__ res, long long polys, int
   const u64 v = u64((theta + half) >> 64);
   if (v != u64((theta + u128(2 * count) + half) >> 64)) {
     native_reduce_one<MAXW>(z, R.n, count, o, 0, 0, R);
+    if (kFinish) native_finish_one<kW, kFinish == 2>(ops, poly, i, fin, R);
     return;
   }
   u64 borrow = 0;  // a -= v pq (stays >= 0: v <= count and pq < q)
@@ -1503,6 +1546,7 @@ __global__ void k_native_mod_q(const u64* __restrict__ res, long long polys, int
   }
 #pragma unroll
   for (int k = 0; k < kW; ++k) o[k] = a[k];
+  if (kFinish) native_finish_one<kW, kFinish == 2>(ops, poly, i, fin, R);
 }
 
 // Mode-1 (scale-and-round) reduction from the residues of the tensor primes:
@@ -1778,13 +1822,6 @@ __global__ void k_words_automorphism(const u64* __restrict__ in, u64* __restrict
 // Per-ciphertext descriptors of the native rotate / add steps (two word polys
 // each): permute writes perm = sigma_g(in); finish writes out = (ks0 + perm0,
 // ks1); add writes out = in + perm.
-struct NativeOp {
-  const u64* in;
-  u64* perm;
-  u64* out;
-  const u64* ks;
-};
-
 __device__ __forceinline__ void words_add_modq(const u64* x, const u64* y, u64* o, const RingDev& R) {
   const int W = R.words;
   u64 r[kMaxWords];

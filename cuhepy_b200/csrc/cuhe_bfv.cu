@@ -846,8 +846,11 @@ size_t native_mask_primes(const cuhe_bfv_ring* r, u64 t) {
   return H::prime_count_for(P.primes, bound);
 }
 
+// finish (1, 2 accumulating; mode 0 with the certified tables only): the
+// polys are the key switches of finish_ops, which are finished in the same
+// pass (k_native_mod_q's epilogue) instead of being written to out.
 int native_reduce(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* res, size_t polys, size_t count, u64* out,
-                  int mode, u64 t) {
+                  int mode, u64 t, const NativeOp* finish_ops = nullptr, int finish = 0) {
   if (!polys) return CUHE_OK;
   const unsigned blocks = blocks_for((long long)(polys * r->plan.n), 128);
   if (mode == 1 && r->d_crt && count == r->plan.tensor_count) {
@@ -869,21 +872,33 @@ int native_reduce(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* res, size_t
   }
   if (mode == 0 && r->d_crt) {
     const bool narrow = count <= size_t(kNarrowWords);
-#define CUHE_MOD_Q(KW)                                                                                          \
-  case KW:                                                                                                      \
-    if (narrow)                                                                                                 \
-      k_native_mod_q<KW, kNarrowWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, d); \
-    else                                                                                                        \
-      k_native_mod_q<KW, kWideWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, d);   \
+#define CUHE_MOD_Q_F(KW, F)                                                                                 \
+  if (narrow)                                                                                                   \
+    k_native_mod_q<KW, kNarrowWords, F><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, d, \
+                                                                       finish_ops);                             \
+  else                                                                                                          \
+    k_native_mod_q<KW, kWideWords, F><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, d,   \
+                                                                     finish_ops);
+#define CUHE_MOD_Q(KW)                  \
+  case KW:                              \
+    if (finish == 2) {                  \
+      CUHE_MOD_Q_F(KW, 2)               \
+    } else if (finish == 1) {           \
+      CUHE_MOD_Q_F(KW, 1)               \
+    } else {                            \
+      CUHE_MOD_Q_F(KW, 0)               \
+    }                                   \
     break;
     switch (r->host_dev.words) {
       CUHE_MOD_Q(1) CUHE_MOD_Q(2) CUHE_MOD_Q(3) CUHE_MOD_Q(4) CUHE_MOD_Q(5) CUHE_MOD_Q(6) CUHE_MOD_Q(7)
       default: CUHE_MOD_Q(8)
     }
 #undef CUHE_MOD_Q
+#undef CUHE_MOD_Q_F
     BFV_CUDA(cudaGetLastError(), "native reduce");
     return CUHE_OK;
   }
+  if (finish) return fail(CUHE_INVALID_ARGUMENT, "finishing reduction needs the certified tables");
   if (count <= size_t(kNarrowWords))
     k_native_reduce<kNarrowWords><<<blocks, 128, 0, ln.stream>>>(res, (long long)polys, int(count), out, mode, t, d);
   else
@@ -926,13 +941,13 @@ int native_mul_plain(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const u64* words, s
 // ([ops][2][N][W]); res: [ops][2][S][N] scratch
 int native_switch(cuhe_bfv_ring* r, Lane& ln, RingDev* d, const std::vector<const u64*>& in,
                   const std::vector<const cuhe_bfv_key*>& keys, u64* res, u64* out, SwitchOp* d_sops,
-                  Arena* small = nullptr) {
+                  Arena* small = nullptr, const NativeOp* finish_ops = nullptr, int finish = 0) {
   const size_t n = r->plan.n, S = r->switch_prime_count;
   std::vector<SwitchOp> sops(in.size());
   for (size_t k = 0; k < in.size(); ++k)
     sops[k] = SwitchOp{nullptr, nullptr, in[k], keys[k]->d_key, keys[k]->d_key_q, res + k * 2 * S * n, 1u, 0u};
   if (int rc = run_switch(r, ln, d, {}, sops, nullptr, d_sops, small)) return rc;
-  return native_reduce(r, ln, d, res, in.size() * 2, S, out, 0, 0);
+  return native_reduce(r, ln, d, res, in.size() * 2, S, out, 0, 0, finish_ops, finish);
 }
 
 // rotations of word ciphertexts by g: ops[k].out = (sigma(c0) + KS(sigma(c1))_0,
@@ -953,6 +968,10 @@ int native_rotate(cuhe_bfv_ring* r, Lane& ln, RingDev* d, std::vector<NativeOp> 
   std::vector<const u64*> c1(ops.size());
   std::vector<const cuhe_bfv_key*> keys(ops.size(), key);
   for (size_t k = 0; k < ops.size(); ++k) c1[k] = ops[k].perm + n * W;
+  if (r->d_crt) {
+    // the reduction mod q finishes the rotation in the same pass
+    return native_switch(r, ln, d, c1, keys, res, ks_all, d_sops, small, d_ops, accumulate ? 2 : 1);
+  }
   if (int rc = native_switch(r, ln, d, c1, keys, res, ks_all, d_sops, small)) return rc;
   if (accumulate) k_native_finish<true><<<grid, 256, 0, ln.stream>>>(d_ops, d);
   else k_native_finish<false><<<grid, 256, 0, ln.stream>>>(d_ops, d);
