@@ -244,6 +244,39 @@ Modexp52 direct52(const cuhe_paillier* ctx) {
   return nullptr;
 }
 
+// encode_hamming_server on the FP64 pipe: queries to R52 Montgomery limbs,
+// then one product per output.
+template <int K>
+cudaError_t launch_outer52(cuhe_paillier* ctx, const uint32_t* query, long long nq, double* q52,
+                           const uint32_t* index, long long nx, uint32_t* out) {
+  constexpr int TPI = K / 16, K52 = 5 * K / 8, IPB = cuhe::kBlockThreads / TPI;
+  const size_t csmem = size_t(K + IPB * K) * 4;
+  cuhe::k_to_mont52<K><<<dim3(unsigned((nq + IPB - 1) / IPB)), cuhe::kBlockThreads, csmem, ctx->stream>>>(
+      query, nq, q52, ctx->d_consts, ctx->ks, ctx->d_n52, ctx->d_status);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t smem = size_t(K52 + IPB * K52) * 8;
+  const long long bx = (nx + IPB - 1) / IPB;
+  for (long long q0 = 0; q0 < nq; q0 += 65535) {
+    const long long qn = std::min<long long>(65535, nq - q0);
+    cuhe::k_mulmod_outer52<K><<<dim3(unsigned(bx), unsigned(qn)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+        q52 + q0 * K52, index, nx, out + q0 * nx * K, ctx->d_consts, ctx->d_n52, ctx->ninv52, ctx->d_status);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+using Outer52 = cudaError_t (*)(cuhe_paillier*, const uint32_t*, long long, double*, const uint32_t*, long long,
+                                uint32_t*);
+Outer52 outer52(const cuhe_paillier* ctx) {
+  if (!direct52(ctx)) return nullptr;
+  if (ctx->K == 64) return &launch_outer52<64>;
+  if (ctx->K == 128) return &launch_outer52<128>;
+  if (ctx->K == 256) return &launch_outer52<256>;
+  return nullptr;
+}
+
 template <int K>
 cudaError_t prepare_tasks52(int device, int* grid) {
   const size_t smem = modexp52_smem<K, kCrt52Window>();
@@ -1325,24 +1358,31 @@ int cuhe_paillier_mulmod_outer(cuhe_paillier* ctx, const uint32_t* query, int64_
   // A large host output moves in query-row blocks on the copy stream, each
   // block's download beside the next block's products.
   const bool pipe = obytes >= kPipeBytes && nq >= 2 && !is_device_pointer(out);
+  const Outer52 f52 = outer52(ctx);
   Stager st(ctx);
   st.add(query, size_t(nq) * kb, true, false);
   st.add(index, size_t(nx) * kb, true, false);
   st.add(out, obytes, false, !pipe);
-  st.add_scratch(size_t(nq) * kb);  // queries in Montgomery form
+  st.add_scratch(size_t(nq) * (f52 ? size_t(ctx->K) * 5 : kb));  // queries in Montgomery form (words or 52-bit limbs)
   if (int rc = st.bind()) return rc;
   uint32_t* qm = static_cast<uint32_t*>(st.dev(3));
   uint32_t* d_out = static_cast<uint32_t*>(st.dev(2));
-  CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(0), qm, nq, 1), "query conversion");
+  // the FP64 form converts each query block inside its launch
+  auto outer = [&](int64_t q0, int64_t qn, uint32_t* o) -> cudaError_t {
+    if (f52)
+      return f52(ctx, (const uint32_t*)st.dev(0) + size_t(q0) * ctx->K, qn,
+                 reinterpret_cast<double*>(qm) + size_t(q0) * (5 * size_t(ctx->K) / 8), (const uint32_t*)st.dev(1),
+                 nx, o);
+    return d.outer(ctx, qm + size_t(q0) * ctx->K, qn, (const uint32_t*)st.dev(1), nx, o);
+  };
+  if (!f52) CUHE_CUDA(ctx, d.convert(ctx, (const uint32_t*)st.dev(0), qm, nq, 1), "query conversion");
   if (pipe && st.is_staged(2)) {
     if (int rc = pipeline_streams(ctx)) return rc;
     const int64_t rows = std::max<int64_t>(1, nq / 8);
     const size_t row_words = size_t(nx) * ctx->K;
     for (int64_t q0 = 0; q0 < nq; q0 += rows) {
       const int64_t qn = std::min(rows, nq - q0);
-      CUHE_CUDA(ctx, d.outer(ctx, qm + size_t(q0) * ctx->K, qn, (const uint32_t*)st.dev(1), nx,
-                             d_out + size_t(q0) * row_words),
-                "mulmod_outer launch");
+      CUHE_CUDA(ctx, outer(q0, qn, d_out + size_t(q0) * row_words), "mulmod_outer launch");
       CUHE_CUDA(ctx, stream_after(ctx->copy, ctx->stream), "download order");
       CUHE_CUDA(ctx, cudaMemcpyAsync(out + size_t(q0) * row_words, d_out + size_t(q0) * row_words,
                                      size_t(qn) * row_words * 4, cudaMemcpyDeviceToHost, ctx->copy),
@@ -1350,7 +1390,7 @@ int cuhe_paillier_mulmod_outer(cuhe_paillier* ctx, const uint32_t* query, int64_
     }
     CUHE_CUDA(ctx, stream_after(ctx->stream, ctx->copy), "download join");
   } else {
-    CUHE_CUDA(ctx, d.outer(ctx, qm, nq, (const uint32_t*)st.dev(1), nx, d_out), "mulmod_outer launch");
+    CUHE_CUDA(ctx, outer(0, nq, d_out), "mulmod_outer launch");
   }
   if (int rc = st.finish()) return rc;
   // the scratch slice is reused by the next call: keep host order

@@ -940,6 +940,92 @@ k_modexp52_tasks(const ModexpTask* __restrict__ tasks, int ntasks, long long tot
 }
 
 // ---------------------------------------------------------------------------
+// encode_hamming_server on the FP64 pipe (n^2 of 4096 / 8192 bits):
+// out[q][j] = index[j] * query[q] mod n^2 as one Montgomery product of 52-bit
+// limbs, the query entering in the Montgomery domain of R52
+// (k_to_mont52: query R52 mod n^2, once per query) and the index value and
+// the result crossing between 32-bit words and 52-bit limbs by bit
+// shuffling, so each output costs one product: mont52(index, query R52) =
+// index * query mod n^2, canonical, as k_mulmod_outer's.
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(kBlockThreads)
+k_to_mont52(const uint32_t* __restrict__ in, long long count, double* __restrict__ out,
+            const uint32_t* __restrict__ consts, KeyScalars ks, const double* __restrict__ n52, int* status) {
+  constexpr int TPI = K / 16, L = 16, K52 = 5 * K / 8, L52 = K52 / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_r52r = smem;  // R52 R mod n^2
+  {
+    const uint32_t* r52r = reinterpret_cast<const uint32_t*>(n52 + 2 * K52);
+    for (int i = threadIdx.x; i < K; i += blockDim.x) s_r52r[i] = r52r[i];
+  }
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;
+  uint32_t n2[L], x[L], xr[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load(x, in + inst * K);
+  if (!g.less_than(x, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  g.mont_mul(xr, x, s_r52r, n2, ks.ninv2);  // x R52 mod n^2
+  uint32_t* s_w = smem + K + slot * K;
+  g.publish(s_w, xr);
+#pragma unroll
+  for (int k = 0; k < L52; ++k)
+    out[inst * K52 + g.gl * L52 + k] = cuhe52::to_f64(limb52_from_words(s_w, K, g.gl * L52 + k));
+}
+
+template <int K>
+__global__ void __launch_bounds__(kBlockThreads, 3)
+k_mulmod_outer52(const double* __restrict__ q52, const uint32_t* __restrict__ index, long long nx,
+                 uint32_t* __restrict__ out, const uint32_t* __restrict__ consts, const double* __restrict__ n52,
+                 unsigned long long ninv52, int* status) {
+  constexpr int TPI = K / 16, L = 16, K52 = 5 * K / 8, L52 = K52 / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  extern __shared__ __align__(16) double smd[];
+  double* s_b = smd;          // the query, K52 limbs (Montgomery form)
+  double* s_inst = smd + K52; // per instance K52 doubles: the index words in, the result limbs out
+  const long long qi = blockIdx.y;
+  for (int i = threadIdx.x; i < K52; i += blockDim.x) s_b[i] = q52[qi * K52 + i];
+  __syncthreads();
+  Group<K, TPI> g;
+  cuhe52::Group52<K52, TPI> f;
+  const int slot = threadIdx.x / TPI;
+  const long long j = (long long)blockIdx.x * IPB + slot;
+  if (j >= nx) return;
+  uint32_t n2[L], x[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load_ro(x, index + j * K);
+  if (!g.less_than(x, n2)) {
+    if (g.gl == 0) atomicOr(status, ST_RANGE);
+    return;
+  }
+  uint32_t* s_w = reinterpret_cast<uint32_t*>(s_inst + slot * K52);
+  g.publish(s_w, x);
+  double a52[L52], m52[L52], r52[L52];
+#pragma unroll
+  for (int k = 0; k < L52; ++k) {
+    a52[k] = cuhe52::to_f64(limb52_from_words(s_w, K, f.gl * L52 + k));
+    m52[k] = __ldg(n52 + f.gl * L52 + k);
+  }
+  f.mont_mul(r52, a52, s_b, m52, ninv52);
+  uint64_t* s_l = reinterpret_cast<uint64_t*>(s_inst + slot * K52);
+  __syncwarp(f.mask);
+#pragma unroll
+  for (int k = 0; k < L52; ++k) s_l[f.gl * L52 + k] = cuhe52::to_u64(r52[k]);
+  __syncwarp(f.mask);
+  uint32_t w[L];
+#pragma unroll
+  for (int t = 0; t < L; ++t) w[t] = word_from_limbs52(s_l, K52, g.gl * L + t);
+  g.store(out + (qi * nx + j) * K, w);
+}
+
+// ---------------------------------------------------------------------------
 // Modular exponentiation with a per-instance exponent (fixed 4-bit windows, so
 // every group of a warp follows the same schedule):
 //   out[i] = base[i]^exps[i] mod n^2, exps[i] held in exp_words words.

@@ -123,8 +123,8 @@ def test_fp64_pipe_equals_integer_pipe(name):
     """The exponentiations as 52-bit-limb products on the FP64 pipe give the
     integer-pipe kernels' results: by the CRT (decrypt and decode) and mod
     n^2 itself (decrypt and decode without the factors, encryption, public
-    powers), on ciphertexts and on awkward values (several waves of a device
-    batch)."""
+    powers) and the server's products, on ciphertexts and on awkward values
+    (several waves of a device batch)."""
     import torch
 
     data = load_golden(name)
@@ -164,19 +164,35 @@ def test_fp64_pipe_equals_integer_pipe(name):
     rs = [rng.randrange(1, n) for _ in range(len(ms))]
     exps = [0, 1, 2, 3, n, rng.getrandbits(300), rng.getrandbits(2 * n.bit_length())]
     bases = [rng.randrange(n2) for _ in range(300)] + [0, 1, n2 - 1]
+    # encode_hamming_server products: a device batch, and a host output
+    # large enough for the piecewise download
+    queries = [rng.randrange(n2) for _ in range(5)] + [0, 1, n2 - 1]
+    qx = torch.from_numpy(direct.limbs(queries).view(np.int32)).cuda()
+    big_q = 2 + (64 << 20) // (len(vals) * direct.words * 4)
+    bq = np.ascontiguousarray(np.repeat(direct.limbs(queries[:1]), big_q, axis=0))
     got = []
     for fp64 in (2, 0):
         direct.set_fp64(fp64)
         out = torch.zeros((len(vals), direct.words), dtype=torch.int32, device="cuda")
         dist = torch.full((len(vals) // 2,), -1, dtype=torch.int64, device="cuda")
+        outer = torch.zeros((len(queries) * len(vals), direct.words), dtype=torch.int32, device="cuda")
         direct.decrypt_array(limbs, out, len(vals))
         direct.decode_array(limbs, len(vals) // 2, 2, 64, dist)
+        direct.mulmod_outer_array(qx, len(queries), limbs, len(vals), outer)
         direct.synchronize()
-        got.append((out, dist, direct.encrypt(ms, rs), [direct.modexp(bases, e) for e in exps]))
+        host_out = np.zeros((big_q * len(vals), direct.words), dtype=np.uint32)
+        direct.mulmod_outer_array(bq, big_q, direct.limbs(vals), len(vals), host_out)
+        got.append((out, dist, direct.encrypt(ms, rs), [direct.modexp(bases, e) for e in exps], outer, host_out))
     direct.set_fp64(1)
-    (o2, d2, c2, p2), (o0, d0, c0, p0) = got
+    (o2, d2, c2, p2, x2, h2), (o0, d0, c0, p0, x0, h0) = got
     assert torch.equal(o2, o0) and torch.equal(d2, d0) and torch.equal(o2, outs[0])
     assert c2 == c0 and p2 == p0
+    assert torch.equal(x2, x0) and np.array_equal(h2, h0)
+    xs = from_limbs(x2.cpu().numpy().view(np.uint32))
+    for qi in (0, len(queries) - 1):
+        for k in (0, 9, len(vals) - 1):
+            assert xs[qi * len(vals) + k] == queries[qi] * vals[k] % n2
+    assert from_limbs(h2[:3]) == [queries[0] * v % n2 for v in vals[:3]]
     for k in (0, 5, len(ms) - 1):
         assert c2[k] == (1 + ms[k] * n) * pow(rs[k], n, n2) % n2
     for e, row in zip(exps, p2):
