@@ -98,7 +98,7 @@ struct cuhe_paillier {
   int nops_sec52 = 0;
   uint32_t* d_crt = nullptr;  // CRT constant block, present once the factors are installed
   double* d_crt52 = nullptr;  // per side: M and R52 mod M as 52-bit limbs (FP64-pipe CRT kernel)
-  double* d_n52 = nullptr;    // n^2 and R52 mod n^2 as 52-bit limbs, then R52 R mod n^2 in words (k_modexp52)
+  double* d_n52 = nullptr;    // n^2 and R52 mod n^2 as 52-bit limbs, then R52 R and R52 mod n^2 in words
   unsigned long long ninv52 = 0;  // -(n^2)^-1 mod 2^52
   int32_t* d_ops_n52 = nullptr;   // the schedule of n for k_modexp52's window
   int nops_n52 = 0;
@@ -109,6 +109,8 @@ struct cuhe_paillier {
   uint32_t* d_gtab = nullptr;
   int message_chunks = 0;
   uint32_t* d_wide = nullptr;  // 16-bit-digit table W[j][D], built on demand (see cuhe_lookup_set_wide_table)
+  double* d_wide52 = nullptr;  // ... as 52-bit limbs in the R52 domain (FP64-pipe encryption), with
+  double* d_noise52 = nullptr; // the noise table likewise
   int wide_mode = 1;           // 0 never, 1 for large batches when it fits, 2 always
   uint32_t* d_noise = nullptr;
   int noise_entries = 0;
@@ -252,7 +254,8 @@ cudaError_t launch_outer52(cuhe_paillier* ctx, const uint32_t* query, long long 
   constexpr int TPI = K / 16, K52 = 5 * K / 8, IPB = cuhe::kBlockThreads / TPI;
   const size_t csmem = size_t(K + IPB * K) * 4;
   cuhe::k_to_mont52<K><<<dim3(unsigned((nq + IPB - 1) / IPB)), cuhe::kBlockThreads, csmem, ctx->stream>>>(
-      query, nq, q52, ctx->d_consts, ctx->ks, ctx->d_n52, ctx->d_status);
+      query, nq, q52, ctx->d_consts, ctx->ks, reinterpret_cast<const uint32_t*>(ctx->d_n52 + 2 * K52),
+      ctx->d_status);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t smem = size_t(K52 + IPB * K52) * 8;
@@ -275,6 +278,55 @@ Outer52 outer52(const cuhe_paillier* ctx) {
   if (ctx->K == 128) return &launch_outer52<128>;
   if (ctx->K == 256) return &launch_outer52<256>;
   return nullptr;
+}
+
+// The 16-bit-digit table and the noise table as 52-bit limbs in the R52
+// domain (k_wide_table52 row by row, k_to_mont52 from the 32-bit Montgomery
+// form), and encryption from them.
+template <int K>
+cudaError_t build_wide52(cuhe_paillier* ctx, double* wide52, double* noise52) {
+  constexpr int TPI = K / 16, K52 = 5 * K / 8, IPB = cuhe::kBlockThreads / TPI;
+  const uint32_t* r52w = reinterpret_cast<const uint32_t*>(ctx->d_n52 + 2 * K52) + K;
+  const size_t smem = size_t(K + IPB * K) * 4;
+  for (int j = 0; j < (ctx->message_chunks + 1) / 2; ++j) {
+    cuhe::k_wide_table52<K><<<dim3(65536 / IPB), cuhe::kBlockThreads, smem, ctx->stream>>>(
+        ctx->d_gtab, ctx->message_chunks, j, wide52, ctx->d_consts, ctx->ks, r52w);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  cuhe::k_to_mont52<K><<<dim3(unsigned((ctx->noise_entries + IPB - 1) / IPB)), cuhe::kBlockThreads, smem,
+                         ctx->stream>>>(ctx->d_noise, ctx->noise_entries, noise52, ctx->d_consts, ctx->ks, r52w,
+                                        ctx->d_status);
+  return cudaGetLastError();
+}
+
+template <int K>
+cudaError_t launch_lookup52(cuhe_paillier* ctx, const uint8_t* bits, int embed_len, int chunk_len, int chunk_num,
+                            const uint32_t* plain, long long count, const uint8_t* idx, uint32_t* out) {
+  constexpr int TPI = K / 16, K52 = 5 * K / 8, IPB = cuhe::kBlockThreads / TPI;
+  const size_t rows_bytes = size_t(IPB) * cuhe::lookup_rows_stride(ctx->message_chunks) * 2;
+  const size_t smem = size_t(K52 + IPB * (K52 + 2)) * 8 + ((rows_bytes + 15) & ~size_t(15));
+  cudaError_t e = cudaFuncSetAttribute(cuhe::k_lookup_encrypt52<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  cuhe::k_lookup_encrypt52<K><<<dim3(unsigned((count + IPB - 1) / IPB)), cuhe::kBlockThreads, smem, ctx->stream>>>(
+      bits, embed_len, chunk_len, chunk_num, plain, K, count, ctx->message_chunks, ctx->d_wide52, ctx->d_noise52,
+      ctx->noise_entries, idx, out, ctx->d_n52, ctx->ninv52, ctx->d_status);
+  return cudaGetLastError();
+}
+
+struct Lookup52 {
+  cudaError_t (*build)(cuhe_paillier*, double*, double*);
+  cudaError_t (*launch)(cuhe_paillier*, const uint8_t*, int, int, int, const uint32_t*, long long, const uint8_t*,
+                        uint32_t*);
+};
+bool lookup52(const cuhe_paillier* ctx, Lookup52* l) {
+  if (!direct52(ctx)) return false;
+  if (ctx->K == 64) *l = {&build_wide52<64>, &launch_lookup52<64>};
+  else if (ctx->K == 128) *l = {&build_wide52<128>, &launch_lookup52<128>};
+  else if (ctx->K == 256) *l = {&build_wide52<256>, &launch_lookup52<256>};
+  else return false;
+  return true;
 }
 
 template <int K>
@@ -632,7 +684,7 @@ int setup_direct52(cuhe_paillier* ctx) {
   const size_t k = size_t(ctx->K), k52 = 5 * k / 8;
   Limbs one(k, 0u);
   one[0] = 1u;
-  std::vector<double> block(2 * k52 + k / 2, 0.0);
+  std::vector<double> block(2 * k52 + k, 0.0);
   auto put52 = [&](size_t row, const Limbs& v) {
     for (size_t i = 0; i < k52; ++i) {
       uint64_t limb = 0;
@@ -647,6 +699,8 @@ int setup_direct52(cuhe_paillier* ctx) {
   put52(1, cuhe::host::shift_mod(one, 52 * k52, ctx->n2));
   const Limbs r52r = cuhe::host::shift_mod(one, 52 * k52 + 32 * k, ctx->n2);
   std::memcpy(block.data() + 2 * k52, r52r.data(), 4 * k);
+  const Limbs r52 = cuhe::host::shift_mod(one, 52 * k52, ctx->n2);
+  std::memcpy(block.data() + 2 * k52 + k / 2, r52.data(), 4 * k);
   const uint64_t m0 = (uint64_t(ctx->n2[1]) << 32) | ctx->n2[0];
   uint64_t inv = m0;
   for (int it = 0; it < 6; ++it) inv *= 2 - m0 * inv;
@@ -785,6 +839,8 @@ void cuhe_paillier_destroy(cuhe_paillier* ctx) {
   cudaFree(ctx->d_ops_n52);
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_wide);
+  cudaFree(ctx->d_wide52);
+  cudaFree(ctx->d_noise52);
   cudaFree(ctx->d_noise);
   for (cudaStream_t st : {ctx->copy, ctx->side})
     if (st) cudaStreamSynchronize(st);
@@ -1412,9 +1468,13 @@ int cuhe_lookup_set_tables(cuhe_paillier* ctx, const uint32_t* g_table, int mess
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_noise);
   cudaFree(ctx->d_wide);
+  cudaFree(ctx->d_wide52);
+  cudaFree(ctx->d_noise52);
   ctx->d_gtab = nullptr;
   ctx->d_noise = nullptr;
   ctx->d_wide = nullptr;
+  ctx->d_wide52 = nullptr;
+  ctx->d_noise52 = nullptr;
   ctx->message_chunks = 0;
   ctx->noise_entries = 0;
   CUHE_CUDA(ctx, cudaMalloc(&ctx->d_gtab, gbytes), "table allocation");
@@ -1471,8 +1531,12 @@ int cuhe_lookup_build_tables(cuhe_paillier* ctx, const uint32_t* g, int message_
   CUHE_CUDA(ctx, d.convert(ctx, b, (uint32_t*)bm.ptr, message_chunks, 1), "row conversion");
   cudaFree(ctx->d_gtab);
   cudaFree(ctx->d_wide);
+  cudaFree(ctx->d_wide52);
+  cudaFree(ctx->d_noise52);
   ctx->d_gtab = nullptr;
   ctx->d_wide = nullptr;
+  ctx->d_wide52 = nullptr;
+  ctx->d_noise52 = nullptr;
   ctx->message_chunks = 0;
   CUHE_CUDA(ctx, cudaMalloc(&ctx->d_gtab, size_t(message_chunks) * 256 * kb), "table allocation");
   CUHE_CUDA(ctx, d.table_rows(ctx, (const uint32_t*)bm.ptr, message_chunks, ctx->d_gtab), "table rows");
@@ -1519,27 +1583,42 @@ int cuhe_lookup_get_g_table(cuhe_paillier* ctx, uint32_t* out) {
 namespace {
 
 int ensure_wide_table(cuhe_paillier* ctx, const Dispatch& d, long long items) {
-  if (ctx->d_wide || ctx->wide_mode == 0 || !ctx->d_gtab) return CUHE_OK;
+  if (ctx->d_wide || ctx->d_wide52 || ctx->wide_mode == 0 || !ctx->d_gtab) return CUHE_OK;
   if (ctx->wide_mode == 1 && items < kWideMinItems) return CUHE_OK;
-  const size_t bytes = size_t((ctx->message_chunks + 1) / 2) * 65536 * size_t(ctx->K) * 4;
+  // the table as the selected pipe takes it: 52-bit limbs (doubles, K52 =
+  // 5K/8 a row) for the FP64 pipe, else 32-bit words
+  Lookup52 l52{};
+  const bool fp52 = lookup52(ctx, &l52);
+  const size_t entry = fp52 ? size_t(5 * ctx->K / 8) * 8 : size_t(ctx->K) * 4;
+  const size_t bytes = size_t((ctx->message_chunks + 1) / 2) * 65536 * entry;
   if (ctx->wide_mode == 1) {
     size_t free_bytes = 0, total_bytes = 0;
     CUHE_CUDA(ctx, cudaMemGetInfo(&free_bytes, &total_bytes), "free memory");
     if (bytes > kWideMaxBytes || bytes > free_bytes / 4) return CUHE_OK;
   }
-  uint32_t* wide = nullptr;
+  void* wide = nullptr;
+  void* noise52 = nullptr;
   cudaError_t e = cudaMalloc(&wide, bytes);
+  if (e == cudaSuccess && fp52) e = cudaMalloc(&noise52, size_t(ctx->noise_entries) * entry);
   if (e != cudaSuccess) {
     cudaGetLastError();
+    cudaFree(wide);
     if (ctx->wide_mode == 2) return fail(ctx, CUHE_OUT_OF_MEMORY, "wide table allocation");
     return CUHE_OK;
   }
-  e = d.wide_table(ctx, wide);
+  e = fp52 ? l52.build(ctx, static_cast<double*>(wide), static_cast<double*>(noise52))
+           : d.wide_table(ctx, static_cast<uint32_t*>(wide));
   if (e != cudaSuccess) {
     cudaFree(wide);
+    cudaFree(noise52);
     return cuda_fail(ctx, e, "wide table build");
   }
-  ctx->d_wide = wide;
+  if (fp52) {
+    ctx->d_wide52 = static_cast<double*>(wide);
+    ctx->d_noise52 = static_cast<double*>(noise52);
+  } else {
+    ctx->d_wide = static_cast<uint32_t*>(wide);
+  }
   return CUHE_OK;
 }
 
@@ -1552,15 +1631,19 @@ int cuhe_lookup_set_wide_table(cuhe_paillier* ctx, int mode) {
   DeviceGuard guard(ctx->device);
   std::lock_guard<std::mutex> lock(ctx->mu);
   ctx->wide_mode = mode;
-  if (mode == 0 && ctx->d_wide) {
+  if (mode == 0 && (ctx->d_wide || ctx->d_wide52)) {
     CUHE_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "wide table release");
     cudaFree(ctx->d_wide);
+    cudaFree(ctx->d_wide52);
+    cudaFree(ctx->d_noise52);
     ctx->d_wide = nullptr;
+    ctx->d_wide52 = nullptr;
+    ctx->d_noise52 = nullptr;
   }
   return CUHE_OK;
 }
 
-int cuhe_lookup_wide_table_ready(const cuhe_paillier* ctx) { return ctx && ctx->d_wide ? 1 : 0; }
+int cuhe_lookup_wide_table_ready(const cuhe_paillier* ctx) { return ctx && (ctx->d_wide || ctx->d_wide52) ? 1 : 0; }
 
 int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t vectors, int embed_len, int chunk_len,
                              int chunk_num, const uint8_t* noise_index, uint32_t* out) {
@@ -1582,8 +1665,10 @@ int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t ve
   st.add(noise_index, size_t(total) * cuhe::kNoiseMultiples, true, false);
   st.add(out, size_t(total) * ctx->K * 4, false, true);
   if (int rc = st.bind()) return rc;
-  CUHE_CUDA(ctx, d.lookup(ctx, (const uint8_t*)st.dev(0), embed_len, chunk_len, chunk_num, nullptr, total,
-                          (const uint8_t*)st.dev(1), (uint32_t*)st.dev(2)),
+  Lookup52 l52{};
+  const bool fp52 = ctx->d_wide52 && lookup52(ctx, &l52);
+  CUHE_CUDA(ctx, (fp52 ? l52.launch : d.lookup)(ctx, (const uint8_t*)st.dev(0), embed_len, chunk_len, chunk_num, nullptr,
+                                               total, (const uint8_t*)st.dev(1), (uint32_t*)st.dev(2)),
             "lookup encrypt launch");
   if (int rc = st.finish()) return rc;
   return check_status(ctx, st.staged());
@@ -1605,8 +1690,10 @@ int cuhe_lookup_encrypt_ints(cuhe_paillier* ctx, const uint32_t* m, int64_t coun
   st.add(noise_index, size_t(count) * cuhe::kNoiseMultiples, true, false);
   st.add(out, size_t(count) * ctx->K * 4, false, true);
   if (int rc = st.bind()) return rc;
-  CUHE_CUDA(ctx, d.lookup(ctx, nullptr, 0, 0, 1, (const uint32_t*)st.dev(0), count, (const uint8_t*)st.dev(1),
-                          (uint32_t*)st.dev(2)),
+  Lookup52 l52{};
+  const bool fp52 = ctx->d_wide52 && lookup52(ctx, &l52);
+  CUHE_CUDA(ctx, (fp52 ? l52.launch : d.lookup)(ctx, nullptr, 0, 0, 1, (const uint32_t*)st.dev(0), count,
+                                               (const uint8_t*)st.dev(1), (uint32_t*)st.dev(2)),
             "lookup encrypt launch");
   if (int rc = st.finish()) return rc;
   return check_status(ctx, st.staged());

@@ -948,18 +948,17 @@ k_modexp52_tasks(const ModexpTask* __restrict__ tasks, int ntasks, long long tot
 // shuffling, so each output costs one product: mont52(index, query R52) =
 // index * query mod n^2, canonical, as k_mulmod_outer's.
 // ---------------------------------------------------------------------------
+// row: R52 R mod n^2 for plain inputs, R52 mod n^2 for inputs already in
+// the 32-bit Montgomery form (x R): either way out = x R52 mod n^2.
 template <int K>
 __global__ void __launch_bounds__(kBlockThreads)
 k_to_mont52(const uint32_t* __restrict__ in, long long count, double* __restrict__ out,
-            const uint32_t* __restrict__ consts, KeyScalars ks, const double* __restrict__ n52, int* status) {
+            const uint32_t* __restrict__ consts, KeyScalars ks, const uint32_t* __restrict__ row, int* status) {
   constexpr int TPI = K / 16, L = 16, K52 = 5 * K / 8, L52 = K52 / TPI;
   constexpr int IPB = kBlockThreads / TPI;
   extern __shared__ __align__(16) uint32_t smem[];
-  uint32_t* s_r52r = smem;  // R52 R mod n^2
-  {
-    const uint32_t* r52r = reinterpret_cast<const uint32_t*>(n52 + 2 * K52);
-    for (int i = threadIdx.x; i < K; i += blockDim.x) s_r52r[i] = r52r[i];
-  }
+  uint32_t* s_r52r = smem;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) s_r52r[i] = row[i];
   __syncthreads();
   Group<K, TPI> g;
   const int slot = threadIdx.x / TPI;
@@ -979,6 +978,7 @@ k_to_mont52(const uint32_t* __restrict__ in, long long count, double* __restrict
   for (int k = 0; k < L52; ++k)
     out[inst * K52 + g.gl * L52 + k] = cuhe52::to_f64(limb52_from_words(s_w, K, g.gl * L52 + k));
 }
+
 
 template <int K>
 __global__ void __launch_bounds__(kBlockThreads, 3)
@@ -1363,6 +1363,59 @@ constexpr int kNoiseMultiples = 14;
 // 16-bit entries of row list per instance: message_chunks rounded up to even
 __host__ __device__ constexpr int lookup_rows_stride(int message_chunks) { return (message_chunks + 1) & ~1; }
 
+// The table rows of an instance's nonzero digits (one lane): 8-bit digits as
+// i * 256 + d into rows16, or with kWide 16-bit digits as j * 65536 + D into
+// rows32 (the same storage); returns their count.  Digits come from a binary
+// embedding (Hamming padding "0b" per bit, MSB-first chunks of chunk_len
+// bits) or from little-endian plaintext words.
+template <bool kWide>
+__device__ __forceinline__ int lookup_digit_rows(const uint8_t* __restrict__ bits, int embed_len, int chunk_len,
+                                                 int chunk_num, const uint32_t* __restrict__ plain, int plain_words,
+                                                 long long inst, int message_chunks, uint16_t* s_rows16) {
+  uint32_t* s_rows32 = reinterpret_cast<uint32_t*>(s_rows16);
+  int cnt = 0;
+  int pending = 0;  // kWide: the low byte of the current 16-bit digit
+  auto push = [&](int i, int d) {
+    if (kWide) {
+      if ((i & 1) == 0) {
+        pending = d;
+        if (i + 1 == message_chunks && d) s_rows32[cnt++] = uint32_t(i / 2) * 65536u + uint32_t(d);
+      } else if (pending | d) {
+        s_rows32[cnt++] = uint32_t(i / 2) * 65536u + uint32_t(pending + 256 * d);
+      }
+    } else if (d) {
+      s_rows16[cnt++] = uint16_t(i * 256 + d);
+    }
+  };
+  if (bits) {
+    const long long vec = inst / chunk_num;
+    const int chunk = int(inst % chunk_num);
+    const int padded_total = 2 * embed_len;
+    const int cbase = chunk * chunk_len;
+    int avail = padded_total - cbase;
+    if (avail > chunk_len) avail = chunk_len;
+    if (avail < 0) avail = 0;
+    const uint8_t* vb = bits + vec * embed_len;
+    for (int i = 0; i < message_chunks; ++i) {
+      int d = 0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int e = 8 * i + b;  // exponent within the chunk value
+        if (e < avail) {
+          const int p = cbase + (avail - 1 - e);  // padded MSB-first position
+          if (p & 1) d |= (vb[p >> 1] & 1) << b;
+        }
+      }
+      push(i, d);
+    }
+  } else {
+    const uint8_t* mb = reinterpret_cast<const uint8_t*>(plain + inst * plain_words);
+    const int bytes = plain_words * 4 < message_chunks ? plain_words * 4 : message_chunks;
+    for (int i = 0; i < message_chunks; ++i) push(i, i < bytes ? int(mb[i]) : 0);
+  }
+  return cnt;
+}
+
 template <int K, int TPI, bool kWide = false>
 __global__ void __launch_bounds__(kBlockThreads)
 k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len, int chunk_num,
@@ -1394,49 +1447,9 @@ k_lookup_encrypt(const uint8_t* __restrict__ bits, int embed_len, int chunk_len,
   __shared__ int s_count[IPB];
 
   // nonzero digits -> list of table rows (lane 0 of the group)
-  if (g.gl == 0) {
-    int cnt = 0;
-    int pending = 0;  // kWide: the low byte of the current 16-bit digit
-    auto push = [&](int i, int d) {
-      if (kWide) {
-        if ((i & 1) == 0) {
-          pending = d;
-          if (i + 1 == message_chunks && d) s_rows32[cnt++] = uint32_t(i / 2) * 65536u + uint32_t(d);
-        } else if (pending | d) {
-          s_rows32[cnt++] = uint32_t(i / 2) * 65536u + uint32_t(pending + 256 * d);
-        }
-      } else if (d) {
-        s_rows16[cnt++] = uint16_t(i * 256 + d);
-      }
-    };
-    if (bits) {
-      const long long vec = inst / chunk_num;
-      const int chunk = int(inst % chunk_num);
-      const int padded_total = 2 * embed_len;
-      const int cbase = chunk * chunk_len;
-      int avail = padded_total - cbase;
-      if (avail > chunk_len) avail = chunk_len;
-      if (avail < 0) avail = 0;
-      const uint8_t* vb = bits + vec * embed_len;
-      for (int i = 0; i < message_chunks; ++i) {
-        int d = 0;
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-          const int e = 8 * i + b;  // exponent within the chunk value
-          if (e < avail) {
-            const int p = cbase + (avail - 1 - e);  // padded MSB-first position
-            if (p & 1) d |= (vb[p >> 1] & 1) << b;
-          }
-        }
-        push(i, d);
-      }
-    } else {
-      const uint8_t* mb = reinterpret_cast<const uint8_t*>(plain + inst * plain_words);
-      const int bytes = plain_words * 4 < message_chunks ? plain_words * 4 : message_chunks;
-      for (int i = 0; i < message_chunks; ++i) push(i, i < bytes ? int(mb[i]) : 0);
-    }
-    s_count[slot] = cnt;
-  }
+  if (g.gl == 0)
+    s_count[slot] = lookup_digit_rows<kWide>(bits, embed_len, chunk_len, chunk_num, plain, plain_words, inst,
+                                             message_chunks, s_rows16);
   __syncwarp(g.mask);
   const int cnt = s_count[slot];
   auto row_of = [&](int j) -> long long { return kWide ? (long long)s_rows32[j] : (long long)s_rows16[j]; };
@@ -1496,6 +1509,123 @@ k_wide_table(const uint32_t* __restrict__ gtab, int message_chunks, uint32_t* __
   g.publish(s_b, hi);
   g.mont_mul(r, lo, s_b, n2, ks.ninv2);
   g.store(wide + inst * K, r);
+}
+
+// The 16-bit-digit table in 52-bit limbs, R52 domain, one row j at a time:
+// W[j][D] = G[2j][D mod 256] G[2j+1][D / 256] R52 mod n^2 from the 8-bit
+// table (32-bit Montgomery form): one 32-bit product for the pair, one with
+// R52 mod n^2 (r52w) into the R52 domain.
+template <int K>
+__global__ void __launch_bounds__(kBlockThreads)
+k_wide_table52(const uint32_t* __restrict__ gtab, int message_chunks, int j, double* __restrict__ wide52,
+               const uint32_t* __restrict__ consts, KeyScalars ks, const uint32_t* __restrict__ r52w) {
+  constexpr int TPI = K / 16, L = 16, K52 = 5 * K / 8, L52 = K52 / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_r52 = smem;
+  for (int i = threadIdx.x; i < K; i += blockDim.x) s_r52[i] = r52w[i];
+  __syncthreads();
+  Group<K, TPI> g;
+  const int slot = threadIdx.x / TPI;
+  const int D = blockIdx.x * IPB + slot;
+  if (D >= 65536) return;
+  uint32_t* s_b = smem + K + slot * K;
+  uint32_t n2[L], lo[L], hi[L], p[L];
+  g.load_ro(n2, consts + C_N2 * K);
+  g.load_ro(lo, gtab + ((long long)(2 * j) * 256 + (D & 255)) * K);
+  if (2 * j + 1 < message_chunks) g.load_ro(hi, gtab + ((long long)(2 * j + 1) * 256 + (D >> 8)) * K);
+  else g.load_ro(hi, consts + C_RM * K);
+  g.publish(s_b, hi);
+  g.mont_mul(p, lo, s_b, n2, ks.ninv2);      // the pair, 32-bit Montgomery form
+  g.mont_mul(lo, p, s_r52, n2, ks.ninv2);    // x R52 mod n^2
+  g.publish(s_b, lo);
+  double* o = wide52 + ((long long)j * 65536 + D) * K52;
+#pragma unroll
+  for (int k = 0; k < L52; ++k) o[g.gl * L52 + k] = cuhe52::to_f64(limb52_from_words(s_b, K, g.gl * L52 + k));
+}
+
+// Paillier-Lookup encryption with the 16-bit-digit table on the FP64 pipe
+// (n^2 of 4096 / 8192 bits): the table and the noise entries as 52-bit limbs
+// in the R52 domain, the product accumulated as in k_modexp52 (the next row
+// loaded during each product), the result re-cut into words: the
+// ciphertexts of k_lookup_encrypt.
+template <int K>
+__global__ void __launch_bounds__(kBlockThreads, 3)
+k_lookup_encrypt52(const uint8_t* __restrict__ bits, int embed_len, int chunk_len, int chunk_num,
+                   const uint32_t* __restrict__ plain, int plain_words, long long count, int message_chunks,
+                   const double* __restrict__ wide52, const double* __restrict__ noise52, int noise_entries,
+                   const uint8_t* __restrict__ noise_idx, uint32_t* __restrict__ out,
+                   const double* __restrict__ n52, unsigned long long ninv52, int* status) {
+  constexpr int TPI = K / 16, L = 16, K52 = 5 * K / 8, L52 = K52 / TPI;
+  constexpr int IPB = kBlockThreads / TPI;
+  extern __shared__ __align__(16) double smd[];
+  double* s_one52 = smd;         // 1
+  double* s_accs = smd + K52;    // per instance: the accumulator (b operand), K52 + 2 doubles
+  __shared__ int s_count[IPB];
+  for (int i = threadIdx.x; i < K52; i += blockDim.x) s_one52[i] = i == 0 ? 1.0 : 0.0;
+  __syncthreads();
+  Group<K, TPI> g;
+  cuhe52::Group52<K52, TPI> f;
+  const int slot = threadIdx.x / TPI;
+  const long long inst = (long long)blockIdx.x * IPB + slot;
+  if (inst >= count) return;
+  uint16_t* s_rows16 =
+      reinterpret_cast<uint16_t*>(s_accs + IPB * (K52 + 2)) + slot * lookup_rows_stride(message_chunks);
+  const uint32_t* s_rows32 = reinterpret_cast<const uint32_t*>(s_rows16);
+  if (g.gl == 0)
+    s_count[slot] = lookup_digit_rows<true>(bits, embed_len, chunk_len, chunk_num, plain, plain_words, inst,
+                                            message_chunks, s_rows16);
+  __syncwarp(f.mask);
+  const int cnt = s_count[slot];
+  double* s_b = s_accs + slot * (K52 + 2);
+  double acc[L52], a[L52], nx[L52], m52[L52];
+  auto load_row = [&](double (&v)[L52], const double* row) {
+    const double2* r2 = reinterpret_cast<const double2*>(row + f.gl * L52);
+#pragma unroll
+    for (int k = 0; k < L52 / 2; ++k) {
+      const double2 t = __ldg(r2 + k);
+      v[2 * k] = t.x;
+      v[2 * k + 1] = t.y;
+    }
+  };
+#pragma unroll
+  for (int k = 0; k < L52; ++k) {
+    m52[k] = __ldg(n52 + f.gl * L52 + k);
+    acc[k] = __ldg(n52 + K52 + f.gl * L52 + k);  // R52 mod n^2: one in the R52 domain
+  }
+  f.publish(s_b, acc);
+  if (cnt > 0) load_row(a, wide52 + (long long)s_rows32[0] * K52);
+#pragma unroll 1
+  for (int j = 0; j < cnt; ++j) {
+    if (j + 1 < cnt) load_row(nx, wide52 + (long long)s_rows32[j + 1] * K52);
+    f.mont_mul(acc, a, s_b, m52, ninv52);
+    f.publish(s_b, acc);
+#pragma unroll
+    for (int k = 0; k < L52; ++k) a[k] = nx[k];
+  }
+  const uint8_t* idx = noise_idx + inst * kNoiseMultiples;
+#pragma unroll 1
+  for (int k = 0; k < kNoiseMultiples; ++k) {
+    const int r = idx[k];
+    if (r >= noise_entries) {
+      if (g.gl == 0) atomicOr(status, ST_RANGE);
+      return;
+    }
+    load_row(a, noise52 + (long long)r * K52);
+    f.mont_mul(acc, a, s_b, m52, ninv52);
+    f.publish(s_b, acc);
+  }
+  double res[L52];
+  f.mont_mul(res, acc, s_one52, m52, ninv52);  // canonical
+  uint64_t* s_l = reinterpret_cast<uint64_t*>(s_b);
+  __syncwarp(f.mask);
+#pragma unroll
+  for (int k = 0; k < L52; ++k) s_l[f.gl * L52 + k] = cuhe52::to_u64(res[k]);
+  __syncwarp(f.mask);
+  uint32_t w[L];
+#pragma unroll
+  for (int t = 0; t < L; ++t) w[t] = word_from_limbs52(s_l, K52, g.gl * L + t);
+  g.store(out + inst * K, w);
 }
 
 // ---------------------------------------------------------------------------

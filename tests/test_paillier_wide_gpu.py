@@ -1,6 +1,7 @@
 """The 16-bit-digit encryption table (cuhe_lookup_set_wide_table): one table
 entry per pair of 8-bit digits gives the same ciphertexts as the 8-bit
-table, for the reference's golden vectors, random embeddings over several
+table, as 32-bit words on the integer pipe and as 52-bit limbs on the FP64
+pipe, for the reference's golden vectors, random embeddings over several
 chunks, random plaintext words and an odd number of digit rows; and the
 table is built only when asked or for a large call.  Integer work: every
 comparison is exact."""
@@ -57,6 +58,18 @@ def test_wide_table_gives_the_same_ciphertexts(name):
             assert ctx.lookup_encrypt_bits(bits, 2 * key_len, 1, hidx) == [[hx(v["c"][0])] for v in vectors]
         assert ctx.lookup_encrypt_bits(vecs, chunk_len, chunk_num, vidx) == narrow_bits
         assert ctx.lookup_encrypt_ints(plain, pidx) == narrow_ints
+        # the other pipe's table (n^2 of 4096 bits: FP64 by default, 52-bit
+        # limbs; 2048 bits: the FP64 pipe only when asked for)
+        other = 0 if ctx.fp64 == 1 and ctx.words >= 128 else 2
+        ctx.set_wide_table(0)
+        ctx.set_fp64(other)
+        ctx.set_wide_table(2)
+        assert ctx.lookup_encrypt_ints(ms, idx) == [hx(c["c"]) for c in data["encrypt"]]
+        assert ctx.lookup_encrypt_bits(vecs, chunk_len, chunk_num, vidx) == narrow_bits
+        assert ctx.lookup_encrypt_ints(plain, pidx) == narrow_ints
+        ctx.set_wide_table(0)
+        ctx.set_fp64(1)
+        ctx.set_wide_table(2)
         # and the 8-bit path is still the oracle's
         table = ctx.g_table()
         for k in (0, 7, len(plain) - 1):
@@ -86,6 +99,11 @@ def test_wide_table_with_an_odd_digit_count_and_the_build_policy():
         ctx.set_wide_table(2)
         assert ctx.lookup_encrypt_ints(plain, pidx) == narrow
         assert ctx.wide_table_ready()
+        ctx.set_wide_table(0)
+        ctx.set_fp64(2)  # the table as 52-bit limbs on the FP64 pipe
+        ctx.set_wide_table(2)
+        assert ctx.lookup_encrypt_ints(plain, pidx) == narrow
+        ctx.set_fp64(1)
 
         # mode 1 (the default): a small call keeps the 8-bit table, a call of
         # 65,536 ciphertexts builds the wide one, with the same results
