@@ -212,8 +212,11 @@ int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t ve
  * looked up as one entry W[j][D] = G[2j][D mod 256] * G[2j+1][D / 256] (mod
  * n^2, Montgomery form), so each ciphertext takes half the table products and
  * the ciphertexts are the same.  The table holds (message_chunks + 1) / 2 *
- * 65,536 entries of K words (4 GiB at key_len 1024) and costs one product per
- * entry to build, which about 150,000 encryptions repay.  mode 1 (the
+ * 65,536 entries, K words each (4 GiB at key_len 1024), or 5K/8 doubles each
+ * when the FP64 pipe is selected (cuhe_paillier_set_fp64; 5 GiB at key_len
+ * 1024, with the noise table converted likewise, and the products then run
+ * on that pipe), and costs one or two products per entry to build, which
+ * about 150,000 encryptions repay.  mode 1 (the
  * default) builds it during an encryption call of at least 65,536
  * ciphertexts, when it takes at most 8 GiB and a quarter of the free device
  * memory; mode 2 builds it at the next encryption call of any size
