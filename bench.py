@@ -1320,6 +1320,7 @@ def profile_case(which: str) -> None:
         ctx.set_factors(*factors_from_phi(pk["n"], sk["phi"]))
         ctx.set_fp64(1 if which == "paillier" else 0)
         ctx.set_tables([keys["g_table"][i] for i in range(keys["message_chunks"])], keys["noise_table"])
+        ctx.set_wide_table(2)  # the bench step's table (16-bit digits), built even for this small case
         stream = torch.cuda.Stream()
         ctx.set_stream(stream.cuda_stream)
         vectors = 8192
