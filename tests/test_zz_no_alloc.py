@@ -9,7 +9,8 @@ workspace.  Here it is called through the C ABI, several calls in a row, on
 the direct and on the CRT decryption kernel, at up to exactly its stated
 maximum, and compared with cuhe_paillier_decode_hamming on the same
 ciphertexts; the device's free memory is checked unchanged across the calls
-(a growing workspace or any other device allocation would lower it).  This
+(a growing workspace or any other device allocation would lower it), and
+one call is captured in a CUDA graph and replayed.  This
 file is collected last on purpose, so that a run stopping at the first
 failure has already run every other test; it creates its own contexts, so it
 also passes alone in a fresh process.
@@ -100,6 +101,28 @@ def test_static_scratch_decode_matches_allocating_decode(crt):
     for i in (0, 1, 2, 2, 1, 0):  # calls in a row; the shared array keeps the last call's counts
         static(i)
     assert torch.cuda.mem_get_info()[0] == free_before
+
+    # the same call captured in a CUDA graph on the context stream and
+    # replayed: a capture in global mode ends with an error at any device
+    # allocation or synchronisation inside the call
+    vectors, chunk_num, _, c_dev = cases[1]
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream, capture_error_mode="global"):
+        rc = lib.cuhe_paillier_decode_hamming_static(ctx._ctx, c_dev.data_ptr(), vectors, chunk_num, chunk_len,
+                                                     gots[1].data_ptr())
+    assert rc == 0, lib.cuhe_last_error(ctx._ctx)
+    graph.replay()
+    torch.cuda.synchronize()
+    free_graph = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        gots[1].fill_(-2)
+        torch.cuda.synchronize()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(gots[1], wants[1])
+    assert torch.cuda.mem_get_info()[0] == free_graph
+    ctx.synchronize()
+    del graph
     # independent check of a few distances against the plaintexts
     for (vectors, chunk_num, ms, _), want in zip(cases[:2], wants[:2]):
         want_h = want.cpu().tolist()
