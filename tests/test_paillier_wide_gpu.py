@@ -3,7 +3,8 @@ entry per pair of 8-bit digits gives the same ciphertexts as the 8-bit
 table, as 32-bit words on the integer pipe and as 52-bit limbs on the FP64
 pipe, for the reference's golden vectors, random embeddings over several
 chunks, random plaintext words and an odd number of digit rows; and the
-table is built only when asked or for a large call.  Integer work: every
+table is built only when asked or for a large call; a noise index past a
+short noise table is a range error on both pipes.  Integer work: every
 comparison is exact."""
 
 import random
@@ -123,5 +124,35 @@ def test_wide_table_with_an_odd_digit_count_and_the_build_policy():
         assert torch.equal(big[:64], small)
         with pytest.raises(ValueError):
             ctx.set_wide_table(3)
+    finally:
+        ctx.close()
+
+
+@pytest.mark.parametrize("fp64", [1, 0], ids=["fp64", "integer"])
+def test_noise_index_beyond_a_short_noise_table_is_a_range_error(fp64):
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    data = load_golden("lookup_1024.json")
+    pk = {k: hx(v) for k, v in data["pk"].items()}
+    ctx = PaillierDevice(pk["n"])
+    try:
+        ctx.set_fp64(fp64)
+        entries = 16
+        noise = oracle.noise_table(pk["g"], pk["n"], [hx(r) for r in data["noise_exponents"][:entries]])
+        ctx.build_tables(pk["g"], data["message_chunks"], noise)
+        table = ctx.g_table()
+        ms = [hx(c["m"]) for c in data["encrypt"][:4]]
+        good = np.array([[(3 * i + k) % entries for k in range(14)] for i in range(len(ms))], dtype=np.uint8)
+        want = [oracle.lookup_encrypt(m, pk, table, noise, list(good[i]), len(table)) for i, m in enumerate(ms)]
+        bad = good.copy()
+        bad[2, 5] = entries  # the first index past the table
+        for wide in (0, 2):  # the 8-bit table, then the 16-bit-digit table
+            ctx.set_wide_table(wide)
+            assert ctx.lookup_encrypt_ints(ms, good) == want
+            with pytest.raises(ValueError, match="noise index"):
+                ctx.lookup_encrypt_ints(ms, bad)
+            # the status is cleared and the context stays usable
+            assert ctx.lookup_encrypt_ints(ms, good) == want
+            assert ctx.wide_table_ready() == (wide == 2)
     finally:
         ctx.close()
