@@ -2,7 +2,8 @@
 entry per pair of 8-bit digits gives the same ciphertexts as the 8-bit
 table, as 32-bit words on the integer pipe and as 52-bit limbs on the FP64
 pipe, for the reference's golden vectors, random embeddings over several
-chunks, random plaintext words and an odd number of digit rows; and the
+chunks, random plaintext words, an odd number of digit rows and n² of 8192
+bits; and the
 table is built only when asked or for a large call; a noise index past a
 short noise table is a range error on both pipes.  Integer work: every
 comparison is exact."""
@@ -154,5 +155,36 @@ def test_noise_index_beyond_a_short_noise_table_is_a_range_error(fp64):
             # the status is cleared and the context stays usable
             assert ctx.lookup_encrypt_ints(ms, good) == want
             assert ctx.wide_table_ready() == (wide == 2)
+    finally:
+        ctx.close()
+
+
+def test_wide_table_at_n_squared_of_8192_bits():
+    """n of 4096 bits (key_len 2048, 256 words, 160 limbs of 52 bits) with 9
+    message digits (five 16-bit rows, the last one half empty), so that both
+    tables stay small; Montgomery arithmetic needs only an odd n."""
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    rng = random.Random(8192)
+    n = rng.getrandbits(4096) | (1 << 4095) | 1
+    pk = {"n": n, "g": n + 1, "n_squared": n * n}
+    ctx = PaillierDevice(n)
+    try:
+        assert ctx.words == 256
+        chunks, entries = 9, 32
+        noise = oracle.noise_table(pk["g"], n, [rng.getrandbits(256) for _ in range(entries)])
+        ctx.build_tables(pk["g"], chunks, noise)
+        table = ctx.g_table()
+        plain = [rng.getrandbits(8 * chunks) for _ in range(20)] + [0, (1 << (8 * chunks)) - 1, 1 << (8 * chunks - 1)]
+        idx = np.array([[rng.randrange(entries) for _ in range(14)] for _ in plain], dtype=np.uint8)
+        want = [oracle.lookup_encrypt(m, pk, table, noise, list(idx[i]), len(table)) for i, m in enumerate(plain)]
+        for fp64 in (1, 0):  # 52-bit limbs on the FP64 pipe (the default at this width), then words
+            ctx.set_fp64(fp64)
+            for wide in (0, 2):
+                ctx.set_wide_table(wide)
+                assert ctx.lookup_encrypt_ints(plain, idx) == want, (fp64, wide)
+                assert ctx.wide_table_ready() == (wide == 2)
+            ctx.set_wide_table(0)
+        ctx.set_fp64(1)
     finally:
         ctx.close()
