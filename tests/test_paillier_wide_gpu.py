@@ -3,10 +3,9 @@ entry per pair of 8-bit digits gives the same ciphertexts as the 8-bit
 table, as 32-bit words on the integer pipe and as 52-bit limbs on the FP64
 pipe, for the reference's golden vectors, random embeddings over several
 chunks, random plaintext words, an odd number of digit rows and n² of 8192
-bits; and the
-table is built only when asked or for a large call; a noise index past a
-short noise table is a range error on both pipes.  Integer work: every
-comparison is exact."""
+bits; and the table is built only when asked or for a large call; a noise
+index past a short noise table is a range error on both pipes.  Integer
+work: every comparison is exact."""
 
 import random
 
