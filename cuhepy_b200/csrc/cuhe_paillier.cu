@@ -294,6 +294,8 @@ cudaError_t build_wide52(cuhe_paillier* ctx, double* wide52, double* noise52) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+  // no noise table: encryption reports every noise index as out of range
+  if (ctx->noise_entries == 0) return cudaSuccess;
   cuhe::k_to_mont52<K><<<dim3(unsigned((ctx->noise_entries + IPB - 1) / IPB)), cuhe::kBlockThreads, smem,
                          ctx->stream>>>(ctx->d_noise, ctx->noise_entries, noise52, ctx->d_consts, ctx->ks, r52w,
                                         ctx->d_status);
@@ -1599,7 +1601,8 @@ int ensure_wide_table(cuhe_paillier* ctx, const Dispatch& d, long long items) {
   void* wide = nullptr;
   void* noise52 = nullptr;
   cudaError_t e = cudaMalloc(&wide, bytes);
-  if (e == cudaSuccess && fp52) e = cudaMalloc(&noise52, size_t(ctx->noise_entries) * entry);
+  if (e == cudaSuccess && fp52 && ctx->noise_entries > 0)
+    e = cudaMalloc(&noise52, size_t(ctx->noise_entries) * entry);
   if (e != cudaSuccess) {
     cudaGetLastError();
     cudaFree(wide);
