@@ -221,9 +221,13 @@ int cuhe_lookup_encrypt_bits(cuhe_paillier* ctx, const uint8_t* bits, int64_t ve
  * ciphertexts, when it takes at most 8 GiB and a quarter of the free device
  * memory; mode 2 builds it at the next encryption call of any size
  * (CUHE_OUT_OF_MEMORY without the memory); mode 0 frees it and keeps the
- * 8-bit table.  Installing new tables drops it.  ready returns 1 once it is
- * built.  No reference counterpart (the reference multiplies one entry per
- * 8-bit digit, lookup.py:213-252). */
+ * 8-bit table.  Installing new tables drops it.  The table is built for the
+ * pipe selected at that time.  If cuhe_paillier_set_fp64 later selects the
+ * other pipe, the table is kept; FP64-form limbs are then left unused and the
+ * 8-bit table serves, while a word table still serves the FP64 selection on
+ * the integer pipe.  Call mode 0, then mode 2, to rebuild it for the new
+ * pipe.  ready returns 1 once it is built.  No reference counterpart (the
+ * reference multiplies one entry per 8-bit digit, lookup.py:213-252). */
 int cuhe_lookup_set_wide_table(cuhe_paillier* ctx, int mode);
 int cuhe_lookup_wide_table_ready(const cuhe_paillier* ctx);
 
