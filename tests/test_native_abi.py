@@ -117,3 +117,24 @@ def test_limb_roundtrip():
         to_limbs([1 << 4096], 128)
     with pytest.raises(ValueError):
         to_limbs([-1], 4)
+
+
+def test_no_cpu_fallback_without_a_device():
+    """Without a CUDA device every entry point raises; nothing computes on the
+    host in its place (on a machine with a GPU this test has nothing to show)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from cuhepy_b200.bfv import _bfv_rns
+    from cuhepy_b200.hamming.paillier_lookup import PaillierLookupClient
+    from cuhepy_b200.paillier.gpu import PaillierDevice
+
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        PaillierDevice(10**30 + 1)
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        PaillierLookupClient(key_len=512, device="gpu")
+    with pytest.raises(RuntimeError, match="no CUDA device"):
+        _bfv_rns.create_ring(16, "ffffffffffffffc5", 4, True, True)
+    with pytest.raises(NotImplementedError):
+        PaillierLookupClient(key_len=512, device="cpu")
