@@ -19,6 +19,29 @@ def declared(header: str) -> list[str]:
     return sorted(set(re.findall(r"\b(cuhe_[a-z0-9_]+)\s*\(", text)))
 
 
+def parameter_counts(header: str) -> dict[str, int]:
+    """Number of parameters of every prototype the header declares."""
+    text = (REPO / "include" / header).read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", "", text)
+    counts = {}
+    for m in re.finditer(r"\b(cuhe_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        args = m.group(2).strip()
+        counts[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return counts
+
+
+@pytest.mark.parametrize("header", ["cuhe_paillier.h", "cuhe_bfv.h"])
+def test_ctypes_signatures_take_the_declared_parameter_counts(header):
+    from cuhepy_b200.bfv import _bfv_rns
+
+    table = _native.PAILLIER_SIGNATURES if header == "cuhe_paillier.h" else _bfv_rns.BFV_SIGNATURES
+    counts = parameter_counts(header)
+    assert sorted(counts) == declared(header)  # every declaration parsed
+    for name, count in counts.items():
+        assert len(table[name][1]) == count, name
+
+
 def test_paillier_library_exports_every_declared_symbol():
     lib = _native.paillier_lib()
     names = declared("cuhe_paillier.h")
