@@ -1,5 +1,6 @@
-"""The C ABI library loads, exports every declared symbol, and its host-only
-logic behaves; no kernel is launched here."""
+"""The C ABI library loads, exports every declared symbol with the declared
+number of parameters, its host-only logic behaves, and without a CUDA device
+every entry point raises; no kernel is launched here."""
 
 import ctypes
 import random
