@@ -1,6 +1,7 @@
 """The C ABI library loads, exports every declared symbol with the declared
 number of parameters, its host-only logic behaves, and without a CUDA device
-every entry point raises; no kernel is launched here."""
+the Paillier context, the client and the BFV ring refuse to start; no kernel
+is launched here."""
 
 import ctypes
 import random
@@ -144,8 +145,9 @@ def test_limb_roundtrip():
 
 
 def test_no_cpu_fallback_without_a_device():
-    """Without a CUDA device every entry point raises; nothing computes on the
-    host in its place (on a machine with a GPU this test has nothing to show)."""
+    """Without a CUDA device the Paillier context, the client and the BFV ring
+    raise instead of computing on the host (on a machine with a GPU this test
+    has nothing to show)."""
     import torch
 
     if torch.cuda.is_available():
