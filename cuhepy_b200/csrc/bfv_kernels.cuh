@@ -1792,33 +1792,6 @@ __global__ void k_words_addsub(const u64* __restrict__ a, long long a_stride, co
   for (int k = 0; k < W; ++k) o[k] = r[k];
 }
 
-// out[poly] = sigma_g(in[poly]) on words mod q: coefficient i moves to
-// g i mod 2N, negated when that wraps past N (rns_ntt.h:656-664).
-__global__ void k_words_automorphism(const u64* __restrict__ in, u64* __restrict__ out, long long polys, unsigned g,
-                                     const RingDev* __restrict__ ring) {
-  const RingDev& R = *ring;
-  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= polys * R.n) return;
-  const long long poly = idx / R.n;
-  const int i = int(idx % R.n);
-  const int W = R.words;
-  const unsigned at = unsigned((unsigned long long)i * g % (2u * unsigned(R.n)));
-  const u64* x = in + idx * W;
-  u64* o = out + (poly * R.n + (at % unsigned(R.n))) * W;
-  bool nonzero = false;
-  for (int k = 0; k < W; ++k) nonzero |= x[k] != 0;
-  if (at >= unsigned(R.n) && nonzero) {
-    u64 borrow = 0;
-    for (int k = 0; k < W; ++k) {
-      const u128 d = u128(R.q_words[k]) - x[k] - borrow;
-      o[k] = u64(d);
-      borrow = u64(d >> 64) ? 1 : 0;
-    }
-  } else {
-    for (int k = 0; k < W; ++k) o[k] = x[k];
-  }
-}
-
 // Per-ciphertext descriptors of the native rotate / add steps (two word polys
 // each): permute writes perm = sigma_g(in); finish writes out = (ks0 + perm0,
 // ks1); add writes out = in + perm.
@@ -1848,6 +1821,8 @@ __device__ __forceinline__ void words_add_modq(const u64* x, const u64* y, u64* 
   for (int k = 0; k < W; ++k) o[k] = r[k];
 }
 
+// perm = sigma_g(in) on words mod q: coefficient i moves to g i mod 2N,
+// negated when that wraps past N (rns_ntt.h:656-664).
 // grid: (blocks over 2N coefficients, ops)
 __global__ void k_native_permute(const NativeOp* __restrict__ ops, unsigned g, const RingDev* __restrict__ ring) {
   const RingDev& R = *ring;
